@@ -1,0 +1,396 @@
+"""Benchmark: 8192^3 DGEMM GFLOP/s at FP64 accuracy, Ozaki-INT8 vs native FP64.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--size 8192]
+
+One step = one C = A*B (alpha=1, beta=0, M=N=K=size, FP64, uniform[-1,1)
+synthetic inputs from a fixed seed) through libjlcgpu.  `value` is the
+FP64-accurate rate of the Ozaki-INT8 route (FP64-equivalent 2*M*N*K/t); the
+native FP64 DMMA route is measured in the same run and reported beside it.
+Inputs are 3 x 512 MiB, larger than the 126 MB L2, so no flush is needed
+between steps.  For N > 1 (torchrun) every rank computes its own row block of
+an (N*size) x size product (weak scaling, no data-path collective); the time is
+the max over ranks.
+
+--impl reference times the reference's CPU algorithm (the oracle's restatement
+of OptimizedBLAS3's PARALLEL_MICRO path, all host threads) on a bounded sample
+of the same workload; under torchrun only rank 0 runs it.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "8192^3 DGEMM GFLOP/s at FP64 accuracy: Ozaki-INT8 vs native FP64, % of peak"
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=5)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--size", type=int, default=8192)
+    p.add_argument("--cpu-seconds", type=float, default=12.0, help="target length of one CPU baseline sample")
+    p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    return p.parse_args()
+
+
+def dist_env():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+# ----------------------------------------------------------------------------- clocks
+class ClockSampler:
+    """Samples SM clock, power and clock-event reasons through NVML during the
+    timed region (read-only queries)."""
+
+    REASONS = {0x4: "sw_power_cap", 0x8: "hw_slowdown", 0x20: "sw_thermal_slowdown",
+               0x40: "hw_thermal_slowdown", 0x80: "hw_power_brake_slowdown", 0x1: "gpu_idle",
+               0x2: "applications_clocks_setting", 0x10: "sync_boost"}
+
+    def __init__(self, torch_device: int):
+        self.samples = []
+        self.max_mhz = None
+        self._stop = threading.Event()
+        self._thread = None
+        try:
+            import pynvml
+            pynvml.nvmlInit()
+            self.nv = pynvml
+            self.h = self._handle(torch_device)
+            self.max_mhz = pynvml.nvmlDeviceGetMaxClockInfo(self.h, pynvml.NVML_CLOCK_SM)
+        except Exception as e:  # NVML missing: report no clocks rather than guess
+            self.nv = None
+            self.error = str(e)
+
+    def _handle(self, dev):
+        import torch
+        nv = self.nv
+        props = torch.cuda.get_device_properties(dev)
+        try:
+            bus = "%08x:%02x:%02x.0" % (props.pci_domain_id, props.pci_bus_id, props.pci_device_id)
+            return nv.nvmlDeviceGetHandleByPciBusId_v2(bus)
+        except Exception:
+            vis = os.environ.get("CUDA_VISIBLE_DEVICES")
+            idx = int(vis.split(",")[dev]) if vis else dev
+            return nv.nvmlDeviceGetHandleByIndex(idx)
+
+    def _run(self):
+        nv = self.nv
+        while not self._stop.is_set():
+            try:
+                sm = nv.nvmlDeviceGetClockInfo(self.h, nv.NVML_CLOCK_SM)
+                pw = nv.nvmlDeviceGetPowerUsage(self.h) / 1000.0
+                try:
+                    rs = nv.nvmlDeviceGetCurrentClocksEventReasons(self.h)
+                except Exception:
+                    rs = nv.nvmlDeviceGetCurrentClocksThrottleReasons(self.h)
+                self.samples.append((sm, pw, rs))
+            except Exception:
+                pass
+            self._stop.wait(0.1)
+
+    def __enter__(self):
+        if self.nv is not None:
+            self._thread = threading.Thread(target=self._run, daemon=True)
+            self._thread.start()
+        return self
+
+    def __exit__(self, *exc):
+        self._stop.set()
+        if self._thread:
+            self._thread.join()
+
+    def summary(self):
+        if self.nv is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvml unavailable"]}
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": self.max_mhz, "reasons": []}
+        reasons = set()
+        for _, _, rs in self.samples:
+            for bit, name in self.REASONS.items():
+                if rs & bit and name != "gpu_idle":
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(s[0] for s in self.samples), "sm_max_mhz": self.max_mhz,
+                "reasons": sorted(reasons), "power_w_max": max(s[1] for s in self.samples),
+                "samples": len(self.samples)}
+
+
+# ----------------------------------------------------------------------------- helpers
+def measured_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            return json.load(f)
+    return None
+
+
+def profile_traffic(name):
+    """DRAM bytes per launch from a committed ncu summary (profiles/<name>.txt,
+    line 'dram_bytes_per_launch: <bytes>'), or None."""
+    path = os.path.join(ROOT, "profiles", name + ".txt")
+    if not os.path.exists(path):
+        return None
+    with open(path) as f:
+        for line in f:
+            if line.startswith("dram_bytes_per_launch:"):
+                try:
+                    return float(line.split(":", 1)[1])
+                except ValueError:
+                    return None
+    return None
+
+
+def cpu_baseline(size, seconds, threads=None):
+    """The oracle's restatement of OptimizedBLAS3 PARALLEL_MICRO (packed, tiled,
+    threaded; bit-exact with the Java path) on a row sample of the size^3
+    product, timed on this host's cores."""
+    import numpy as np
+    from oracle import oracle as O
+    threads = threads or (os.cpu_count() or 1)
+    rng = np.random.default_rng(20260604)
+    B = rng.uniform(-1.0, 1.0, (size, size))
+    probe_rows = 64
+    A = rng.uniform(-1.0, 1.0, (probe_rows, size))
+    C = np.zeros((probe_rows, size))
+    t0 = time.perf_counter()
+    O.gemm_packed_parallel(A, B, C, 1.0, 0.0, threads=threads)
+    dt = time.perf_counter() - t0
+    rate = 2.0 * probe_rows * size * size / max(dt, 1e-9)
+    rows = int(max(64, min(size, seconds * rate / (2.0 * size * size))))
+    rows = max(64, rows // 64 * 64)
+    A = rng.uniform(-1.0, 1.0, (rows, size))
+    C = np.zeros((rows, size))
+    t0 = time.perf_counter()
+    O.gemm_packed_parallel(A, B, C, 1.0, 0.0, threads=threads)
+    dt = time.perf_counter() - t0
+    gflops = 2.0 * rows * size * size / dt / 1e9
+    return {"value": round(gflops, 2), "unit": "GFLOP/s", "cores": threads, "kind": "port",
+            "sample": f"rows 0..{rows} of the {size}^3 product ({rows}x{size}x{size}, alpha=1, beta=0) through "
+                      f"the C restatement of OptimizedBLAS3 PARALLEL_MICRO (MC/KC/NC=2048/128/128, 6x8 "
+                      f"microkernel, bit-exact fma chain), {threads} threads, {dt:.1f} s"}
+
+
+# ----------------------------------------------------------------------------- reference arm
+def run_reference(args):
+    world, rank, _ = dist_env()
+    if rank != 0:
+        return 0
+    size = args.size
+    threads = os.cpu_count() or 1
+    vals = []
+    for i in range(args.warmup + args.steps):
+        r = cpu_baseline(size, args.cpu_seconds / 2 if i < args.warmup else args.cpu_seconds, threads)
+        if i >= args.warmup:
+            vals.append(r)
+    v = statistics.median(x["value"] for x in vals)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": v, "unit": "GFLOP/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic uniform[-1,1), seed 20260604",
+        "config": {"workload": f"DGEMM M=N=K={size}, alpha=1, beta=0, row-major, FP64 (CPU sample)",
+                   "l2": "n/a (CPU)"},
+        "cpu_baseline": {"value": v, "unit": "GFLOP/s", "cores": threads, "kind": "port",
+                         "sample": vals[-1]["sample"]},
+        "e2e": {"value": v, "unit": "GFLOP/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "note": "the reference path is Java (OptimizedBLAS3); no JDK exists in this image, so its algorithm "
+                "is timed through the C restatement in oracle/ on all host threads",
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ----------------------------------------------------------------------------- our arm
+def run_ours(args):
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+
+    import jlc_b200
+    from jlc_b200 import JLC_PREC_NATIVE, JLC_PREC_OZAKI
+
+    world, rank, local = dist_env()
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=torch.device("cuda", local))
+    torch.cuda.set_device(local)
+    size = args.size
+    M = N = K = size
+    flops = 2.0 * M * N * K
+
+    ctx = jlc_b200.Context(local)
+    stream = torch.cuda.Stream()
+    ctx.set_stream(stream.cuda_stream)
+
+    peaks = ctx.measure_peaks()
+    g = torch.Generator(device="cuda")
+    g.manual_seed(20260604 + 7919 * rank)  # rank r owns row block r of the (world*size) x size product
+    with torch.cuda.stream(stream):
+        A = torch.rand((M, K), dtype=torch.float64, device="cuda", generator=g) * 2 - 1
+        B = torch.rand((K, N), dtype=torch.float64, device="cuda", generator=g) * 2 - 1
+        Cn = torch.zeros((M, N), dtype=torch.float64, device="cuda")
+        Co = torch.zeros((M, N), dtype=torch.float64, device="cuda")
+    stream.synchronize()
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def step(prec, C):
+        return ctx.dgemm_device(0, 0, M, N, K, 1.0, A.data_ptr(), K, B.data_ptr(), N, 0.0, C.data_ptr(), N,
+                                precision=prec)
+
+    def timed(prec, C, clocks=None):
+        for _ in range(args.warmup):
+            rep = step(prec, C)
+        ctx.synchronize()
+        ctx.profile_collect()
+        ctx.set_profiling(True)
+        launches0 = ctx.launch_count()
+        barrier()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.steps):
+            rep = step(prec, C)
+        e1.record(stream)
+        e1.synchronize()
+        torch.cuda.synchronize()
+        barrier()
+        ms = e0.elapsed_time(e1)
+        launches = ctx.launch_count() - launches0
+        recs = ctx.profile_collect()
+        ctx.set_profiling(False)
+        if world > 1:
+            t = torch.tensor([ms], device="cuda", dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = float(t.item())
+        phases = {}
+        for name, pms in recs:
+            phases.setdefault(name, []).append(pms)
+        return ms / args.steps, rep, launches, phases
+
+    # native FP64 first, then the Ozaki route (the headline) under the clock sampler
+    nat_ms, nat_rep, nat_launches, nat_phases = timed(JLC_PREC_NATIVE, Cn)
+    with ClockSampler(local) as clk:
+        oz_ms, oz_rep, oz_launches, oz_phases = timed(JLC_PREC_OZAKI, Co)
+    clocks = clk.summary()
+
+    # accuracy of both results on sampled entries against the device double-double check
+    rng = np.random.default_rng(17 + rank)
+    rows = np.concatenate([rng.integers(0, M, 4096), [0, M - 1, 127, 128, M - 1]])
+    cols = np.concatenate([rng.integers(0, N, 4096), [0, N - 1, 255, 256, 0]])
+    acc_oz = ctx.check_fp64_bound_device(0, 0, M, N, K, 1.0, A.data_ptr(), K, B.data_ptr(), N, 0.0, None, N,
+                                         Co.data_ptr(), N, rows, cols)
+    acc_nat = ctx.check_fp64_bound_device(0, 0, M, N, K, 1.0, A.data_ptr(), K, B.data_ptr(), N, 0.0, None, N,
+                                          Cn.data_ptr(), N, rows, cols)
+
+    # end to end through the public host entry (pinned host buffers, copies timed on the device)
+    e2e = None
+    if not args.no_e2e:
+        Ah = A.cpu().pin_memory()
+        Bh = B.cpu().pin_memory()
+        Ch = torch.zeros((M, N), dtype=torch.float64).pin_memory()
+        a_np, b_np, c_np = Ah.numpy(), Bh.numpy(), Ch.numpy()
+        for _ in range(max(1, min(args.warmup, 2))):
+            ctx.gemm(a_np, b_np, c_np, 1.0, 0.0, precision=JLC_PREC_OZAKI)
+        dev_ms, wall = [], []
+        for _ in range(args.steps):
+            t0 = time.perf_counter()
+            rep = ctx.gemm(a_np, b_np, c_np, 1.0, 0.0, precision=JLC_PREC_OZAKI)
+            wall.append((time.perf_counter() - t0) * 1e3)
+            dev_ms.append(rep["device_ms"])
+        e2e_ms = statistics.mean(dev_ms)
+        if world > 1:
+            t = torch.tensor([e2e_ms], device="cuda", dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            e2e_ms = float(t.item())
+        e2e = {"value": round(world * flops / (e2e_ms * 1e-3) / 1e9, 1), "unit": "GFLOP/s",
+               "h2d_bytes_per_step": int(rep["h2d_bytes"]), "d2h_bytes_per_step": int(rep["d2h_bytes"]),
+               "ms_per_step": round(e2e_ms, 3), "wall_ms_per_step": round(statistics.mean(wall), 3),
+               "path": "jlc_gemm (host pointers, pinned), Ozaki precision, H2D+D2H inside the timed region"}
+
+    if rank != 0:
+        return 0
+
+    nat_gflops = flops / (nat_ms * 1e-3) / 1e9
+    oz_gflops = flops / (oz_ms * 1e-3) / 1e9
+    P = oz_rep["products"]
+    gemm_ms = statistics.mean(oz_phases.get("ozaki_gemm", [float("nan")]))
+    split_ms = statistics.mean(oz_phases.get("ozaki_split", [float("nan")]))
+    dmma_ms = statistics.mean(nat_phases.get("dmma", [float("nan")]))
+    int8_ops_per_launch = 2.0 * M * N * K * P
+    achieved_tops = int8_ops_per_launch / (gemm_ms * 1e-3) / 1e12
+    mp = measured_peaks()
+    traffic = profile_traffic(f"ozaki_gemm_{size}")
+    line = {
+        "metric": METRIC,
+        "value": round(world * oz_gflops, 1),
+        "unit": "GFLOP/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": round(oz_ms, 3),
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64 (INT8 slice products, INT32 accumulation, FP64 recombination)",
+        "data": "synthetic uniform[-1,1) (torch Philox, seed 20260604 + 7919*rank), device resident",
+        "config": {"workload": f"DGEMM M=N=K={size}, alpha=1, beta=0, row-major A/B/C, FP64-accurate "
+                               f"(Ozaki-INT8, s={oz_rep['slices']})",
+                   "global_M": world * M, "N": N, "K": K, "parallelism": f"dp{world} (row blocks of C)",
+                   "l2": "inputs 1.5 GiB > 126 MB L2, no flush"},
+        "gpu_launches": int(oz_launches),
+        "clocks": clocks,
+        "accuracy": {"ozaki": acc_oz, "native": acc_nat,
+                     "check": "device double-double on 4101 sampled entries, bound 2ku|A||B|"},
+        "native_fp64": {"value": round(world * nat_gflops, 1), "unit": "GFLOP/s", "ms_per_step": round(nat_ms, 3),
+                        "kernel_ms": round(dmma_ms, 3),
+                        "frac_of_dmma_peak": round(flops / (dmma_ms * 1e-3) / 1e12 / peaks["fp64_dmma_tflops"], 4),
+                        "gpu_launches": int(nat_launches)},
+        "ozaki": {"slices": oz_rep["slices"], "products": P, "est_err_ratio": oz_rep["est_err_ratio"],
+                  "split_ms": round(split_ms, 3), "gemm_ms": round(gemm_ms, 3),
+                  "speedup_vs_native": round(oz_gflops / nat_gflops, 3)},
+        "peaks_probed": {k: round(v, 2) for k, v in peaks.items()},
+        "roofline": {"bound": "tensor", "kernel": "ozaki_gemm_kernel (tcgen05 kind::i8)",
+                     "achieved": round(achieved_tops, 1), "peak": round(peaks["int8_tops"], 1),
+                     "unit": "TFLOP/s", "frac": round(achieved_tops / peaks["int8_tops"], 4),
+                     "traffic": traffic,
+                     "peak_source": "INT8 dense tcgen05 rate measured by the in-library probe in this run "
+                                    "(MEASURED_PEAKS.json has no INT8 figure)",
+                     "bf16_probe_vs_measured_peaks": (round(peaks["bf16_tflops"] / mp["bf16_tflops"], 3)
+                                                      if mp and mp.get("bf16_tflops") else None),
+                     "ops_per_launch": int8_ops_per_launch},
+        "e2e": e2e,
+    }
+    if world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(size, args.cpu_seconds)
+    print(json.dumps(line), flush=True)
+    ctx.close()
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

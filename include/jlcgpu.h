@@ -1,0 +1,204 @@
+/*
+ * jlcgpu.h -- C ABI of libjlcgpu, the B200 (sm_100a) GEMM engine behind JLC's
+ * GPU route.  Plain C types only: pointers, 64-bit sizes, doubles.  A Java 21
+ * Panama FFM binding (or ctypes, JNA, ...) binds these symbols directly.
+ *
+ * Every matrix is FP64.  Unless a function says "device", pointers are HOST
+ * pointers (heap copies or OffHeapMatrix MemorySegment addresses); the
+ * library stages them through its own device buffers, runs its own kernels
+ * (no cuBLAS, no CPU fallback) and returns when C is written back.
+ *
+ * Semantics shared by all GEMM entries (C <- alpha*op(A)*op(B) + beta*C):
+ *  - beta == 0: C is not read (NaN/Inf already in C are cleared).
+ *  - alpha == 0 or k == 0: A and B are not read; C <- beta*C.
+ *  - m == 0 or n == 0: nothing is touched.
+ *  - C elements outside the logical m x n window (ld padding) are never written.
+ *  - No zero-skip: 0*Inf contributes NaN as IEEE arithmetic says.
+ * Return value: JLC_OK (0) or a negative JLC_E_* code; jlc_last_error() then
+ * holds a message.  Argument errors mirror the IllegalArgumentException cases
+ * of the reference (null matrices, inner or output dimension mismatch).
+ *
+ * Thread safety: a jlc_ctx is owned by one thread at a time (the Java side
+ * keeps one per thread, as GemmWorkspace does).  Different contexts may be
+ * used concurrently.
+ */
+#ifndef JLCGPU_H
+#define JLCGPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define JLCGPU_VERSION 1
+
+#if defined(__GNUC__)
+#define JLC_API __attribute__((visibility("default")))
+#else
+#define JLC_API
+#endif
+
+/* status codes */
+#define JLC_OK 0
+#define JLC_E_ARG (-1)         /* invalid argument (IllegalArgumentException in the reference) */
+#define JLC_E_NODEV (-2)       /* no usable sm_100 device */
+#define JLC_E_OOM (-3)         /* device or pinned allocation failed */
+#define JLC_E_LAUNCH (-4)      /* kernel launch failed */
+#define JLC_E_TIMEOUT (-5)     /* a bounded device wait expired; results are not valid */
+#define JLC_E_UNSUPPORTED (-6) /* combination not supported */
+#define JLC_E_CUDA (-7)        /* other CUDA runtime error */
+
+/* storage order of an operand (OffHeapMatrix.Order, OffHeapMatrix.java:15-70) */
+#define JLC_ROW_MAJOR 0
+#define JLC_COL_MAJOR 1
+
+/* arithmetic used for the product */
+#define JLC_PREC_NATIVE 0 /* FP64 DMMA tensor-core kernel */
+#define JLC_PREC_OZAKI 1  /* Ozaki split: INT8 slices on tcgen05, FP64 recombination */
+#define JLC_PREC_AUTO 2   /* library picks (Ozaki for large, well-formed products) */
+
+/* kernel classes reported back (GemmDispatch.Kernel, GemmDispatch.java:40-47, on the GPU) */
+#define JLC_KERNEL_NONE 0    /* nothing to multiply (alpha==0, k==0, empty) */
+#define JLC_KERNEL_DMMA 1    /* tiled FP64 DMMA GEMM */
+#define JLC_KERNEL_GEMV 2    /* HBM-bound matrix-vector (n == 1 or m == 1) */
+#define JLC_KERNEL_OZAKI 3   /* INT8 tcgen05 slice products */
+#define JLC_KERNEL_GROUPED 4 /* persistent grouped launch */
+
+typedef struct jlc_ctx jlc_ctx;
+
+/* Per-call report (all fields written on success). */
+typedef struct jlc_report {
+    int32_t precision;     /* JLC_PREC_NATIVE or JLC_PREC_OZAKI actually used */
+    int32_t kernel;        /* JLC_KERNEL_* */
+    int32_t slices;        /* Ozaki slice count s (0 for native) */
+    int32_t products;      /* INT8 slice products run (s(s+1)/2 for Ozaki) */
+    double est_err_ratio;  /* Ozaki a-priori error estimate / FP64 bound (0 for native) */
+    double device_ms;      /* device time of the call, CUDA events (host entries only) */
+    int64_t h2d_bytes;     /* bytes copied host -> device by this call */
+    int64_t d2h_bytes;     /* bytes copied device -> host by this call */
+} jlc_report;
+
+/* ---------------------------------------------------------------- context */
+JLC_API int jlc_version(void);
+/* number of visible devices that can run libjlcgpu (sm_100) */
+JLC_API int jlc_device_count(int* count);
+/* Replaces CudaSupport.isCudaAvailable() probing (CudaSupport.java:34-76) and
+ * the placeholder CudaContext (CudaContext.java:11-56): a persistent context
+ * with its own stream, device buffer pool and pinned staging. */
+JLC_API int jlc_init(int device, jlc_ctx** out);
+JLC_API void jlc_destroy(jlc_ctx* ctx);
+/* message of the last failing call on this context ("" if none) */
+JLC_API const char* jlc_last_error(const jlc_ctx* ctx);
+/* run this context's device work on a caller-supplied cudaStream_t (NULL:
+ * back to the context's own stream) */
+JLC_API int jlc_set_stream(jlc_ctx* ctx, void* cuda_stream);
+JLC_API int jlc_synchronize(jlc_ctx* ctx);
+/* page-lock caller memory (e.g. an OffHeapMatrix segment) so host entries
+ * copy it by DMA; unregister before freeing it */
+JLC_API int jlc_host_register(jlc_ctx* ctx, void* ptr, size_t bytes);
+JLC_API int jlc_host_unregister(jlc_ctx* ctx, void* ptr);
+
+/* ---------------------------------------------------------------- host GEMM entries */
+/* CudaGemm.gemm(Matrix a, Matrix b, Matrix c, double alpha, double beta)
+ * (CudaGemm.java:53-134): dense row-major a (m x k), b (k x n), c (m x n). */
+JLC_API int jlc_gemm(jlc_ctx* ctx, const double* a, const double* b, double* c, int64_t m, int64_t k, int64_t n,
+             double alpha, double beta, int precision, jlc_report* rep);
+
+/* BLAS3Kernels.gemmStrided (BLAS3Kernels.java:244-251) and
+ * OptimizedBLAS3.gemmStrided (OptimizedBLAS3.java:135-179):
+ * C[m x n] = alpha*A[m x k]*B[k x n] + beta*C, row-major, element offsets and
+ * leading dimensions as in the reference (a[aOff + i*lda + p]). */
+JLC_API int jlc_gemm_strided(jlc_ctx* ctx, const double* a, int64_t a_off, int64_t lda, const double* b, int64_t b_off,
+                     int64_t ldb, double* c, int64_t c_off, int64_t ldc, int64_t m, int64_t k, int64_t n,
+                     double alpha, double beta, int precision, jlc_report* rep);
+
+/* BLAS3Kernels.gemmStridedTransA (BLAS3Kernels.java:272-279): A is m x k and
+ * B is m x n (row-major); the output is k x n: C = alpha*A^T*B + beta*C. */
+JLC_API int jlc_gemm_strided_transa(jlc_ctx* ctx, const double* a, int64_t a_off, int64_t lda, const double* b,
+                            int64_t b_off, int64_t ldb, double* c, int64_t c_off, int64_t ldc, int64_t m,
+                            int64_t k, int64_t n, double alpha, double beta, int precision, jlc_report* rep);
+
+/* BLAS3Kernels.gemmStridedColMajorA (BLAS3Kernels.java:284-291):
+ * A(i,p) = a[aOff + p*lda + i]; B and C row-major. */
+JLC_API int jlc_gemm_strided_colmajor_a(jlc_ctx* ctx, const double* a, int64_t a_off, int64_t lda, const double* b,
+                                int64_t b_off, int64_t ldb, double* c, int64_t c_off, int64_t ldc, int64_t m,
+                                int64_t k, int64_t n, double alpha, double beta, int precision,
+                                jlc_report* rep);
+
+/* BLAS3Kernels.gemmStridedColMajorB (BLAS3Kernels.java:296-303):
+ * B(p,j) = b[bOff + j*ldb + p]; A and C row-major. */
+JLC_API int jlc_gemm_strided_colmajor_b(jlc_ctx* ctx, const double* a, int64_t a_off, int64_t lda, const double* b,
+                                int64_t b_off, int64_t ldb, double* c, int64_t c_off, int64_t ldc, int64_t m,
+                                int64_t k, int64_t n, double alpha, double beta, int precision,
+                                jlc_report* rep);
+
+/* General host form: op(A) is m x k stored with layout_a (JLC_ROW_MAJOR:
+ * a[i*lda + p]; JLC_COL_MAJOR: a[p*lda + i]), op(B) is k x n with layout_b,
+ * C is row-major m x n with ldc.  Covers OffHeapMatrix operands of either
+ * order (OffHeapMatrix.order()/ld(), OffHeapMatrix.java:122-148). */
+JLC_API int jlc_dgemm(jlc_ctx* ctx, int layout_a, int layout_b, int64_t m, int64_t n, int64_t k, double alpha,
+              const double* a, int64_t lda, const double* b, int64_t ldb, double beta, double* c, int64_t ldc,
+              int precision, jlc_report* rep);
+
+/* ---------------------------------------------------------------- device entries */
+/* Same as jlc_dgemm on DEVICE pointers, enqueued on the context stream and
+ * returning without synchronising (benchmarks, device-resident callers,
+ * CUDA-graph capture). */
+JLC_API int jlc_dgemm_device(jlc_ctx* ctx, int layout_a, int layout_b, int64_t m, int64_t n, int64_t k, double alpha,
+                     const double* a, int64_t lda, const double* b, int64_t ldb, double beta, double* c,
+                     int64_t ldc, int precision, jlc_report* rep);
+
+/* Ozaki split-precision GEMM on device pointers with an explicit slice count
+ * (slices in [3,8]; 0 = choose per call from the inputs' scale statistics). */
+JLC_API int jlc_dgemm_ozaki_device(jlc_ctx* ctx, int layout_a, int layout_b, int64_t m, int64_t n, int64_t k,
+                           double alpha, const double* a, int64_t lda, const double* b, int64_t ldb, double beta,
+                           double* c, int64_t ldc, int slices, jlc_report* rep);
+
+/* Reads and clears the context's device status word after synchronising:
+ * JLC_OK, or JLC_E_TIMEOUT if a kernel gave up on a bounded wait. */
+JLC_API int jlc_device_status(jlc_ctx* ctx);
+
+/* ---------------------------------------------------------------- measurement */
+/* phases the profiler records (one CUDA event pair per phase and call) */
+#define JLC_PHASE_DMMA 1        /* FP64 DMMA GEMM kernel */
+#define JLC_PHASE_GEMV 2        /* matrix-vector kernel(s) */
+#define JLC_PHASE_OZAKI_GEMM 3  /* INT8 tcgen05 slice-product GEMM + FP64 recombination */
+#define JLC_PHASE_OZAKI_SPLIT 5 /* exponent scaling + INT8 slicing of A and B */
+#define JLC_PHASE_SCALE 6       /* beta-only update of C */
+#define JLC_PHASE_FP64_GATED 7  /* FP64 kernel behind an Ozaki call (runs only on Inf/NaN input) */
+#define JLC_PHASE_H2D 8         /* host -> device operand copies */
+#define JLC_PHASE_D2H 9         /* device -> host copy of C */
+/* Turn event-pair recording around each phase on (1) or off (0).  Records
+ * accumulate (up to 4096) until collected. */
+JLC_API int jlc_set_profiling(jlc_ctx* ctx, int on);
+/* Synchronises, then writes up to max (phase, milliseconds) records in launch
+ * order, clears them and returns how many were written (or a JLC_E_* code). */
+JLC_API int jlc_profile_collect(jlc_ctx* ctx, int* phases, double* ms, int max);
+/* Number of kernels this context has launched since jlc_init. */
+JLC_API int jlc_launch_count(jlc_ctx* ctx, int64_t* launches);
+
+/* A-posteriori accuracy check of a finished device GEMM (no reference
+ * counterpart; the reference's GemmReference oracle is a plain FP64 loop).
+ * For count sampled entries (rows[e], cols[e]) (HOST arrays) it evaluates
+ * alpha*op(A)*op(B) + beta*C_in in double-double on the device and writes
+ *   *max_ratio = max_e |C_out - C_dd| / (2 k u (|alpha| (|A||B|)_e + |beta| |C_in|_e))
+ *   *max_abs   = max_e |C_out - C_dd|,  *over = entries with ratio > 1.
+ * c_in may be NULL when beta == 0.  Synchronous. */
+JLC_API int jlc_check_fp64_bound_device(jlc_ctx* ctx, int layout_a, int layout_b, int64_t m, int64_t n, int64_t k,
+                                        double alpha, const double* a, int64_t lda, const double* b, int64_t ldb,
+                                        double beta, const double* c_in, int64_t ldc_in, const double* c_out,
+                                        int64_t ldc_out, int64_t count, const int64_t* rows, const int64_t* cols,
+                                        double* max_ratio, double* max_abs, int64_t* over);
+
+/* Measures the running GPU's throughput ceilings (TFLOP/s or TOPS) with probe
+ * kernels: [0] FP64 on mma.sync .f64 (DMMA), [1] FP64 on DFMA, [2] INT8 on
+ * tcgen05 (dense), [3] BF16 on tcgen05 (dense).  Takes about a second. */
+JLC_API int jlc_measure_peaks(jlc_ctx* ctx, double* out4);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* JLCGPU_H */

@@ -1,0 +1,701 @@
+// libjlcgpu C ABI: contexts, argument validation, host staging and dispatch.
+//
+// The host entries replace net.faulj.compute.CudaGemm (CudaGemm.java:53-134),
+// which paid cublasCreate + cudaMalloc x3 + free x3 on every call: here a
+// context keeps its stream, its device buffers (grow-only) and its workspace
+// across calls, and only the copies of the operands remain per call.
+#include <cudaTypedefs.h>
+
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <mutex>
+
+#include "jlc_internal.h"
+
+using namespace jlc;
+
+struct DevBuf {
+    void* ptr = nullptr;
+    size_t bytes = 0;
+};
+
+struct jlc_ctx {
+    int device = 0;
+    int sm_count = 0;
+    cudaStream_t own_stream = nullptr;
+    cudaStream_t stream = nullptr;
+    int* d_status = nullptr;  // status word written by kernels (JLC_DEV_* bits)
+    int* d_flags = nullptr;   // control flags (e.g. the Ozaki non-finite gate)
+    DevBuf bufA, bufB, bufC;
+    Workspace ws;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    int dmma_k = 8;
+    // profiler: event pairs around phases, reused from a pool
+    bool profiling = false;
+    static constexpr int kMaxRec = 4096;
+    int nrec = 0;
+    int rec_phase[kMaxRec];
+    cudaEvent_t rec_ev[2 * kMaxRec] = {};
+    int64_t launches = 0;
+    char err[512] = {0};
+};
+
+namespace {
+
+int set_err(jlc_ctx* ctx, int code, const char* fmt, ...) {
+    if (ctx) {
+        va_list ap;
+        va_start(ap, fmt);
+        vsnprintf(ctx->err, sizeof(ctx->err), fmt, ap);
+        va_end(ap);
+    }
+    return code;
+}
+
+int cuda_err(jlc_ctx* ctx, cudaError_t e, const char* what) {
+    if (e == cudaErrorMemoryAllocation) return set_err(ctx, JLC_E_OOM, "%s: %s", what, cudaGetErrorString(e));
+    return set_err(ctx, JLC_E_CUDA, "%s: %s", what, cudaGetErrorString(e));
+}
+
+int reserve(jlc_ctx* ctx, DevBuf& b, size_t bytes, const char* what) {
+    if (bytes <= b.bytes) return JLC_OK;
+    if (b.ptr) cudaFree(b.ptr);
+    b.ptr = nullptr;
+    b.bytes = 0;
+    size_t want = bytes + bytes / 8;  // grow with slack, like GemmWorkspace's grow-only buffers
+    cudaError_t e = cudaMalloc(&b.ptr, want);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        e = cudaMalloc(&b.ptr, bytes);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            b.ptr = nullptr;
+            return cuda_err(ctx, e, what);
+        }
+        want = bytes;
+    }
+    b.bytes = want;
+    return JLC_OK;
+}
+
+inline long long round_up(long long v, long long m) { return (v + m - 1) / m * m; }
+
+// Phase markers for the profiler: begin() records the start event of a new
+// record, end() its stop event.  Both are no-ops when profiling is off or the
+// record buffer is full.
+struct Phase {
+    jlc_ctx* ctx;
+    int idx = -1;
+    Phase(jlc_ctx* c, int phase) : ctx(c) {
+        if (!ctx->profiling || ctx->nrec >= jlc_ctx::kMaxRec) return;
+        idx = ctx->nrec++;
+        for (int e = 0; e < 2; ++e)
+            if (!ctx->rec_ev[2 * idx + e]) cudaEventCreate(&ctx->rec_ev[2 * idx + e]);
+        ctx->rec_phase[idx] = phase;
+        cudaEventRecord(ctx->rec_ev[2 * idx], ctx->stream);
+    }
+    ~Phase() {
+        if (idx >= 0) cudaEventRecord(ctx->rec_ev[2 * idx + 1], ctx->stream);
+    }
+};
+
+// Validation shared by host and device entries: the IllegalArgumentException
+// cases of CudaGemm.gemm / OptimizedBLAS3.gemm (null matrices, negative sizes,
+// leading dimensions too small for the declared shape).
+int validate(jlc_ctx* ctx, int la, int lb, long long m, long long n, long long k, const void* a, long long lda,
+             const void* b, long long ldb, const void* c, long long ldc) {
+    if (!ctx) return JLC_E_ARG;
+    if (m < 0 || n < 0 || k < 0) return set_err(ctx, JLC_E_ARG, "dimensions must be non-negative");
+    if ((la != JLC_ROW_MAJOR && la != JLC_COL_MAJOR) || (lb != JLC_ROW_MAJOR && lb != JLC_COL_MAJOR))
+        return set_err(ctx, JLC_E_ARG, "layout must be JLC_ROW_MAJOR or JLC_COL_MAJOR");
+    if (m > 0 && n > 0 && c == nullptr) return set_err(ctx, JLC_E_ARG, "Matrices must not be null");
+    if (m > 0 && n > 0 && ldc < n) return set_err(ctx, JLC_E_ARG, "ldc (%lld) < n (%lld)", ldc, n);
+    if (m > 0 && n > 0 && k > 0) {
+        if (a == nullptr || b == nullptr) return set_err(ctx, JLC_E_ARG, "Matrices must not be null");
+        const long long need_a = la == JLC_ROW_MAJOR ? k : m;
+        const long long need_b = lb == JLC_ROW_MAJOR ? n : k;
+        if (lda < need_a) return set_err(ctx, JLC_E_ARG, "lda (%lld) too small (need >= %lld)", lda, need_a);
+        if (ldb < need_b) return set_err(ctx, JLC_E_ARG, "ldb (%lld) too small (need >= %lld)", ldb, need_b);
+    }
+    if (m > INT32_MAX / 2 || n > INT32_MAX / 2 || k > INT32_MAX / 2)
+        return set_err(ctx, JLC_E_UNSUPPORTED, "dimension above 2^30");
+    return JLC_OK;
+}
+
+void report_init(jlc_report* rep) {
+    if (rep) memset(rep, 0, sizeof(*rep));
+}
+
+// Ozaki slice count from the a-priori model (see ozaki.cu): the smallest s in
+// [5,8] whose worst-case error estimate stays inside the FP64 bound for
+// inputs whose |A||B| is not far below rowmax*colmax*k.
+int auto_slices(long long k) {
+    // (s+3) * 2^-7s <= 2u * k * rho^2 with rho = 1/4 (uniform-like rows/cols)
+    const double u = std::ldexp(1.0, -53);
+    for (int s = 5; s <= 8; ++s) {
+        const double lhs = (s + 3) * std::ldexp(1.0, -7 * s);
+        const double rhs = 2.0 * u * (double)k / 16.0;
+        if (lhs <= rhs) return s;
+    }
+    return 8;
+}
+
+bool use_ozaki(int precision, long long m, long long n, long long k) {
+    if (precision == JLC_PREC_OZAKI) return true;
+    if (precision == JLC_PREC_NATIVE) return false;
+    return m >= 2048 && n >= 2048 && k >= 1024;  // AUTO: large products only
+}
+
+// Device dispatch on already-validated device operands.
+int run_device(jlc_ctx* ctx, const GemmDesc& g0, int precision, int slices, jlc_report* rep) {
+    GemmDesc g = g0;
+    if (rep) rep->precision = JLC_PREC_NATIVE;
+    if (g.m == 0 || g.n == 0) {
+        if (rep) rep->kernel = JLC_KERNEL_NONE;
+        return JLC_OK;
+    }
+    if (g.alpha == 0.0 || g.k == 0) {
+        if (rep) rep->kernel = JLC_KERNEL_NONE;
+        if (g.beta == 1.0) return JLC_OK;
+        Phase ph(ctx, JLC_PHASE_SCALE);
+        ctx->launches += 1;
+        int rc = launch_scale_c(g.c, g.ldc, g.m, g.n, g.beta, ctx->stream);
+        return rc ? set_err(ctx, rc, "scale kernel launch failed") : JLC_OK;
+    }
+    if (g.n == 1 || g.m == 1) {
+        GemvDesc v;
+        if (g.n == 1) {
+            // y = C(:,0), rows of op(A) dotted with x = B(:,0)
+            v.rows = g.m;
+            v.cols = g.k;
+            v.mat = g.a;
+            v.rs = g.layout_a == JLC_ROW_MAJOR ? g.lda : 1;
+            v.cs = g.layout_a == JLC_ROW_MAJOR ? 1 : g.lda;
+            v.x = g.b;
+            v.incx = g.layout_b == JLC_ROW_MAJOR ? g.ldb : 1;
+            v.y = g.c;
+            v.incy = g.ldc;
+        } else {
+            // y^T = C(0,:) = A(0,:) * B  ->  y = B^T x with x = A(0,:)
+            v.rows = g.n;
+            v.cols = g.k;
+            v.mat = g.b;
+            v.rs = g.layout_b == JLC_ROW_MAJOR ? 1 : g.ldb;
+            v.cs = g.layout_b == JLC_ROW_MAJOR ? g.ldb : 1;
+            v.x = g.a;
+            v.incx = g.layout_a == JLC_ROW_MAJOR ? 1 : g.lda;
+            v.y = g.c;
+            v.incy = 1;
+        }
+        v.alpha = g.alpha;
+        v.beta = g.beta;
+        if (v.cs != 1 && v.rs != 1) {
+            // single row/column with both strides > 1 cannot happen for a
+            // matrix operand; k == 1 makes either stride irrelevant
+            if (v.cols == 1) v.cs = 1;
+            else if (v.rows == 1) v.rs = 1;
+        }
+        size_t need = gemv_scratch_bytes(v, ctx->sm_count);
+        if (need) {
+            int rc = workspace_reserve(ctx->ws, need, ctx->err, sizeof(ctx->err));
+            if (rc) return rc;
+        }
+        if (rep) rep->kernel = JLC_KERNEL_GEMV;
+        Phase ph(ctx, JLC_PHASE_GEMV);
+        ctx->launches += v.cs == 1 ? 1 : 2;
+        return launch_gemv(v, ctx->ws.ptr, ctx->stream, ctx->sm_count, ctx->err, sizeof(ctx->err));
+    }
+    const bool ozaki = use_ozaki(precision, g.m, g.n, g.k);
+    int rc = JLC_OK;
+    if (ozaki) {
+        const int s = slices > 0 ? slices : auto_slices(g.k);
+        size_t need = ozaki_workspace_bytes(g.m, g.n, g.k, s, ctx->sm_count);
+        rc = workspace_reserve(ctx->ws, need, ctx->err, sizeof(ctx->err));
+        if (rc) return rc;
+        {
+            Phase ph(ctx, JLC_PHASE_OZAKI_SPLIT);
+            ctx->launches += (g.layout_a == JLC_ROW_MAJOR ? 1 : 2) + (g.layout_b == JLC_COL_MAJOR ? 1 : 2);
+            rc = launch_ozaki_split(g, s, ctx->ws.ptr, ctx->ws.bytes, ctx->stream, ctx->sm_count, ctx->d_flags,
+                                    ctx->err, sizeof(ctx->err));
+        }
+        if (rc) return rc;
+        {
+            Phase ph(ctx, JLC_PHASE_OZAKI_GEMM);
+            ctx->launches += 1;
+            rc = launch_ozaki_gemm(g, s, ctx->ws.ptr, ctx->ws.bytes, ctx->stream, ctx->sm_count, ctx->d_status,
+                                   ctx->d_flags, ctx->err, sizeof(ctx->err));
+        }
+        if (rc) return rc;
+        if (rep) {
+            rep->precision = JLC_PREC_OZAKI;
+            rep->kernel = JLC_KERNEL_OZAKI;
+            rep->slices = s;
+            rep->products = s * (s + 1) / 2;
+            const double u = std::ldexp(1.0, -53);
+            rep->est_err_ratio = (s + 3) * std::ldexp(1.0, -7 * s) / (2.0 * u * (double)g.k / 16.0);
+        }
+    }
+    // the DMMA kernel reads A/B through TMA: 16-byte aligned bases, even lds
+    if (!dmma_operand_ok(g.a, g.lda)) {
+        const long long rows = g.layout_a == JLC_ROW_MAJOR ? g.m : g.k;
+        const long long cols = g.layout_a == JLC_ROW_MAJOR ? g.k : g.m;
+        const long long ld = round_up(cols, 8);
+        if ((rc = reserve(ctx, ctx->bufA, (size_t)(rows * ld) * 8, "repack A"))) return rc;
+        cudaError_t e = cudaMemcpy2DAsync(ctx->bufA.ptr, ld * 8, g.a, g.lda * 8, cols * 8, rows,
+                                          cudaMemcpyDeviceToDevice, ctx->stream);
+        if (e != cudaSuccess) return cuda_err(ctx, e, "repack A");
+        g.a = (const double*)ctx->bufA.ptr;
+        g.lda = ld;
+    }
+    if (!dmma_operand_ok(g.b, g.ldb)) {
+        const long long rows = g.layout_b == JLC_ROW_MAJOR ? g.k : g.n;
+        const long long cols = g.layout_b == JLC_ROW_MAJOR ? g.n : g.k;
+        const long long ld = round_up(cols, 8);
+        if ((rc = reserve(ctx, ctx->bufB, (size_t)(rows * ld) * 8, "repack B"))) return rc;
+        cudaError_t e = cudaMemcpy2DAsync(ctx->bufB.ptr, ld * 8, g.b, g.ldb * 8, cols * 8, rows,
+                                          cudaMemcpyDeviceToDevice, ctx->stream);
+        if (e != cudaSuccess) return cuda_err(ctx, e, "repack B");
+        g.b = (const double*)ctx->bufB.ptr;
+        g.ldb = ld;
+    }
+    if (!ozaki && rep) rep->kernel = JLC_KERNEL_DMMA;
+    // After an Ozaki launch the FP64 kernel is gated on the split's
+    // non-finite flag: it only runs when Inf/NaN made slicing impossible.
+    Phase ph(ctx, ozaki ? JLC_PHASE_FP64_GATED : JLC_PHASE_DMMA);
+    ctx->launches += 1;
+    return launch_dgemm_dmma(g, ctx->stream, ctx->sm_count, ctx->d_status, ozaki ? ctx->d_flags : nullptr,
+                             ctx->dmma_k, ctx->err, sizeof(ctx->err));
+}
+
+int finish_sync(jlc_ctx* ctx) {
+    cudaError_t e = cudaStreamSynchronize(ctx->stream);
+    if (e != cudaSuccess) return cuda_err(ctx, e, "stream synchronize");
+    int st = 0;
+    e = cudaMemcpy(&st, ctx->d_status, sizeof(int), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return cuda_err(ctx, e, "status read");
+    if (st != 0) {
+        cudaMemset(ctx->d_status, 0, sizeof(int));
+        if (st & JLC_DEV_TIMEOUT) return set_err(ctx, JLC_E_TIMEOUT, "a device wait timed out (status 0x%x)", st);
+        return set_err(ctx, JLC_E_CUDA, "device status 0x%x", st);
+    }
+    return JLC_OK;
+}
+
+// Host entry: stage op(A), op(B) (and C when beta != 0) into context buffers
+// with 16-byte-aligned, padded leading dimensions, run, copy C back into the
+// caller's m x n window only.
+int run_host(jlc_ctx* ctx, int la, int lb, long long m, long long n, long long k, double alpha, const double* a,
+             long long lda, const double* b, long long ldb, double beta, double* c, long long ldc, int precision,
+             jlc_report* rep) {
+    report_init(rep);
+    int rc = validate(ctx, la, lb, m, n, k, a, lda, b, ldb, c, ldc);
+    if (rc) return rc;
+    if (m == 0 || n == 0) return JLC_OK;
+    ctx->err[0] = 0;
+    cudaError_t e;
+    const bool need_ab = alpha != 0.0 && k > 0;
+    const long long a_rows = la == JLC_ROW_MAJOR ? m : k, a_cols = la == JLC_ROW_MAJOR ? k : m;
+    const long long b_rows = lb == JLC_ROW_MAJOR ? k : n, b_cols = lb == JLC_ROW_MAJOR ? n : k;
+    const long long dlda = round_up(a_cols, 8), dldb = round_up(b_cols, 8), dldc = round_up(n, 8);
+    int64_t h2d = 0, d2h = 0;
+    if (need_ab) {
+        if ((rc = reserve(ctx, ctx->bufA, (size_t)(a_rows * dlda) * 8, "device A"))) return rc;
+        if ((rc = reserve(ctx, ctx->bufB, (size_t)(b_rows * dldb) * 8, "device B"))) return rc;
+    }
+    if ((rc = reserve(ctx, ctx->bufC, (size_t)(m * dldc) * 8, "device C"))) return rc;
+    cudaEventRecord(ctx->ev0, ctx->stream);
+    {
+    Phase ph(ctx, JLC_PHASE_H2D);
+    if (need_ab) {
+        e = cudaMemcpy2DAsync(ctx->bufA.ptr, dlda * 8, a, lda * 8, a_cols * 8, a_rows, cudaMemcpyHostToDevice,
+                              ctx->stream);
+        if (e != cudaSuccess) return cuda_err(ctx, e, "copy A to device");
+        e = cudaMemcpy2DAsync(ctx->bufB.ptr, dldb * 8, b, ldb * 8, b_cols * 8, b_rows, cudaMemcpyHostToDevice,
+                              ctx->stream);
+        if (e != cudaSuccess) return cuda_err(ctx, e, "copy B to device");
+        h2d += (a_rows * a_cols + b_rows * b_cols) * 8;
+    }
+    if (beta != 0.0) {
+        e = cudaMemcpy2DAsync(ctx->bufC.ptr, dldc * 8, c, ldc * 8, n * 8, m, cudaMemcpyHostToDevice, ctx->stream);
+        if (e != cudaSuccess) return cuda_err(ctx, e, "copy C to device");
+        h2d += m * n * 8;
+    }
+    }
+    GemmDesc g{la, lb, m, n, k, alpha, beta, (const double*)ctx->bufA.ptr, dlda, (const double*)ctx->bufB.ptr,
+               dldb, (double*)ctx->bufC.ptr, dldc};
+    rc = run_device(ctx, g, precision, 0, rep);
+    if (rc) {
+        cudaStreamSynchronize(ctx->stream);
+        return rc;
+    }
+    {
+        Phase ph(ctx, JLC_PHASE_D2H);
+        e = cudaMemcpy2DAsync(c, ldc * 8, ctx->bufC.ptr, dldc * 8, n * 8, m, cudaMemcpyDeviceToHost, ctx->stream);
+    }
+    if (e != cudaSuccess) return cuda_err(ctx, e, "copy C to host");
+    d2h += m * n * 8;
+    cudaEventRecord(ctx->ev1, ctx->stream);
+    rc = finish_sync(ctx);
+    if (rc) return rc;
+    if (rep) {
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
+        rep->device_ms = ms;
+        rep->h2d_bytes = h2d;
+        rep->d2h_bytes = d2h;
+    }
+    return JLC_OK;
+}
+
+}  // namespace
+
+namespace jlc {
+
+int workspace_reserve(Workspace& w, size_t bytes, char* err, size_t errlen) {
+    if (bytes <= w.bytes) return JLC_OK;
+    if (w.ptr) cudaFree(w.ptr);
+    w.ptr = nullptr;
+    w.bytes = 0;
+    cudaError_t e = cudaMalloc(&w.ptr, bytes);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        w.ptr = nullptr;
+        snprintf(err, errlen, "workspace allocation of %zu bytes failed: %s", bytes, cudaGetErrorString(e));
+        return JLC_E_OOM;
+    }
+    w.bytes = bytes;
+    return JLC_OK;
+}
+
+static PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    });
+    return fn;
+}
+
+int make_tmap_2d(CUtensorMap* map, CUtensorMapDataType dt, int elem_bytes, void* base, uint64_t inner,
+                 uint64_t outer, uint64_t ld_elems, uint32_t box_inner, uint32_t box_outer, CUtensorMapSwizzle sw,
+                 char* err, size_t errlen) {
+    auto fn = encode_fn();
+    if (!fn) {
+        snprintf(err, errlen, "cuTensorMapEncodeTiled unavailable");
+        return JLC_E_CUDA;
+    }
+    cuuint64_t dims[2] = {inner, outer};
+    cuuint64_t strides[1] = {ld_elems * (uint64_t)elem_bytes};
+    cuuint32_t box[2] = {box_inner, box_outer};
+    cuuint32_t estr[2] = {1, 1};
+    CUresult r = fn(map, dt, 2, base, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, sw,
+                    CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) {
+        snprintf(err, errlen, "cuTensorMapEncodeTiled(2d) failed (%d): dims %llu x %llu ld %llu box %u x %u",
+                 (int)r, (unsigned long long)inner, (unsigned long long)outer, (unsigned long long)ld_elems,
+                 box_inner, box_outer);
+        return JLC_E_CUDA;
+    }
+    return JLC_OK;
+}
+
+int make_tmap_3d(CUtensorMap* map, CUtensorMapDataType dt, int elem_bytes, void* base, uint64_t d0, uint64_t d1,
+                 uint64_t d2, uint64_t stride1_elems, uint64_t stride2_elems, uint32_t b0, uint32_t b1, uint32_t b2,
+                 CUtensorMapSwizzle sw, char* err, size_t errlen) {
+    auto fn = encode_fn();
+    if (!fn) {
+        snprintf(err, errlen, "cuTensorMapEncodeTiled unavailable");
+        return JLC_E_CUDA;
+    }
+    cuuint64_t dims[3] = {d0, d1, d2};
+    cuuint64_t strides[2] = {stride1_elems * (uint64_t)elem_bytes, stride2_elems * (uint64_t)elem_bytes};
+    cuuint32_t box[3] = {b0, b1, b2};
+    cuuint32_t estr[3] = {1, 1, 1};
+    CUresult r = fn(map, dt, 3, base, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, sw,
+                    CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) {
+        snprintf(err, errlen, "cuTensorMapEncodeTiled(3d) failed (%d)", (int)r);
+        return JLC_E_CUDA;
+    }
+    return JLC_OK;
+}
+
+}  // namespace jlc
+
+// ======================================================================== C ABI
+extern "C" {
+
+int jlc_version(void) { return JLCGPU_VERSION; }
+
+int jlc_device_count(int* count) {
+    if (!count) return JLC_E_ARG;
+    *count = 0;
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess) {
+        cudaGetLastError();
+        return JLC_OK;
+    }
+    int usable = 0;
+    for (int d = 0; d < n; ++d) {
+        int major = 0;
+        if (cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, d) == cudaSuccess && major == 10)
+            ++usable;
+    }
+    *count = usable;
+    return JLC_OK;
+}
+
+int jlc_init(int device, jlc_ctx** out) {
+    if (!out) return JLC_E_ARG;
+    *out = nullptr;
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || device < 0 || device >= n) {
+        cudaGetLastError();
+        return JLC_E_NODEV;
+    }
+    int major = 0, minor = 0;
+    cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, device);
+    cudaDeviceGetAttribute(&minor, cudaDevAttrComputeCapabilityMinor, device);
+    if (major != 10 || minor != 0) return JLC_E_NODEV;  // sm_100a code only
+    if (cudaSetDevice(device) != cudaSuccess) return JLC_E_NODEV;
+    jlc_ctx* ctx = new (std::nothrow) jlc_ctx();
+    if (!ctx) return JLC_E_OOM;
+    ctx->device = device;
+    cudaDeviceGetAttribute(&ctx->sm_count, cudaDevAttrMultiProcessorCount, device);
+    if (const char* e = getenv("JLCGPU_DMMA_K")) {
+        int v = atoi(e);
+        if (v == 4 || v == 8 || v == 16) ctx->dmma_k = v;
+    }
+    bool ok = cudaStreamCreateWithFlags(&ctx->own_stream, cudaStreamNonBlocking) == cudaSuccess &&
+              cudaMalloc(&ctx->d_status, 2 * sizeof(int)) == cudaSuccess &&
+              cudaMalloc(&ctx->d_flags, 4 * sizeof(int)) == cudaSuccess &&
+              cudaEventCreate(&ctx->ev0) == cudaSuccess && cudaEventCreate(&ctx->ev1) == cudaSuccess;
+    if (ok) ok = cudaMemset(ctx->d_status, 0, 2 * sizeof(int)) == cudaSuccess &&
+                 cudaMemset(ctx->d_flags, 0, 4 * sizeof(int)) == cudaSuccess;
+    if (!ok) {
+        cudaGetLastError();
+        jlc_destroy(ctx);
+        return JLC_E_CUDA;
+    }
+    ctx->stream = ctx->own_stream;
+    *out = ctx;
+    return JLC_OK;
+}
+
+void jlc_destroy(jlc_ctx* ctx) {
+    if (!ctx) return;
+    cudaSetDevice(ctx->device);
+    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    if (ctx->bufA.ptr) cudaFree(ctx->bufA.ptr);
+    if (ctx->bufB.ptr) cudaFree(ctx->bufB.ptr);
+    if (ctx->bufC.ptr) cudaFree(ctx->bufC.ptr);
+    if (ctx->ws.ptr) cudaFree(ctx->ws.ptr);
+    if (ctx->d_status) cudaFree(ctx->d_status);
+    if (ctx->d_flags) cudaFree(ctx->d_flags);
+    for (int i = 0; i < 2 * jlc_ctx::kMaxRec; ++i)
+        if (ctx->rec_ev[i]) cudaEventDestroy(ctx->rec_ev[i]);
+    if (ctx->ev0) cudaEventDestroy(ctx->ev0);
+    if (ctx->ev1) cudaEventDestroy(ctx->ev1);
+    if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
+    delete ctx;
+}
+
+const char* jlc_last_error(const jlc_ctx* ctx) { return ctx ? ctx->err : "null context"; }
+
+int jlc_set_stream(jlc_ctx* ctx, void* cuda_stream) {
+    if (!ctx) return JLC_E_ARG;
+    ctx->stream = cuda_stream ? static_cast<cudaStream_t>(cuda_stream) : ctx->own_stream;
+    return JLC_OK;
+}
+
+int jlc_synchronize(jlc_ctx* ctx) {
+    if (!ctx) return JLC_E_ARG;
+    cudaSetDevice(ctx->device);
+    return finish_sync(ctx);
+}
+
+int jlc_device_status(jlc_ctx* ctx) { return jlc_synchronize(ctx); }
+
+int jlc_host_register(jlc_ctx* ctx, void* ptr, size_t bytes) {
+    if (!ctx || !ptr || bytes == 0) return set_err(ctx, JLC_E_ARG, "host_register: bad arguments");
+    cudaSetDevice(ctx->device);
+    cudaError_t e = cudaHostRegister(ptr, bytes, cudaHostRegisterPortable);
+    return e == cudaSuccess ? JLC_OK : cuda_err(ctx, e, "cudaHostRegister");
+}
+
+int jlc_host_unregister(jlc_ctx* ctx, void* ptr) {
+    if (!ctx || !ptr) return set_err(ctx, JLC_E_ARG, "host_unregister: bad arguments");
+    cudaSetDevice(ctx->device);
+    cudaError_t e = cudaHostUnregister(ptr);
+    return e == cudaSuccess ? JLC_OK : cuda_err(ctx, e, "cudaHostUnregister");
+}
+
+int jlc_gemm(jlc_ctx* ctx, const double* a, const double* b, double* c, int64_t m, int64_t k, int64_t n,
+             double alpha, double beta, int precision, jlc_report* rep) {
+    if (!ctx) return JLC_E_ARG;
+    cudaSetDevice(ctx->device);
+    return run_host(ctx, JLC_ROW_MAJOR, JLC_ROW_MAJOR, m, n, k, alpha, a, k, b, n, beta, c, n, precision, rep);
+}
+
+int jlc_dgemm(jlc_ctx* ctx, int layout_a, int layout_b, int64_t m, int64_t n, int64_t k, double alpha,
+              const double* a, int64_t lda, const double* b, int64_t ldb, double beta, double* c, int64_t ldc,
+              int precision, jlc_report* rep) {
+    if (!ctx) return JLC_E_ARG;
+    cudaSetDevice(ctx->device);
+    return run_host(ctx, layout_a, layout_b, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc, precision, rep);
+}
+
+static int strided_entry(jlc_ctx* ctx, int la, int lb, const double* a, int64_t a_off, int64_t lda,
+                         const double* b, int64_t b_off, int64_t ldb, double* c, int64_t c_off, int64_t ldc,
+                         int64_t m, int64_t n, int64_t k, double alpha, double beta, int precision,
+                         jlc_report* rep) {
+    if (!ctx) return JLC_E_ARG;
+    if (a_off < 0 || b_off < 0 || c_off < 0) return set_err(ctx, JLC_E_ARG, "offsets must be non-negative");
+    cudaSetDevice(ctx->device);
+    return run_host(ctx, la, lb, m, n, k, alpha, a ? a + a_off : nullptr, lda, b ? b + b_off : nullptr, ldb, beta,
+                    c ? c + c_off : nullptr, ldc, precision, rep);
+}
+
+int jlc_gemm_strided(jlc_ctx* ctx, const double* a, int64_t a_off, int64_t lda, const double* b, int64_t b_off,
+                     int64_t ldb, double* c, int64_t c_off, int64_t ldc, int64_t m, int64_t k, int64_t n,
+                     double alpha, double beta, int precision, jlc_report* rep) {
+    return strided_entry(ctx, JLC_ROW_MAJOR, JLC_ROW_MAJOR, a, a_off, lda, b, b_off, ldb, c, c_off, ldc, m, n, k,
+                         alpha, beta, precision, rep);
+}
+
+int jlc_gemm_strided_transa(jlc_ctx* ctx, const double* a, int64_t a_off, int64_t lda, const double* b,
+                            int64_t b_off, int64_t ldb, double* c, int64_t c_off, int64_t ldc, int64_t m,
+                            int64_t k, int64_t n, double alpha, double beta, int precision, jlc_report* rep) {
+    // output k x n, contraction over m: op(A)(i,p) = A(p,i) = a[p*lda + i] (column-major view)
+    return strided_entry(ctx, JLC_COL_MAJOR, JLC_ROW_MAJOR, a, a_off, lda, b, b_off, ldb, c, c_off, ldc, k, n, m,
+                         alpha, beta, precision, rep);
+}
+
+int jlc_gemm_strided_colmajor_a(jlc_ctx* ctx, const double* a, int64_t a_off, int64_t lda, const double* b,
+                                int64_t b_off, int64_t ldb, double* c, int64_t c_off, int64_t ldc, int64_t m,
+                                int64_t k, int64_t n, double alpha, double beta, int precision,
+                                jlc_report* rep) {
+    return strided_entry(ctx, JLC_COL_MAJOR, JLC_ROW_MAJOR, a, a_off, lda, b, b_off, ldb, c, c_off, ldc, m, n, k,
+                         alpha, beta, precision, rep);
+}
+
+int jlc_gemm_strided_colmajor_b(jlc_ctx* ctx, const double* a, int64_t a_off, int64_t lda, const double* b,
+                                int64_t b_off, int64_t ldb, double* c, int64_t c_off, int64_t ldc, int64_t m,
+                                int64_t k, int64_t n, double alpha, double beta, int precision,
+                                jlc_report* rep) {
+    return strided_entry(ctx, JLC_ROW_MAJOR, JLC_COL_MAJOR, a, a_off, lda, b, b_off, ldb, c, c_off, ldc, m, n, k,
+                         alpha, beta, precision, rep);
+}
+
+int jlc_dgemm_device(jlc_ctx* ctx, int layout_a, int layout_b, int64_t m, int64_t n, int64_t k, double alpha,
+                     const double* a, int64_t lda, const double* b, int64_t ldb, double beta, double* c,
+                     int64_t ldc, int precision, jlc_report* rep) {
+    report_init(rep);
+    int rc = validate(ctx, layout_a, layout_b, m, n, k, a, lda, b, ldb, c, ldc);
+    if (rc) return rc;
+    cudaSetDevice(ctx->device);
+    GemmDesc g{layout_a, layout_b, m, n, k, alpha, beta, a, lda, b, ldb, c, ldc};
+    return run_device(ctx, g, precision, 0, rep);
+}
+
+int jlc_dgemm_ozaki_device(jlc_ctx* ctx, int layout_a, int layout_b, int64_t m, int64_t n, int64_t k,
+                           double alpha, const double* a, int64_t lda, const double* b, int64_t ldb, double beta,
+                           double* c, int64_t ldc, int slices, jlc_report* rep) {
+    report_init(rep);
+    int rc = validate(ctx, layout_a, layout_b, m, n, k, a, lda, b, ldb, c, ldc);
+    if (rc) return rc;
+    if (slices != 0 && (slices < 3 || slices > 8)) return set_err(ctx, JLC_E_ARG, "slices must be 0 or in [3,8]");
+    cudaSetDevice(ctx->device);
+    GemmDesc g{layout_a, layout_b, m, n, k, alpha, beta, a, lda, b, ldb, c, ldc};
+    return run_device(ctx, g, JLC_PREC_OZAKI, slices, rep);
+}
+
+int jlc_set_profiling(jlc_ctx* ctx, int on) {
+    if (!ctx) return JLC_E_ARG;
+    ctx->profiling = on != 0;
+    return JLC_OK;
+}
+
+int jlc_profile_collect(jlc_ctx* ctx, int* phases, double* ms, int max) {
+    if (!ctx || max < 0 || (max > 0 && (!phases || !ms))) return JLC_E_ARG;
+    cudaSetDevice(ctx->device);
+    cudaError_t e = cudaStreamSynchronize(ctx->stream);
+    if (e != cudaSuccess) return cuda_err(ctx, e, "profile synchronize");
+    const int n = ctx->nrec < max ? ctx->nrec : max;
+    for (int i = 0; i < n; ++i) {
+        float t = 0.f;
+        e = cudaEventElapsedTime(&t, ctx->rec_ev[2 * i], ctx->rec_ev[2 * i + 1]);
+        if (e != cudaSuccess) return cuda_err(ctx, e, "profile event");
+        phases[i] = ctx->rec_phase[i];
+        ms[i] = t;
+    }
+    ctx->nrec = 0;
+    return n;
+}
+
+int jlc_check_fp64_bound_device(jlc_ctx* ctx, int layout_a, int layout_b, int64_t m, int64_t n, int64_t k,
+                                double alpha, const double* a, int64_t lda, const double* b, int64_t ldb,
+                                double beta, const double* c_in, int64_t ldc_in, const double* c_out,
+                                int64_t ldc_out, int64_t count, const int64_t* rows, const int64_t* cols,
+                                double* max_ratio, double* max_abs, int64_t* over) {
+    int rc = validate(ctx, layout_a, layout_b, m, n, k, a, lda, b, ldb, c_out, ldc_out);
+    if (rc) return rc;
+    if (count < 0 || (count > 0 && (!rows || !cols)) || !max_ratio || !max_abs || !over)
+        return set_err(ctx, JLC_E_ARG, "check: bad sample arguments");
+    if (beta != 0.0 && (!c_in || ldc_in < n)) return set_err(ctx, JLC_E_ARG, "check: beta != 0 needs C_in");
+    for (int64_t e = 0; e < count; ++e)
+        if (rows[e] < 0 || rows[e] >= m || cols[e] < 0 || cols[e] >= n)
+            return set_err(ctx, JLC_E_ARG, "check: sample entry %lld out of range", (long long)e);
+    cudaSetDevice(ctx->device);
+    const size_t bytes = (size_t)count * 16 + 64;
+    DevBuf tmp;
+    if ((rc = reserve(ctx, tmp, bytes, "check buffers"))) return rc;
+    auto* d_rows = static_cast<long long*>(tmp.ptr);
+    auto* d_cols = d_rows + count;
+    auto* d_out = reinterpret_cast<unsigned long long*>(d_cols + count);
+    cudaError_t e = cudaMemcpyAsync(d_rows, rows, count * 8, cudaMemcpyHostToDevice, ctx->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(d_cols, cols, count * 8, cudaMemcpyHostToDevice, ctx->stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(d_out, 0, 24, ctx->stream);
+    if (e != cudaSuccess) {
+        cudaFree(tmp.ptr);
+        return cuda_err(ctx, e, "check setup");
+    }
+    GemmDesc g{layout_a, layout_b, m, n, k, alpha, beta, a, lda, b, ldb, nullptr, 0};
+    rc = check_fp64_bound(g, c_in, ldc_in, c_out, ldc_out, count, d_rows, d_cols, d_out, ctx->stream);
+    unsigned long long h[3] = {0, 0, 0};
+    if (!rc) e = cudaMemcpyAsync(h, d_out, 24, cudaMemcpyDeviceToHost, ctx->stream);
+    if (!rc && e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    cudaFree(tmp.ptr);
+    if (rc) return set_err(ctx, rc, "check kernel launch failed");
+    if (e != cudaSuccess) return cuda_err(ctx, e, "check");
+    double r, ab;
+    memcpy(&r, &h[0], 8);
+    memcpy(&ab, &h[1], 8);
+    *max_ratio = r;
+    *max_abs = ab;
+    *over = (int64_t)h[2];
+    return JLC_OK;
+}
+
+int jlc_measure_peaks(jlc_ctx* ctx, double* out4) {
+    if (!ctx || !out4) return JLC_E_ARG;
+    cudaSetDevice(ctx->device);
+    int rc = measure_peaks(ctx->sm_count, ctx->stream, ctx->d_status, out4, ctx->err, sizeof(ctx->err));
+    if (rc) return rc;
+    return finish_sync(ctx);
+}
+
+int jlc_launch_count(jlc_ctx* ctx, int64_t* launches) {
+    if (!ctx || !launches) return JLC_E_ARG;
+    *launches = ctx->launches;
+    return JLC_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,370 @@
+// FP64 GEMM on the B200 double-precision tensor path (mma.sync .f64, "DMMA").
+//
+// C[m x n] = alpha * op(A)[m x k] * op(B)[k x n] + beta * C, row-major C.
+// Replaces the packed CPU path of OptimizedBLAS3 (OptimizedBLAS3.java:184-385,
+// PackingUtils.java:37-183, MicroKernel.java:94-271):
+//  * packA/packB become TMA tile loads into 128B-swizzled shared memory
+//    (A row- or column-major, B row- or column-major: the four layouts of
+//    BLAS3Kernels.gemmStrided / TransA / ColMajorA / ColMajorB);
+//  * alpha is folded into the A fragments as they are staged from shared
+//    memory into registers, so every product uses round(alpha*a) exactly as
+//    packA does; beta is applied in the fused epilogue (C is not read when
+//    beta == 0, as PackingUtils.scaleCPanel clears it);
+//  * the VectorMask remainder becomes TMA out-of-bounds zero fill plus masked
+//    epilogue stores.
+//
+// Structure: persistent CTAs (one per SM), warp-specialised, 3 warpgroups.
+// Warpgroup 0 is the producer (one lane issues TMA into a STAGES-deep ring
+// guarded by full/empty mbarriers) and gives registers back with
+// setmaxnreg.dec; warpgroups 1-2 are the 8 consumer warps, arranged 2 (M) x
+// 4 (N), each owning a 64 x 32 slab of the 128 x 128 C tile as 4 x 4 m16n8
+// accumulators, and take the registers with setmaxnreg.inc.
+// Register budget: the launch gives 384 threads x 168 = 64512 registers;
+// after the split 128 x 40 + 256 x 224 = 62464 are in use.
+//
+// K permutation: inside each k-step the logical k index of the mma fragment
+// layout is remapped to a physical column of the shared tile so that the four
+// rows a warp reads per fragment fall into different 64-byte halves of the
+// 128B swizzle pattern; A and B use the same map, so the sum is unchanged and
+// every fragment load is bank-conflict free.
+#include <cstdio>
+
+#include "jlc_device.cuh"
+#include "jlc_internal.h"
+
+namespace jlc {
+namespace dmma {
+
+constexpr int BM = 128, BN = 128, BK = 16;  // BK in doubles: one 128-byte swizzle row
+constexpr int STAGES = 5;
+constexpr int WARPS_M = 2, WARPS_N = 4, MMA_WARPS = WARPS_M * WARPS_N;
+constexpr int WM = BM / WARPS_M, WN = BN / WARPS_N;  // 64 x 32 per warp
+constexpr int MT = WM / 16, NT = WN / 8;              // 4 x 4 m16n8 tiles
+constexpr int PRODUCER_WARPS = 4;  // one full warpgroup, required by setmaxnreg
+constexpr int THREADS = (MMA_WARPS + PRODUCER_WARPS) * 32;
+constexpr int PRODUCER_REGS = 40, CONSUMER_REGS = 224;
+static_assert(PRODUCER_WARPS * 32 * PRODUCER_REGS + MMA_WARPS * 32 * CONSUMER_REGS <= THREADS * 168,
+              "setmaxnreg split exceeds the registers the CTA is launched with");
+constexpr int A_STAGE = BM * BK * 8;  // 16 KB
+constexpr int B_STAGE = BN * BK * 8;  // 16 KB
+constexpr int STAGE_BYTES = A_STAGE + B_STAGE;
+constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024 + 2 * STAGES * 8;
+constexpr int RASTER_GROUP = 8;
+
+struct Params {
+    int M, N, K;
+    double alpha, beta;
+    double* C;
+    long long ldc;
+    int tiles_m, tiles_n, num_tiles, k_blocks;
+    int* status;
+    const int* gate;  // when non-null the kernel runs only if *gate != 0
+};
+
+// Byte offset of element (r, c) in a tile whose rows are 128 bytes (16 doubles)
+// and which TMA wrote with the 128B swizzle (16-byte unit index ^= row & 7).
+__device__ __forceinline__ uint32_t kmajor_off(int r, int c) {
+    return uint32_t(r) * 128u + ((uint32_t((c >> 1) ^ (r & 7)) << 4) | (uint32_t(c & 1) << 3));
+}
+// Byte offset of element (mn, k) in a tile stored as 16-wide MN chunks of
+// [16 k rows][16 mn doubles], each chunk 2 KB, swizzled the same way.
+__device__ __forceinline__ uint32_t mnmajor_off(int mn, int k) {
+    return uint32_t(mn >> 4) * 2048u + uint32_t(k) * 128u +
+           ((uint32_t((((mn & 15) >> 1) ^ (k & 7))) << 4) | (uint32_t(mn & 1) << 3));
+}
+
+template <bool A_KMAJOR>
+__device__ __forceinline__ double lds_a(const char* sA, int m, int k) {
+    return *reinterpret_cast<const double*>(sA + (A_KMAJOR ? kmajor_off(m, k) : mnmajor_off(m, k)));
+}
+template <bool B_KMAJOR>
+__device__ __forceinline__ double lds_b(const char* sB, int k, int n) {
+    return *reinterpret_cast<const double*>(sB + (B_KMAJOR ? kmajor_off(n, k) : mnmajor_off(n, k)));
+}
+
+// Physical k column (0..15 inside the stage) for mma k-step q, thread-in-group
+// t and fragment k-slot j (logical k = 4j + t).
+template <int MMA_K>
+__device__ __forceinline__ int phys_k(int q, int t, int j) {
+    if constexpr (MMA_K == 4) {
+        // q-th k4 step uses physical columns {0,1,4,5} + {0,2,8,10}[q]
+        const int base = (q & 1) * 2 + (q >> 1) * 8;
+        return base + (t & 1) + (t >> 1) * 4;
+    } else if constexpr (MMA_K == 8) {
+        return q * 8 + 2 * t + j;
+    } else {
+        return 4 * t + j;
+    }
+}
+
+template <int MMA_K>
+__device__ __forceinline__ void mma_f64(double (&d)[4], const double* a, const double* b) {
+    if constexpr (MMA_K == 4) {
+        asm volatile(
+            "mma.sync.aligned.m16n8k4.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5}, {%6}, {%0,%1,%2,%3};\n"
+            : "+d"(d[0]), "+d"(d[1]), "+d"(d[2]), "+d"(d[3])
+            : "d"(a[0]), "d"(a[1]), "d"(b[0]));
+    } else if constexpr (MMA_K == 8) {
+        asm volatile(
+            "mma.sync.aligned.m16n8k8.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+            "{%0,%1,%2,%3};\n"
+            : "+d"(d[0]), "+d"(d[1]), "+d"(d[2]), "+d"(d[3])
+            : "d"(a[0]), "d"(a[1]), "d"(a[2]), "d"(a[3]), "d"(b[0]), "d"(b[1]));
+    } else {
+        asm volatile(
+            "mma.sync.aligned.m16n8k16.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5,%6,%7,%8,%9,%10,%11}, "
+            "{%12,%13,%14,%15}, {%0,%1,%2,%3};\n"
+            : "+d"(d[0]), "+d"(d[1]), "+d"(d[2]), "+d"(d[3])
+            : "d"(a[0]), "d"(a[1]), "d"(a[2]), "d"(a[3]), "d"(a[4]), "d"(a[5]), "d"(a[6]), "d"(a[7]),
+              "d"(b[0]), "d"(b[1]), "d"(b[2]), "d"(b[3]));
+    }
+}
+
+// Bounded wait used only while draining: ignores errors recorded by others
+// so that copies this CTA issued have landed before it exits.
+__device__ __forceinline__ void drain_wait(uint64_t* bar, uint32_t parity, int* status) {
+    const uint32_t b = smem_u32(bar);
+    const uint64_t t0 = globaltimer_ns();
+    while (!mbar_try_wait(b, parity)) {
+        if (globaltimer_ns() - t0 > kWaitTimeoutNs) {
+            atomicOr(status, JLC_DEV_TIMEOUT);
+            return;
+        }
+    }
+}
+
+template <bool A_KMAJOR, bool B_KMAJOR, int MMA_K>
+__global__ void __launch_bounds__(THREADS, 1)
+    dgemm_dmma_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB,
+                      const Params p) {
+    if (p.gate != nullptr && *p.gate == 0) return;
+    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    char* smem = reinterpret_cast<char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    uint64_t* full = reinterpret_cast<uint64_t*>(smem + STAGES * STAGE_BYTES);
+    uint64_t* empty = full + STAGES;
+
+    const int warp = warp_id(), lane = lane_id();
+    if (threadIdx.x == 0) {
+        tma_prefetch_desc(&mapA);
+        tma_prefetch_desc(&mapB);
+        for (int s = 0; s < STAGES; ++s) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], MMA_WARPS);
+        }
+        fence_barrier_init();
+    }
+    __syncthreads();
+
+    if (warp < PRODUCER_WARPS) {
+        // ---------------- producer ----------------
+        asm volatile("setmaxnreg.dec.sync.aligned.u32 %0;\n" ::"n"(PRODUCER_REGS));
+        if (warp == 0 && lane == 0) {
+            int stage = 0;
+            uint32_t phase = 0;
+            uint32_t armed = 0, last_parity = 0;  // per-stage bit sets, for the drain
+            bool ok = true;
+            for (int tile = blockIdx.x; tile < p.num_tiles && ok; tile += gridDim.x) {
+                int tm, tn;
+                tile_coords(tile, p.tiles_m, p.tiles_n, RASTER_GROUP, tm, tn);
+                const int m0 = tm * BM, n0 = tn * BN;
+                for (int kb = 0; kb < p.k_blocks; ++kb) {
+                    if (!mbar_wait(&empty[stage], phase ^ 1u, p.status)) {
+                        ok = false;
+                        break;
+                    }
+                    char* sA = smem + stage * STAGE_BYTES;
+                    char* sB = sA + A_STAGE;
+                    const int k0 = kb * BK;
+                    mbar_arrive_expect_tx(&full[stage], STAGE_BYTES);
+                    if constexpr (A_KMAJOR) {
+                        tma_load_2d(sA, &mapA, &full[stage], k0, m0);
+                    } else {
+#pragma unroll
+                        for (int c = 0; c < BM / 16; ++c) tma_load_2d(sA + c * 2048, &mapA, &full[stage], m0 + 16 * c, k0);
+                    }
+                    if constexpr (B_KMAJOR) {
+                        tma_load_2d(sB, &mapB, &full[stage], k0, n0);
+                    } else {
+#pragma unroll
+                        for (int c = 0; c < BN / 16; ++c) tma_load_2d(sB + c * 2048, &mapB, &full[stage], n0 + 16 * c, k0);
+                    }
+                    armed |= 1u << stage;
+                    last_parity = (last_parity & ~(1u << stage)) | (phase << stage);
+                    if (++stage == STAGES) {
+                        stage = 0;
+                        phase ^= 1u;
+                    }
+                }
+            }
+            // drain: every copy this CTA issued must land before it exits
+            for (int s = 0; s < STAGES; ++s)
+                if (armed & (1u << s)) drain_wait(&full[s], (last_parity >> s) & 1u, p.status);
+        }
+        return;
+    }
+
+    // ---------------- consumers ----------------
+    asm volatile("setmaxnreg.inc.sync.aligned.u32 %0;\n" ::"n"(CONSUMER_REGS));
+    const int g = lane >> 2, t = lane & 3;
+    const int cw = warp - PRODUCER_WARPS;
+    const int warp_m = cw / WARPS_N, warp_n = cw % WARPS_N;
+    const bool scale_a = p.alpha != 1.0;
+    int stage = 0;
+    uint32_t phase = 0;
+    constexpr int STEPS = BK / MMA_K;
+    constexpr int AREG = MMA_K / 2;  // doubles of A per m16 tile per step
+    constexpr int BREG = MMA_K / 4;  // doubles of B per n8 tile per step
+
+    for (int tile = blockIdx.x; tile < p.num_tiles; tile += gridDim.x) {
+        int tm, tn;
+        tile_coords(tile, p.tiles_m, p.tiles_n, RASTER_GROUP, tm, tn);
+        double acc[MT][NT][4];
+#pragma unroll
+        for (int i = 0; i < MT; ++i)
+#pragma unroll
+            for (int j = 0; j < NT; ++j)
+#pragma unroll
+                for (int e = 0; e < 4; ++e) acc[i][j][e] = 0.0;
+
+        for (int kb = 0; kb < p.k_blocks; ++kb) {
+            if (!mbar_wait(&full[stage], phase, p.status)) return;
+            const char* sA = smem + stage * STAGE_BYTES;
+            const char* sB = sA + A_STAGE;
+#pragma unroll
+            for (int q = 0; q < STEPS; ++q) {
+                // B fragments of the four n8 tiles stay live for the step; A
+                // fragments are staged one m16 tile at a time.
+                double bf[NT][BREG];
+#pragma unroll
+                for (int nt = 0; nt < NT; ++nt) {
+                    const int c = warp_n * WN + nt * 8 + g;
+#pragma unroll
+                    for (int j = 0; j < BREG; ++j) bf[nt][j] = lds_b<B_KMAJOR>(sB, phys_k<MMA_K>(q, t, j), c);
+                }
+#pragma unroll
+                for (int mt = 0; mt < MT; ++mt) {
+                    const int r = warp_m * WM + mt * 16 + g;
+                    double af[AREG];
+#pragma unroll
+                    for (int i = 0; i < AREG; ++i) {
+                        // register i: row g + 8*(i&1), k-slot i>>1
+                        af[i] = lds_a<A_KMAJOR>(sA, r + 8 * (i & 1), phys_k<MMA_K>(q, t, i >> 1));
+                    }
+                    if (scale_a) {
+#pragma unroll
+                        for (int i = 0; i < AREG; ++i) af[i] *= p.alpha;
+                    }
+#pragma unroll
+                    for (int nt = 0; nt < NT; ++nt) mma_f64<MMA_K>(acc[mt][nt], af, bf[nt]);
+                }
+            }
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&empty[stage]);
+            if (++stage == STAGES) {
+                stage = 0;
+                phase ^= 1u;
+            }
+        }
+
+        // fused epilogue: C = acc + beta * C_old (C_old not read when beta == 0)
+        const int row0 = tm * BM + warp_m * WM;
+        const int col0 = tn * BN + warp_n * WN;
+#pragma unroll
+        for (int mt = 0; mt < MT; ++mt) {
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const int row = row0 + mt * 16 + g + 8 * h;
+                if (row >= p.M) continue;
+                double* crow = p.C + (long long)row * p.ldc;
+#pragma unroll
+                for (int nt = 0; nt < NT; ++nt) {
+#pragma unroll
+                    for (int e = 0; e < 2; ++e) {
+                        const int col = col0 + nt * 8 + 2 * t + e;
+                        if (col < p.N) {
+                            const double v = acc[mt][nt][2 * h + e];
+                            crow[col] = (p.beta == 0.0) ? v : fma(p.beta, crow[col], v);
+                        }
+                    }
+                }
+            }
+        }
+    }
+}
+
+template <bool AK, bool BK_, int MK>
+static int launch_variant(const CUtensorMap& ma, const CUtensorMap& mb, const Params& p, int grid,
+                          cudaStream_t st) {
+    auto kern = dgemm_dmma_kernel<AK, BK_, MK>;
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES);
+    if (e != cudaSuccess) return JLC_E_LAUNCH;
+    kern<<<grid, THREADS, SMEM_BYTES, st>>>(ma, mb, p);
+    return cudaGetLastError() == cudaSuccess ? JLC_OK : JLC_E_LAUNCH;
+}
+
+}  // namespace dmma
+
+bool dmma_operand_ok(const void* ptr, long long ld) {
+    return (reinterpret_cast<uintptr_t>(ptr) % 16 == 0) && ((ld * 8) % 16 == 0) && ld > 0;
+}
+
+int launch_dgemm_dmma(const GemmDesc& g, cudaStream_t st, int sm_count, int* status, const int* gate,
+                      int mma_k, char* err, size_t errlen) {
+    using namespace dmma;
+    if (!dmma_operand_ok(g.a, g.lda) || !dmma_operand_ok(g.b, g.ldb)) {
+        snprintf(err, errlen, "DMMA kernel needs 16-byte aligned A/B and even leading dimensions");
+        return JLC_E_UNSUPPORTED;
+    }
+    const bool a_k = g.layout_a == 0;  // row-major A: k contiguous
+    const bool b_k = g.layout_b == 1;  // column-major B: k contiguous
+    CUtensorMap ma, mb;
+    int rc;
+    if (a_k)
+        rc = make_tmap_2d(&ma, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 8, (void*)g.a, g.k, g.m, g.lda, BK, BM,
+                          CU_TENSOR_MAP_SWIZZLE_128B, err, errlen);
+    else
+        rc = make_tmap_2d(&ma, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 8, (void*)g.a, g.m, g.k, g.lda, 16, BK,
+                          CU_TENSOR_MAP_SWIZZLE_128B, err, errlen);
+    if (rc) return rc;
+    if (b_k)
+        rc = make_tmap_2d(&mb, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 8, (void*)g.b, g.k, g.n, g.ldb, BK, BN,
+                          CU_TENSOR_MAP_SWIZZLE_128B, err, errlen);
+    else
+        rc = make_tmap_2d(&mb, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 8, (void*)g.b, g.n, g.k, g.ldb, 16, BK,
+                          CU_TENSOR_MAP_SWIZZLE_128B, err, errlen);
+    if (rc) return rc;
+
+    Params p;
+    p.M = (int)g.m;
+    p.N = (int)g.n;
+    p.K = (int)g.k;
+    p.alpha = g.alpha;
+    p.beta = g.beta;
+    p.C = g.c;
+    p.ldc = g.ldc;
+    p.tiles_m = (int)((g.m + BM - 1) / BM);
+    p.tiles_n = (int)((g.n + BN - 1) / BN);
+    p.num_tiles = p.tiles_m * p.tiles_n;
+    p.k_blocks = (int)((g.k + BK - 1) / BK);
+    p.status = status;
+    p.gate = gate;
+    const int grid = p.num_tiles < sm_count ? p.num_tiles : sm_count;
+
+#define JLC_DMMA_DISPATCH(MK)                                                     \
+    if (a_k && b_k) rc = launch_variant<true, true, MK>(ma, mb, p, grid, st);      \
+    else if (a_k) rc = launch_variant<true, false, MK>(ma, mb, p, grid, st);       \
+    else if (b_k) rc = launch_variant<false, true, MK>(ma, mb, p, grid, st);       \
+    else rc = launch_variant<false, false, MK>(ma, mb, p, grid, st);
+    if (mma_k == 4) {
+        JLC_DMMA_DISPATCH(4)
+    } else if (mma_k == 16) {
+        JLC_DMMA_DISPATCH(16)
+    } else {
+        JLC_DMMA_DISPATCH(8)
+    }
+#undef JLC_DMMA_DISPATCH
+    if (rc) snprintf(err, errlen, "DMMA kernel launch failed: %s", cudaGetErrorString(cudaGetLastError()));
+    return rc;
+}
+
+}  // namespace jlc

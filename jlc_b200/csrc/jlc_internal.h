@@ -1,0 +1,95 @@
+// Host-side internal interface of libjlcgpu: operand descriptors, tensor-map
+// helpers and kernel launchers.  Not part of the public C ABI.
+#pragma once
+#include <cuda.h>
+#include <cuda_runtime.h>
+
+#include <cstddef>
+#include <cstdint>
+
+#include "jlc_errors.h"
+#include "jlcgpu.h"
+
+namespace jlc {
+
+// One GEMM on device pointers: C[m x n] (row-major, ldc) =
+//   alpha * op(A)[m x k] * op(B)[k x n] + beta * C.
+// layout_a: JLC_ROW_MAJOR -> A(i,p) = a[i*lda + p]; JLC_COL_MAJOR -> a[p*lda + i].
+// layout_b: JLC_ROW_MAJOR -> B(p,j) = b[p*ldb + j]; JLC_COL_MAJOR -> b[j*ldb + p].
+struct GemmDesc {
+    int layout_a, layout_b;
+    long long m, n, k;
+    double alpha, beta;
+    const double* a;
+    long long lda;
+    const double* b;
+    long long ldb;
+    double* c;
+    long long ldc;
+};
+
+// Grow-only device scratch owned by a context.
+struct Workspace {
+    void* ptr = nullptr;
+    size_t bytes = 0;
+};
+int workspace_reserve(Workspace& w, size_t bytes, char* err, size_t errlen);
+
+// TMA descriptors (cuTensorMapEncodeTiled through the runtime's driver entry point).
+int make_tmap_2d(CUtensorMap* map, CUtensorMapDataType dt, int elem_bytes, void* base, uint64_t inner,
+                 uint64_t outer, uint64_t ld_elems, uint32_t box_inner, uint32_t box_outer, CUtensorMapSwizzle sw,
+                 char* err, size_t errlen);
+int make_tmap_3d(CUtensorMap* map, CUtensorMapDataType dt, int elem_bytes, void* base, uint64_t d0, uint64_t d1,
+                 uint64_t d2, uint64_t stride1_elems, uint64_t stride2_elems, uint32_t b0, uint32_t b1, uint32_t b2,
+                 CUtensorMapSwizzle sw, char* err, size_t errlen);
+
+bool dmma_operand_ok(const void* ptr, long long ld);
+
+// FP64 DMMA tiled GEMM.  A/B must be 16-byte aligned with even leading
+// dimensions.  gate != nullptr: the kernel only runs if *gate != 0.
+int launch_dgemm_dmma(const GemmDesc& g, cudaStream_t st, int sm_count, int* status, const int* gate, int mma_k,
+                      char* err, size_t errlen);
+
+// y[i*incy] = alpha * sum_p M(i,p) x[p*incx] + beta * y[i*incy], M(i,p) = mat[i*rs + p*cs]
+// with rs == 1 or cs == 1.  scratch: ceil-split partial sums for the rs == 1 form.
+struct GemvDesc {
+    long long rows, cols;
+    double alpha, beta;
+    const double* mat;
+    long long rs, cs;
+    const double* x;
+    long long incx;
+    double* y;
+    long long incy;
+};
+size_t gemv_scratch_bytes(const GemvDesc& g, int sm_count);
+int launch_gemv(const GemvDesc& g, void* scratch, cudaStream_t st, int sm_count, char* err, size_t errlen);
+
+// C <- beta * C on the m x n window (beta == 0 writes zeros without reading).
+int launch_scale_c(double* c, long long ldc, long long m, long long n, double beta, cudaStream_t st);
+
+// Ozaki split-precision GEMM (INT8 slices on tcgen05, FP64 recombination).
+struct OzakiPlan {
+    int slices;         // s
+    int products;       // s(s+1)/2
+    double est_ratio;   // a-priori error / bound estimate for the chosen s (host-side model)
+};
+size_t ozaki_workspace_bytes(long long m, long long n, long long k, int slices, int sm_count);
+// Phase 1: exponents + INT8 slices of op(A) and op(B) into the workspace; sets
+// flags[0] when an operand holds Inf/NaN.  Phase 2: the tcgen05 slice-product
+// GEMM with FP64 recombination into C (skipped on the device when flags[0]).
+int launch_ozaki_split(const GemmDesc& g, int slices, void* workspace, size_t ws_bytes, cudaStream_t st,
+                       int sm_count, int* flags, char* err, size_t errlen);
+int launch_ozaki_gemm(const GemmDesc& g, int slices, void* workspace, size_t ws_bytes, cudaStream_t st,
+                      int sm_count, int* status, int* flags, char* err, size_t errlen);
+
+// double-double accuracy check of sampled entries (verify.cu); d_out3 holds
+// [max ratio bits, max abs error bits, entries over the bound], zeroed by the caller
+int check_fp64_bound(const GemmDesc& g, const double* c_in, long long ldc_in, const double* c_out, long long ldc_out,
+                     long long count, const long long* d_rows, const long long* d_cols, unsigned long long* d_out3,
+                     cudaStream_t st);
+
+// throughput probes (peaks.cu): out4 = {DMMA FP64, DFMA FP64, INT8 tcgen05, BF16 tcgen05} in T(FL)OP/s
+int measure_peaks(int sm_count, cudaStream_t st, int* status, double* out4, char* err, size_t errlen);
+
+}  // namespace jlc

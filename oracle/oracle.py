@@ -1,0 +1,230 @@
+"""CPU oracle for the JLC FP64 GEMM path -- TEST INFRASTRUCTURE ONLY.
+
+Only tests/, ``__graft_entry__.smoke()`` and bench.py's CPU-baseline leg may
+import this module, and only as the checker or the timed CPU baseline.  The
+shipped library (``jlc_b200``) never imports it.
+
+It wraps ``liboracle.so`` (built from ``jlc_oracle.c`` by the Makefile beside
+it) with numpy-friendly helpers.  The C file documents, per function, which
+reference file and lines it restates:
+
+* ``seeded_array``      -- GemmReference.seededArray (GemmReference.java:14-25)
+* ``gemm_reference``    -- GemmReference.gemm* (GemmReference.java:31-112)
+* ``gemm_fmachain``     -- OptimizedBLAS3 / BLAS3Kernels packed-path order
+* ``opt_gemm``          -- OptimizedBLAS3.gemm dispatch (OptimizedBLAS3.java:61-130)
+* ``gemm_packed_parallel`` -- PARALLEL_MICRO (OptimizedBLAS3.java:295-385)
+* ``gemm_dd``           -- double-double oracle + componentwise FP64 bound
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "liboracle.so")
+_lib = None
+
+_dp = ctypes.POINTER(ctypes.c_double)
+_i64p = ctypes.POINTER(ctypes.c_int64)
+_i64 = ctypes.c_int64
+_d = ctypes.c_double
+
+# kernel classes of GemmDispatch.Kernel (GemmDispatch.java:40-47)
+TINY, SMALL, MATVEC, MICROKERNEL, CUDA, PARALLEL_MICRO = range(6)
+
+
+def build(force: bool = False) -> str:
+    """Compile liboracle.so with the Makefile beside this file."""
+    src = os.path.join(_HERE, "jlc_oracle.c")
+    if force or not os.path.exists(_LIB_PATH) or os.path.getmtime(_LIB_PATH) < os.path.getmtime(src):
+        subprocess.run(["make", "-s", "-C", _HERE], check=True)
+    return _LIB_PATH
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(_LIB_PATH):
+            build()
+        L = ctypes.CDLL(_LIB_PATH)
+        L.orc_splittable_doubles.argtypes = [_dp, _i64, _i64, _d, _d]
+        L.orc_seeded_array.argtypes = [_dp, _i64, _i64]
+        L.orc_normal_array.argtypes = [_dp, _i64, _i64]
+        gemm_args = [_i64, _i64, _i64, _d, _dp, _i64, _i64, _dp, _i64, _i64, _d, _dp, _i64, ctypes.c_int]
+        L.orc_gemm_reference.argtypes = gemm_args
+        L.orc_gemm_fmachain.argtypes = gemm_args
+        L.orc_select_kernel.argtypes = [_i64, _i64, _i64, ctypes.c_int, ctypes.c_int]
+        L.orc_select_kernel.restype = ctypes.c_int
+        L.orc_opt_gemm.argtypes = [_i64, _i64, _i64, _dp, _dp, _dp, _d, _d, ctypes.c_int, ctypes.c_int]
+        L.orc_opt_gemm.restype = ctypes.c_int
+        L.orc_gemm_packed_parallel.argtypes = [_i64, _i64, _i64, _dp, _i64, _dp, _i64, _dp, _i64, _d, _d, ctypes.c_int]
+        L.orc_gemm_dd.argtypes = [_i64, _i64, _i64, _d, _dp, _i64, _i64, _dp, _i64, _i64, _d, _dp, _i64,
+                                  _i64, _i64p, _i64p, _dp, _dp, ctypes.c_int]
+        L.orc_max_err_ratio.argtypes = [_i64, _dp, _dp, _dp, _dp]
+        L.orc_max_err_ratio.restype = ctypes.c_double
+        _lib = L
+    return _lib
+
+
+def _ptr(x: np.ndarray):
+    assert x.dtype == np.float64 and x.flags["C_CONTIGUOUS"], "oracle wants contiguous float64"
+    return x.ctypes.data_as(_dp)
+
+
+def _threads(n):
+    return int(n) if n else (os.cpu_count() or 1)
+
+
+# ------------------------------------------------------------------ generators
+def splittable_doubles(n: int, seed: int, origin: float = -1.0, bound: float = 1.0) -> np.ndarray:
+    out = np.empty(int(n), dtype=np.float64)
+    lib().orc_splittable_doubles(_ptr(out), out.size, int(np.int64(np.uint64(seed & (2**64 - 1)))), origin, bound)
+    return out
+
+
+def seeded_array(n: int, seed: int) -> np.ndarray:
+    """GemmReference.seededArray(length, seed)."""
+    out = np.empty(int(n), dtype=np.float64)
+    lib().orc_seeded_array(_ptr(out), out.size, int(seed))
+    return out
+
+
+def seeded_matrix(rows: int, cols: int, seed: int) -> np.ndarray:
+    return seeded_array(rows * cols, seed).reshape(rows, cols)
+
+
+def uniform(shape, seed: int) -> np.ndarray:
+    """U[-1,1) i.i.d. from the SplitMix64 stream (no zeroed elements)."""
+    n = int(np.prod(shape))
+    return splittable_doubles(n, seed).reshape(shape)
+
+
+def normal(shape, seed: int) -> np.ndarray:
+    n = int(np.prod(shape))
+    out = np.empty(n, dtype=np.float64)
+    lib().orc_normal_array(_ptr(out), n, int(seed))
+    return out.reshape(shape)
+
+
+def ill_scaled(rows: int, cols: int, seed: int, axis: int, emax: int = 20) -> np.ndarray:
+    """U[-1,1) * 2^e with one integer e ~ U{-emax..emax} per row (axis=0) or column (axis=1)."""
+    base = uniform((rows, cols), seed)
+    e = np.floor(splittable_doubles(rows if axis == 0 else cols, seed ^ 0x5DEECE66D, 0.0, 2 * emax + 1)).astype(np.int64) - emax
+    scale = np.ldexp(1.0, e)
+    return base * (scale[:, None] if axis == 0 else scale[None, :])
+
+
+# ------------------------------------------------------------------ GEMM restatements
+def _strides(x: np.ndarray):
+    return x.strides[0] // 8, x.strides[1] // 8
+
+
+def _gemm_call(fn, a_op, b_op, c, alpha, beta, threads):
+    """a_op (m x k) and b_op (k x n) may be strided views of contiguous buffers."""
+    m, k = a_op.shape
+    k2, n = b_op.shape
+    assert k == k2 and c.shape == (m, n) and c.dtype == np.float64
+    abase, bbase = a_op, b_op
+    # ctypes needs the view's first-element address; strides in elements
+    a_rs, a_cs = _strides(a_op) if a_op.ndim == 2 else (k, 1)
+    b_rs, b_cs = _strides(b_op)
+    ap = ctypes.cast(abase.__array_interface__["data"][0], _dp)
+    bp = ctypes.cast(bbase.__array_interface__["data"][0], _dp)
+    assert c.strides[1] == 8
+    cp = ctypes.cast(c.__array_interface__["data"][0], _dp)
+    fn(m, n, k, alpha, ap, a_rs, a_cs, bp, b_rs, b_cs, beta, cp, c.strides[0] // 8, _threads(threads))
+    return c
+
+
+def gemm_reference(a_op, b_op, c, alpha, beta, threads=None):
+    """GemmReference.gemm family: returns a new C (input left untouched)."""
+    out = np.array(c, dtype=np.float64, copy=True, order="C")
+    return _gemm_call(lib().orc_gemm_reference, a_op, b_op, out, alpha, beta, threads)
+
+
+def gemm_fmachain(a_op, b_op, c, alpha, beta, threads=None):
+    """OptimizedBLAS3 packed-path order (bit-exact with the Java MICRO/PARALLEL/SMALL paths)."""
+    out = np.array(c, dtype=np.float64, copy=True, order="C")
+    return _gemm_call(lib().orc_gemm_fmachain, a_op, b_op, out, alpha, beta, threads)
+
+
+def select_kernel(m, n, k, cuda_available=False, threads=1) -> int:
+    return lib().orc_select_kernel(m, n, k, int(cuda_available), int(threads))
+
+
+def opt_gemm(a, b, c, alpha, beta, threads=1, lanes=8):
+    """OptimizedBLAS3.gemm on row-major dense arrays; returns (C, kernel class)."""
+    a = np.ascontiguousarray(a, dtype=np.float64)
+    b = np.ascontiguousarray(b, dtype=np.float64)
+    out = np.array(c, dtype=np.float64, copy=True, order="C")
+    m, k = a.shape
+    n = b.shape[1]
+    kern = lib().orc_opt_gemm(m, n, k, _ptr(a), _ptr(b), _ptr(out), alpha, beta, int(threads), int(lanes))
+    return out, kern
+
+
+def gemm_packed_parallel(a, b, c, alpha, beta, threads=None):
+    """PARALLEL_MICRO restated (the timed CPU baseline); updates c in place."""
+    m, k = a.shape
+    n = b.shape[1]
+    lib().orc_gemm_packed_parallel(m, n, k, _ptr(a), a.strides[0] // 8, _ptr(b), b.strides[0] // 8,
+                                   _ptr(c), c.strides[0] // 8, alpha, beta, _threads(threads))
+    return c
+
+
+def gemm_dd(a_op, b_op, c, alpha, beta, rows=None, cols=None, threads=None):
+    """Double-double alpha*A*B + beta*C at the given entries (all if rows is None).
+
+    Returns (reference values, componentwise FP64 bounds)."""
+    m, k = a_op.shape
+    n = b_op.shape[1]
+    a_rs, a_cs = _strides(a_op)
+    b_rs, b_cs = _strides(b_op)
+    ap = ctypes.cast(a_op.__array_interface__["data"][0], _dp)
+    bp = ctypes.cast(b_op.__array_interface__["data"][0], _dp)
+    if c is None:
+        cp, ldc = None, n
+    else:
+        assert c.strides[1] == 8
+        cp, ldc = ctypes.cast(c.__array_interface__["data"][0], _dp), c.strides[0] // 8
+    if rows is None:
+        count = m * n
+        rp = cpp = None
+    else:
+        rows = np.ascontiguousarray(rows, dtype=np.int64)
+        cols = np.ascontiguousarray(cols, dtype=np.int64)
+        count = rows.size
+        rp, cpp = rows.ctypes.data_as(_i64p), cols.ctypes.data_as(_i64p)
+    out = np.empty(count, dtype=np.float64)
+    bound = np.empty(count, dtype=np.float64)
+    lib().orc_gemm_dd(m, n, k, alpha, ap, a_rs, a_cs, bp, b_rs, b_cs, beta, cp, ldc,
+                      count, rp, cpp, _ptr(out), _ptr(bound), _threads(threads))
+    if rows is None:
+        return out.reshape(m, n), bound.reshape(m, n)
+    return out, bound
+
+
+def max_err_ratio(x, ref, bound):
+    """max_e |x-ref|/bound and max_e |x-ref| over flattened arrays."""
+    x = np.ascontiguousarray(x, dtype=np.float64).ravel()
+    ref = np.ascontiguousarray(ref, dtype=np.float64).ravel()
+    bound = np.ascontiguousarray(bound, dtype=np.float64).ravel()
+    mabs = ctypes.c_double(0.0)
+    r = lib().orc_max_err_ratio(x.size, _ptr(x), _ptr(ref), _ptr(bound), ctypes.byref(mabs))
+    return r, mabs.value
+
+
+def sample_entries(m: int, n: int, count: int, seed: int):
+    """Seeded random output entries plus the four corners and tile-edge rows/cols."""
+    rng = np.random.default_rng(seed)
+    r = rng.integers(0, m, size=count, dtype=np.int64)
+    c = rng.integers(0, n, size=count, dtype=np.int64)
+    extra_r, extra_c = [], []
+    for i in {0, m - 1, min(m - 1, 127), min(m - 1, 128)}:
+        for j in {0, n - 1, min(n - 1, 127), min(n - 1, 128), min(n - 1, 255), min(n - 1, 256)}:
+            extra_r.append(i)
+            extra_c.append(j)
+    return np.concatenate([r, np.array(extra_r, np.int64)]), np.concatenate([c, np.array(extra_c, np.int64)])
