@@ -34,7 +34,7 @@ METRIC = "8192^3 DGEMM GFLOP/s at FP64 accuracy: Ozaki-INT8 vs native FP64, % of
 def parse():
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
-    p.add_argument("--steps", type=int, default=5)
+    p.add_argument("--steps", type=int, default=10)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--size", type=int, default=8192)
@@ -100,7 +100,7 @@ class ClockSampler:
                 self.samples.append((sm, pw, rs))
             except Exception:
                 pass
-            self._stop.wait(0.1)
+            self._stop.wait(0.05)
 
     def __enter__(self):
         if self.nv is not None:
@@ -283,9 +283,10 @@ def run_ours(args):
             phases.setdefault(name, []).append(pms)
         return ms / args.steps, rep, launches, phases
 
-    # native FP64 first, then the Ozaki route (the headline) under the clock sampler
-    nat_ms, nat_rep, nat_launches, nat_phases = timed(JLC_PREC_NATIVE, Cn)
+    # native FP64 first, then the Ozaki route (the headline); clocks are sampled
+    # over both timed regions
     with ClockSampler(local) as clk:
+        nat_ms, nat_rep, nat_launches, nat_phases = timed(JLC_PREC_NATIVE, Cn)
         oz_ms, oz_rep, oz_launches, oz_phases = timed(JLC_PREC_OZAKI, Co)
     clocks = clk.summary()
 
