@@ -197,6 +197,32 @@ JLC_API int jlc_check_fp64_bound_device(jlc_ctx* ctx, int layout_a, int layout_b
  * tcgen05 (dense), [3] BF16 on tcgen05 (dense).  Takes about a second. */
 JLC_API int jlc_measure_peaks(jlc_ctx* ctx, double* out4);
 
+/* ---------------------------------------------------------------- allocation-free entry */
+/* Ozaki-INT8 DGEMM on DEVICE pointers that allocates nothing: no context, no
+ * cudaMalloc/cudaFree, no allocating library call.  (No counterpart in the
+ * reference: its only GPU route allocates three device buffers per call.)
+ * For callers that cannot allocate device memory -- processes whose GPU memory
+ * a caching allocator has already reserved, latency paths where cudaMalloc or
+ * cudaFree may synchronise the device, embedders that forbid driver
+ * allocations after start-up.  Scratch comes from a 64 MiB array compiled into
+ * the library (held by every GPU that loads it until exit); problems whose
+ * INT8 slices, s*(m+n)*roundup(k,16) bytes plus at least one 256 KB FP64 tile,
+ * do not fit return JLC_E_ARG with a message.  Same arguments and semantics as
+ * jlc_dgemm_ozaki_device, plus:
+ *   cuda_stream  stream the work is enqueued on (NULL: legacy default stream);
+ *   dev_status   optional DEVICE int that receives JLC_DEV_* bits if a bounded
+ *                wait times out (NULL: kept inside the library's array);
+ *   err, errlen  optional HOST buffer for an error message.
+ * A and B must have 16-byte aligned bases and even leading dimensions.
+ * The first call on each device looks up the array's device address (with
+ * that device current) and should come before any stream capture.  All calls
+ * on a device share the array: calls that overlap on the GPU race and must be
+ * serialised by the caller.  Returns when the work is enqueued. */
+JLC_API int jlc_dgemm_ozaki_static(int layout_a, int layout_b, int64_t m, int64_t n, int64_t k, double alpha,
+                                   const double* a, int64_t lda, const double* b, int64_t ldb, double beta,
+                                   double* c, int64_t ldc, int slices, void* cuda_stream, int* dev_status,
+                                   char* err, size_t errlen);
+
 #ifdef __cplusplus
 }
 #endif

@@ -85,6 +85,8 @@ SIGNATURES = {
                                          _dp, _i64, _i64, _vp, _vp, ctypes.POINTER(_d), ctypes.POINTER(_d),
                                          ctypes.POINTER(_i64)]),
     "jlc_measure_peaks": (_i, [_vp, ctypes.POINTER(_d)]),
+    "jlc_dgemm_ozaki_static": (_i, [_i, _i, _i64, _i64, _i64, _d, _dp, _i64, _dp, _i64, _d, _dp, _i64, _i, _vp,
+                                    _vp, ctypes.c_char_p, _sz]),
 }
 
 PHASES = {1: "dmma", 2: "gemv", 3: "ozaki_gemm", 5: "ozaki_split", 6: "scale", 7: "fp64_gated", 8: "h2d",
