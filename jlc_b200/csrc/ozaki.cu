@@ -17,17 +17,19 @@
 //     the weight 2^-7(d+2), so their products accumulate into one INT32
 //     accumulator; a run is split whenever (pairs x k) could exceed
 //     2^31 / 127^2 (1040 k-blocks of 128), so INT32 never overflows.
-//  4. Recombination in FP64.  T = sum_d 2^-7d S_d (the only FP64 rounding
-//     besides the final one), then C = alpha * 2^(E_i+F_j-14) * T + beta*C.
+//  4. Recombination in FP64.  T = sum_d 2^-7d S_d, summed from the least
+//     significant diagonal up (the only FP64 rounding besides the final
+//     one), then C = alpha * 2^(E_i+F_j-14) * T + beta*C.
 //
-// Kernel layout: persistent CTAs, 6 warps.  Warp 0 issues TMA loads of the
+// Kernel layout: persistent CTAs, 10 warps.  Warp 0 issues TMA loads of the
 // K-major INT8 slice tiles (A 128x128 B, B 256x128 B, 128B swizzle) into a
 // 4-stage ring; warp 1 allocates TMEM (512 columns = two 128x256 INT32
-// accumulators) and one elected lane issues tcgen05.mma; warps 2-5 drain
+// accumulators) and one elected lane issues tcgen05.mma; warps 2-9 drain
 // the accumulators with tcgen05.ld and keep the FP64 running sum T of the
 // current 128x256 tile in a per-CTA scratch tile (256 KB, L2 resident),
-// writing C after the last anti-diagonal.  Accumulator double buffering lets
-// the epilogue of diagonal d overlap the MMAs of diagonal d+1.  No TMA
+// writing C after the last anti-diagonal.  Diagonals run from the least
+// significant (most pairs) down to d = 0, and accumulator double buffering
+// lets the epilogue of one diagonal overlap the MMAs of the next.  No TMA
 // multicast is used anywhere.
 #include <cstdio>
 
@@ -44,8 +46,8 @@ constexpr int STAGES = 4;
 constexpr int A_STAGE = BM * BKB;  // 16 KB
 constexpr int B_STAGE = BN * BKB;  // 32 KB
 constexpr int STAGE_BYTES = A_STAGE + B_STAGE;
-constexpr int THREADS = 192;
-constexpr int EPI_WARPS = 4;
+constexpr int THREADS = 320;  // warp 0 TMA, warp 1 MMA, warps 2..9 epilogue
+constexpr int EPI_WARPS = 8;
 constexpr int TMEM_COLS = 512;
 constexpr int GROUP_CAP = 1040;  // k-blocks per INT32 run: 1040*128*127*127 < 2^31
 constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024 + 256;
@@ -114,7 +116,7 @@ __global__ void __launch_bounds__(THREADS, 1)
                 int tm, tn;
                 tile_coords(tile, p.tiles_m, p.tiles_n, 8, tm, tn);
                 const int m0 = tm * BM, n0 = tn * BN;
-                for (int d = 0; d < p.s && ok; ++d) {
+                for (int d = p.s - 1; d >= 0 && ok; --d) {
                     for (int pr = 0; pr <= d && ok; ++pr) {
                         const int ia = pr, ib = d - pr;
                         for (int kb = 0; kb < p.KB; ++kb) {
@@ -148,7 +150,7 @@ __global__ void __launch_bounds__(THREADS, 1)
             uint32_t gcount = 0;
             bool ok = true;
             for (int tile = blockIdx.x; tile < p.num_tiles && ok; tile += gridDim.x) {
-                for (int d = 0; d < p.s && ok; ++d) {
+                for (int d = p.s - 1; d >= 0 && ok; --d) {
                     const int nblk = (d + 1) * p.KB;
                     for (int g0 = 0; g0 < nblk && ok; g0 += GROUP_CAP) {
                         const int g1 = min(nblk, g0 + GROUP_CAP);
@@ -190,10 +192,16 @@ __global__ void __launch_bounds__(THREADS, 1)
             drain_wait(mma_done, 0, p.status);
         }
     } else {
-        // ---------------- epilogue (warps 2..5) ----------------
-        const int quarter = warp & 3;  // TMEM lanes this warp may access
+        // ---------------- epilogue (warps 2..9) ----------------
+        // Warp w reads TMEM lanes 32*(w%4)..+31 (one C row per thread); the
+        // two warps sharing a lane quarter split the 256 columns in halves.
+        const int quarter = warp & 3;
+        const int half = (warp - 2) >> 2;
         const int row = quarter * 32 + lane;
-        double* scratch = p.scratch + (size_t)blockIdx.x * SCRATCH_DOUBLES;
+        // FP64 running sums of this CTA's tile, laid out [col/2][row][2] so a
+        // warp's 16-byte accesses for one column pair are contiguous
+        double2* scratch = reinterpret_cast<double2*>(p.scratch + (size_t)blockIdx.x * SCRATCH_DOUBLES);
+        const bool c_vec = ((reinterpret_cast<uintptr_t>(p.C) & 15) == 0) && ((p.ldc & 1) == 0);
         uint32_t gcount = 0;
         bool ok = true;
         for (int tile = blockIdx.x; tile < p.num_tiles && ok; tile += gridDim.x) {
@@ -203,7 +211,7 @@ __global__ void __launch_bounds__(THREADS, 1)
             const int grow = m0 + row;
             const bool row_ok = grow < p.M;
             const int ei = row_ok ? p.ea[grow] : 0;
-            for (int d = 0; d < p.s && ok; ++d) {
+            for (int d = p.s - 1; d >= 0 && ok; --d) {
                 const int nblk = (d + 1) * p.KB;
                 const int ngroups = (nblk + GROUP_CAP - 1) / GROUP_CAP;
                 const double w = ldexp(1.0, -7 * d);
@@ -214,34 +222,62 @@ __global__ void __launch_bounds__(THREADS, 1)
                         break;
                     }
                     tc_fence_after();
-                    const bool first = (d == 0 && gi == 0);
-                    const bool last = (d == p.s - 1 && gi == ngroups - 1);
-                    const uint32_t taddr = tmem_base + ((uint32_t)(quarter * 32) << 16) + buf * BN;
+                    // least significant diagonal first: the FP64 sum grows from
+                    // its smallest terms, and the tile's last (C-writing) pass
+                    // overlaps the next tile's longest MMA phase
+                    const bool first = (d == p.s - 1 && gi == 0);
+                    const bool last = (d == 0 && gi == ngroups - 1);
+                    const uint32_t taddr = tmem_base + ((uint32_t)(quarter * 32) << 16) + buf * BN + half * (BN / 2);
 #pragma unroll 1
-                    for (int ch = 0; ch < BN / 32; ++ch) {
+                    for (int ch = 0; ch < BN / 64; ++ch) {
+                        const int c0 = half * (BN / 2) + ch * 32;  // first column of this chunk in the tile
                         uint32_t r[32];
                         tmem_ld32(taddr + ch * 32, r);
                         tmem_wait_ld();
+                        double2* sp = scratch + (size_t)(c0 >> 1) * BM + row;
                         if (!last) {
 #pragma unroll
-                            for (int j = 0; j < 32; ++j) {
-                                double* sp = scratch + (size_t)(ch * 32 + j) * BM + row;
-                                double v = (double)(int)r[j] * w;
-                                if (!first) v += *sp;
-                                *sp = v;
+                            for (int j = 0; j < 16; ++j) {
+                                double2 v = make_double2((double)(int)r[2 * j] * w, (double)(int)r[2 * j + 1] * w);
+                                if (!first) {
+                                    const double2 o = sp[(size_t)j * BM];
+                                    v.x += o.x;
+                                    v.y += o.y;
+                                }
+                                sp[(size_t)j * BM] = v;
                             }
                         } else if (row_ok) {
-                            double* crow = p.C + (long long)grow * p.ldc;
+                            double* crow = p.C + (long long)grow * p.ldc + n0 + c0;
+                            const int ncols = min(32, p.N - (n0 + c0));
+                            double out[32];
 #pragma unroll
-                            for (int j = 0; j < 32; ++j) {
-                                const int col = n0 + ch * 32 + j;
-                                double* sp = scratch + (size_t)(ch * 32 + j) * BM + row;
-                                double v = (double)(int)r[j] * w;
-                                if (!first) v += *sp;
-                                if (col < p.N) {
-                                    const double cv = p.alpha * ldexp(v, ei + p.eb[col] - 14);
-                                    crow[col] = (p.beta == 0.0) ? cv : fma(p.beta, crow[col], cv);
+                            for (int j = 0; j < 16; ++j) {
+                                double2 v = make_double2((double)(int)r[2 * j] * w, (double)(int)r[2 * j + 1] * w);
+                                if (!first) {
+                                    const double2 o = sp[(size_t)j * BM];
+                                    v.x += o.x;
+                                    v.y += o.y;
                                 }
+                                const int col0 = n0 + c0 + 2 * j;
+                                out[2 * j] = col0 < p.N ? p.alpha * ldexp(v.x, ei + p.eb[col0] - 14) : 0.0;
+                                out[2 * j + 1] = col0 + 1 < p.N ? p.alpha * ldexp(v.y, ei + p.eb[col0 + 1] - 14) : 0.0;
+                            }
+                            if (c_vec && ncols == 32) {
+                                double2* c2 = reinterpret_cast<double2*>(crow);
+#pragma unroll
+                                for (int j = 0; j < 16; ++j) {
+                                    double2 v = make_double2(out[2 * j], out[2 * j + 1]);
+                                    if (p.beta != 0.0) {
+                                        const double2 o = c2[j];
+                                        v.x = fma(p.beta, o.x, v.x);
+                                        v.y = fma(p.beta, o.y, v.y);
+                                    }
+                                    c2[j] = v;
+                                }
+                            } else {
+#pragma unroll
+                                for (int j = 0; j < 32; ++j)
+                                    if (j < ncols) crow[j] = (p.beta == 0.0) ? out[j] : fma(p.beta, crow[j], out[j]);
                             }
                         }
                     }
