@@ -165,6 +165,7 @@ JLC_API int jlc_device_status(jlc_ctx* ctx);
 #define JLC_PHASE_DMMA 1        /* FP64 DMMA GEMM kernel */
 #define JLC_PHASE_GEMV 2        /* matrix-vector kernel(s) */
 #define JLC_PHASE_OZAKI_GEMM 3  /* INT8 tcgen05 slice-product GEMM + FP64 recombination */
+#define JLC_PHASE_GROUPED 4     /* persistent grouped launch */
 #define JLC_PHASE_OZAKI_SPLIT 5 /* exponent scaling + INT8 slicing of A and B */
 #define JLC_PHASE_SCALE 6       /* beta-only update of C */
 #define JLC_PHASE_FP64_GATED 7  /* FP64 kernel behind an Ozaki call (runs only on Inf/NaN input) */
@@ -196,6 +197,41 @@ JLC_API int jlc_check_fp64_bound_device(jlc_ctx* ctx, int layout_a, int layout_b
  * kernels: [0] FP64 on mma.sync .f64 (DMMA), [1] FP64 on DFMA, [2] INT8 on
  * tcgen05 (dense), [3] BF16 on tcgen05 (dense).  Takes about a second. */
 JLC_API int jlc_measure_peaks(jlc_ctx* ctx, double* out4);
+
+/* ---------------------------------------------------------------- grouped batches */
+/* One GEMM of a batch: C = alpha*op(A)*op(B) + beta*C on DEVICE pointers, the
+ * same layouts and semantics as jlc_dgemm_device. */
+typedef struct jlc_problem {
+    int64_t m, n, k;
+    int32_t layout_a, layout_b;
+    int64_t lda, ldb, ldc;
+    double alpha, beta;
+    const double* a;
+    const double* b;
+    double* c;
+} jlc_problem;
+
+typedef struct jlc_grouped_plan jlc_grouped_plan;
+#define JLC_GROUPED_GRAPH 1    /* capture the launch into a CUDA graph; run replays it */
+#define JLC_GROUPED_AUTOTUNE 2 /* time the tile shapes of each shape class now and cache the choice */
+
+/* Replaces the reference's per-call loop over many small GEMMs (the TINY and
+ * SMALL dispatch classes, GemmDispatch.java:76-106, and the blocked QR /
+ * Hessenberg panel and trailing updates, HouseholderQR.java:167-210,
+ * BlockedHessenbergQR.java:277-345) with one persistent launch.  The plan
+ * copies the problem table to the device; later runs reuse the same device
+ * pointers (update the data in place and run again).  precision must be
+ * JLC_PREC_NATIVE or JLC_PREC_AUTO. */
+JLC_API int jlc_grouped_plan_create(jlc_ctx* ctx, const jlc_problem* probs, int64_t count, int precision, int flags,
+                                    jlc_grouped_plan** out);
+/* enqueue one run on the context stream (graph replay when captured) */
+JLC_API int jlc_grouped_plan_run(jlc_grouped_plan* plan);
+JLC_API int jlc_grouped_plan_info(const jlc_grouped_plan* plan, int64_t* work_items, double* flops, int* tile_small,
+                                  int* tile_large);
+JLC_API void jlc_grouped_plan_destroy(jlc_grouped_plan* plan);
+/* one-shot: plan, run, synchronise, destroy */
+JLC_API int jlc_dgemm_grouped_device(jlc_ctx* ctx, const jlc_problem* probs, int64_t count, int precision,
+                                     jlc_report* rep);
 
 /* ---------------------------------------------------------------- allocation-free entry */
 /* Ozaki-INT8 DGEMM on DEVICE pointers that allocates nothing: no context, no

@@ -54,7 +54,22 @@ class Report(ctypes.Structure):
         return {f: getattr(self, f) for f, _ in self._fields_}
 
 
+class Problem(ctypes.Structure):
+    """jlc_problem: one GEMM of a grouped batch (device pointers)."""
+    _fields_ = [
+        ("m", ctypes.c_int64), ("n", ctypes.c_int64), ("k", ctypes.c_int64),
+        ("layout_a", ctypes.c_int32), ("layout_b", ctypes.c_int32),
+        ("lda", ctypes.c_int64), ("ldb", ctypes.c_int64), ("ldc", ctypes.c_int64),
+        ("alpha", ctypes.c_double), ("beta", ctypes.c_double),
+        ("a", ctypes.c_void_p), ("b", ctypes.c_void_p), ("c", ctypes.c_void_p),
+    ]
+
+
+JLC_GROUPED_GRAPH = 1
+JLC_GROUPED_AUTOTUNE = 2
+
 _REP = ctypes.POINTER(Report)
+_PROB = ctypes.POINTER(Problem)
 _STRIDED = [_vp, _dp, _i64, _i64, _dp, _i64, _i64, _dp, _i64, _i64, _i64, _i64, _i64, _d, _d, _i, _REP]
 _GENERAL = [_vp, _i, _i, _i64, _i64, _i64, _d, _dp, _i64, _dp, _i64, _d, _dp, _i64, _i, _REP]
 
@@ -85,11 +100,17 @@ SIGNATURES = {
                                          _dp, _i64, _i64, _vp, _vp, ctypes.POINTER(_d), ctypes.POINTER(_d),
                                          ctypes.POINTER(_i64)]),
     "jlc_measure_peaks": (_i, [_vp, ctypes.POINTER(_d)]),
+    "jlc_grouped_plan_create": (_i, [_vp, _PROB, _i64, _i, _i, ctypes.POINTER(_vp)]),
+    "jlc_grouped_plan_run": (_i, [_vp]),
+    "jlc_grouped_plan_info": (_i, [_vp, ctypes.POINTER(_i64), ctypes.POINTER(_d), ctypes.POINTER(_i),
+                                   ctypes.POINTER(_i)]),
+    "jlc_grouped_plan_destroy": (None, [_vp]),
+    "jlc_dgemm_grouped_device": (_i, [_vp, _PROB, _i64, _i, _REP]),
     "jlc_dgemm_ozaki_static": (_i, [_i, _i, _i64, _i64, _i64, _d, _dp, _i64, _dp, _i64, _d, _dp, _i64, _i, _vp,
                                     _vp, ctypes.c_char_p, _sz]),
 }
 
-PHASES = {1: "dmma", 2: "gemv", 3: "ozaki_gemm", 5: "ozaki_split", 6: "scale", 7: "fp64_gated", 8: "h2d",
+PHASES = {1: "dmma", 2: "gemv", 3: "ozaki_gemm", 4: "grouped", 5: "ozaki_split", 6: "scale", 7: "fp64_gated", 8: "h2d",
           9: "d2h"}
 
 _lib = None

@@ -102,6 +102,18 @@ class Context:
         return {"fp64_dmma_tflops": out[0], "fp64_dfma_tflops": out[1], "int8_tops": out[2],
                 "bf16_tflops": out[3]}
 
+    # -- grouped batches ---------------------------------------------------
+    def grouped_plan(self, problems, precision=L.JLC_PREC_NATIVE, graph=False, autotune=False) -> "GroupedPlan":
+        """Plan one persistent launch over a list of problems (dicts or
+        Problem structs with device pointers)."""
+        return GroupedPlan(self, problems, precision, graph, autotune)
+
+    def dgemm_grouped_device(self, problems, precision=L.JLC_PREC_NATIVE) -> dict:
+        arr = _problem_array(problems)
+        rep = L.Report()
+        self.check(self.lib.jlc_dgemm_grouped_device(self.h, arr, len(arr), int(precision), ctypes.byref(rep)))
+        return rep.as_dict()
+
     def launch_count(self) -> int:
         v = ctypes.c_int64(0)
         self.check(self.lib.jlc_launch_count(self.h, ctypes.byref(v)))
@@ -174,6 +186,52 @@ class Context:
                                              ctypes.byref(rep))
         self.check(rc)
         return rep.as_dict()
+
+
+def _problem_array(problems):
+    arr = (L.Problem * len(problems))()
+    for i, p in enumerate(problems):
+        if isinstance(p, L.Problem):
+            arr[i] = p
+        else:
+            q = arr[i]
+            for k, v in p.items():
+                setattr(q, k, v)
+    return arr
+
+
+class GroupedPlan:
+    """jlc_grouped_plan: a reusable persistent launch over a fixed problem table."""
+
+    def __init__(self, ctx: Context, problems, precision, graph, autotune):
+        self.ctx = ctx
+        self.problems = _problem_array(problems)
+        flags = (L.JLC_GROUPED_GRAPH if graph else 0) | (L.JLC_GROUPED_AUTOTUNE if autotune else 0)
+        h = ctypes.c_void_p()
+        ctx.check(ctx.lib.jlc_grouped_plan_create(ctx.h, self.problems, len(self.problems), int(precision), flags,
+                                                  ctypes.byref(h)))
+        self.h = h
+
+    def run(self):
+        self.ctx.check(self.ctx.lib.jlc_grouped_plan_run(self.h))
+
+    def info(self) -> dict:
+        items, flops = ctypes.c_int64(), ctypes.c_double()
+        ts, tl = ctypes.c_int(), ctypes.c_int()
+        self.ctx.check(self.ctx.lib.jlc_grouped_plan_info(self.h, ctypes.byref(items), ctypes.byref(flops),
+                                                          ctypes.byref(ts), ctypes.byref(tl)))
+        return {"work_items": items.value, "flops": flops.value, "tile_small": ts.value, "tile_large": tl.value}
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.ctx.lib.jlc_grouped_plan_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def _f64c(x):

@@ -17,32 +17,6 @@
 
 using namespace jlc;
 
-struct DevBuf {
-    void* ptr = nullptr;
-    size_t bytes = 0;
-};
-
-struct jlc_ctx {
-    int device = 0;
-    int sm_count = 0;
-    cudaStream_t own_stream = nullptr;
-    cudaStream_t stream = nullptr;
-    int* d_status = nullptr;  // status word written by kernels (JLC_DEV_* bits)
-    int* d_flags = nullptr;   // control flags (e.g. the Ozaki non-finite gate)
-    DevBuf bufA, bufB, bufC;
-    Workspace ws;
-    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
-    int dmma_k = 8;
-    // profiler: event pairs around phases, reused from a pool
-    bool profiling = false;
-    static constexpr int kMaxRec = 4096;
-    int nrec = 0;
-    int rec_phase[kMaxRec];
-    cudaEvent_t rec_ev[2 * kMaxRec] = {};
-    int64_t launches = 0;
-    char err[512] = {0};
-};
-
 namespace {
 
 int set_err(jlc_ctx* ctx, int code, const char* fmt, ...) {

@@ -1,0 +1,617 @@
+// Grouped FP64 GEMM: thousands of independent, unevenly shaped problems in one
+// persistent launch.
+//
+// The reference runs such batches as separate CPU calls: the tiny and SMALL
+// dispatch classes (GemmDispatch.java:76-106, SpecializedKernels.java:79-271)
+// and the panel / trailing updates of blocked Householder QR, Hessenberg and
+// bidiagonalisation (HouseholderQR.java:167-210, BlockedHessenbergQR.java:
+// 277-345), each a gemm / gemmStrided* call.  Here a plan turns a problem
+// table into a work list once; every run is a single launch (optionally a
+// CUDA graph replay) in which persistent CTAs pull work items from an atomic
+// counter:
+//   * tile items: one 32x32 or 64x64 tile of C of one problem, FP64
+//     mma.sync (m16n8k8) over double-buffered cp.async stages of 16 k-values,
+//     with both operands stored K-major in swizzled shared memory (the layout
+//     and K permutation of the tiled DMMA kernel), alpha folded into the A
+//     fragments, beta fused in the epilogue;
+//   * tiny items: a batch of problems with m*n <= 64 and k <= 64 (the TINY
+//     and small SMALL shapes), one thread per output element running the
+//     reference's small-GEMM order (C <- beta*C, then an fma chain over p
+//     with alpha*a).
+// Items are ordered by decreasing cost (longest-processing-time first).  The
+// tile shape of each shape class is chosen by an autotuner that times both
+// shapes on the plan's own problem shapes and caches the choice on disk,
+// keyed by device, SM count, library version and class.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <fstream>
+#include <map>
+#include <mutex>
+#include <sstream>
+#include <string>
+#include <vector>
+
+#include <sys/stat.h>
+
+#include "jlc_device.cuh"
+#include "jlc_dmma.cuh"
+#include "jlc_internal.h"
+
+namespace jlc {
+namespace grp {
+
+constexpr int THREADS = 128;
+constexpr int GBK = 16;  // k-values per stage (one 128-byte swizzled row per tile row)
+constexpr int TINY_ELEMS = THREADS;
+constexpr int KIND_TINY = 0, KIND_T32 = 1, KIND_T64 = 2;
+constexpr int SMEM_BYTES = 2 * (64 + 64) * 128 + 128;
+
+struct Item {
+    int prob;  // problem index, or first index into the tiny list
+    int tm;    // tile row, or number of tiny problems
+    int tn;    // tile column
+    int kind;
+};
+
+__device__ __forceinline__ void cp_async8(void* smem_dst, const void* src, bool valid) {
+    const uint32_t d = smem_u32(smem_dst);
+    const int n = valid ? 8 : 0;  // 0: zero-fill without reading
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(d), "l"(src), "r"(n) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+__device__ __forceinline__ double elem_a(const jlc_problem& P, long long i, long long p) {
+    return P.layout_a == JLC_ROW_MAJOR ? P.a[i * P.lda + p] : P.a[p * P.lda + i];
+}
+__device__ __forceinline__ double elem_b(const jlc_problem& P, long long p, long long j) {
+    return P.layout_b == JLC_ROW_MAJOR ? P.b[p * P.ldb + j] : P.b[j * P.ldb + p];
+}
+
+// Stages one k-block of A (BM rows) and B (BN columns) into K-major swizzled
+// shared memory; threads walk the source's contiguous direction.
+template <int BM, int BN>
+__device__ __forceinline__ void load_stage(const jlc_problem& P, char* sA, char* sB, long long m0, long long n0,
+                                           long long k0) {
+    const int tid = threadIdx.x;
+    const bool a_row = P.layout_a == JLC_ROW_MAJOR;
+#pragma unroll 4
+    for (int e = tid; e < BM * GBK; e += THREADS) {
+        const int r = a_row ? e / GBK : e % BM;
+        const int c = a_row ? e % GBK : e / BM;
+        const long long gi = m0 + r, gk = k0 + c;
+        const bool ok = gi < P.m && gk < P.k;
+        const double* src = ok ? (a_row ? P.a + gi * P.lda + gk : P.a + gk * P.lda + gi) : P.a;
+        cp_async8(sA + dmma::kmajor_off(r, c), src, ok);
+    }
+    const bool b_row = P.layout_b == JLC_ROW_MAJOR;
+#pragma unroll 4
+    for (int e = tid; e < BN * GBK; e += THREADS) {
+        const int nn = b_row ? e % BN : e / GBK;
+        const int c = b_row ? e / BN : e % GBK;
+        const long long gj = n0 + nn, gk = k0 + c;
+        const bool ok = gj < P.n && gk < P.k;
+        const double* src = ok ? (b_row ? P.b + gk * P.ldb + gj : P.b + gj * P.ldb + gk) : P.b;
+        cp_async8(sB + dmma::kmajor_off(nn, c), src, ok);
+    }
+    cp_async_commit();
+}
+
+template <int BM, int BN>
+__device__ void tile_item(const jlc_problem& P, int tm, int tn, char* smem) {
+    constexpr int WM = BM / 2, WN = BN / 2;  // 2 x 2 warps
+    constexpr int MT = WM / 16, NT = WN / 8;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int g = lane >> 2, t = lane & 3;
+    const int warp_m = warp >> 1, warp_n = warp & 1;
+    const long long m0 = (long long)tm * BM, n0 = (long long)tn * BN;
+    // stage s: A tile at smem + s*(BM+BN)*128, B tile right after it
+    constexpr int STAGE = (BM + BN) * 128;
+    const int kblocks = P.alpha == 0.0 ? 0 : (int)((P.k + GBK - 1) / GBK);
+    const bool scale_a = P.alpha != 1.0;
+
+    double acc[MT][NT][4];
+#pragma unroll
+    for (int i = 0; i < MT; ++i)
+#pragma unroll
+        for (int j = 0; j < NT; ++j)
+#pragma unroll
+            for (int e = 0; e < 4; ++e) acc[i][j][e] = 0.0;
+
+    if (kblocks > 0) load_stage<BM, BN>(P, smem, smem + BM * 128, m0, n0, 0);
+    for (int kb = 0; kb < kblocks; ++kb) {
+        const int cur = kb & 1;
+        const char* sA = smem + cur * STAGE;
+        const char* sB = sA + BM * 128;
+        if (kb + 1 < kblocks) {
+            char* nA = smem + (cur ^ 1) * STAGE;
+            load_stage<BM, BN>(P, nA, nA + BM * 128, m0, n0, (long long)(kb + 1) * GBK);
+            cp_async_wait<1>();
+        } else {
+            cp_async_wait<0>();
+        }
+        __syncthreads();
+#pragma unroll
+        for (int q = 0; q < GBK / 8; ++q) {
+            double bf[NT][2];
+#pragma unroll
+            for (int nt = 0; nt < NT; ++nt) {
+                const int c = warp_n * WN + nt * 8 + g;
+#pragma unroll
+                for (int j = 0; j < 2; ++j) bf[nt][j] = dmma::lds_b<true>(sB, dmma::phys_k<8>(q, t, j), c);
+            }
+#pragma unroll
+            for (int mt = 0; mt < MT; ++mt) {
+                const int r = warp_m * WM + mt * 16 + g;
+                double af[4];
+#pragma unroll
+                for (int i = 0; i < 4; ++i) af[i] = dmma::lds_a<true>(sA, r + 8 * (i & 1), dmma::phys_k<8>(q, t, i >> 1));
+                if (scale_a) {
+#pragma unroll
+                    for (int i = 0; i < 4; ++i) af[i] *= P.alpha;
+                }
+#pragma unroll
+                for (int nt = 0; nt < NT; ++nt) dmma::mma_f64<8>(acc[mt][nt], af, bf[nt]);
+            }
+        }
+        __syncthreads();  // the stage is refilled two iterations later
+    }
+
+#pragma unroll
+    for (int mt = 0; mt < MT; ++mt)
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const long long row = m0 + warp_m * WM + mt * 16 + g + 8 * h;
+            if (row >= P.m) continue;
+            double* crow = P.c + row * P.ldc;
+#pragma unroll
+            for (int nt = 0; nt < NT; ++nt)
+#pragma unroll
+                for (int e = 0; e < 2; ++e) {
+                    const long long col = n0 + warp_n * WN + nt * 8 + 2 * t + e;
+                    if (col < P.n) {
+                        const double v = acc[mt][nt][2 * h + e];
+                        crow[col] = (P.beta == 0.0) ? v : fma(P.beta, crow[col], v);
+                    }
+                }
+        }
+}
+
+// A batch of tiny problems, one thread per output element.
+__device__ void tiny_item(const jlc_problem* probs, const int* tiny_ids, int start, int count) {
+    int off = 0;
+    for (int q = 0; q < count; ++q) {
+        const jlc_problem& P = probs[tiny_ids[start + q]];
+        const int sz = (int)(P.m * P.n);
+        const int e = threadIdx.x - off;
+        if (e >= 0 && e < sz) {
+            const long long i = e / P.n, j = e % P.n;
+            double* cij = P.c + i * P.ldc + j;
+            double acc = (P.beta == 0.0) ? 0.0 : (P.beta == 1.0 ? *cij : *cij * P.beta);
+            if (P.alpha != 0.0)
+                for (long long p = 0; p < P.k; ++p) acc = fma(P.alpha * elem_a(P, i, p), elem_b(P, p, j), acc);
+            *cij = acc;
+            return;
+        }
+        off += sz;
+    }
+}
+
+__global__ void __launch_bounds__(THREADS, 3) grouped_kernel(const jlc_problem* probs, const Item* items, int nitems,
+                                                          const int* tiny_ids, int* counter) {
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    char* smem = reinterpret_cast<char*>((reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~uintptr_t(127));
+    __shared__ int s_item;
+    for (;;) {
+        if (threadIdx.x == 0) s_item = atomicAdd(counter, 1);
+        __syncthreads();
+        const int it = s_item;
+        __syncthreads();
+        if (it >= nitems) return;
+        const Item w = items[it];
+        if (w.kind == KIND_TINY) {
+            tiny_item(probs, tiny_ids, w.prob, w.tm);
+        } else {
+            const jlc_problem P = probs[w.prob];
+            if (w.kind == KIND_T64) tile_item<64, 64>(P, w.tm, w.tn, smem);
+            else tile_item<32, 32>(P, w.tm, w.tn, smem);
+        }
+    }
+}
+
+// ------------------------------------------------------------------ host side
+bool is_tiny(const jlc_problem& p) { return p.m * p.n <= 64 && p.k <= 64; }
+int shape_class(const jlc_problem& p) { return std::max(p.m, p.n) <= 48 ? 0 : 1; }
+
+struct WorkList {
+    std::vector<Item> items;
+    std::vector<int> tiny;
+    double flops = 0.0;
+};
+
+void build_work(const std::vector<jlc_problem>& probs, const int cfg[2], int only_class, WorkList& wl) {
+    struct Costed {
+        Item it;
+        double cost;
+    };
+    std::vector<Costed> v;
+    int batch_start = -1, batch_count = 0, batch_elems = 0;
+    double batch_cost = 0.0;
+    auto flush_batch = [&] {
+        if (batch_count > 0) v.push_back({Item{batch_start, batch_count, 0, KIND_TINY}, batch_cost});
+        batch_start = -1;
+        batch_count = batch_elems = 0;
+        batch_cost = 0.0;
+    };
+    for (int i = 0; i < (int)probs.size(); ++i) {
+        const jlc_problem& p = probs[i];
+        if (p.m == 0 || p.n == 0) continue;
+        const double kk = p.alpha == 0.0 ? 0.0 : (double)p.k;
+        wl.flops += 2.0 * p.m * p.n * kk;
+        if (is_tiny(p)) {
+            if (only_class >= 0) continue;
+            const int sz = (int)(p.m * p.n);
+            if (batch_elems + sz > TINY_ELEMS) flush_batch();
+            if (batch_count == 0) batch_start = (int)wl.tiny.size();
+            wl.tiny.push_back(i);
+            ++batch_count;
+            batch_elems += sz;
+            batch_cost += (double)sz * (kk + 1.0);
+            continue;
+        }
+        const int cls = shape_class(p);
+        if (only_class >= 0 && cls != only_class) continue;
+        const int ts = cfg[cls];
+        const int kind = ts == 64 ? KIND_T64 : KIND_T32;
+        const int tmn = (int)((p.m + ts - 1) / ts), tnn = (int)((p.n + ts - 1) / ts);
+        for (int a = 0; a < tmn; ++a)
+            for (int b = 0; b < tnn; ++b) v.push_back({Item{i, a, b, kind}, (double)ts * ts * (kk + 16.0)});
+    }
+    flush_batch();
+    std::stable_sort(v.begin(), v.end(), [](const Costed& x, const Costed& y) { return x.cost > y.cost; });
+    wl.items.reserve(v.size());
+    for (auto& c : v) wl.items.push_back(c.it);
+}
+
+std::string tune_cache_path() {
+    if (const char* p = getenv("JLCGPU_TUNE_CACHE")) return p;
+    const char* home = getenv("HOME");
+    return std::string(home ? home : "/tmp") + "/.cache/jlcgpu/grouped_tune.txt";
+}
+
+std::mutex g_tune_mu;
+
+std::string tune_key(int device, int sm_count, int cls) {
+    cudaDeviceProp prop;
+    cudaGetDeviceProperties(&prop, device);
+    std::ostringstream os;
+    std::string name = prop.name;
+    for (auto& ch : name)
+        if (ch == ' ') ch = '_';
+    os << name << "|sm" << sm_count << "|v" << JLCGPU_VERSION << "|grouped-fp64|class" << cls;
+    return os.str();
+}
+
+int tune_lookup(const std::string& key) {
+    std::lock_guard<std::mutex> lock(g_tune_mu);
+    std::ifstream f(tune_cache_path());
+    std::string k;
+    int v;
+    int found = 0;
+    while (f >> k >> v)
+        if (k == key) found = v;
+    return found;
+}
+
+void mkdirs_for(const std::string& path) {
+    for (size_t i = 1; i < path.size(); ++i)
+        if (path[i] == '/') ::mkdir(path.substr(0, i).c_str(), 0755);
+}
+
+void tune_store(const std::string& key, int value) {
+    std::lock_guard<std::mutex> lock(g_tune_mu);
+    const std::string path = tune_cache_path();
+    mkdirs_for(path);
+    std::map<std::string, int> all;
+    {
+        std::ifstream f(path);
+        std::string k;
+        int v;
+        while (f >> k >> v) all[k] = v;
+    }
+    all[key] = value;
+    std::ofstream f(path, std::ios::trunc);
+    for (auto& kv : all) f << kv.first << " " << kv.second << "\n";
+}
+
+}  // namespace grp
+}  // namespace jlc
+
+struct jlc_grouped_plan {
+    jlc_ctx* ctx = nullptr;
+    int64_t count = 0;
+    jlc_problem* d_probs = nullptr;
+    jlc::grp::Item* d_items = nullptr;
+    int* d_tiny = nullptr;
+    int* d_counter = nullptr;
+    int nitems = 0;
+    int grid = 0;
+    double flops = 0.0;
+    int cfg[2] = {32, 64};
+    bool use_graph = false;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+};
+
+namespace {
+
+using namespace jlc;
+using namespace jlc::grp;
+
+int gerr(jlc_ctx* ctx, int code, const char* fmt, ...) {
+    if (ctx) {
+        va_list ap;
+        va_start(ap, fmt);
+        vsnprintf(ctx->err, sizeof(ctx->err), fmt, ap);
+        va_end(ap);
+    }
+    return code;
+}
+
+int check_problem(jlc_ctx* ctx, const jlc_problem& p, int64_t i) {
+    if (p.m < 0 || p.n < 0 || p.k < 0) return gerr(ctx, JLC_E_ARG, "problem %lld: negative dimension", (long long)i);
+    if ((p.layout_a != JLC_ROW_MAJOR && p.layout_a != JLC_COL_MAJOR) ||
+        (p.layout_b != JLC_ROW_MAJOR && p.layout_b != JLC_COL_MAJOR))
+        return gerr(ctx, JLC_E_ARG, "problem %lld: bad layout", (long long)i);
+    if (p.m == 0 || p.n == 0) return JLC_OK;
+    if (!p.c || p.ldc < p.n) return gerr(ctx, JLC_E_ARG, "problem %lld: C null or ldc < n", (long long)i);
+    if (p.k > 0 && p.alpha != 0.0) {
+        if (!p.a || !p.b) return gerr(ctx, JLC_E_ARG, "problem %lld: Matrices must not be null", (long long)i);
+        if (p.lda < (p.layout_a == JLC_ROW_MAJOR ? p.k : p.m) || p.ldb < (p.layout_b == JLC_ROW_MAJOR ? p.n : p.k))
+            return gerr(ctx, JLC_E_ARG, "problem %lld: leading dimension too small", (long long)i);
+    }
+    if (p.m > (1 << 30) || p.n > (1 << 30) || p.k > (1 << 30))
+        return gerr(ctx, JLC_E_UNSUPPORTED, "problem %lld: dimension above 2^30", (long long)i);
+    return JLC_OK;
+}
+
+void free_plan_buffers(jlc_grouped_plan* pl) {
+    if (pl->exec) cudaGraphExecDestroy(pl->exec);
+    if (pl->graph) cudaGraphDestroy(pl->graph);
+    if (pl->d_probs) cudaFree(pl->d_probs);
+    if (pl->d_items) cudaFree(pl->d_items);
+    if (pl->d_tiny) cudaFree(pl->d_tiny);
+    if (pl->d_counter) cudaFree(pl->d_counter);
+    pl->exec = nullptr;
+    pl->graph = nullptr;
+    pl->d_probs = nullptr;
+    pl->d_items = nullptr;
+    pl->d_tiny = nullptr;
+    pl->d_counter = nullptr;
+}
+
+int upload(jlc_grouped_plan* pl, const std::vector<jlc_problem>& probs, const WorkList& wl) {
+    jlc_ctx* ctx = pl->ctx;
+    cudaStream_t st = ctx->stream;
+    auto alloc_copy = [&](void** dst, const void* src, size_t bytes) -> cudaError_t {
+        cudaError_t e = cudaMalloc(dst, bytes ? bytes : 16);
+        if (e != cudaSuccess) return e;
+        return bytes ? cudaMemcpyAsync(*dst, src, bytes, cudaMemcpyHostToDevice, st) : cudaSuccess;
+    };
+    cudaError_t e = alloc_copy((void**)&pl->d_probs, probs.data(), probs.size() * sizeof(jlc_problem));
+    if (e == cudaSuccess) e = alloc_copy((void**)&pl->d_items, wl.items.data(), wl.items.size() * sizeof(Item));
+    if (e == cudaSuccess) e = alloc_copy((void**)&pl->d_tiny, wl.tiny.data(), wl.tiny.size() * sizeof(int));
+    if (e == cudaSuccess) e = cudaMalloc((void**)&pl->d_counter, sizeof(int));
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);  // host vectors are pageable and short-lived
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return gerr(ctx, e == cudaErrorMemoryAllocation ? JLC_E_OOM : JLC_E_CUDA, "grouped plan upload: %s",
+                    cudaGetErrorString(e));
+    }
+    pl->nitems = (int)wl.items.size();
+    int per_sm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, grouped_kernel, THREADS, SMEM_BYTES);
+    if (per_sm < 1) per_sm = 1;
+    pl->grid = std::max(1, std::min(pl->nitems, ctx->sm_count * per_sm));
+    return JLC_OK;
+}
+
+int launch_plan(jlc_grouped_plan* pl, cudaStream_t st) {
+    if (pl->nitems == 0) return JLC_OK;
+    if (cudaMemsetAsync(pl->d_counter, 0, sizeof(int), st) != cudaSuccess) return JLC_E_CUDA;
+    grouped_kernel<<<pl->grid, THREADS, SMEM_BYTES, st>>>(pl->d_probs, pl->d_items, pl->nitems, pl->d_tiny,
+                                                         pl->d_counter);
+    return cudaGetLastError() == cudaSuccess ? JLC_OK : JLC_E_LAUNCH;
+}
+
+// Times both tile shapes of one shape class on synthetic operands with the
+// plan's problem shapes (the caller's C is never touched) and returns the
+// faster tile size, or 0 when the class is empty.
+int autotune_class(jlc_ctx* ctx, const std::vector<jlc_problem>& probs, int cls) {
+    size_t ma = 0, mb = 0, mc = 0;
+    std::vector<jlc_problem> syn;
+    for (const auto& p : probs) {
+        if (p.m == 0 || p.n == 0 || is_tiny(p) || shape_class(p) != cls) continue;
+        syn.push_back(p);
+        ma = std::max(ma, (size_t)(p.m * p.k));
+        mb = std::max(mb, (size_t)(p.k * p.n));
+        mc = std::max(mc, (size_t)(p.m * p.n));
+    }
+    if (syn.empty()) return 0;
+    double* buf = nullptr;
+    if (cudaMalloc(&buf, (ma + mb + mc + 3) * sizeof(double)) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    cudaMemsetAsync(buf, 0x3f, (ma + mb + mc + 3) * sizeof(double), ctx->stream);
+    for (auto& p : syn) {
+        p.a = buf;
+        p.b = buf + ma + 1;
+        p.c = buf + ma + mb + 2;
+        p.lda = p.layout_a == JLC_ROW_MAJOR ? p.k : p.m;
+        p.ldb = p.layout_b == JLC_ROW_MAJOR ? p.n : p.k;
+        p.ldc = p.n;
+        p.beta = 0.0;
+        if (p.alpha == 0.0) p.alpha = 1.0;
+    }
+    int best = 0;
+    float best_ms = 1e30f;
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    for (int ts : {32, 64}) {
+        int cfg[2] = {ts, ts};
+        WorkList wl;
+        build_work(syn, cfg, cls, wl);
+        jlc_grouped_plan tmp;
+        tmp.ctx = ctx;
+        if (upload(&tmp, syn, wl) != JLC_OK) {
+            free_plan_buffers(&tmp);
+            continue;
+        }
+        launch_plan(&tmp, ctx->stream);  // warm-up
+        float t = 1e30f;
+        for (int rep = 0; rep < 3; ++rep) {
+            cudaEventRecord(e0, ctx->stream);
+            launch_plan(&tmp, ctx->stream);
+            cudaEventRecord(e1, ctx->stream);
+            cudaEventSynchronize(e1);
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, e0, e1);
+            t = std::min(t, ms);
+        }
+        if (t < best_ms) {
+            best_ms = t;
+            best = ts;
+        }
+        free_plan_buffers(&tmp);
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaFree(buf);
+    cudaGetLastError();
+    return best;
+}
+
+}  // namespace
+
+extern "C" {
+
+int jlc_grouped_plan_create(jlc_ctx* ctx, const jlc_problem* probs, int64_t count, int precision, int flags,
+                            jlc_grouped_plan** out) {
+    if (!ctx || !out) return JLC_E_ARG;
+    *out = nullptr;
+    if (count < 0 || (count > 0 && !probs)) return gerr(ctx, JLC_E_ARG, "grouped: bad problem table");
+    if (count > (1 << 28)) return gerr(ctx, JLC_E_UNSUPPORTED, "grouped: too many problems");
+    if (precision == JLC_PREC_OZAKI)
+        return gerr(ctx, JLC_E_UNSUPPORTED, "grouped: Ozaki precision is not available for grouped launches");
+    cudaSetDevice(ctx->device);
+    std::vector<jlc_problem> v(probs, probs + count);
+    for (int64_t i = 0; i < count; ++i) {
+        int rc = check_problem(ctx, v[i], i);
+        if (rc) return rc;
+    }
+    jlc_grouped_plan* pl = new (std::nothrow) jlc_grouped_plan();
+    if (!pl) return JLC_E_OOM;
+    pl->ctx = ctx;
+    pl->count = count;
+    for (int cls = 0; cls < 2; ++cls) {
+        const std::string key = tune_key(ctx->device, ctx->sm_count, cls);
+        int ts = (flags & JLC_GROUPED_AUTOTUNE) ? autotune_class(ctx, v, cls) : 0;
+        if (ts) tune_store(key, ts);
+        else ts = tune_lookup(key);
+        if (ts == 32 || ts == 64) pl->cfg[cls] = ts;
+    }
+    WorkList wl;
+    build_work(v, pl->cfg, -1, wl);
+    pl->flops = wl.flops;
+    int rc = upload(pl, v, wl);
+    if (rc) {
+        free_plan_buffers(pl);
+        delete pl;
+        return rc;
+    }
+    if (flags & JLC_GROUPED_GRAPH) {
+        cudaError_t e = cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal);
+        if (e == cudaSuccess) {
+            rc = launch_plan(pl, ctx->stream);
+            e = cudaStreamEndCapture(ctx->stream, &pl->graph);
+        }
+        if (e == cudaSuccess && rc == JLC_OK) e = cudaGraphInstantiate(&pl->exec, pl->graph, 0);
+        if (e != cudaSuccess || rc != JLC_OK) {
+            cudaGetLastError();
+            free_plan_buffers(pl);
+            delete pl;
+            return gerr(ctx, JLC_E_CUDA, "grouped: graph capture failed: %s", cudaGetErrorString(e));
+        }
+        pl->use_graph = true;
+    }
+    *out = pl;
+    return JLC_OK;
+}
+
+int jlc_grouped_plan_run(jlc_grouped_plan* plan) {
+    if (!plan || !plan->ctx) return JLC_E_ARG;
+    jlc_ctx* ctx = plan->ctx;
+    cudaSetDevice(ctx->device);
+    if (plan->nitems == 0) return JLC_OK;
+    ctx->launches += 1;
+    if (plan->use_graph) {
+        cudaError_t e = cudaGraphLaunch(plan->exec, ctx->stream);
+        return e == cudaSuccess ? JLC_OK : gerr(ctx, JLC_E_LAUNCH, "graph launch: %s", cudaGetErrorString(e));
+    }
+    int rc = launch_plan(plan, ctx->stream);
+    return rc ? gerr(ctx, rc, "grouped launch failed") : JLC_OK;
+}
+
+int jlc_grouped_plan_info(const jlc_grouped_plan* plan, int64_t* work_items, double* flops, int* tile_small,
+                          int* tile_large) {
+    if (!plan) return JLC_E_ARG;
+    if (work_items) *work_items = plan->nitems;
+    if (flops) *flops = plan->flops;
+    if (tile_small) *tile_small = plan->cfg[0];
+    if (tile_large) *tile_large = plan->cfg[1];
+    return JLC_OK;
+}
+
+void jlc_grouped_plan_destroy(jlc_grouped_plan* plan) {
+    if (!plan) return;
+    if (plan->ctx) {
+        cudaSetDevice(plan->ctx->device);
+        cudaStreamSynchronize(plan->ctx->stream);
+    }
+    free_plan_buffers(plan);
+    delete plan;
+}
+
+int jlc_dgemm_grouped_device(jlc_ctx* ctx, const jlc_problem* probs, int64_t count, int precision, jlc_report* rep) {
+    if (rep) memset(rep, 0, sizeof(*rep));
+    jlc_grouped_plan* pl = nullptr;
+    int rc = jlc_grouped_plan_create(ctx, probs, count, precision, 0, &pl);
+    if (rc) return rc;
+    cudaEventRecord(ctx->ev0, ctx->stream);
+    rc = jlc_grouped_plan_run(pl);
+    cudaEventRecord(ctx->ev1, ctx->stream);
+    cudaError_t e = cudaStreamSynchronize(ctx->stream);
+    if (!rc && e != cudaSuccess) rc = gerr(ctx, JLC_E_CUDA, "grouped: %s", cudaGetErrorString(e));
+    if (!rc && rep) {
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
+        rep->precision = JLC_PREC_NATIVE;
+        rep->kernel = JLC_KERNEL_GROUPED;
+        rep->device_ms = ms;
+    }
+    jlc_grouped_plan_destroy(pl);
+    return rc;
+}
+
+}  // extern "C"

@@ -1,0 +1,140 @@
+"""GPU parity of grouped launches (many uneven GEMMs in one persistent launch).
+
+Mirrors the reference's batched use: the TINY/SMALL dispatch shapes
+(GemmDispatch.java:76-106) and blocked-factorisation updates issued as many
+independent gemm calls.  Every problem's result must sit inside the FP64
+componentwise bound of the double-double oracle.
+"""
+import os
+
+import numpy as np
+import pytest
+
+from parity import assert_fp64_bound
+
+pytestmark = pytest.mark.gpu
+
+
+def make_batch(oracle, shapes, seed, layouts=None, alphas=None, betas=None):
+    """Allocates every operand in one device arena; returns (problems, host copies, arena)."""
+    import torch
+    rng = np.random.default_rng(seed)
+    host, sizes = [], []
+    for idx, (m, n, k) in enumerate(shapes):
+        la, lb = layouts[idx] if layouts else (int(rng.integers(0, 2)), int(rng.integers(0, 2)))
+        alpha = alphas[idx] if alphas else float(rng.uniform(-2, 2))
+        beta = betas[idx] if betas else float(rng.uniform(-2, 2))
+        A = oracle.uniform((m, k), seed * 1000 + 3 * idx)
+        B = oracle.uniform((k, n), seed * 1000 + 3 * idx + 1)
+        C = oracle.uniform((m, n), seed * 1000 + 3 * idx + 2)
+        host.append((m, n, k, la, lb, alpha, beta, A, B, C))
+        sizes.append(m * k + k * n + m * n)
+    arena = torch.zeros(int(sum(sizes)) + 8, dtype=torch.float64, device="cuda")
+    probs, off = [], 0
+    base = arena.data_ptr()
+    for (m, n, k, la, lb, alpha, beta, A, B, C) in host:
+        a_store = A if la == 0 else np.ascontiguousarray(A.T)
+        b_store = B if lb == 0 else np.ascontiguousarray(B.T)
+        pa = off
+        arena[pa:pa + m * k] = torch.from_numpy(a_store.ravel())
+        pb = pa + m * k
+        arena[pb:pb + k * n] = torch.from_numpy(b_store.ravel())
+        pc = pb + k * n
+        arena[pc:pc + m * n] = torch.from_numpy(C.ravel())
+        off = pc + m * n
+        probs.append(dict(m=m, n=n, k=k, layout_a=la, layout_b=lb,
+                          lda=max(1, a_store.shape[1]), ldb=max(1, b_store.shape[1]), ldc=max(1, n),
+                          alpha=alpha, beta=beta, a=base + 8 * pa, b=base + 8 * pb, c=base + 8 * pc))
+    return probs, host, arena
+
+
+def check_batch(oracle, probs, host, arena, label):
+    flat = arena.cpu().numpy()
+    worst = 0.0
+    for p, (m, n, k, la, lb, alpha, beta, A, B, C) in zip(probs, host):
+        if m == 0 or n == 0:
+            continue
+        off = (p["c"] - arena.data_ptr()) // 8
+        got = flat[off:off + m * n].reshape(m, n)
+        worst = max(worst, assert_fp64_bound(f"{label} {m}x{n}x{k}", np.ascontiguousarray(got), A, B, C,
+                                             alpha, beta))
+    return worst
+
+
+def mixed_shapes(rng, count):
+    shapes = []
+    for i in range(count):
+        r = rng.random()
+        if r < 0.3:
+            s = int(rng.integers(2, 5))
+            shapes.append((s, s, s))
+        elif r < 0.5:
+            shapes.append(tuple(int(x) for x in rng.integers(1, 49, size=3)))
+        else:
+            shapes.append(tuple(int(x) for x in np.exp(rng.uniform(np.log(8), np.log(300), size=3)).round()))
+    return shapes
+
+
+def test_grouped_mixed_batch(ctx, oracle):
+    rng = np.random.default_rng(3)
+    shapes = mixed_shapes(rng, 300) + [(0, 5, 3), (5, 0, 3), (7, 9, 0), (1, 1, 1), (1, 200, 70), (200, 1, 70)]
+    alphas = [float(x) for x in rng.uniform(-2, 2, size=len(shapes))]
+    alphas[10] = 0.0  # alpha == 0: A and B are not read
+    probs, host, arena = make_batch(oracle, shapes, 5, alphas=alphas)
+    rep = ctx.dgemm_grouped_device(probs)
+    assert rep["kernel"] == 4
+    check_batch(oracle, probs, host, arena, "grouped")
+
+
+def test_grouped_plan_graph_replay_sees_new_data(ctx, oracle):
+    import torch
+    rng = np.random.default_rng(7)
+    shapes = mixed_shapes(rng, 120)
+    probs, host, arena = make_batch(oracle, shapes, 9, betas=[0.0] * len(shapes))
+    plan = ctx.grouped_plan(probs, graph=True)
+    info = plan.info()
+    assert info["work_items"] > 0 and info["flops"] > 0
+    plan.run()
+    ctx.synchronize()
+    check_batch(oracle, probs, host, arena, "graph run 1")
+    # new A data written in place; the same plan (same pointers) replays
+    host2 = []
+    for p, (m, n, k, la, lb, alpha, beta, A, B, C) in zip(probs, host):
+        A2 = -2.0 * A
+        a_store = A2 if la == 0 else np.ascontiguousarray(A2.T)
+        off = (p["a"] - arena.data_ptr()) // 8
+        arena[off:off + m * k] = torch.from_numpy(a_store.ravel())
+        host2.append((m, n, k, la, lb, alpha, beta, A2, B, C))
+    torch.cuda.synchronize()
+    plan.run()
+    ctx.synchronize()
+    check_batch(oracle, probs, host2, arena, "graph run 2")
+    plan.close()
+
+
+def test_grouped_autotune_writes_cache(ctx, oracle, tmp_path):
+    cache = tmp_path / "tune.txt"
+    os.environ["JLCGPU_TUNE_CACHE"] = str(cache)
+    try:
+        rng = np.random.default_rng(11)
+        shapes = [tuple(int(x) for x in rng.integers(20, 48, size=3)) for _ in range(40)] + \
+                 [tuple(int(x) for x in rng.integers(60, 260, size=3)) for _ in range(40)]
+        probs, host, arena = make_batch(oracle, shapes, 13)
+        plan = ctx.grouped_plan(probs, autotune=True)
+        info = plan.info()
+        assert info["tile_small"] in (32, 64) and info["tile_large"] in (32, 64)
+        text = cache.read_text()
+        assert "class0" in text and "class1" in text
+        plan.run()
+        ctx.synchronize()
+        check_batch(oracle, probs, host, arena, "autotuned")
+        plan.close()
+    finally:
+        os.environ.pop("JLCGPU_TUNE_CACHE", None)
+
+
+def test_grouped_rejects_bad_problem(ctx):
+    from jlc_b200 import IllegalArgumentException
+    bad = [dict(m=4, n=4, k=4, layout_a=0, layout_b=0, lda=2, ldb=4, ldc=4, alpha=1.0, beta=0.0, a=8, b=8, c=8)]
+    with pytest.raises(IllegalArgumentException):
+        ctx.dgemm_grouped_device(bad)
