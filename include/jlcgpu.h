@@ -198,6 +198,22 @@ JLC_API int jlc_check_fp64_bound_device(jlc_ctx* ctx, int layout_a, int layout_b
  * tcgen05 (dense), [3] BF16 on tcgen05 (dense).  Takes about a second. */
 JLC_API int jlc_measure_peaks(jlc_ctx* ctx, double* out4);
 
+/* ---------------------------------------------------------------- adjoint */
+/* Reverse-mode derivative of C_out = alpha*A*B + beta*C_in (no reference
+ * counterpart; the forward is OptimizedBLAS3.gemm, OptimizedBLAS3.java:61-130),
+ * all DEVICE pointers, row-major, A m x k, B k x n, C_in / dC m x n:
+ *   dA = alpha*dC*B^T, dB = alpha*A^T*dC, *dalpha = <dC, A*B> = <A, dC*B^T>,
+ *   *dbeta = <dC, C_in>, and dC_in = beta*dC when dc_in is not NULL.
+ * dalpha / dbeta are DEVICE doubles.  dA and d(alpha) come from one GEMM with a
+ * fused epilogue (scale + dot), dB from a second GEMM with A read transposed;
+ * reductions are deterministic.  precision as for jlc_dgemm_device.
+ * Enqueued on the context stream. */
+JLC_API int jlc_dgemm_adjoint_device(jlc_ctx* ctx, int64_t m, int64_t n, int64_t k, double alpha, double beta,
+                                     const double* a, int64_t lda, const double* b, int64_t ldb, const double* c_in,
+                                     int64_t ldc_in, const double* dc, int64_t lddc, double* da, int64_t ldda,
+                                     double* db, int64_t lddb, double* dalpha, double* dbeta, double* dc_in,
+                                     int64_t lddc_in, int precision, jlc_report* rep);
+
 /* ---------------------------------------------------------------- grouped batches */
 /* One GEMM of a batch: C = alpha*op(A)*op(B) + beta*C on DEVICE pointers, the
  * same layouts and semantics as jlc_dgemm_device. */

@@ -102,6 +102,18 @@ class Context:
         return {"fp64_dmma_tflops": out[0], "fp64_dfma_tflops": out[1], "int8_tops": out[2],
                 "bf16_tflops": out[3]}
 
+    def adjoint_device(self, m, n, k, alpha, beta, a_ptr, lda, b_ptr, ldb, cin_ptr, ldc_in, dc_ptr, lddc,
+                       da_ptr, ldda, db_ptr, lddb, dalpha_ptr, dbeta_ptr, dcin_ptr=None, lddc_in=0,
+                       precision=L.JLC_PREC_NATIVE) -> dict:
+        """jlc_dgemm_adjoint_device: gradients of C_out = alpha*A*B + beta*C_in (device pointers)."""
+        rep = L.Report()
+        rc = self.lib.jlc_dgemm_adjoint_device(self.h, m, n, k, float(alpha), float(beta), a_ptr, lda, b_ptr, ldb,
+                                               cin_ptr, ldc_in, dc_ptr, lddc, da_ptr, ldda, db_ptr, lddb,
+                                               dalpha_ptr, dbeta_ptr, dcin_ptr, lddc_in, int(precision),
+                                               ctypes.byref(rep))
+        self.check(rc)
+        return rep.as_dict()
+
     # -- grouped batches ---------------------------------------------------
     def grouped_plan(self, problems, precision=L.JLC_PREC_NATIVE, graph=False, autotune=False) -> "GroupedPlan":
         """Plan one persistent launch over a list of problems (dicts or

@@ -470,6 +470,7 @@ void jlc_destroy(jlc_ctx* ctx) {
     if (ctx->bufA.ptr) cudaFree(ctx->bufA.ptr);
     if (ctx->bufB.ptr) cudaFree(ctx->bufB.ptr);
     if (ctx->bufC.ptr) cudaFree(ctx->bufC.ptr);
+    if (ctx->bufR.ptr) cudaFree(ctx->bufR.ptr);
     if (ctx->ws.ptr) cudaFree(ctx->ws.ptr);
     if (ctx->d_status) cudaFree(ctx->d_status);
     if (ctx->d_flags) cudaFree(ctx->d_flags);
@@ -655,6 +656,78 @@ int jlc_check_fp64_bound_device(jlc_ctx* ctx, int layout_a, int layout_b, int64_
     *max_ratio = r;
     *max_abs = ab;
     *over = (int64_t)h[2];
+    return JLC_OK;
+}
+
+int jlc_dgemm_adjoint_device(jlc_ctx* ctx, int64_t m, int64_t n, int64_t k, double alpha, double beta,
+                             const double* a, int64_t lda, const double* b, int64_t ldb, const double* c_in,
+                             int64_t ldc_in, const double* dc, int64_t lddc, double* da, int64_t ldda, double* db,
+                             int64_t lddb, double* dalpha, double* dbeta, double* dc_in, int64_t lddc_in,
+                             int precision, jlc_report* rep) {
+    report_init(rep);
+    if (!ctx) return JLC_E_ARG;
+    if (m < 0 || n < 0 || k < 0) return set_err(ctx, JLC_E_ARG, "dimensions must be non-negative");
+    if (!dalpha || !dbeta) return set_err(ctx, JLC_E_ARG, "dalpha and dbeta must not be null");
+    if (m > 0 && n > 0 && (!dc || lddc < n || !c_in || ldc_in < n))
+        return set_err(ctx, JLC_E_ARG, "dC and C_in must not be null and their ld must be >= n");
+    if (m > 0 && k > 0 && (!a || lda < k || !da || ldda < k))
+        return set_err(ctx, JLC_E_ARG, "A and dA must not be null and their ld must be >= k");
+    if (k > 0 && n > 0 && (!b || ldb < n || !db || lddb < n))
+        return set_err(ctx, JLC_E_ARG, "B and dB must not be null and their ld must be >= n");
+    if (dc_in && lddc_in < n) return set_err(ctx, JLC_E_ARG, "lddc_in must be >= n");
+    if (m > INT32_MAX / 2 || n > INT32_MAX / 2 || k > INT32_MAX / 2)
+        return set_err(ctx, JLC_E_UNSUPPORTED, "dimension above 2^30");
+    cudaSetDevice(ctx->device);
+    ctx->err[0] = 0;
+    cudaStream_t st = ctx->stream;
+    const int np = ctx->sm_count > 0 ? ctx->sm_count : 1;  // the GEMM kernels never launch more CTAs
+    int rc = reserve(ctx, ctx->bufR, (size_t)(4 * np) * sizeof(double), "reduction partials");
+    if (rc) return rc;
+    double* parts_a = static_cast<double*>(ctx->bufR.ptr);
+    double* parts_b = parts_a + 2 * np;
+    jlc_report sub;
+
+    // 1) G = dC * B^T (m x k, contraction n): dA = alpha * G, dalpha = <A, G>
+    if (m > 0 && k > 0 && n > 0) {
+        GemmDesc g{JLC_ROW_MAJOR, JLC_COL_MAJOR, m, k, n, 1.0, 0.0, dc, lddc, b, ldb, da, ldda};
+        const bool gemv_shape = (k == 1 || m == 1);
+        if (!gemv_shape) {
+            // fused: the GEMM epilogue scales and reduces; partials of a kernel
+            // that did not run (the gated FP64 twin of an Ozaki call) stay 0
+            if (cudaMemsetAsync(parts_a, 0, np * sizeof(double), st) != cudaSuccess)
+                return set_err(ctx, JLC_E_CUDA, "partials reset failed");
+            g.epi_scale = alpha;
+            g.dot_mat = a;
+            g.dot_ld = lda;
+            g.dot_partials = parts_a;
+            rc = run_device(ctx, g, precision, 0, &sub);
+            if (!rc) rc = launch_sum(parts_a, np, dalpha, st);
+        } else {
+            rc = run_device(ctx, g, precision, 0, &sub);
+            if (!rc) rc = launch_dot2d(a, lda, da, ldda, m, k, parts_a, 2 * np, dalpha, st);
+            if (!rc && alpha != 1.0) rc = launch_scale_copy(da, ldda, da, ldda, m, k, alpha, st);
+        }
+        if (rc) return rc;
+    } else {
+        if (m > 0 && k > 0) {
+            rc = launch_scale_c(da, ldda, m, k, 0.0, st);  // n == 0: dA = 0
+            if (rc) return set_err(ctx, rc, "dA reset failed");
+        }
+        if (cudaMemsetAsync(dalpha, 0, sizeof(double), st) != cudaSuccess)
+            return set_err(ctx, JLC_E_CUDA, "dalpha reset failed");
+    }
+    if (rep) *rep = sub;
+    // 2) dB = alpha * A^T * dC (k x n, contraction m)
+    if (k > 0 && n > 0) {
+        GemmDesc g2{JLC_COL_MAJOR, JLC_ROW_MAJOR, k, n, m, alpha, 0.0, a, lda, dc, lddc, db, lddb};
+        rc = run_device(ctx, g2, precision, 0, &sub);
+        if (rc) return rc;
+    }
+    // 3) dbeta = <dC, C_in>;  4) dC_in = beta * dC
+    rc = launch_dot2d(dc, lddc, c_in, ldc_in, m, n, parts_b, 2 * np, dbeta, st);
+    if (!rc && dc_in) rc = launch_scale_copy(dc_in, lddc_in, dc, lddc, m, n, beta, st);
+    if (rc) return set_err(ctx, rc, "adjoint reduction launch failed");
+    ctx->launches += 3;
     return JLC_OK;
 }
 

@@ -49,12 +49,16 @@ static_assert(PRODUCER_WARPS * 32 * PRODUCER_REGS + MMA_WARPS * 32 * CONSUMER_RE
 constexpr int A_STAGE = BM * BK * 8;  // 16 KB
 constexpr int B_STAGE = BN * BK * 8;  // 16 KB
 constexpr int STAGE_BYTES = A_STAGE + B_STAGE;
-constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024 + 2 * STAGES * 8;
+constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024 + 2 * STAGES * 8 + MMA_WARPS * 8;
 constexpr int RASTER_GROUP = 8;
 
 struct Params {
     int M, N, K;
     double alpha, beta;
+    double epi_scale;
+    const double* dot_mat;
+    long long dot_ld;
+    double* dot_partials;
     double* C;
     long long ldc;
     int tiles_m, tiles_n, num_tiles, k_blocks;
@@ -153,11 +157,13 @@ __global__ void __launch_bounds__(THREADS, 1)
     const bool scale_a = p.alpha != 1.0;
     int stage = 0;
     uint32_t phase = 0;
+    double dot_acc = 0.0;
     constexpr int STEPS = BK / MMA_K;
     constexpr int AREG = MMA_K / 2;  // doubles of A per m16 tile per step
     constexpr int BREG = MMA_K / 4;  // doubles of B per n8 tile per step
 
-    for (int tile = blockIdx.x; tile < p.num_tiles; tile += gridDim.x) {
+    bool failed = false;
+    for (int tile = blockIdx.x; tile < p.num_tiles && !failed; tile += gridDim.x) {
         int tm, tn;
         tile_coords(tile, p.tiles_m, p.tiles_n, RASTER_GROUP, tm, tn);
         double acc[MT][NT][4];
@@ -169,7 +175,10 @@ __global__ void __launch_bounds__(THREADS, 1)
                 for (int e = 0; e < 4; ++e) acc[i][j][e] = 0.0;
 
         for (int kb = 0; kb < p.k_blocks; ++kb) {
-            if (!mbar_wait(&full[stage], phase, p.status)) return;
+            if (!mbar_wait(&full[stage], phase, p.status)) {
+                failed = true;  // status word reports it; still reach the reduction barrier below
+                break;
+            }
             const char* sA = smem + stage * STAGE_BYTES;
             const char* sB = sA + A_STAGE;
 #pragma unroll
@@ -208,7 +217,9 @@ __global__ void __launch_bounds__(THREADS, 1)
             }
         }
 
-        // fused epilogue: C = acc + beta * C_old (C_old not read when beta == 0)
+        if (failed) break;
+        // fused epilogue: C = epi_scale*acc + beta * C_old (C_old not read when
+        // beta == 0); optional dot with dot_mat for the adjoint's d(alpha)
         const int row0 = tm * BM + warp_m * WM;
         const int col0 = tn * BN + warp_n * WN;
 #pragma unroll
@@ -218,18 +229,34 @@ __global__ void __launch_bounds__(THREADS, 1)
                 const int row = row0 + mt * 16 + g + 8 * h;
                 if (row >= p.M) continue;
                 double* crow = p.C + (long long)row * p.ldc;
+                const double* drow = p.dot_mat ? p.dot_mat + (long long)row * p.dot_ld : nullptr;
 #pragma unroll
                 for (int nt = 0; nt < NT; ++nt) {
 #pragma unroll
                     for (int e = 0; e < 2; ++e) {
                         const int col = col0 + nt * 8 + 2 * t + e;
                         if (col < p.N) {
-                            const double v = acc[mt][nt][2 * h + e];
+                            const double a = acc[mt][nt][2 * h + e];
+                            if (drow) dot_acc = fma(drow[col], a, dot_acc);
+                            const double v = p.epi_scale == 1.0 ? a : p.epi_scale * a;
                             crow[col] = (p.beta == 0.0) ? v : fma(p.beta, crow[col], v);
                         }
                     }
                 }
             }
+        }
+    }
+    if (p.dot_partials) {
+        // deterministic CTA reduction over the 8 consumer warps (named barrier 1)
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) dot_acc += __shfl_xor_sync(0xffffffffu, dot_acc, o);
+        double* red = reinterpret_cast<double*>(empty + STAGES);
+        if (lane == 0) red[cw] = dot_acc;
+        asm volatile("bar.sync 1, %0;" ::"n"(MMA_WARPS * 32) : "memory");
+        if (cw == 0 && lane == 0) {
+            double s = 0.0;
+            for (int w = 0; w < MMA_WARPS; ++w) s += red[w];
+            p.dot_partials[blockIdx.x] = s;
         }
     }
 }
@@ -245,6 +272,11 @@ static int launch_variant(const CUtensorMap& ma, const CUtensorMap& mb, const Pa
 }
 
 }  // namespace dmma
+
+int dmma_grid(long long m, long long n, int sm_count) {
+    const long long tiles = ((m + dmma::BM - 1) / dmma::BM) * ((n + dmma::BN - 1) / dmma::BN);
+    return (int)(tiles < sm_count ? tiles : sm_count);
+}
 
 bool dmma_operand_ok(const void* ptr, long long ld) {
     return (reinterpret_cast<uintptr_t>(ptr) % 16 == 0) && ((ld * 8) % 16 == 0) && ld > 0;
@@ -284,6 +316,10 @@ int launch_dgemm_dmma(const GemmDesc& g, cudaStream_t st, int sm_count, int* sta
     p.beta = g.beta;
     p.C = g.c;
     p.ldc = g.ldc;
+    p.epi_scale = g.epi_scale;
+    p.dot_mat = g.dot_mat;
+    p.dot_ld = g.dot_ld;
+    p.dot_partials = g.dot_partials;
     p.tiles_m = (int)((g.m + BM - 1) / BM);
     p.tiles_n = (int)((g.n + BN - 1) / BN);
     p.num_tiles = p.tiles_m * p.tiles_n;

@@ -26,7 +26,21 @@ struct GemmDesc {
     long long ldb;
     double* c;
     long long ldc;
+    // Optional fused epilogue extras (the adjoint uses them):
+    //  epi_scale multiplies the product when it is written (C = epi_scale *
+    //  alpha*op(A)op(B) + beta*C); dot_mat, when set, makes every CTA add
+    //  sum_ij dot_mat(i,j) * (alpha*op(A)op(B))_ij over the tiles it wrote into
+    //  dot_partials[blockIdx.x] (deterministic order; the caller reduces).
+    double epi_scale = 1.0;
+    const double* dot_mat = nullptr;
+    long long dot_ld = 0;
+    double* dot_partials = nullptr;
 };
+
+// number of CTAs the DMMA / Ozaki GEMM kernels launch for this shape (the
+// length of dot_partials they fill)
+int dmma_grid(long long m, long long n, int sm_count);
+int ozaki_grid(long long m, long long n, int sm_count);
 
 // Grow-only device scratch owned by a context.
 struct Workspace {
@@ -89,6 +103,14 @@ int check_fp64_bound(const GemmDesc& g, const double* c_in, long long ldc_in, co
                      long long count, const long long* d_rows, const long long* d_cols, unsigned long long* d_out3,
                      cudaStream_t st);
 
+// adjoint helpers (adjoint.cu): out[0] = <x, y> over a rows x cols window
+// (nparts block partials, fixed order); out[0] = sum of n partials; dst = s * src
+int launch_dot2d(const double* x, long long ldx, const double* y, long long ldy, long long rows, long long cols,
+                 double* partials, int nparts, double* out, cudaStream_t st);
+int launch_sum(const double* partials, int n, double* out, cudaStream_t st);
+int launch_scale_copy(double* dst, long long ldd, const double* src, long long lds, long long rows, long long cols,
+                      double s, cudaStream_t st);
+
 // throughput probes (peaks.cu): out4 = {DMMA FP64, DFMA FP64, INT8 tcgen05, BF16 tcgen05} in T(FL)OP/s
 int measure_peaks(int sm_count, cudaStream_t st, int* status, double* out4, char* err, size_t errlen);
 
@@ -109,6 +131,7 @@ struct jlc_ctx {
     int* d_status = nullptr;  // status word written by kernels (JLC_DEV_* bits)
     int* d_flags = nullptr;   // control flags (e.g. the Ozaki non-finite gate)
     DevBuf bufA, bufB, bufC;
+    DevBuf bufR;  // reduction partials (adjoint)
     Workspace ws;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     int dmma_k = 8;

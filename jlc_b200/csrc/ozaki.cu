@@ -64,6 +64,10 @@ struct Params {
     double* scratch;
     int* status;
     const int* nonfinite;
+    double epi_scale;
+    const double* dot_mat;
+    long long dot_ld;
+    double* dot_partials;
 };
 
 // Instruction descriptor: kind::i8, D = S32, A = B = signed INT8, both K-major, 128 x 256.
@@ -81,6 +85,7 @@ __global__ void __launch_bounds__(THREADS, 1)
     uint64_t* acc_empty = acc_full + 2;
     uint64_t* mma_done = acc_empty + 2;
     uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(mma_done + 1);
+    double* red = reinterpret_cast<double*>(mma_done + 2);  // EPI_WARPS partial dots
 
     const int warp = warp_id(), lane = lane_id();
     if (threadIdx.x == 0) {
@@ -202,6 +207,8 @@ __global__ void __launch_bounds__(THREADS, 1)
         // warp's 16-byte accesses for one column pair are contiguous
         double2* scratch = reinterpret_cast<double2*>(p.scratch + (size_t)blockIdx.x * SCRATCH_DOUBLES);
         const bool c_vec = ((reinterpret_cast<uintptr_t>(p.C) & 15) == 0) && ((p.ldc & 1) == 0);
+        const double out_scale = p.epi_scale == 1.0 ? p.alpha : p.alpha * p.epi_scale;
+        double dot_acc = 0.0;
         uint32_t gcount = 0;
         bool ok = true;
         for (int tile = blockIdx.x; tile < p.num_tiles && ok; tile += gridDim.x) {
@@ -248,6 +255,7 @@ __global__ void __launch_bounds__(THREADS, 1)
                             }
                         } else if (row_ok) {
                             double* crow = p.C + (long long)grow * p.ldc + n0 + c0;
+                            const double* drow = p.dot_mat ? p.dot_mat + (long long)grow * p.dot_ld + n0 + c0 : nullptr;
                             const int ncols = min(32, p.N - (n0 + c0));
                             double out[32];
 #pragma unroll
@@ -259,8 +267,14 @@ __global__ void __launch_bounds__(THREADS, 1)
                                     v.y += o.y;
                                 }
                                 const int col0 = n0 + c0 + 2 * j;
-                                out[2 * j] = col0 < p.N ? p.alpha * ldexp(v.x, ei + p.eb[col0] - 14) : 0.0;
-                                out[2 * j + 1] = col0 + 1 < p.N ? p.alpha * ldexp(v.y, ei + p.eb[col0 + 1] - 14) : 0.0;
+                                const double g0 = col0 < p.N ? ldexp(v.x, ei + p.eb[col0] - 14) : 0.0;
+                                const double g1 = col0 + 1 < p.N ? ldexp(v.y, ei + p.eb[col0 + 1] - 14) : 0.0;
+                                if (drow) {
+                                    if (col0 < p.N) dot_acc = fma(drow[2 * j], p.alpha * g0, dot_acc);
+                                    if (col0 + 1 < p.N) dot_acc = fma(drow[2 * j + 1], p.alpha * g1, dot_acc);
+                                }
+                                out[2 * j] = out_scale * g0;
+                                out[2 * j + 1] = out_scale * g1;
                             }
                             if (c_vec && ncols == 32) {
                                 double2* c2 = reinterpret_cast<double2*>(crow);
@@ -286,6 +300,18 @@ __global__ void __launch_bounds__(THREADS, 1)
                     if (lane == 0) mbar_arrive(&acc_empty[buf]);
                     ++gcount;
                 }
+            }
+        }
+        if (p.dot_partials) {
+            // deterministic CTA reduction over the epilogue warps (named barrier 1)
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) dot_acc += __shfl_xor_sync(0xffffffffu, dot_acc, o);
+            if (lane == 0) red[warp - 2] = dot_acc;
+            asm volatile("bar.sync 1, %0;" ::"n"(EPI_WARPS * 32) : "memory");
+            if (warp == 2 && lane == 0) {
+                double sum = 0.0;
+                for (int w = 0; w < EPI_WARPS; ++w) sum += red[w];
+                p.dot_partials[blockIdx.x] = sum;
             }
         }
     }
@@ -475,6 +501,11 @@ int split_operand(const double* src, long long ld, bool kmajor, int rows, int K,
 
 }  // namespace oz
 
+int ozaki_grid(long long m, long long n, int sm_count) {
+    const long long tiles = ((m + oz::BM - 1) / oz::BM) * ((n + oz::BN - 1) / oz::BN);
+    return (int)(tiles < sm_count ? tiles : sm_count);
+}
+
 size_t ozaki_workspace_bytes(long long m, long long n, long long k, int slices, int sm_count) {
     const long long tiles = ((m + oz::BM - 1) / oz::BM) * ((n + oz::BN - 1) / oz::BN);
     const int grid = (int)(tiles < sm_count ? tiles : sm_count);
@@ -566,6 +597,10 @@ int launch_ozaki_gemm(const GemmDesc& g, int s, void* workspace, size_t ws_bytes
     p.scratch = reinterpret_cast<double*>(ws + b.L.scratch);
     p.status = status;
     p.nonfinite = flags;
+    p.epi_scale = g.epi_scale;
+    p.dot_mat = g.dot_mat;
+    p.dot_ld = g.dot_ld;
+    p.dot_partials = g.dot_partials;
     cudaError_t e = cudaFuncSetAttribute(ozaki_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES);
     if (e != cudaSuccess) {
         snprintf(err, errlen, "Ozaki smem attribute: %s", cudaGetErrorString(e));
