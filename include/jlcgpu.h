@@ -57,7 +57,8 @@ extern "C" {
 /* arithmetic used for the product */
 #define JLC_PREC_NATIVE 0 /* FP64 DMMA tensor-core kernel */
 #define JLC_PREC_OZAKI 1  /* Ozaki split: INT8 slices on tcgen05, FP64 recombination */
-#define JLC_PREC_AUTO 2   /* library picks (Ozaki for large, well-formed products) */
+#define JLC_PREC_AUTO 2   /* library picks (Ozaki residues for large products, else native) */
+#define JLC_PREC_OZAKI_CRT 3 /* Ozaki residues: INT8 residues mod coprime m_l on tcgen05, exact CRT in FP64 */
 
 /* kernel classes reported back (GemmDispatch.Kernel, GemmDispatch.java:40-47, on the GPU) */
 #define JLC_KERNEL_NONE 0    /* nothing to multiply (alpha==0, k==0, empty) */
@@ -72,8 +73,8 @@ typedef struct jlc_ctx jlc_ctx;
 typedef struct jlc_report {
     int32_t precision;     /* JLC_PREC_NATIVE or JLC_PREC_OZAKI actually used */
     int32_t kernel;        /* JLC_KERNEL_* */
-    int32_t slices;        /* Ozaki slice count s (0 for native) */
-    int32_t products;      /* INT8 slice products run (s(s+1)/2 for Ozaki) */
+    int32_t slices;        /* Ozaki slice count s, or number of moduli N (0 for native) */
+    int32_t products;      /* INT8 products run: s(s+1)/2 slice pairs, or N residue products */
     double est_err_ratio;  /* Ozaki a-priori error estimate / FP64 bound (0 for native) */
     double device_ms;      /* device time of the call, CUDA events (host entries only) */
     int64_t h2d_bytes;     /* bytes copied host -> device by this call */
@@ -155,6 +156,12 @@ JLC_API int jlc_dgemm_device(jlc_ctx* ctx, int layout_a, int layout_b, int64_t m
 JLC_API int jlc_dgemm_ozaki_device(jlc_ctx* ctx, int layout_a, int layout_b, int64_t m, int64_t n, int64_t k,
                            double alpha, const double* a, int64_t lda, const double* b, int64_t ldb, double beta,
                            double* c, int64_t ldc, int slices, jlc_report* rep);
+
+/* Ozaki residue (CRT) GEMM on device pointers with an explicit number of
+ * moduli (moduli in [2,15]; 0 = choose per call from k). */
+JLC_API int jlc_dgemm_ozaki_crt_device(jlc_ctx* ctx, int layout_a, int layout_b, int64_t m, int64_t n, int64_t k,
+                                       double alpha, const double* a, int64_t lda, const double* b, int64_t ldb,
+                                       double beta, double* c, int64_t ldc, int moduli, jlc_report* rep);
 
 /* Reads and clears the context's device status word after synchronising:
  * JLC_OK, or JLC_E_TIMEOUT if a kernel gave up on a bounded wait. */

@@ -7,7 +7,8 @@ compute entry point without the built library raises ``JlcLibraryMissing``;
 nothing falls back to the CPU.
 """
 from ._lib import (JLC_COL_MAJOR, JLC_KERNEL_DMMA, JLC_KERNEL_GEMV, JLC_KERNEL_GROUPED, JLC_KERNEL_NONE,
-                   JLC_KERNEL_OZAKI, JLC_PREC_AUTO, JLC_PREC_NATIVE, JLC_PREC_OZAKI, JLC_ROW_MAJOR,
+                   JLC_KERNEL_OZAKI, JLC_PREC_AUTO, JLC_PREC_NATIVE, JLC_PREC_OZAKI, JLC_PREC_OZAKI_CRT,
+                   JLC_ROW_MAJOR,
                    JlcLibraryMissing, LIB_PATH, load)
 from .compute import (BLAS3Kernels, Context, CudaGemm, DispatchPolicy, IllegalArgumentException, JlcError, Matrix,
                       OffHeapMatrix, OptimizedBLAS3, default_context)
@@ -15,6 +16,6 @@ from .compute import (BLAS3Kernels, Context, CudaGemm, DispatchPolicy, IllegalAr
 __all__ = [
     "BLAS3Kernels", "Context", "CudaGemm", "DispatchPolicy", "IllegalArgumentException", "JlcError",
     "JlcLibraryMissing", "Matrix", "OffHeapMatrix", "OptimizedBLAS3", "default_context", "load", "LIB_PATH",
-    "JLC_ROW_MAJOR", "JLC_COL_MAJOR", "JLC_PREC_NATIVE", "JLC_PREC_OZAKI", "JLC_PREC_AUTO", "JLC_KERNEL_NONE",
+    "JLC_ROW_MAJOR", "JLC_COL_MAJOR", "JLC_PREC_NATIVE", "JLC_PREC_OZAKI", "JLC_PREC_OZAKI_CRT", "JLC_PREC_AUTO", "JLC_KERNEL_NONE",
     "JLC_KERNEL_DMMA", "JLC_KERNEL_GEMV", "JLC_KERNEL_OZAKI", "JLC_KERNEL_GROUPED",
 ]

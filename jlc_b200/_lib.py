@@ -22,6 +22,7 @@ JLC_COL_MAJOR = 1
 JLC_PREC_NATIVE = 0
 JLC_PREC_OZAKI = 1
 JLC_PREC_AUTO = 2
+JLC_PREC_OZAKI_CRT = 3
 
 JLC_KERNEL_NONE = 0
 JLC_KERNEL_DMMA = 1
@@ -92,6 +93,8 @@ SIGNATURES = {
     "jlc_dgemm_device": (_i, _GENERAL),
     "jlc_dgemm_ozaki_device": (_i, [_vp, _i, _i, _i64, _i64, _i64, _d, _dp, _i64, _dp, _i64, _d, _dp, _i64, _i,
                                     _REP]),
+    "jlc_dgemm_ozaki_crt_device": (_i, [_vp, _i, _i, _i64, _i64, _i64, _d, _dp, _i64, _dp, _i64, _d, _dp, _i64,
+                                        _i, _REP]),
     "jlc_device_status": (_i, [_vp]),
     "jlc_set_profiling": (_i, [_vp, _i]),
     "jlc_profile_collect": (_i, [_vp, ctypes.POINTER(_i), ctypes.POINTER(_d), _i]),

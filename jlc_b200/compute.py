@@ -102,6 +102,15 @@ class Context:
         return {"fp64_dmma_tflops": out[0], "fp64_dfma_tflops": out[1], "int8_tops": out[2],
                 "bf16_tflops": out[3]}
 
+    def ozaki_crt_device(self, layout_a, layout_b, m, n, k, alpha, a_ptr, lda, b_ptr, ldb, beta, c_ptr, ldc,
+                         moduli=0) -> dict:
+        rep = L.Report()
+        rc = self.lib.jlc_dgemm_ozaki_crt_device(self.h, int(layout_a), int(layout_b), m, n, k, float(alpha), a_ptr,
+                                                 lda, b_ptr, ldb, float(beta), c_ptr, ldc, int(moduli),
+                                                 ctypes.byref(rep))
+        self.check(rc)
+        return rep.as_dict()
+
     def adjoint_device(self, m, n, k, alpha, beta, a_ptr, lda, b_ptr, ldb, cin_ptr, ldc_in, dc_ptr, lddc,
                        da_ptr, ldda, db_ptr, lddb, dalpha_ptr, dbeta_ptr, dcin_ptr=None, lddc_in=0,
                        precision=L.JLC_PREC_NATIVE) -> dict:

@@ -118,7 +118,7 @@ int auto_slices(long long k) {
 }
 
 bool use_ozaki(int precision, long long m, long long n, long long k) {
-    if (precision == JLC_PREC_OZAKI) return true;
+    if (precision == JLC_PREC_OZAKI || precision == JLC_PREC_OZAKI_CRT) return true;
     if (precision == JLC_PREC_NATIVE) return false;
     return m >= 2048 && n >= 2048 && k >= 1024;  // AUTO: large products only
 }
@@ -183,33 +183,36 @@ int run_device(jlc_ctx* ctx, const GemmDesc& g0, int precision, int slices, jlc_
         return launch_gemv(v, ctx->ws.ptr, ctx->stream, ctx->sm_count, ctx->err, sizeof(ctx->err));
     }
     const bool ozaki = use_ozaki(precision, g.m, g.n, g.k);
+    // AUTO takes the residue scheme: fewer INT8 products for the same bound
+    const bool crt = ozaki && precision != JLC_PREC_OZAKI;
     int rc = JLC_OK;
     if (ozaki) {
-        const int s = slices > 0 ? slices : auto_slices(g.k);
-        size_t need = ozaki_workspace_bytes(g.m, g.n, g.k, s, ctx->sm_count);
+        const int s = slices > 0 ? slices : (crt ? ozaki_crt_auto_moduli(g.k) : auto_slices(g.k));
+        size_t need = ozaki_workspace_bytes(g.m, g.n, g.k, s, ctx->sm_count, crt);
         rc = workspace_reserve(ctx->ws, need, ctx->err, sizeof(ctx->err));
         if (rc) return rc;
         {
             Phase ph(ctx, JLC_PHASE_OZAKI_SPLIT);
             ctx->launches += (g.layout_a == JLC_ROW_MAJOR ? 1 : 2) + (g.layout_b == JLC_COL_MAJOR ? 1 : 2);
             rc = launch_ozaki_split(g, s, ctx->ws.ptr, ctx->ws.bytes, ctx->stream, ctx->sm_count, ctx->d_flags,
-                                    ctx->err, sizeof(ctx->err));
+                                    ctx->err, sizeof(ctx->err), crt);
         }
         if (rc) return rc;
         {
             Phase ph(ctx, JLC_PHASE_OZAKI_GEMM);
             ctx->launches += 1;
             rc = launch_ozaki_gemm(g, s, ctx->ws.ptr, ctx->ws.bytes, ctx->stream, ctx->sm_count, ctx->d_status,
-                                   ctx->d_flags, ctx->err, sizeof(ctx->err));
+                                   ctx->d_flags, ctx->err, sizeof(ctx->err), crt);
         }
         if (rc) return rc;
         if (rep) {
-            rep->precision = JLC_PREC_OZAKI;
+            rep->precision = crt ? JLC_PREC_OZAKI_CRT : JLC_PREC_OZAKI;
             rep->kernel = JLC_KERNEL_OZAKI;
             rep->slices = s;
-            rep->products = s * (s + 1) / 2;
+            rep->products = crt ? s : s * (s + 1) / 2;
             const double u = std::ldexp(1.0, -53);
-            rep->est_err_ratio = (s + 3) * std::ldexp(1.0, -7 * s) / (2.0 * u * (double)g.k / 16.0);
+            rep->est_err_ratio = crt ? ozaki_crt_est_ratio(s, g.k)
+                                     : (s + 3) * std::ldexp(1.0, -7 * s) / (2.0 * u * (double)g.k / 16.0);
         }
     }
     // the DMMA kernel reads A/B through TMA: 16-byte aligned bases, even lds
@@ -578,6 +581,18 @@ int jlc_dgemm_device(jlc_ctx* ctx, int layout_a, int layout_b, int64_t m, int64_
     cudaSetDevice(ctx->device);
     GemmDesc g{layout_a, layout_b, m, n, k, alpha, beta, a, lda, b, ldb, c, ldc};
     return run_device(ctx, g, precision, 0, rep);
+}
+
+int jlc_dgemm_ozaki_crt_device(jlc_ctx* ctx, int layout_a, int layout_b, int64_t m, int64_t n, int64_t k,
+                               double alpha, const double* a, int64_t lda, const double* b, int64_t ldb, double beta,
+                               double* c, int64_t ldc, int moduli, jlc_report* rep) {
+    report_init(rep);
+    int rc = validate(ctx, layout_a, layout_b, m, n, k, a, lda, b, ldb, c, ldc);
+    if (rc) return rc;
+    if (moduli != 0 && (moduli < 2 || moduli > 15)) return set_err(ctx, JLC_E_ARG, "moduli must be 0 or in [2,15]");
+    cudaSetDevice(ctx->device);
+    GemmDesc g{layout_a, layout_b, m, n, k, alpha, beta, a, lda, b, ldb, c, ldc};
+    return run_device(ctx, g, JLC_PREC_OZAKI_CRT, moduli, rep);
 }
 
 int jlc_dgemm_ozaki_device(jlc_ctx* ctx, int layout_a, int layout_b, int64_t m, int64_t n, int64_t k,

@@ -82,20 +82,20 @@ int launch_gemv(const GemvDesc& g, void* scratch, cudaStream_t st, int sm_count,
 // C <- beta * C on the m x n window (beta == 0 writes zeros without reading).
 int launch_scale_c(double* c, long long ldc, long long m, long long n, double beta, cudaStream_t st);
 
-// Ozaki split-precision GEMM (INT8 slices on tcgen05, FP64 recombination).
-struct OzakiPlan {
-    int slices;         // s
-    int products;       // s(s+1)/2
-    double est_ratio;   // a-priori error / bound estimate for the chosen s (host-side model)
-};
-size_t ozaki_workspace_bytes(long long m, long long n, long long k, int slices, int sm_count);
-// Phase 1: exponents + INT8 slices of op(A) and op(B) into the workspace; sets
-// flags[0] when an operand holds Inf/NaN.  Phase 2: the tcgen05 slice-product
-// GEMM with FP64 recombination into C (skipped on the device when flags[0]).
-int launch_ozaki_split(const GemmDesc& g, int slices, void* workspace, size_t ws_bytes, cudaStream_t st,
-                       int sm_count, int* flags, char* err, size_t errlen);
-int launch_ozaki_gemm(const GemmDesc& g, int slices, void* workspace, size_t ws_bytes, cudaStream_t st,
-                      int sm_count, int* status, int* flags, char* err, size_t errlen);
+// Ozaki split-precision GEMM (INT8 on tcgen05, FP64 recombination).  count
+// is the slice count s (slice scheme) or the number of moduli N (residue
+// scheme, crt = true).
+size_t ozaki_workspace_bytes(long long m, long long n, long long k, int count, int sm_count, bool crt = false);
+int ozaki_crt_auto_moduli(long long k);
+double ozaki_crt_est_ratio(int nmod, long long k);
+// Phase 1: exponents + INT8 slices / residues of op(A) and op(B) into the
+// workspace; sets flags[0] when an operand holds Inf/NaN.  Phase 2: the
+// tcgen05 GEMM with FP64 recombination into C (skipped on the device when
+// flags[0] is set).
+int launch_ozaki_split(const GemmDesc& g, int count, void* workspace, size_t ws_bytes, cudaStream_t st,
+                       int sm_count, int* flags, char* err, size_t errlen, bool crt = false);
+int launch_ozaki_gemm(const GemmDesc& g, int count, void* workspace, size_t ws_bytes, cudaStream_t st,
+                      int sm_count, int* status, int* flags, char* err, size_t errlen, bool crt = false);
 
 // double-double accuracy check of sampled entries (verify.cu); d_out3 holds
 // [max ratio bits, max abs error bits, entries over the bound], zeroed by the caller

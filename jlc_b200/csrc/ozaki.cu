@@ -1,10 +1,12 @@
 // Ozaki split-precision FP64 GEMM on the B200 INT8 tensor cores (tcgen05).
 //
-// Method (Ozaki, Ogita, Oishi, Rump, "Error-free transformations of matrix
-// multiplication by using fast routines of matrix multiplication and its
-// applications", Numer. Algorithms 59, 2012; INT8 variant after Ootomo, Ozaki
-// and Yokota, "DGEMM on integer matrix multiplication unit", IJHPCA 2024):
+// Two schemes share one persistent tcgen05 kernel (template parameter CRT):
 //
+// Slice pairs (JLC_PREC_OZAKI; Ozaki, Ogita, Oishi, Rump, "Error-free
+// transformations of matrix multiplication by using fast routines of matrix
+// multiplication and its applications", Numer. Algorithms 59, 2012; INT8
+// variant after Ootomo, Ozaki and Yokota, "DGEMM on integer matrix
+// multiplication unit", IJHPCA 2024):
 //  1. Exponent scaling.  Row i of op(A) gets E_i with max_p |a_ip| < 2^E_i,
 //     column j of op(B) gets F_j likewise.  a * 2^-E_i lies in (-1, 1); the
 //     scaling is exact (a power of two).
@@ -21,20 +23,41 @@
 //     significant diagonal up (the only FP64 rounding besides the final
 //     one), then C = alpha * 2^(E_i+F_j-14) * T + beta*C.
 //
+// Residues (JLC_PREC_OZAKI_CRT; after Ozaki, Uchino and Imamura, "Ozaki
+// Scheme II: a GEMM-oriented emulation of floating-point matrix
+// multiplication using an integer modular technique", 2025):
+//  1. The same exponents, then integers A' = rint(a * 2^(p-E_i)),
+//     B' = rint(b * 2^(q-F_j)) with |A'| <= 2^p, |B'| <= 2^q, where p + q is
+//     chosen so that M = m_1 * ... * m_N exceeds 2 k 2^(p+q).
+//  2. For each pairwise coprime modulus m_l <= 256 the symmetric residues of
+//     A' and B' are INT8 matrices; their product runs on tcgen05 with exact
+//     INT32 accumulation and is reduced mod m_l in the epilogue (one byte
+//     per element; runs longer than 1023 k-blocks are reduced chunk-wise).
+//  3. After the last modulus the integer product A'B' is reconstructed
+//     exactly by the Chinese remainder theorem: sum_l r_l W_l is kept as
+//     three FP64 words of 41-bit digits (every product and partial sum is
+//     an exact integer below 2^53), one multiple of M is removed to land in
+//     (-M/2, M/2], and C = alpha * 2^(E_i+F_j-p-q) * A'B' + beta*C.
+//  N moduli replace s(s+1)/2 slice pairs: 13 products instead of 28 for
+//  the same FP64 accuracy at k = 8192, and the error comes only from the
+//  rounding of A' and B' (round-to-nearest, so it is unbiased).
+//
 // Kernel layout: persistent CTAs, 10 warps.  Warp 0 issues TMA loads of the
-// K-major INT8 slice tiles (A 128x128 B, B 256x128 B, 128B swizzle) into a
+// K-major INT8 tiles (A 128x128 B, B 256x128 B, 128B swizzle) into a
 // 4-stage ring; warp 1 allocates TMEM (512 columns = two 128x256 INT32
 // accumulators) and one elected lane issues tcgen05.mma; warps 2-9 drain
-// the accumulators with tcgen05.ld and keep the FP64 running sum T of the
-// current 128x256 tile in a per-CTA scratch tile (256 KB, L2 resident),
-// writing C after the last anti-diagonal.  Diagonals run from the least
-// significant (most pairs) down to d = 0, and accumulator double buffering
-// lets the epilogue of one diagonal overlap the MMAs of the next.  No TMA
-// multicast is used anywhere.
+// the accumulators with tcgen05.ld into a per-CTA scratch tile (FP64 running
+// sums, or residue bytes) and write C after the tile's last run.  In the
+// slice scheme diagonals run from the least significant (most pairs) down
+// to d = 0; accumulator double buffering lets the epilogue of one run
+// overlap the MMAs of the next.  No TMA multicast is used anywhere.
+#include <cmath>
 #include <cstdio>
+#include <cstring>
 
 #include "jlc_device.cuh"
 #include "jlc_internal.h"
+#include "jlc_crt.cuh"
 #include "jlc_tcgen05.cuh"
 
 namespace jlc {
@@ -49,9 +72,27 @@ constexpr int STAGE_BYTES = A_STAGE + B_STAGE;
 constexpr int THREADS = 320;  // warp 0 TMA, warp 1 MMA, warps 2..9 epilogue
 constexpr int EPI_WARPS = 8;
 constexpr int TMEM_COLS = 512;
-constexpr int GROUP_CAP = 1040;  // k-blocks per INT32 run: 1040*128*127*127 < 2^31
+constexpr int GROUP_CAP = 1040;      // k-blocks per INT32 run: 1040*128*127*127 < 2^31
+constexpr int GROUP_CAP_CRT = 1023;  // residues up to 128 in magnitude: 1023*128*128*128 < 2^31
 constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024 + 256;
-constexpr int SCRATCH_DOUBLES = BM * BN;  // per CTA
+constexpr int SCRATCH_DOUBLES = BM * BN;  // per CTA, slice scheme (FP64 running sums)
+constexpr int MAX_MODULI = 15;            // product of 15 moduli < 2^123 = three 41-bit digits
+constexpr int RECON_GROUPS = BN / 2 / 4;  // groups of 4 columns per epilogue thread and tile
+constexpr int CRT_SLOT_WORDS = (BN / 4) * BM;  // one residue byte per element, 4 per word
+
+// Pairwise coprime moduli, largest first; residues are symmetric INT8.
+__constant__ int kModuli[MAX_MODULI] = {256, 255, 253, 251, 247, 241, 239, 233, 229, 227, 223, 211, 199, 197, 193};
+// 1/m_l rounded to nearest (host-compiler IEEE division of constants)
+__constant__ double kInvModuli[MAX_MODULI] = {1.0 / 256, 1.0 / 255, 1.0 / 253, 1.0 / 251, 1.0 / 247,
+                                              1.0 / 241, 1.0 / 239, 1.0 / 233, 1.0 / 229, 1.0 / 227,
+                                              1.0 / 223, 1.0 / 211, 1.0 / 199, 1.0 / 197, 1.0 / 193};
+static const int kModuliHost[MAX_MODULI] = {256, 255, 253, 251, 247, 241, 239, 233, 229, 227, 223, 211, 199, 197,
+                                            193};
+
+// Constants of the CRT reconstruction for N moduli (written per call into
+// the workspace): W_l = (M/m_l) * ((M/m_l)^-1 mod m_l) mod M and M itself as
+// three 41-bit digits (value = d0*2^82 + d1*2^41 + d2).
+using CrtConsts = crt::Consts;
 
 struct Params {
     int M, N, K, KB, s;
@@ -68,11 +109,47 @@ struct Params {
     const double* dot_mat;
     long long dot_ld;
     double* dot_partials;
+    CrtConsts crt;  // residue scheme only (by value: read from the constant bank)
 };
 
 // Instruction descriptor: kind::i8, D = S32, A = B = signed INT8, both K-major, 128 x 256.
 constexpr uint32_t kIdescI8 = make_idesc(2u, 1u, BM, BN);
 
+// Run structure shared by the three roles.  A tile is a sequence of
+// "diagonals"; diagonal di holds npairs(di) slice pairs whose INT8 products
+// accumulate into one INT32 accumulator (split into runs of at most cap
+// k-blocks).  Slice scheme: diagonals d = s-1 .. 0, pairs (t, d-t).
+// Residue scheme: diagonal l = modulus l, one pair (l, l).
+template <bool CRT>
+struct Runs {
+    int ndiag, KB;
+    __device__ __forceinline__ int diag(int di) const { return CRT ? di : ndiag - 1 - di; }
+    __device__ __forceinline__ int npairs(int d) const { return CRT ? 1 : d + 1; }
+    __device__ __forceinline__ int slice_a(int d, int pr) const { return CRT ? d : pr; }
+    __device__ __forceinline__ int slice_b(int d, int pr) const { return CRT ? d : d - pr; }
+    static constexpr int cap = CRT ? GROUP_CAP_CRT : GROUP_CAP;
+};
+
+// 2^s as the product of two doubles (each a power of two that is a normal
+// double), so that x * lo * hi == x * 2^s exactly whenever the result is a
+// normal double, for any s in [-1074, 1126].
+struct Pow2 {
+    double lo, hi;
+};
+__device__ __forceinline__ Pow2 pow2_split(int s) {
+    const int s1 = s > 1000 ? s - 1000 : (s < -1000 ? -1000 : s);
+    const int s2 = s - s1;
+    return {__longlong_as_double((long long)(s1 + 1023) << 52), __longlong_as_double((long long)(s2 + 1023) << 52)};
+}
+
+// v * 2^s for an integer-valued v: one exact multiply while 2^s is a normal
+// double (then v * 2^s is normal too, or zero), ldexp beyond that
+__device__ __forceinline__ double scale_pow2(double v, int s) {
+    if (s >= -1022 && s <= 1023) return v * __longlong_as_double((long long)(s + 1023) << 52);
+    return ldexp(v, s);
+}
+
+template <bool CRT>
 __global__ void __launch_bounds__(THREADS, 1)
     ozaki_gemm_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB,
                       const Params p) {
@@ -86,6 +163,7 @@ __global__ void __launch_bounds__(THREADS, 1)
     uint64_t* mma_done = acc_empty + 2;
     uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(mma_done + 1);
     double* red = reinterpret_cast<double*>(mma_done + 2);  // EPI_WARPS partial dots
+    const Runs<CRT> runs{p.s, p.KB};
 
     const int warp = warp_id(), lane = lane_id();
     if (threadIdx.x == 0) {
@@ -121,9 +199,10 @@ __global__ void __launch_bounds__(THREADS, 1)
                 int tm, tn;
                 tile_coords(tile, p.tiles_m, p.tiles_n, 8, tm, tn);
                 const int m0 = tm * BM, n0 = tn * BN;
-                for (int d = p.s - 1; d >= 0 && ok; --d) {
-                    for (int pr = 0; pr <= d && ok; ++pr) {
-                        const int ia = pr, ib = d - pr;
+                for (int di = 0; di < runs.ndiag && ok; ++di) {
+                    const int d = runs.diag(di);
+                    for (int pr = 0; pr < runs.npairs(d) && ok; ++pr) {
+                        const int ia = runs.slice_a(d, pr), ib = runs.slice_b(d, pr);
                         for (int kb = 0; kb < p.KB; ++kb) {
                             if (!mbar_wait(&empty[stage], phase ^ 1u, p.status)) {
                                 ok = false;
@@ -155,10 +234,10 @@ __global__ void __launch_bounds__(THREADS, 1)
             uint32_t gcount = 0;
             bool ok = true;
             for (int tile = blockIdx.x; tile < p.num_tiles && ok; tile += gridDim.x) {
-                for (int d = p.s - 1; d >= 0 && ok; --d) {
-                    const int nblk = (d + 1) * p.KB;
-                    for (int g0 = 0; g0 < nblk && ok; g0 += GROUP_CAP) {
-                        const int g1 = min(nblk, g0 + GROUP_CAP);
+                for (int di = 0; di < runs.ndiag && ok; ++di) {
+                    const int nblk = runs.npairs(runs.diag(di)) * p.KB;
+                    for (int g0 = 0; g0 < nblk && ok; g0 += Runs<CRT>::cap) {
+                        const int g1 = min(nblk, g0 + Runs<CRT>::cap);
                         const uint32_t buf = gcount & 1u, accphase = (gcount >> 1) & 1u;
                         if (!mbar_wait(&acc_empty[buf], accphase ^ 1u, p.status)) {
                             ok = false;
@@ -203,12 +282,103 @@ __global__ void __launch_bounds__(THREADS, 1)
         const int quarter = warp & 3;
         const int half = (warp - 2) >> 2;
         const int row = quarter * 32 + lane;
-        // FP64 running sums of this CTA's tile, laid out [col/2][row][2] so a
-        // warp's 16-byte accesses for one column pair are contiguous
-        double2* scratch = reinterpret_cast<double2*>(p.scratch + (size_t)blockIdx.x * SCRATCH_DOUBLES);
         const bool c_vec = ((reinterpret_cast<uintptr_t>(p.C) & 15) == 0) && ((p.ldc & 1) == 0);
         const double out_scale = p.epi_scale == 1.0 ? p.alpha : p.alpha * p.epi_scale;
         double dot_acc = 0.0;
+        uint32_t* crt_base = reinterpret_cast<uint32_t*>(p.scratch) + (size_t)blockIdx.x * 2 * MAX_MODULI * CRT_SLOT_WORDS;
+        // writes 32 columns of row grow from tile column c0; out holds alpha-free values
+        auto write_out = [&](int grow, int n0, int c0, double(&out)[32]) {
+            double* crow = p.C + (long long)grow * p.ldc + n0 + c0;
+            const double* drow = p.dot_mat ? p.dot_mat + (long long)grow * p.dot_ld + n0 + c0 : nullptr;
+            const int ncols = min(32, p.N - (n0 + c0));
+            if (drow) {
+#pragma unroll
+                for (int j = 0; j < 32; ++j)
+                    if (j < ncols) dot_acc = fma(drow[j], p.alpha * out[j], dot_acc);
+            }
+#pragma unroll
+            for (int j = 0; j < 32; ++j) out[j] *= out_scale;
+            if (c_vec && ncols == 32) {
+                double2* c2 = reinterpret_cast<double2*>(crow);
+#pragma unroll
+                for (int j = 0; j < 16; ++j) {
+                    double2 v = make_double2(out[2 * j], out[2 * j + 1]);
+                    if (p.beta != 0.0) {
+                        const double2 o = c2[j];
+                        v.x = fma(p.beta, o.x, v.x);
+                        v.y = fma(p.beta, o.y, v.y);
+                    }
+                    c2[j] = v;
+                }
+            } else {
+#pragma unroll
+                for (int j = 0; j < 32; ++j)
+                    if (j < ncols) crow[j] = (p.beta == 0.0) ? out[j] : fma(p.beta, crow[j], out[j]);
+            }
+        };
+        // writes 4 columns of row grow from tile column c; out holds alpha-free values
+        auto write_out4 = [&](int grow, int n0, int c, double(&out)[4]) {
+            const int ncols = min(4, p.N - (n0 + c));
+            if (ncols <= 0) return;
+            double* crow = p.C + (long long)grow * p.ldc + n0 + c;
+            if (p.dot_mat) {
+                const double* drow = p.dot_mat + (long long)grow * p.dot_ld + n0 + c;
+#pragma unroll
+                for (int j = 0; j < 4; ++j)
+                    if (j < ncols) dot_acc = fma(drow[j], p.alpha * out[j], dot_acc);
+            }
+#pragma unroll
+            for (int j = 0; j < 4; ++j) out[j] *= out_scale;
+            if (c_vec && ncols == 4) {
+                double2* c2 = reinterpret_cast<double2*>(crow);
+#pragma unroll
+                for (int j = 0; j < 2; ++j) {
+                    double2 v = make_double2(out[2 * j], out[2 * j + 1]);
+                    if (p.beta != 0.0) {
+                        const double2 o = c2[j];
+                        v.x = fma(p.beta, o.x, v.x);
+                        v.y = fma(p.beta, o.y, v.y);
+                    }
+                    c2[j] = v;
+                }
+            } else {
+#pragma unroll
+                for (int j = 0; j < 4; ++j)
+                    if (j < ncols) crow[j] = (p.beta == 0.0) ? out[j] : fma(p.beta, crow[j], out[j]);
+            }
+        };
+        // Residue scheme: a finished tile's Chinese remainder reconstruction is
+        // spread over the next tile's runs (a share after each accumulator is
+        // released), so the MMAs never wait for it.  Each thread owns one row
+        // and 128 columns of the tile: RECON_GROUPS groups of 4 columns.
+        int pend_left = 0, pend_n0 = 0, pend_grow = 0, pend_ei = 0;
+        bool pend_row_ok = false;
+        const uint32_t* pend_slots = crt_base;
+        int local_tile = 0;
+        const int runs_per_tile = CRT ? p.crt.nmod * ((p.KB + Runs<CRT>::cap - 1) / Runs<CRT>::cap) : 1;
+        const int per_run = (RECON_GROUPS + runs_per_tile - 1) / runs_per_tile;
+        auto recon_group = [&](int g) {
+            if (!pend_row_ok) return;
+            const CrtConsts& cc = p.crt;
+            const int c = half * (BN / 2) + 4 * g;
+            const uint32_t* gbase = pend_slots + (size_t)(c >> 2) * BM + row;
+            // every residue word of the group is requested before any is used
+            uint32_t cur[MAX_MODULI];
+#pragma unroll
+            for (int l = 0; l < MAX_MODULI; ++l) cur[l] = l < cc.nmod ? gbase[(size_t)l * CRT_SLOT_WORDS] : 0u;
+            int scale[4];
+#pragma unroll
+            for (int e = 0; e < 4; ++e) {
+                const int col = pend_n0 + c + e;
+                scale[e] = pend_ei + (col < p.N ? p.eb[col] : 0) - cc.p - cc.q;
+            }
+            double out[4];
+            crt::reconstruct4(cc, cur, scale, out);
+#pragma unroll
+            for (int e = 0; e < 4; ++e)
+                if (pend_n0 + c + e >= p.N) out[e] = 0.0;
+            write_out4(pend_grow, pend_n0, c, out);
+        };
         uint32_t gcount = 0;
         bool ok = true;
         for (int tile = blockIdx.x; tile < p.num_tiles && ok; tile += gridDim.x) {
@@ -218,10 +388,13 @@ __global__ void __launch_bounds__(THREADS, 1)
             const int grow = m0 + row;
             const bool row_ok = grow < p.M;
             const int ei = row_ok ? p.ea[grow] : 0;
-            for (int d = p.s - 1; d >= 0 && ok; --d) {
-                const int nblk = (d + 1) * p.KB;
-                const int ngroups = (nblk + GROUP_CAP - 1) / GROUP_CAP;
-                const double w = ldexp(1.0, -7 * d);
+            // residue scheme: tiles alternate between two slot banks, so a finished
+            // tile's residues stay intact while the next tile writes its own
+            uint32_t* tile_slots = crt_base + (size_t)(local_tile & 1) * MAX_MODULI * CRT_SLOT_WORDS;
+            for (int di = 0; di < runs.ndiag && ok; ++di) {
+                const int d = runs.diag(di);
+                const int nblk = runs.npairs(d) * p.KB;
+                const int ngroups = (nblk + Runs<CRT>::cap - 1) / Runs<CRT>::cap;
                 for (int gi = 0; gi < ngroups; ++gi) {
                     const uint32_t buf = gcount & 1u, accphase = (gcount >> 1) & 1u;
                     if (!mbar_wait(&acc_full[buf], accphase, p.status)) {
@@ -229,11 +402,7 @@ __global__ void __launch_bounds__(THREADS, 1)
                         break;
                     }
                     tc_fence_after();
-                    // least significant diagonal first: the FP64 sum grows from
-                    // its smallest terms, and the tile's last (C-writing) pass
-                    // overlaps the next tile's longest MMA phase
-                    const bool first = (d == p.s - 1 && gi == 0);
-                    const bool last = (d == 0 && gi == ngroups - 1);
+                    const bool last = (di == runs.ndiag - 1 && gi == ngroups - 1);
                     const uint32_t taddr = tmem_base + ((uint32_t)(quarter * 32) << 16) + buf * BN + half * (BN / 2);
 #pragma unroll 1
                     for (int ch = 0; ch < BN / 64; ++ch) {
@@ -241,23 +410,31 @@ __global__ void __launch_bounds__(THREADS, 1)
                         uint32_t r[32];
                         tmem_ld32(taddr + ch * 32, r);
                         tmem_wait_ld();
-                        double2* sp = scratch + (size_t)(c0 >> 1) * BM + row;
-                        if (!last) {
-#pragma unroll
-                            for (int j = 0; j < 16; ++j) {
-                                double2 v = make_double2((double)(int)r[2 * j] * w, (double)(int)r[2 * j + 1] * w);
-                                if (!first) {
-                                    const double2 o = sp[(size_t)j * BM];
-                                    v.x += o.x;
-                                    v.y += o.y;
-                                }
-                                sp[(size_t)j * BM] = v;
-                            }
-                        } else if (row_ok) {
-                            double* crow = p.C + (long long)grow * p.ldc + n0 + c0;
-                            const double* drow = p.dot_mat ? p.dot_mat + (long long)grow * p.dot_ld + n0 + c0 : nullptr;
-                            const int ncols = min(32, p.N - (n0 + c0));
+                        if constexpr (!CRT) {
                             double out[32];
+                            // FP64 running sums, laid out [col/2][row][2] so a warp's
+                            // 16-byte accesses for one column pair are contiguous
+                            double2* sp = reinterpret_cast<double2*>(p.scratch + (size_t)blockIdx.x * SCRATCH_DOUBLES) +
+                                          (size_t)(c0 >> 1) * BM + row;
+                            const double w = ldexp(1.0, -7 * d);
+                            // least significant diagonal first: the FP64 sum grows from
+                            // its smallest terms, and the tile's last (C-writing) pass
+                            // overlaps the next tile's longest MMA phase
+                            const bool first = (di == 0 && gi == 0);
+                            if (!last) {
+#pragma unroll
+                                for (int j = 0; j < 16; ++j) {
+                                    double2 v = make_double2((double)(int)r[2 * j] * w, (double)(int)r[2 * j + 1] * w);
+                                    if (!first) {
+                                        const double2 o = sp[(size_t)j * BM];
+                                        v.x += o.x;
+                                        v.y += o.y;
+                                    }
+                                    sp[(size_t)j * BM] = v;
+                                }
+                                continue;
+                            }
+                            if (!row_ok) continue;
 #pragma unroll
                             for (int j = 0; j < 16; ++j) {
                                 double2 v = make_double2((double)(int)r[2 * j] * w, (double)(int)r[2 * j + 1] * w);
@@ -267,40 +444,72 @@ __global__ void __launch_bounds__(THREADS, 1)
                                     v.y += o.y;
                                 }
                                 const int col0 = n0 + c0 + 2 * j;
-                                const double g0 = col0 < p.N ? ldexp(v.x, ei + p.eb[col0] - 14) : 0.0;
-                                const double g1 = col0 + 1 < p.N ? ldexp(v.y, ei + p.eb[col0 + 1] - 14) : 0.0;
-                                if (drow) {
-                                    if (col0 < p.N) dot_acc = fma(drow[2 * j], p.alpha * g0, dot_acc);
-                                    if (col0 + 1 < p.N) dot_acc = fma(drow[2 * j + 1], p.alpha * g1, dot_acc);
-                                }
-                                out[2 * j] = out_scale * g0;
-                                out[2 * j + 1] = out_scale * g1;
+                                out[2 * j] = col0 < p.N ? ldexp(v.x, ei + p.eb[col0] - 14) : 0.0;
+                                out[2 * j + 1] = col0 + 1 < p.N ? ldexp(v.y, ei + p.eb[col0 + 1] - 14) : 0.0;
                             }
-                            if (c_vec && ncols == 32) {
-                                double2* c2 = reinterpret_cast<double2*>(crow);
+                            write_out(grow, n0, c0, out);
+                        } else {
+                            // residues: reduce this run mod m_d (adding the earlier
+                            // runs of the same modulus), one byte per element in
+                            // slot d of the scratch, laid out [slot][col/4][row]
+                            const int m = p.crt.m[d];
+                            const uint32_t mu = p.crt.mu[d], off = p.crt.off[d];
+                            uint32_t* my = tile_slots + (size_t)d * CRT_SLOT_WORDS + (size_t)(c0 >> 2) * BM + row;
+                            int res[32];
 #pragma unroll
-                                for (int j = 0; j < 16; ++j) {
-                                    double2 v = make_double2(out[2 * j], out[2 * j + 1]);
-                                    if (p.beta != 0.0) {
-                                        const double2 o = c2[j];
-                                        v.x = fma(p.beta, o.x, v.x);
-                                        v.y = fma(p.beta, o.y, v.y);
+                            for (int j = 0; j < 32; ++j) res[j] = crt::mod_pos((int)r[j], (uint32_t)m, mu, off);
+                            if (gi > 0) {
+#pragma unroll
+                                for (int w4 = 0; w4 < 8; ++w4) {
+                                    const uint32_t old = my[(size_t)w4 * BM];
+#pragma unroll
+                                    for (int e = 0; e < 4; ++e) {
+                                        int v = res[4 * w4 + e] + (int)((old >> (8 * e)) & 0xFFu);
+                                        res[4 * w4 + e] = v >= m ? v - m : v;
                                     }
-                                    c2[j] = v;
                                 }
-                            } else {
-#pragma unroll
-                                for (int j = 0; j < 32; ++j)
-                                    if (j < ncols) crow[j] = (p.beta == 0.0) ? out[j] : fma(p.beta, crow[j], out[j]);
                             }
+#pragma unroll
+                            for (int w4 = 0; w4 < 8; ++w4)
+                                my[(size_t)w4 * BM] = (uint32_t)res[4 * w4] | ((uint32_t)res[4 * w4 + 1] << 8) |
+                                                      ((uint32_t)res[4 * w4 + 2] << 16) |
+                                                      ((uint32_t)res[4 * w4 + 3] << 24);
                         }
                     }
+                    // the accumulator is free once every chunk has been read
                     tc_fence_before();
                     __syncwarp();
                     if (lane == 0) mbar_arrive(&acc_empty[buf]);
                     ++gcount;
+                    if constexpr (CRT) {
+                        // the previous tile's reconstruction advances by a share
+                        // that completes it within this tile's runs
+                        if (ok) {
+                            const int todo = min(pend_left, per_run);
+                            for (int i = 0; i < todo; ++i) recon_group(RECON_GROUPS - pend_left + i);
+                            pend_left -= todo;
+                        }
+                        if (last) {
+                            pend_left = RECON_GROUPS;
+                            pend_n0 = n0;
+                            pend_grow = grow;
+                            pend_ei = ei;
+                            pend_row_ok = row_ok;
+                            pend_slots = tile_slots;
+                            // slots written many runs ago have usually left L2 under the
+                            // operand stream: pull them back before the first group is due
+                            if (warp == 2 && lane == 0)
+                                for (int l = 0; l < p.crt.nmod; ++l)
+                                    l2_prefetch_bulk(tile_slots + (size_t)l * CRT_SLOT_WORDS, CRT_SLOT_WORDS * 4);
+                        }
+                    }
                 }
             }
+            ++local_tile;
+        }
+        if constexpr (CRT) {
+            if (ok)
+                for (; pend_left > 0; --pend_left) recon_group(RECON_GROUPS - pend_left);
         }
         if (p.dot_partials) {
             // deterministic CTA reduction over the epilogue warps (named barrier 1)
@@ -335,29 +544,70 @@ __device__ __forceinline__ int frexp_exp(double mx) {
     return e;
 }
 
-// Slices four consecutive values (already scaled into (-1, 1)) into s packed
-// INT8 words: byte u of word t is q_t of value u.
-__device__ __forceinline__ void slice4(double (&v)[4], int s, uint32_t (&word)[8]) {
+constexpr double kMagic = 0x1.8p52;  // adding it rounds |x| < 2^51 to an integer held in the low bits
+
+// Encodes four consecutive values of one row (already multiplied by 2^-E, or
+// by 2^(shift-E) in the residue scheme) into `count` packed INT8 words, word t
+// stored at dst + t * stride bytes: byte u of word t is digit t of value u.
+//   slice scheme:   v <- 128 v, q <- trunc(v), v <- v - q   (exact steps)
+//   residue scheme: x = rint(v) (|x| <= 2^51), digit t = x - m_t * rint(x / m_t),
+//                   which lies in [-m_t/2, m_t/2] and is congruent to x mod m_t.
+//                   rint(x / m_t) is taken as rint(x * inv_t): inv_t's relative
+//                   error 2^-53 moves x * inv_t by at most 2^51/m_t * 2^-53 =
+//                   1/(4 m_t), less than the 1/(2 m_t) gap between x/m_t and a
+//                   rounding tie for odd m_t (m_t = 256 has an exact inverse),
+//                   so the digit never leaves [-128, 128]; +128 only arises for
+//                   m_t = 256, where the byte 0x80 is still congruent.
+//                   All steps are exact: x + kMagic, m_t * q and their
+//                   difference are integers below 2^53, and the low byte of
+//                   kMagic + digit is the digit's two's-complement byte.
+template <bool CRT>
+__device__ __forceinline__ void encode4(double (&v)[4], int count, uint8_t* dst, size_t stride) {
+    if constexpr (!CRT) {
 #pragma unroll
-    for (int t = 0; t < 8; ++t) word[t] = 0u;
+        for (int t = 0; t < 8; ++t) {
+            if (t < count) {
+                uint32_t word = 0u;
 #pragma unroll
-    for (int t = 0; t < 8; ++t) {
-        if (t < s) {
+                for (int u = 0; u < 4; ++u) {
+                    v[u] *= 128.0;
+                    const int q = __double2int_rz(v[u]);
+                    v[u] -= (double)q;
+                    word |= ((uint32_t)q & 0xFFu) << (8 * u);
+                }
+                *reinterpret_cast<uint32_t*>(dst + (size_t)t * stride) = word;
+            }
+        }
+    } else {
+        double xm[4], x[4];
 #pragma unroll
-            for (int u = 0; u < 4; ++u) {
-                v[u] *= 128.0;
-                const int q = __double2int_rz(v[u]);
-                v[u] -= (double)q;
-                word[t] |= ((uint32_t)q & 0xFFu) << (8 * u);
+        for (int u = 0; u < 4; ++u) {
+            xm[u] = v[u] + kMagic;  // kMagic + rint(v)
+            x[u] = xm[u] - kMagic;  // rint(v)
+        }
+#pragma unroll
+        for (int t = 0; t < MAX_MODULI; ++t) {
+            if (t < count) {
+                const double m = (double)kModuli[t];
+                const double inv = kInvModuli[t];
+                uint32_t b[4];
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    const double qd = fma(x[u], inv, kMagic) - kMagic;  // rint(x / m)
+                    b[u] = (uint32_t)__double2loint(fma(-m, qd, xm[u]));
+                }
+                *reinterpret_cast<uint32_t*>(dst + (size_t)t * stride) =
+                    __byte_perm(__byte_perm(b[0], b[1], 0x0040), __byte_perm(b[2], b[3], 0x0040), 0x5410);
             }
         }
     }
 }
 
 // K-major source: row r is src[r*ld + p], p < K.  One block per row.
+template <bool CRT>
 __global__ void __launch_bounds__(SPLIT_THREADS) split_rows_kernel(const double* src, long long ld, int rows, int K,
-                                                                    int Kp, int s, uint8_t* out, int* exps,
-                                                                    int* nonfinite) {
+                                                                    int Kp, int count, int shift, uint8_t* out,
+                                                                    int* exps, int* nonfinite) {
     __shared__ double red[SPLIT_THREADS / 32];
     __shared__ int bad_sh;
     const int r = blockIdx.x;
@@ -393,15 +643,12 @@ __global__ void __launch_bounds__(SPLIT_THREADS) split_rows_kernel(const double*
     }
     const int e = frexp_exp(red[0]);
     if (threadIdx.x == 0) exps[r] = e;
+    const Pow2 sc = pow2_split(shift - e);
     for (int p4 = threadIdx.x * 4; p4 < K; p4 += SPLIT_THREADS * 4) {
         double v[4];
 #pragma unroll
-        for (int u = 0; u < 4; ++u) v[u] = (p4 + u < K) ? ldexp(row[p4 + u], -e) : 0.0;
-        uint32_t word[8];
-        slice4(v, s, word);
-#pragma unroll
-        for (int t = 0; t < 8; ++t)
-            if (t < s) *reinterpret_cast<uint32_t*>(out + ((size_t)t * rows + r) * Kp + p4) = word[t];
+        for (int u = 0; u < 4; ++u) v[u] = (p4 + u < K) ? row[p4 + u] * sc.lo * sc.hi : 0.0;
+        encode4<CRT>(v, count, out + (size_t)r * Kp + p4, (size_t)rows * Kp);
     }
 }
 
@@ -425,15 +672,30 @@ __global__ void __launch_bounds__(SPLIT_THREADS) colmax_kernel(const double* src
 
 // Pass 2: 32 (i) x 128 (p) tiles through shared memory, written K-major.
 constexpr int TR_I = 32, TR_P = 128;
-__global__ void __launch_bounds__(SPLIT_THREADS) split_cols_kernel(const double* src, long long ld, int cols, int K,
-                                                                    int Kp, int s, const unsigned long long* maxbits,
-                                                                    uint8_t* out, int* exps) {
-    __shared__ double tile[TR_P][TR_I + 1];
+static_assert(TR_P / 4 <= TR_I && (TR_I & (TR_I - 1)) == 0, "swizzle needs p/4 < TR_I");
+template <bool CRT>
+__global__ void __launch_bounds__(SPLIT_THREADS, 4) split_cols_kernel(const double* src, long long ld, int cols, int K,
+                                                                    int Kp, int count, int shift,
+                                                                    const unsigned long long* maxbits, uint8_t* out,
+                                                                    int* exps) {
+    // element (p, i) sits at column i ^ (p/4): the loads (lanes along i) and
+    // the encoder's reads (lanes along p/4) both hit 32 distinct banks pairs
+    __shared__ double tile[TR_P][TR_I];
     const int i0 = blockIdx.x * TR_I, p0 = blockIdx.y * TR_P;
-    for (int e = threadIdx.x; e < TR_I * TR_P; e += SPLIT_THREADS) {
+    constexpr int LOADS = TR_I * TR_P / SPLIT_THREADS;
+    double ld_v[LOADS];  // every load of the tile is in flight before the first store
+#pragma unroll
+    for (int it = 0; it < LOADS; ++it) {
+        const int e = threadIdx.x + it * SPLIT_THREADS;
         const int pi = e / TR_I, ii = e % TR_I;
         const int gi = i0 + ii, gp = p0 + pi;
-        tile[pi][ii] = (gi < cols && gp < K) ? src[(long long)gp * ld + gi] : 0.0;
+        ld_v[it] = (gi < cols && gp < K) ? src[(long long)gp * ld + gi] : 0.0;
+    }
+#pragma unroll
+    for (int it = 0; it < LOADS; ++it) {
+        const int e = threadIdx.x + it * SPLIT_THREADS;
+        const int pi = e / TR_I, ii = e % TR_I;
+        tile[pi][ii ^ ((pi >> 2) & (TR_I - 1))] = ld_v[it];
     }
     __syncthreads();
     for (int e = threadIdx.x; e < TR_I * (TR_P / 4); e += SPLIT_THREADS) {
@@ -442,14 +704,11 @@ __global__ void __launch_bounds__(SPLIT_THREADS) split_cols_kernel(const double*
         if (gi >= cols || gp >= K) continue;
         const int ex = frexp_exp(__longlong_as_double((long long)maxbits[gi]));
         if (blockIdx.y == 0 && q == 0) exps[gi] = ex;
+        const Pow2 sc = pow2_split(shift - ex);
         double v[4];
 #pragma unroll
-        for (int u = 0; u < 4; ++u) v[u] = ldexp(tile[4 * q + u][ii], -ex);
-        uint32_t word[8];
-        slice4(v, s, word);
-#pragma unroll
-        for (int t = 0; t < 8; ++t)
-            if (t < s) *reinterpret_cast<uint32_t*>(out + ((size_t)t * cols + gi) * Kp + gp) = word[t];
+        for (int u = 0; u < 4; ++u) v[u] = tile[4 * q + u][ii ^ (q & (TR_I - 1))] * sc.lo * sc.hi;
+        encode4<CRT>(v, count, out + (size_t)gi * Kp + gp, (size_t)cols * Kp);
     }
 }
 
@@ -459,14 +718,15 @@ struct Layout {
 
 inline size_t up(size_t v, size_t a) { return (v + a - 1) / a * a; }
 
-Layout plan_layout(long long m, long long n, long long k, int s, int grid) {
+// count: slices (slice scheme) or moduli (residue scheme)
+Layout plan_layout(long long m, long long n, long long k, int count, int grid, bool crt) {
     const size_t kp = up((size_t)k, 16);
     Layout L;
     size_t off = 0;
     L.sa = off;
-    off = up(off + (size_t)s * m * kp, 1024);
+    off = up(off + (size_t)count * m * kp, 1024);
     L.sb = off;
-    off = up(off + (size_t)s * n * kp, 1024);
+    off = up(off + (size_t)count * n * kp, 1024);
     L.ea = off;
     off = up(off + (size_t)m * 4, 256);
     L.eb = off;
@@ -474,16 +734,25 @@ Layout plan_layout(long long m, long long n, long long k, int s, int grid) {
     L.maxb = off;
     off = up(off + (size_t)(m > n ? m : n) * 8, 256);
     L.scratch = off;
-    off = up(off + (size_t)grid * SCRATCH_DOUBLES * 8, 1024);
+    // residue scheme: two banks of slots per CTA (the tile being accumulated and
+    // the one being reconstructed)
+    const size_t per_cta = crt ? (size_t)2 * MAX_MODULI * CRT_SLOT_WORDS * 4 : (size_t)SCRATCH_DOUBLES * 8;
+    off = up(off + (size_t)grid * per_cta, 1024);
     L.total = off;
     return L;
 }
 
 // Split one operand given as K-major (rows contiguous along k) or MN-major.
-int split_operand(const double* src, long long ld, bool kmajor, int rows, int K, int Kp, int s, uint8_t* out,
-                  int* exps, unsigned long long* maxbits, int* nonfinite, cudaStream_t st, int sm_count) {
+int split_operand(const double* src, long long ld, bool kmajor, int rows, int K, int Kp, int count, int shift,
+                  bool crt, uint8_t* out, int* exps, unsigned long long* maxbits, int* nonfinite, cudaStream_t st,
+                  int sm_count) {
     if (kmajor) {
-        split_rows_kernel<<<rows, SPLIT_THREADS, 0, st>>>(src, ld, rows, K, Kp, s, out, exps, nonfinite);
+        if (crt)
+            split_rows_kernel<true><<<rows, SPLIT_THREADS, 0, st>>>(src, ld, rows, K, Kp, count, shift, out, exps,
+                                                                   nonfinite);
+        else
+            split_rows_kernel<false><<<rows, SPLIT_THREADS, 0, st>>>(src, ld, rows, K, Kp, count, 0, out, exps,
+                                                                    nonfinite);
     } else {
         cudaMemsetAsync(maxbits, 0, (size_t)rows * 8, st);
         const int cblocks = (rows + SPLIT_THREADS - 1) / SPLIT_THREADS;
@@ -493,10 +762,44 @@ int split_operand(const double* src, long long ld, bool kmajor, int rows, int K,
         if (kchunk < 16) kchunk = 16;
         ksplit = (K + kchunk - 1) / kchunk;
         colmax_kernel<<<dim3(cblocks, ksplit), SPLIT_THREADS, 0, st>>>(src, ld, rows, K, kchunk, maxbits, nonfinite);
-        split_cols_kernel<<<dim3((rows + TR_I - 1) / TR_I, (K + TR_P - 1) / TR_P), SPLIT_THREADS, 0, st>>>(
-            src, ld, rows, K, Kp, s, maxbits, out, exps);
+        const dim3 grid((rows + TR_I - 1) / TR_I, (K + TR_P - 1) / TR_P);
+        if (crt)
+            split_cols_kernel<true><<<grid, SPLIT_THREADS, 0, st>>>(src, ld, rows, K, Kp, count, shift, maxbits, out,
+                                                                   exps);
+        else
+            split_cols_kernel<false><<<grid, SPLIT_THREADS, 0, st>>>(src, ld, rows, K, Kp, count, 0, maxbits, out,
+                                                                    exps);
     }
     return cudaGetLastError() == cudaSuccess ? JLC_OK : JLC_E_LAUNCH;
+}
+
+// ---------------------------------------------------------------- CRT constants
+typedef unsigned __int128 u128;
+
+u128 modulus_product(int nmod) {
+    u128 M = 1;
+    for (int i = 0; i < nmod; ++i) M *= (u128)kModuliHost[i];
+    return M;
+}
+
+double u128_to_double(u128 x) { return (double)(uint64_t)(x >> 64) * 0x1p64 + (double)(uint64_t)x; }
+
+double log2_u128(u128 x) { return std::log2(u128_to_double(x)); }
+
+// p + q budget: M > 2 k 2^(p+q)
+void crt_pq(int nmod, long long k, int& p, int& q) {
+    const double budget = log2_u128(modulus_product(nmod)) - std::log2(2.0 * (double)(k > 0 ? k : 1));
+    int b = (int)std::floor(budget - 1e-9);
+    if (b > 102) b = 102;  // |A'|, |B'| <= 2^51: the split's exact integer tricks hold
+    p = b / 2;
+    q = b - p;
+}
+
+
+void crt_constants(int nmod, long long k, CrtConsts& c) {
+    int p = 0, q = 0;
+    crt_pq(nmod, k, p, q);
+    crt::build_consts(nmod, p, q, kModuliHost, c);
 }
 
 }  // namespace oz
@@ -506,10 +809,26 @@ int ozaki_grid(long long m, long long n, int sm_count) {
     return (int)(tiles < sm_count ? tiles : sm_count);
 }
 
-size_t ozaki_workspace_bytes(long long m, long long n, long long k, int slices, int sm_count) {
-    const long long tiles = ((m + oz::BM - 1) / oz::BM) * ((n + oz::BN - 1) / oz::BN);
-    const int grid = (int)(tiles < sm_count ? tiles : sm_count);
-    return oz::plan_layout(m, n, k, slices, grid).total;
+size_t ozaki_workspace_bytes(long long m, long long n, long long k, int count, int sm_count, bool crt) {
+    return oz::plan_layout(m, n, k, count, ozaki_grid(m, n, sm_count), crt).total;
+}
+
+int ozaki_crt_auto_moduli(long long k) {
+    // smallest N whose worst-case rounding error 2^-min(p,q) stays inside
+    // 2 k u / 16 (rows/columns whose mean |a| is at least 1/4 of their max)
+    const double rhs = 2.0 * std::ldexp(1.0, -53) * (double)k / 16.0;
+    for (int n = 2; n <= oz::MAX_MODULI; ++n) {
+        int p, q;
+        oz::crt_pq(n, k, p, q);
+        if (std::ldexp(1.0, -(p < q ? p : q)) <= rhs) return n;
+    }
+    return oz::MAX_MODULI;
+}
+
+double ozaki_crt_est_ratio(int nmod, long long k) {
+    int p, q;
+    oz::crt_pq(nmod, k, p, q);
+    return std::ldexp(1.0, -(p < q ? p : q)) / (2.0 * std::ldexp(1.0, -53) * (double)k / 16.0);
 }
 
 struct OzakiBufs {
@@ -518,18 +837,17 @@ struct OzakiBufs {
     long long tiles_m, tiles_n;
 };
 
-static int ozaki_bufs(const GemmDesc& g, int s, size_t ws_bytes, int sm_count, OzakiBufs& b, char* err,
-                      size_t errlen) {
+static int ozaki_bufs(const GemmDesc& g, int count, size_t ws_bytes, int sm_count, bool crt, OzakiBufs& b,
+                      char* err, size_t errlen) {
     using namespace oz;
-    if (s < 1 || s > 8) {
-        snprintf(err, errlen, "slice count %d outside [1,8]", s);
+    if (count < 1 || count > (crt ? MAX_MODULI : 8)) {
+        snprintf(err, errlen, "%s count %d out of range", crt ? "modulus" : "slice", count);
         return JLC_E_ARG;
     }
     b.tiles_m = (g.m + BM - 1) / BM;
     b.tiles_n = (g.n + BN - 1) / BN;
-    const long long num_tiles = b.tiles_m * b.tiles_n;
-    b.grid = (int)(num_tiles < sm_count ? num_tiles : sm_count);
-    b.L = plan_layout(g.m, g.n, g.k, s, b.grid);
+    b.grid = ozaki_grid(g.m, g.n, sm_count);
+    b.L = plan_layout(g.m, g.n, g.k, count, b.grid, crt);
     b.Kp = (int)up((size_t)g.k, 16);
     if (b.L.total > ws_bytes) {
         snprintf(err, errlen, "Ozaki workspace too small (%zu < %zu)", ws_bytes, b.L.total);
@@ -538,45 +856,49 @@ static int ozaki_bufs(const GemmDesc& g, int s, size_t ws_bytes, int sm_count, O
     return JLC_OK;
 }
 
-int launch_ozaki_split(const GemmDesc& g, int s, void* workspace, size_t ws_bytes, cudaStream_t st, int sm_count,
-                       int* flags, char* err, size_t errlen) {
+int launch_ozaki_split(const GemmDesc& g, int count, void* workspace, size_t ws_bytes, cudaStream_t st,
+                       int sm_count, int* flags, char* err, size_t errlen, bool crt) {
     using namespace oz;
     OzakiBufs b;
-    int rc = ozaki_bufs(g, s, ws_bytes, sm_count, b, err, errlen);
+    int rc = ozaki_bufs(g, count, ws_bytes, sm_count, crt, b, err, errlen);
     if (rc) return rc;
     char* ws = static_cast<char*>(workspace);
     auto* maxb = reinterpret_cast<unsigned long long*>(ws + b.L.maxb);
     int* nonfinite = flags;
+    int p = 0, q = 0;
+    if (crt) crt_pq(count, g.k, p, q);
     if (cudaMemsetAsync(nonfinite, 0, sizeof(int), st) != cudaSuccess) {
         snprintf(err, errlen, "flag reset failed");
         return JLC_E_CUDA;
     }
     // op(A) rows are contiguous along k when A is row-major; op(B) "rows"
     // (columns j of B) are contiguous along k when B is column-major.
-    rc = split_operand(g.a, g.lda, g.layout_a == JLC_ROW_MAJOR, (int)g.m, (int)g.k, b.Kp, s,
+    rc = split_operand(g.a, g.lda, g.layout_a == JLC_ROW_MAJOR, (int)g.m, (int)g.k, b.Kp, count, p, crt,
                        reinterpret_cast<uint8_t*>(ws + b.L.sa), reinterpret_cast<int*>(ws + b.L.ea), maxb,
                        nonfinite, st, sm_count);
     if (!rc)
-        rc = split_operand(g.b, g.ldb, g.layout_b == JLC_COL_MAJOR, (int)g.n, (int)g.k, b.Kp, s,
+        rc = split_operand(g.b, g.ldb, g.layout_b == JLC_COL_MAJOR, (int)g.n, (int)g.k, b.Kp, count, q, crt,
                            reinterpret_cast<uint8_t*>(ws + b.L.sb), reinterpret_cast<int*>(ws + b.L.eb), maxb,
                            nonfinite, st, sm_count);
     if (rc) snprintf(err, errlen, "Ozaki split launch failed: %s", cudaGetErrorString(cudaGetLastError()));
     return rc;
 }
 
-int launch_ozaki_gemm(const GemmDesc& g, int s, void* workspace, size_t ws_bytes, cudaStream_t st, int sm_count,
-                      int* status, int* flags, char* err, size_t errlen) {
+int launch_ozaki_gemm(const GemmDesc& g, int count, void* workspace, size_t ws_bytes, cudaStream_t st,
+                      int sm_count, int* status, int* flags, char* err, size_t errlen, bool crt) {
     using namespace oz;
     OzakiBufs b;
-    int rc = ozaki_bufs(g, s, ws_bytes, sm_count, b, err, errlen);
+    int rc = ozaki_bufs(g, count, ws_bytes, sm_count, crt, b, err, errlen);
     if (rc) return rc;
     char* ws = static_cast<char*>(workspace);
     CUtensorMap ma, mb;
-    rc = make_tmap_3d(&ma, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, ws + b.L.sa, (uint64_t)g.k, (uint64_t)g.m, (uint64_t)s,
-                      (uint64_t)b.Kp, (uint64_t)g.m * b.Kp, BKB, BM, 1, CU_TENSOR_MAP_SWIZZLE_128B, err, errlen);
+    rc = make_tmap_3d(&ma, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, ws + b.L.sa, (uint64_t)g.k, (uint64_t)g.m,
+                      (uint64_t)count, (uint64_t)b.Kp, (uint64_t)g.m * b.Kp, BKB, BM, 1, CU_TENSOR_MAP_SWIZZLE_128B,
+                      err, errlen);
     if (rc) return rc;
-    rc = make_tmap_3d(&mb, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, ws + b.L.sb, (uint64_t)g.k, (uint64_t)g.n, (uint64_t)s,
-                      (uint64_t)b.Kp, (uint64_t)g.n * b.Kp, BKB, BN, 1, CU_TENSOR_MAP_SWIZZLE_128B, err, errlen);
+    rc = make_tmap_3d(&mb, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, ws + b.L.sb, (uint64_t)g.k, (uint64_t)g.n,
+                      (uint64_t)count, (uint64_t)b.Kp, (uint64_t)g.n * b.Kp, BKB, BN, 1, CU_TENSOR_MAP_SWIZZLE_128B,
+                      err, errlen);
     if (rc) return rc;
 
     Params p;
@@ -584,7 +906,7 @@ int launch_ozaki_gemm(const GemmDesc& g, int s, void* workspace, size_t ws_bytes
     p.N = (int)g.n;
     p.K = (int)g.k;
     p.KB = (int)((g.k + BKB - 1) / BKB);
-    p.s = s;
+    p.s = count;
     p.tiles_m = (int)b.tiles_m;
     p.tiles_n = (int)b.tiles_n;
     p.num_tiles = (int)(b.tiles_m * b.tiles_n);
@@ -601,12 +923,15 @@ int launch_ozaki_gemm(const GemmDesc& g, int s, void* workspace, size_t ws_bytes
     p.dot_mat = g.dot_mat;
     p.dot_ld = g.dot_ld;
     p.dot_partials = g.dot_partials;
-    cudaError_t e = cudaFuncSetAttribute(ozaki_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES);
+    p.crt = CrtConsts{};
+    if (crt) crt_constants(count, g.k, p.crt);
+    auto kern = crt ? ozaki_gemm_kernel<true> : ozaki_gemm_kernel<false>;
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES);
     if (e != cudaSuccess) {
         snprintf(err, errlen, "Ozaki smem attribute: %s", cudaGetErrorString(e));
         return JLC_E_LAUNCH;
     }
-    ozaki_gemm_kernel<<<b.grid, THREADS, SMEM_BYTES, st>>>(ma, mb, p);
+    kern<<<b.grid, THREADS, SMEM_BYTES, st>>>(ma, mb, p);
     e = cudaGetLastError();
     if (e != cudaSuccess) {
         snprintf(err, errlen, "Ozaki GEMM launch failed: %s", cudaGetErrorString(e));
