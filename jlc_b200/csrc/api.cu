@@ -62,17 +62,18 @@ inline long long round_up(long long v, long long m) { return (v + m - 1) / m * m
 // record buffer is full.
 struct Phase {
     jlc_ctx* ctx;
+    cudaStream_t st;
     int idx = -1;
-    Phase(jlc_ctx* c, int phase) : ctx(c) {
+    Phase(jlc_ctx* c, int phase, cudaStream_t s = nullptr) : ctx(c), st(s ? s : c->stream) {
         if (!ctx->profiling || ctx->nrec >= jlc_ctx::kMaxRec) return;
         idx = ctx->nrec++;
         for (int e = 0; e < 2; ++e)
             if (!ctx->rec_ev[2 * idx + e]) cudaEventCreate(&ctx->rec_ev[2 * idx + e]);
         ctx->rec_phase[idx] = phase;
-        cudaEventRecord(ctx->rec_ev[2 * idx], ctx->stream);
+        cudaEventRecord(ctx->rec_ev[2 * idx], st);
     }
     ~Phase() {
-        if (idx >= 0) cudaEventRecord(ctx->rec_ev[2 * idx + 1], ctx->stream);
+        if (idx >= 0) cudaEventRecord(ctx->rec_ev[2 * idx + 1], st);
     }
 };
 
@@ -182,13 +183,14 @@ int run_device(jlc_ctx* ctx, const GemmDesc& g0, int precision, int slices, jlc_
         ctx->launches += v.cs == 1 ? 1 : 2;
         return launch_gemv(v, ctx->ws.ptr, ctx->stream, ctx->sm_count, ctx->err, sizeof(ctx->err));
     }
-    const bool ozaki = use_ozaki(precision, g.m, g.n, g.k);
+    // a row block of a pipelined product follows the whole product's choice
+    const bool ozaki = use_ozaki(precision, g.ws_m > g.m ? g.ws_m : g.m, g.n, g.k);
     // AUTO takes the residue scheme: fewer INT8 products for the same bound
     const bool crt = ozaki && precision != JLC_PREC_OZAKI;
     int rc = JLC_OK;
     if (ozaki) {
         const int s = slices > 0 ? slices : (crt ? ozaki_crt_auto_moduli(g.k) : auto_slices(g.k));
-        size_t need = ozaki_workspace_bytes(g.m, g.n, g.k, s, ctx->sm_count, crt);
+        size_t need = ozaki_workspace_bytes(g.ws_m > g.m ? g.ws_m : g.m, g.n, g.k, s, ctx->sm_count, crt);
         rc = workspace_reserve(ctx->ws, need, ctx->err, sizeof(ctx->err));
         if (rc) return rc;
         {
@@ -264,6 +266,117 @@ int finish_sync(jlc_ctx* ctx) {
 // Host entry: stage op(A), op(B) (and C when beta != 0) into context buffers
 // with 16-byte-aligned, padded leading dimensions, run, copy C back into the
 // caller's m x n window only.
+// Smallest row block of the host-entry pipeline: below two of these (or for a
+// matrix-vector shape) the copies and the GEMM run back to back.
+constexpr long long kPipeBlockRows = 512;
+
+int pipe_ready(jlc_ctx* ctx) {
+    if (!ctx->cin && cudaStreamCreateWithFlags(&ctx->cin, cudaStreamNonBlocking) != cudaSuccess)
+        return cuda_err(ctx, cudaGetLastError(), "copy stream");
+    if (!ctx->cout && cudaStreamCreateWithFlags(&ctx->cout, cudaStreamNonBlocking) != cudaSuccess)
+        return cuda_err(ctx, cudaGetLastError(), "copy stream");
+    for (cudaEvent_t& ev : ctx->pev)
+        if (!ev && cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) != cudaSuccess)
+            return cuda_err(ctx, cudaGetLastError(), "pipeline event");
+    return JLC_OK;
+}
+
+// Host entry in row blocks of C: B (whole) and then the rows of op(A) (and of
+// C when beta != 0) of each block go to the device on a copy-in stream, each
+// block's GEMM runs on the context stream as soon as its rows have arrived,
+// and its rows of C return on a copy-out stream while later blocks compute.
+// PCIe is full duplex, so the time approaches the larger of the two copy
+// directions plus one block.  Every block computes exactly what the
+// single-shot path computes for its rows (same kernels, per-row and
+// per-column Ozaki scaling, same k order), so results are bitwise identical.
+// The Ozaki split of B is made once, by the first block, and reused.
+int run_host_pipelined(jlc_ctx* ctx, int la, int lb, long long m, long long n, long long k, double alpha,
+                       const double* a, long long lda, const double* b, long long ldb, double beta, double* c,
+                       long long ldc, int precision, jlc_report* rep, long long dlda, long long dldb, long long dldc,
+                       int64_t& h2d, int64_t& d2h) {
+    int rc = pipe_ready(ctx);
+    if (rc) return rc;
+    const int maxb = jlc_ctx::kPipeMaxBlocks;
+    long long rb = round_up((m + maxb - 1) / maxb, 128);
+    if (rb < kPipeBlockRows) rb = kPipeBlockRows;
+    const int nb = (int)((m + rb - 1) / rb);
+    const long long b_rows = lb == JLC_ROW_MAJOR ? k : n, b_cols = lb == JLC_ROW_MAJOR ? n : k;
+    cudaStream_t cs = ctx->stream, ci = ctx->cin, co = ctx->cout;
+    auto drain = [&] {
+        cudaStreamSynchronize(ci);
+        cudaStreamSynchronize(cs);
+        cudaStreamSynchronize(co);
+    };
+    cudaError_t e = cudaEventRecord(ctx->ev0, cs);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(ci, ctx->ev0, 0);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(co, ctx->ev0, 0);
+    if (e != cudaSuccess) return cuda_err(ctx, e, "pipeline start");
+    {
+        Phase ph(ctx, JLC_PHASE_H2D, ci);
+        e = cudaMemcpy2DAsync(ctx->bufB.ptr, dldb * 8, b, ldb * 8, b_cols * 8, b_rows, cudaMemcpyHostToDevice, ci);
+    }
+    if (e != cudaSuccess) {
+        drain();
+        return cuda_err(ctx, e, "copy B to device");
+    }
+    h2d += b_rows * b_cols * 8;
+    double* dA = static_cast<double*>(ctx->bufA.ptr);
+    double* dC = static_cast<double*>(ctx->bufC.ptr);
+    for (int i = 0; i < nb; ++i) {
+        const long long r0 = (long long)i * rb, mr = (m - r0 < rb) ? m - r0 : rb;
+        const double* blk_a;
+        {
+            Phase ph(ctx, JLC_PHASE_H2D, ci);
+            if (la == JLC_ROW_MAJOR) {
+                e = cudaMemcpy2DAsync(dA + r0 * dlda, dlda * 8, a + r0 * lda, lda * 8, k * 8, mr,
+                                      cudaMemcpyHostToDevice, ci);
+                blk_a = dA + r0 * dlda;
+            } else {
+                e = cudaMemcpy2DAsync(dA + r0, dlda * 8, a + r0, lda * 8, mr * 8, k, cudaMemcpyHostToDevice, ci);
+                blk_a = dA + r0;
+            }
+            if (e == cudaSuccess && beta != 0.0)
+                e = cudaMemcpy2DAsync(dC + r0 * dldc, dldc * 8, c + r0 * ldc, ldc * 8, n * 8, mr,
+                                      cudaMemcpyHostToDevice, ci);
+        }
+        if (e == cudaSuccess) e = cudaEventRecord(ctx->pev[i], ci);
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(cs, ctx->pev[i], 0);
+        if (e != cudaSuccess) {
+            drain();
+            return cuda_err(ctx, e, "copy A block to device");
+        }
+        h2d += mr * k * 8 + (beta != 0.0 ? mr * n * 8 : 0);
+        GemmDesc g{la, lb, mr, n, k, alpha, beta, blk_a, dlda, (const double*)ctx->bufB.ptr, dldb, dC + r0 * dldc,
+                   dldc};
+        g.ws_m = m;
+        g.b_split_ready = i > 0;
+        rc = run_device(ctx, g, precision, 0, rep);
+        if (rc) {
+            drain();
+            return rc;
+        }
+        e = cudaEventRecord(ctx->pev[maxb + i], cs);
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(co, ctx->pev[maxb + i], 0);
+        if (e == cudaSuccess) {
+            Phase ph(ctx, JLC_PHASE_D2H, co);
+            e = cudaMemcpy2DAsync(c + r0 * ldc, ldc * 8, dC + r0 * dldc, dldc * 8, n * 8, mr,
+                                  cudaMemcpyDeviceToHost, co);
+        }
+        if (e != cudaSuccess) {
+            drain();
+            return cuda_err(ctx, e, "copy C block to host");
+        }
+        d2h += mr * n * 8;
+    }
+    e = cudaEventRecord(ctx->pev[2 * maxb], co);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(cs, ctx->pev[2 * maxb], 0);
+    if (e != cudaSuccess) {
+        drain();
+        return cuda_err(ctx, e, "pipeline end");
+    }
+    return JLC_OK;
+}
+
 int run_host(jlc_ctx* ctx, int la, int lb, long long m, long long n, long long k, double alpha, const double* a,
              long long lda, const double* b, long long ldb, double beta, double* c, long long ldc, int precision,
              jlc_report* rep) {
@@ -283,6 +396,22 @@ int run_host(jlc_ctx* ctx, int la, int lb, long long m, long long n, long long k
         if ((rc = reserve(ctx, ctx->bufB, (size_t)(b_rows * dldb) * 8, "device B"))) return rc;
     }
     if ((rc = reserve(ctx, ctx->bufC, (size_t)(m * dldc) * 8, "device C"))) return rc;
+    if (need_ab && n > 1 && m >= 2 * kPipeBlockRows) {
+        rc = run_host_pipelined(ctx, la, lb, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc, precision, rep, dlda,
+                                dldb, dldc, h2d, d2h);
+        if (rc) return rc;
+        cudaEventRecord(ctx->ev1, ctx->stream);
+        rc = finish_sync(ctx);
+        if (rc) return rc;
+        if (rep) {
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
+            rep->device_ms = ms;
+            rep->h2d_bytes = h2d;
+            rep->d2h_bytes = d2h;
+        }
+        return JLC_OK;
+    }
     cudaEventRecord(ctx->ev0, ctx->stream);
     {
     Phase ph(ctx, JLC_PHASE_H2D);
@@ -481,6 +610,10 @@ void jlc_destroy(jlc_ctx* ctx) {
         if (ctx->rec_ev[i]) cudaEventDestroy(ctx->rec_ev[i]);
     if (ctx->ev0) cudaEventDestroy(ctx->ev0);
     if (ctx->ev1) cudaEventDestroy(ctx->ev1);
+    for (cudaEvent_t ev : ctx->pev)
+        if (ev) cudaEventDestroy(ev);
+    if (ctx->cin) cudaStreamDestroy(ctx->cin);
+    if (ctx->cout) cudaStreamDestroy(ctx->cout);
     if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
     delete ctx;
 }

@@ -63,7 +63,7 @@ struct Params {
     long long ldc;
     int tiles_m, tiles_n, num_tiles, k_blocks;
     int* status;
-    const int* gate;  // when non-null the kernel runs only if *gate != 0
+    const int* gate;  // when non-null the kernel runs only if gate[0] or gate[1] is set
 };
 
 // Bounded wait used only while draining: ignores errors recorded by others
@@ -83,7 +83,7 @@ template <bool A_KMAJOR, bool B_KMAJOR, int MMA_K>
 __global__ void __launch_bounds__(THREADS, 1)
     dgemm_dmma_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB,
                       const Params p) {
-    if (p.gate != nullptr && *p.gate == 0) return;
+    if (p.gate != nullptr && (p.gate[0] | p.gate[1]) == 0) return;
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     char* smem = reinterpret_cast<char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
     uint64_t* full = reinterpret_cast<uint64_t*>(smem + STAGES * STAGE_BYTES);

@@ -32,6 +32,12 @@ struct GemmDesc {
     //  sum_ij dot_mat(i,j) * (alpha*op(A)op(B))_ij over the tiles it wrote into
     //  dot_partials[blockIdx.x] (deterministic order; the caller reduces).
     double epi_scale = 1.0;
+    // Row-block pipelines (the host entry's copy/compute overlap): ws_m sizes
+    // the Ozaki workspace for the whole product so that every block finds the
+    // split of B at the same place, and b_split_ready says a previous block of
+    // the same product has left that split there.
+    long long ws_m = 0;
+    bool b_split_ready = false;
     const double* dot_mat = nullptr;
     long long dot_ld = 0;
     double* dot_partials = nullptr;
@@ -60,7 +66,8 @@ int make_tmap_3d(CUtensorMap* map, CUtensorMapDataType dt, int elem_bytes, void*
 bool dmma_operand_ok(const void* ptr, long long ld);
 
 // FP64 DMMA tiled GEMM.  A/B must be 16-byte aligned with even leading
-// dimensions.  gate != nullptr: the kernel only runs if *gate != 0.
+// dimensions.  gate != nullptr: the kernel only runs if gate[0] or gate[1] is
+// nonzero (the Ozaki split's non-finite flags for A and B).
 int launch_dgemm_dmma(const GemmDesc& g, cudaStream_t st, int sm_count, int* status, const int* gate, int mma_k,
                       char* err, size_t errlen);
 
@@ -134,6 +141,11 @@ struct jlc_ctx {
     DevBuf bufR;  // reduction partials (adjoint)
     Workspace ws;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    // host-entry pipeline: copy-in and copy-out streams beside `stream`, and
+    // ordering events (created on first use)
+    static constexpr int kPipeMaxBlocks = 8;
+    cudaStream_t cin = nullptr, cout = nullptr;
+    cudaEvent_t pev[2 * kPipeMaxBlocks + 1] = {};
     int dmma_k = 8;
     // profiler: event pairs around phases, reused from a pool
     bool profiling = false;

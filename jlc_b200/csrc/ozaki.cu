@@ -153,7 +153,7 @@ template <bool CRT>
 __global__ void __launch_bounds__(THREADS, 1)
     ozaki_gemm_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB,
                       const Params p) {
-    if (*p.nonfinite != 0) return;
+    if ((p.nonfinite[0] | p.nonfinite[1]) != 0) return;
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     char* smem = reinterpret_cast<char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
     uint64_t* full = reinterpret_cast<uint64_t*>(smem + STAGES * STAGE_BYTES);
@@ -847,7 +847,8 @@ static int ozaki_bufs(const GemmDesc& g, int count, size_t ws_bytes, int sm_coun
     b.tiles_m = (g.m + BM - 1) / BM;
     b.tiles_n = (g.n + BN - 1) / BN;
     b.grid = ozaki_grid(g.m, g.n, sm_count);
-    b.L = plan_layout(g.m, g.n, g.k, count, b.grid, crt);
+    const long long lm = g.ws_m > g.m ? g.ws_m : g.m;
+    b.L = plan_layout(lm, g.n, g.k, count, ozaki_grid(lm, g.n, sm_count), crt);
     b.Kp = (int)up((size_t)g.k, 16);
     if (b.L.total > ws_bytes) {
         snprintf(err, errlen, "Ozaki workspace too small (%zu < %zu)", ws_bytes, b.L.total);
@@ -864,10 +865,10 @@ int launch_ozaki_split(const GemmDesc& g, int count, void* workspace, size_t ws_
     if (rc) return rc;
     char* ws = static_cast<char*>(workspace);
     auto* maxb = reinterpret_cast<unsigned long long*>(ws + b.L.maxb);
-    int* nonfinite = flags;
+    // flags[0]: A held Inf/NaN, flags[1]: B did (kept while B's split is reused)
     int p = 0, q = 0;
     if (crt) crt_pq(count, g.k, p, q);
-    if (cudaMemsetAsync(nonfinite, 0, sizeof(int), st) != cudaSuccess) {
+    if (cudaMemsetAsync(flags, 0, (g.b_split_ready ? 1 : 2) * sizeof(int), st) != cudaSuccess) {
         snprintf(err, errlen, "flag reset failed");
         return JLC_E_CUDA;
     }
@@ -875,11 +876,11 @@ int launch_ozaki_split(const GemmDesc& g, int count, void* workspace, size_t ws_
     // (columns j of B) are contiguous along k when B is column-major.
     rc = split_operand(g.a, g.lda, g.layout_a == JLC_ROW_MAJOR, (int)g.m, (int)g.k, b.Kp, count, p, crt,
                        reinterpret_cast<uint8_t*>(ws + b.L.sa), reinterpret_cast<int*>(ws + b.L.ea), maxb,
-                       nonfinite, st, sm_count);
-    if (!rc)
+                       flags, st, sm_count);
+    if (!rc && !g.b_split_ready)
         rc = split_operand(g.b, g.ldb, g.layout_b == JLC_COL_MAJOR, (int)g.n, (int)g.k, b.Kp, count, q, crt,
                            reinterpret_cast<uint8_t*>(ws + b.L.sb), reinterpret_cast<int*>(ws + b.L.eb), maxb,
-                           nonfinite, st, sm_count);
+                           flags + 1, st, sm_count);
     if (rc) snprintf(err, errlen, "Ozaki split launch failed: %s", cudaGetErrorString(cudaGetLastError()));
     return rc;
 }
