@@ -345,7 +345,7 @@ def run_ours(args):
     int8_ops_per_launch = 2.0 * M * N * K * P
     achieved_tops = int8_ops_per_launch / (gemm_ms * 1e-3) / 1e12
     mp = measured_peaks()
-    traffic = profile_traffic(f"ozaki_gemm_{size}")
+    traffic = profile_traffic(f"ozaki_crt_gemm_{size}")
     line = {
         "metric": METRIC,
         "value": round(world * oz_gflops, 1),
