@@ -113,6 +113,18 @@ __device__ __forceinline__ void l2_prefetch_bulk(const void* src, uint32_t bytes
                  : "memory");
 }
 
+// 3-D tile load by one CTA of a pair whose completion (bytes) is signalled on
+// an mbarrier given by its shared::cluster address, which may sit in the
+// other CTA of the pair (no multicast: the data lands in this CTA only)
+__device__ __forceinline__ void tma_load_3d_pair(void* smem_dst, const CUtensorMap* map, uint32_t bar_cluster,
+                                                 int32_t x, int32_t y, int32_t z) {
+    asm volatile(
+        "cp.async.bulk.tensor.3d.cta_group::2.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, "
+        "{%3, %4, %5}], [%2];" ::"r"(smem_u32(smem_dst)),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(bar_cluster), "r"(x), "r"(y), "r"(z)
+        : "memory");
+}
+
 __device__ __forceinline__ int warp_id() { return threadIdx.x >> 5; }
 __device__ __forceinline__ int lane_id() { return threadIdx.x & 31; }
 

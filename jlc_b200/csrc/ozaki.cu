@@ -34,23 +34,30 @@
 //     INT32 accumulation and is reduced mod m_l in the epilogue (one byte
 //     per element; runs longer than 1023 k-blocks are reduced chunk-wise).
 //  3. After the last modulus the integer product A'B' is reconstructed
-//     exactly by the Chinese remainder theorem: sum_l r_l W_l is kept as
-//     three FP64 words of 41-bit digits (every product and partial sum is
-//     an exact integer below 2^53), one multiple of M is removed to land in
-//     (-M/2, M/2], and C = alpha * 2^(E_i+F_j-p-q) * A'B' + beta*C.
+//     exactly by the Chinese remainder theorem in integer arithmetic
+//     (jlc_crt.cuh: 128-bit sum_l r_l W_l, one multiple of M removed to land
+//     in (-M/2, M/2], nearest double assembled from the bits), spread over
+//     the next tile's runs, and C = alpha * 2^(E_i+F_j-p-q) * A'B' + beta*C.
 //  N moduli replace s(s+1)/2 slice pairs: 13 products instead of 28 for
 //  the same FP64 accuracy at k = 8192, and the error comes only from the
 //  rounding of A' and B' (round-to-nearest, so it is unbiased).
 //
-// Kernel layout: persistent CTAs, 10 warps.  Warp 0 issues TMA loads of the
-// K-major INT8 tiles (A 128x128 B, B 256x128 B, 128B swizzle) into a
-// 4-stage ring; warp 1 allocates TMEM (512 columns = two 128x256 INT32
-// accumulators) and one elected lane issues tcgen05.mma; warps 2-9 drain
-// the accumulators with tcgen05.ld into a per-CTA scratch tile (FP64 running
-// sums, or residue bytes) and write C after the tile's last run.  In the
-// slice scheme diagonals run from the least significant (most pairs) down
-// to d = 0; accumulator double buffering lets the epilogue of one run
-// overlap the MMAs of the next.  No TMA multicast is used anywhere.
+// Kernel layout: persistent CTA pairs (clusters of 2 on neighbouring SMs),
+// 10 warps per CTA, one 256 x 256 tile of C per pair.  Warp 0 of each CTA
+// issues TMA loads of its K-major INT8 tiles (its 128 rows of A and 128 of
+// the 256 rows of op(B)^T, 128 bytes of K, 128B swizzle) into a 6-stage
+// ring; both signal the leader CTA's barrier.  Warp 1 allocates TMEM in both
+// CTAs (512 columns = two 128x256 INT32 accumulators each) and one lane of
+// the leader issues tcgen05.mma.cta_group::2 (M=256, N=256, K=32), which
+// reads both CTAs' shared memory and writes both CTAs' TMEM; each CTA's B
+// half is read once for both.  Against one CTA per 128x256 tile this moves a
+// third less operand data from L2 per flop, which is what pays under the
+// 1000 W cap.  Warps 2-9 of each CTA drain their 128 accumulator rows with
+// tcgen05.ld into per-CTA scratch (FP64 running sums, or residue bytes) and
+// write C.  In the slice scheme diagonals run from the least significant
+// (most pairs) down to d = 0; accumulator double buffering lets the
+// epilogue of one run overlap the MMAs of the next.  No TMA multicast is
+// used anywhere.
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -63,12 +70,14 @@
 namespace jlc {
 namespace oz {
 
-constexpr int BM = 128, BN = 256, BKB = 128;  // BKB: k-bytes (INT8 elements) per stage
+// A CTA pair computes a PM x BN tile of C: each CTA owns BM rows (its half of
+// A, its 128 accumulator lanes) and loads BNH of the BN rows of op(B)^T.
+constexpr int BM = 128, PM = 256, BN = 256, BNH = 128, BKB = 128;  // BKB: k-bytes (INT8) per stage
 constexpr int UMMA_K = 32;
-constexpr int STAGES = 4;
-constexpr int A_STAGE = BM * BKB;  // 16 KB
-constexpr int B_STAGE = BN * BKB;  // 32 KB
-constexpr int STAGE_BYTES = A_STAGE + B_STAGE;
+constexpr int STAGES = 6;
+constexpr int A_STAGE = BM * BKB;   // 16 KB
+constexpr int B_STAGE = BNH * BKB;  // 16 KB
+constexpr int STAGE_BYTES = A_STAGE + B_STAGE;  // per CTA; a stage of the pair completes 2x this
 constexpr int THREADS = 320;  // warp 0 TMA, warp 1 MMA, warps 2..9 epilogue
 constexpr int EPI_WARPS = 8;
 constexpr int TMEM_COLS = 512;
@@ -96,7 +105,7 @@ using CrtConsts = crt::Consts;
 
 struct Params {
     int M, N, K, KB, s;
-    int tiles_m, tiles_n, num_tiles;
+    int tiles_m, tiles_n, num_tiles;  // pair tiles (PM x BN)
     const int* ea;
     const int* eb;
     double alpha, beta;
@@ -112,8 +121,8 @@ struct Params {
     CrtConsts crt;  // residue scheme only (by value: read from the constant bank)
 };
 
-// Instruction descriptor: kind::i8, D = S32, A = B = signed INT8, both K-major, 128 x 256.
-constexpr uint32_t kIdescI8 = make_idesc(2u, 1u, BM, BN);
+// Instruction descriptor: kind::i8, D = S32, A = B = signed INT8, both K-major, 256 x 256 (pair).
+constexpr uint32_t kIdescI8 = make_idesc(2u, 1u, PM, BN);
 
 // Run structure shared by the three roles.  A tile is a sequence of
 // "diagonals"; diagonal di holds npairs(di) slice pairs whose INT8 products
@@ -150,9 +159,10 @@ __device__ __forceinline__ double scale_pow2(double v, int s) {
 }
 
 template <bool CRT>
-__global__ void __launch_bounds__(THREADS, 1)
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(THREADS, 1)
     ozaki_gemm_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB,
                       const Params p) {
+    // both CTAs of a pair read the same flags, so both leave here or neither
     if ((p.nonfinite[0] | p.nonfinite[1]) != 0) return;
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     char* smem = reinterpret_cast<char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
@@ -166,6 +176,13 @@ __global__ void __launch_bounds__(THREADS, 1)
     const Runs<CRT> runs{p.s, p.KB};
 
     const int warp = warp_id(), lane = lane_id();
+    // Pair protocol.  full[s] of the leader (rank 0) collects both CTAs' TMA
+    // bytes of stage s (the leader arms it for 2 * STAGE_BYTES); the leader's
+    // MMA commit arrives on empty[s] of both CTAs, whose producers wait on
+    // their own copy; acc_full[b] is signalled in both CTAs by the leader's
+    // commit; acc_empty[b] of the leader counts the epilogue warps of both.
+    const uint32_t rank = cluster_ctarank();
+    const bool leader = rank == 0;
     if (threadIdx.x == 0) {
         tma_prefetch_desc(&mapA);
         tma_prefetch_desc(&mapB);
@@ -175,19 +192,20 @@ __global__ void __launch_bounds__(THREADS, 1)
         }
         for (int b = 0; b < 2; ++b) {
             mbar_init(&acc_full[b], 1);
-            mbar_init(&acc_empty[b], EPI_WARPS);
+            mbar_init(&acc_empty[b], 2 * EPI_WARPS);
         }
         mbar_init(mma_done, 1);
         fence_barrier_init();
     }
     if (warp == 1) {
-        tmem_alloc(tmem_slot, TMEM_COLS);
-        tmem_relinquish();
+        tmem_alloc_pair(tmem_slot, TMEM_COLS);
+        tmem_relinquish_pair();
     }
     tc_fence_before();
-    __syncthreads();
+    cluster_sync();  // barriers initialised and TMEM allocated in both CTAs
     tc_fence_after();
     const uint32_t tmem_base = *tmem_slot;
+    const int cluster = blockIdx.x >> 1, nclusters = gridDim.x >> 1;
 
     if (warp == 0) {
         // ---------------- TMA producer ----------------
@@ -195,10 +213,11 @@ __global__ void __launch_bounds__(THREADS, 1)
             int stage = 0;
             uint32_t phase = 0, armed = 0, last_parity = 0;
             bool ok = true;
-            for (int tile = blockIdx.x; tile < p.num_tiles && ok; tile += gridDim.x) {
+            const uint32_t full0_leader = mapa_shared(smem_u32(full), 0);
+            for (int tile = cluster; tile < p.num_tiles && ok; tile += nclusters) {
                 int tm, tn;
                 tile_coords(tile, p.tiles_m, p.tiles_n, 8, tm, tn);
-                const int m0 = tm * BM, n0 = tn * BN;
+                const int m0 = tm * PM + (int)rank * BM, n0 = tn * BN + (int)rank * BNH;
                 for (int di = 0; di < runs.ndiag && ok; ++di) {
                     const int d = runs.diag(di);
                     for (int pr = 0; pr < runs.npairs(d) && ok; ++pr) {
@@ -210,9 +229,10 @@ __global__ void __launch_bounds__(THREADS, 1)
                             }
                             char* sA = smem + stage * STAGE_BYTES;
                             char* sB = sA + A_STAGE;
-                            mbar_arrive_expect_tx(&full[stage], STAGE_BYTES);
-                            tma_load_3d(sA, &mapA, &full[stage], kb * BKB, m0, ia);
-                            tma_load_3d(sB, &mapB, &full[stage], kb * BKB, n0, ib);
+                            if (leader) mbar_arrive_expect_tx(&full[stage], 2 * STAGE_BYTES);
+                            const uint32_t fb = full0_leader + 8u * (uint32_t)stage;
+                            tma_load_3d_pair(sA, &mapA, fb, kb * BKB, m0, ia);
+                            tma_load_3d_pair(sB, &mapB, fb, kb * BKB, n0, ib);
                             armed |= 1u << stage;
                             last_parity = (last_parity & ~(1u << stage)) | (phase << stage);
                             if (++stage == STAGES) {
@@ -223,17 +243,24 @@ __global__ void __launch_bounds__(THREADS, 1)
                     }
                 }
             }
-            for (int s = 0; s < STAGES; ++s)
-                if (armed & (1u << s)) drain_wait(&full[s], (last_parity >> s) & 1u, p.status);
+            // the leader's full barriers see both CTAs' copies complete; the
+            // peer's copies are covered by the leader's wait and the final
+            // cluster barrier
+            if (leader)
+                for (int s = 0; s < STAGES; ++s)
+                    if (armed & (1u << s)) drain_wait(&full[s], (last_parity >> s) & 1u, p.status);
         }
     } else if (warp == 1) {
-        // ---------------- MMA issuer ----------------
-        if (lane == 0) {
+        // ---------------- MMA issuer (leader CTA of the pair) ----------------
+        if (lane == 0 && leader) {
             int stage = 0;
             uint32_t phase = 0;
             uint32_t gcount = 0;
             bool ok = true;
-            for (int tile = blockIdx.x; tile < p.num_tiles && ok; tile += gridDim.x) {
+            // stage 0's A descriptor; the 14-bit address field (smem byte
+            // address / 16 < 2^14) never carries into the other fields
+            const uint64_t adesc0 = sw128_kmajor_desc(smem_u32(smem));
+            for (int tile = cluster; tile < p.num_tiles && ok; tile += nclusters) {
                 for (int di = 0; di < runs.ndiag && ok; ++di) {
                     const int nblk = runs.npairs(runs.diag(di)) * p.KB;
                     for (int g0 = 0; g0 < nblk && ok; g0 += Runs<CRT>::cap) {
@@ -251,28 +278,28 @@ __global__ void __launch_bounds__(THREADS, 1)
                                 break;
                             }
                             tc_fence_after();
-                            const uint32_t sA = smem_u32(smem + stage * STAGE_BYTES);
-                            const uint32_t sB = sA + A_STAGE;
+                            // descriptors: stage base + K offset (address field counts 16 B)
+                            const uint64_t ad = adesc0 + (uint64_t)(stage * (STAGE_BYTES >> 4));
+                            const uint64_t bd = ad + (uint64_t)(A_STAGE >> 4);
 #pragma unroll
-                            for (int kk = 0; kk < BKB / UMMA_K; ++kk) {
-                                const uint64_t ad = sw128_kmajor_desc(sA + kk * UMMA_K);
-                                const uint64_t bd = sw128_kmajor_desc(sB + kk * UMMA_K);
-                                umma_i8(tmem_d, ad, bd, kIdescI8, (f == g0 && kk == 0) ? 0u : 1u);
-                            }
-                            umma_commit(&empty[stage]);
+                            for (int kk = 0; kk < BKB / UMMA_K; ++kk)
+                                umma_i8_pair(tmem_d, ad + (uint64_t)(kk * (UMMA_K >> 4)),
+                                             bd + (uint64_t)(kk * (UMMA_K >> 4)), kIdescI8,
+                                             (f == g0 && kk == 0) ? 0u : 1u);
+                            umma_commit_pair_mc(&empty[stage], 0x3);
                             if (++stage == STAGES) {
                                 stage = 0;
                                 phase ^= 1u;
                             }
                         }
                         if (!ok) break;
-                        umma_commit(&acc_full[buf]);
+                        umma_commit_pair_mc(&acc_full[buf], 0x3);
                         ++gcount;
                     }
                 }
             }
             // every MMA this thread issued has completed before TMEM is freed
-            umma_commit(mma_done);
+            umma_commit_pair(mma_done);
             drain_wait(mma_done, 0, p.status);
         }
     } else {
@@ -381,10 +408,11 @@ __global__ void __launch_bounds__(THREADS, 1)
         };
         uint32_t gcount = 0;
         bool ok = true;
-        for (int tile = blockIdx.x; tile < p.num_tiles && ok; tile += gridDim.x) {
+        const uint32_t acc_empty_leader = mapa_shared(smem_u32(acc_empty), 0);
+        for (int tile = cluster; tile < p.num_tiles && ok; tile += nclusters) {
             int tm, tn;
             tile_coords(tile, p.tiles_m, p.tiles_n, 8, tm, tn);
-            const int m0 = tm * BM, n0 = tn * BN;
+            const int m0 = tm * PM + (int)rank * BM, n0 = tn * BN;
             const int grow = m0 + row;
             const bool row_ok = grow < p.M;
             const int ei = row_ok ? p.ea[grow] : 0;
@@ -479,7 +507,7 @@ __global__ void __launch_bounds__(THREADS, 1)
                     // the accumulator is free once every chunk has been read
                     tc_fence_before();
                     __syncwarp();
-                    if (lane == 0) mbar_arrive(&acc_empty[buf]);
+                    if (lane == 0) mbar_arrive_cluster(acc_empty_leader + buf * 8u);
                     ++gcount;
                     if constexpr (CRT) {
                         // the previous tile's reconstruction advances by a share
@@ -527,10 +555,12 @@ __global__ void __launch_bounds__(THREADS, 1)
 
     __syncwarp();  // lanes that skipped a single-lane role wait for it here
     tc_fence_before();
-    __syncthreads();
+    // neither CTA leaves (or frees TMEM) while the leader's MMAs may still read
+    // the peer's shared memory or write its TMEM
+    cluster_sync();
     if (warp == 1) {
         tc_fence_after();
-        tmem_dealloc(tmem_base, TMEM_COLS);
+        tmem_dealloc_pair(tmem_base, TMEM_COLS);
     }
 }
 
@@ -804,9 +834,14 @@ void crt_constants(int nmod, long long k, CrtConsts& c) {
 
 }  // namespace oz
 
+// CTAs of the persistent Ozaki GEMM: one pair per PM x BN tile, at most one
+// CTA per SM, always a whole number of pairs.
 int ozaki_grid(long long m, long long n, int sm_count) {
-    const long long tiles = ((m + oz::BM - 1) / oz::BM) * ((n + oz::BN - 1) / oz::BN);
-    return (int)(tiles < sm_count ? tiles : sm_count);
+    const long long tiles = ((m + oz::PM - 1) / oz::PM) * ((n + oz::BN - 1) / oz::BN);
+    long long pairs = sm_count / 2;
+    if (pairs < 1) pairs = 1;
+    if (tiles < pairs) pairs = tiles < 1 ? 1 : tiles;
+    return (int)(2 * pairs);
 }
 
 size_t ozaki_workspace_bytes(long long m, long long n, long long k, int count, int sm_count, bool crt) {
@@ -844,7 +879,7 @@ static int ozaki_bufs(const GemmDesc& g, int count, size_t ws_bytes, int sm_coun
         snprintf(err, errlen, "%s count %d out of range", crt ? "modulus" : "slice", count);
         return JLC_E_ARG;
     }
-    b.tiles_m = (g.m + BM - 1) / BM;
+    b.tiles_m = (g.m + PM - 1) / PM;
     b.tiles_n = (g.n + BN - 1) / BN;
     b.grid = ozaki_grid(g.m, g.n, sm_count);
     const long long lm = g.ws_m > g.m ? g.ws_m : g.m;
@@ -898,7 +933,7 @@ int launch_ozaki_gemm(const GemmDesc& g, int count, void* workspace, size_t ws_b
                       err, errlen);
     if (rc) return rc;
     rc = make_tmap_3d(&mb, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, ws + b.L.sb, (uint64_t)g.k, (uint64_t)g.n,
-                      (uint64_t)count, (uint64_t)b.Kp, (uint64_t)g.n * b.Kp, BKB, BN, 1, CU_TENSOR_MAP_SWIZZLE_128B,
+                      (uint64_t)count, (uint64_t)b.Kp, (uint64_t)g.n * b.Kp, BKB, BNH, 1, CU_TENSOR_MAP_SWIZZLE_128B,
                       err, errlen);
     if (rc) return rc;
 
