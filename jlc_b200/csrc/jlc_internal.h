@@ -143,7 +143,7 @@ struct jlc_ctx {
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     // host-entry pipeline: copy-in and copy-out streams beside `stream`, and
     // ordering events (created on first use)
-    static constexpr int kPipeMaxBlocks = 8;
+    static constexpr int kPipeMaxBlocks = 16;
     cudaStream_t cin = nullptr, cout = nullptr;
     cudaEvent_t pev[2 * kPipeMaxBlocks + 1] = {};
     int dmma_k = 8;
