@@ -41,8 +41,9 @@ def parse():
     p.add_argument("--cpu-seconds", type=float, default=12.0, help="target length of one CPU baseline sample")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu-baseline", action="store_true")
-    p.add_argument("--workload", default="dgemm", choices=["dgemm", "grouped"],
-                   help="dgemm: the 8192^3 headline; grouped: 20,000 uneven problems in one launch")
+    p.add_argument("--workload", default="dgemm", choices=["dgemm", "grouped", "configs"],
+                   help="dgemm: the 8192^3 headline; grouped: 20,000 uneven problems in one launch; "
+                        "configs: one line per C1-C5 shape (rate and accuracy), one GPU")
     return p.parse_args()
 
 
@@ -472,12 +473,134 @@ def run_grouped(args):
     return 0
 
 
+def run_configs(args):
+    """One JSON line per configuration of the five workload families: C1
+    (1024^3, alpha 1.5, beta 0.5), C2 (DMMA square sweep, beta 0 and 1,
+    rectangular shapes, matrix-vector, transposed / column-major operand
+    layouts), C3 (Ozaki at 4096/8192/16384 on uniform and ill-scaled inputs),
+    C5 (adjoint, native and Ozaki).  Each line: device time per call (CUDA
+    events, warm), FP64-equivalent GFLOP/s, algorithmic GB/s, and the max
+    |err|/bound over sampled entries from the device double-double check."""
+    import numpy as np
+    import torch
+    import jlc_b200
+    from jlc_b200 import JLC_COL_MAJOR, JLC_PREC_AUTO, JLC_PREC_NATIVE, JLC_PREC_OZAKI_CRT, JLC_ROW_MAJOR
+    torch.cuda.set_device(0)
+    ctx = jlc_b200.Context(0)
+    stream = torch.cuda.Stream()
+    ctx.set_stream(stream.cuda_stream)
+    g = torch.Generator(device="cuda")
+    g.manual_seed(20260604)
+    reps = max(3, min(args.steps, 10))
+
+    def uniform(shape):
+        with torch.cuda.stream(stream):
+            t = torch.rand(shape, dtype=torch.float64, device="cuda", generator=g) * 2 - 1
+        return t
+
+    def timed(fn):
+        for _ in range(2):
+            fn()
+        stream.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(reps):
+            rep = fn()
+        e1.record(stream)
+        e1.synchronize()
+        return e0.elapsed_time(e1) / reps, rep
+
+    def accuracy(la, lb, m, n, k, alpha, A, lda, B, ldb, beta, Cin, C):
+        rng = np.random.default_rng(5)
+        rows = np.concatenate([rng.integers(0, m, 1024), [0, m - 1]])
+        cols = np.concatenate([rng.integers(0, n, 1024), [0, n - 1]])
+        if n == 1:
+            cols[:] = 0
+        return ctx.check_fp64_bound_device(la, lb, m, n, k, alpha, A.data_ptr(), lda, B.data_ptr(), ldb, beta,
+                                           Cin.data_ptr() if Cin is not None else None, C.shape[1] if C.dim() > 1
+                                           else 1, C.data_ptr(), C.shape[1] if C.dim() > 1 else 1, rows,
+                                           cols)["max_ratio"]
+
+    def gemm_case(name, m, n, k, alpha=1.0, beta=0.0, la=JLC_ROW_MAJOR, lb=JLC_ROW_MAJOR, precision=JLC_PREC_NATIVE,
+                  scaled=False):
+        A = uniform((m, k) if la == JLC_ROW_MAJOR else (k, m))
+        B = uniform((k, n) if lb == JLC_ROW_MAJOR else (n, k))
+        if scaled:  # 2^e, e uniform in [-20, 20], per row of A and per column of B
+            ea = torch.randint(-20, 21, (m,), device="cuda", generator=g).double()
+            eb = torch.randint(-20, 21, (n,), device="cuda", generator=g).double()
+            A *= torch.pow(2.0, ea)[:, None] if la == JLC_ROW_MAJOR else torch.pow(2.0, ea)[None, :]
+            B *= torch.pow(2.0, eb)[None, :] if lb == JLC_ROW_MAJOR else torch.pow(2.0, eb)[:, None]
+        C0 = uniform((m, n))
+        C = C0.clone()
+        lda = A.shape[1]
+        ldb = B.shape[1]
+        ms, rep = timed(lambda: ctx.dgemm_device(la, lb, m, n, k, alpha, A.data_ptr(), lda, B.data_ptr(), ldb,
+                                                 beta, C.data_ptr(), n, precision=precision))
+        # accuracy of one fresh call on the original C
+        C.copy_(C0)
+        ctx.dgemm_device(la, lb, m, n, k, alpha, A.data_ptr(), lda, B.data_ptr(), ldb, beta, C.data_ptr(), n,
+                         precision=precision)
+        ctx.synchronize()
+        ratio = accuracy(la, lb, m, n, k, alpha, A, lda, B, ldb, beta, C0 if beta != 0.0 else None, C)
+        flops = 2.0 * m * n * k
+        nbytes = 8.0 * (m * k + k * n + m * n * (2 if beta != 0.0 else 1))
+        line = {"config": name, "m": m, "n": n, "k": k, "alpha": alpha, "beta": beta,
+                "layout_a": "col" if la == JLC_COL_MAJOR else "row", "layout_b": "col" if lb == JLC_COL_MAJOR
+                else "row", "route": {0: "native", 1: "ozaki-slices", 3: "ozaki-crt"}.get(rep["precision"]),
+                "kernel": rep["kernel"], "ms": round(ms, 4), "gflops": round(flops / (ms * 1e-3) / 1e9, 1),
+                "gbs": round(nbytes / (ms * 1e-3) / 1e9, 1), "max_err_ratio": ratio}
+        if scaled:
+            line["inputs"] = "ill-scaled 2^e, e in [-20,20] per row of A / column of B"
+        print(json.dumps(line), flush=True)
+        del A, B, C, C0
+        torch.cuda.empty_cache()
+
+    gemm_case("C1", 1024, 1024, 1024, alpha=1.5, beta=0.5)
+    for sz in (2048, 4096, 8192):
+        for beta in (0.0, 1.0):
+            gemm_case("C2 square", sz, sz, sz, beta=beta)
+    gemm_case("C2 rectangular", 8192, 256, 8192)
+    gemm_case("C2 rectangular", 8192, 8192, 256)
+    gemm_case("C2 matvec", 16384, 1, 16384)
+    gemm_case("C2 TransA (A^T B, A stored k x m)", 4096, 4096, 4096, la=JLC_COL_MAJOR)
+    gemm_case("C2 ColMajorB", 4096, 4096, 4096, lb=JLC_COL_MAJOR)
+    for sz in (4096, 8192, 16384):
+        gemm_case("C3 Ozaki uniform", sz, sz, sz, precision=JLC_PREC_AUTO)
+        gemm_case("C3 Ozaki ill-scaled", sz, sz, sz, precision=JLC_PREC_OZAKI_CRT, scaled=True)
+
+    # C5: adjoint of C_out = A B + C_in, A 4096x2048, B 2048x4096, N(0,1)
+    m, k, n = 4096, 2048, 4096
+    for prec, pname in ((JLC_PREC_NATIVE, "native"), (JLC_PREC_OZAKI_CRT, "ozaki-crt")):
+        with torch.cuda.stream(stream):
+            A = torch.randn((m, k), dtype=torch.float64, device="cuda", generator=g)
+            B = torch.randn((k, n), dtype=torch.float64, device="cuda", generator=g)
+            Cin = torch.randn((m, n), dtype=torch.float64, device="cuda", generator=g)
+            dC = torch.randn((m, n), dtype=torch.float64, device="cuda", generator=g)
+            dA = torch.empty((m, k), dtype=torch.float64, device="cuda")
+            dB = torch.empty((k, n), dtype=torch.float64, device="cuda")
+            sc = torch.zeros(2, dtype=torch.float64, device="cuda")
+        ms, _ = timed(lambda: ctx.adjoint_device(m, n, k, 1.0, 1.0, A.data_ptr(), k, B.data_ptr(), n,
+                                                 Cin.data_ptr(), n, dC.data_ptr(), n, dA.data_ptr(), k,
+                                                 dB.data_ptr(), n, sc.data_ptr(), sc.data_ptr() + 8,
+                                                 precision=prec))
+        flops = 2.0 * (2.0 * m * n * k) + 2.0 * m * n
+        print(json.dumps({"config": "C5 adjoint", "m": m, "n": n, "k": k, "route": pname, "ms": round(ms, 4),
+                          "gflops": round(flops / (ms * 1e-3) / 1e9, 1),
+                          "outputs": "dA, dB, dalpha, dbeta"}), flush=True)
+        del A, B, Cin, dC, dA, dB
+        torch.cuda.empty_cache()
+    ctx.close()
+    return 0
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         return run_reference(args)
     if args.workload == "grouped":
         return run_grouped(args)
+    if args.workload == "configs":
+        return run_configs(args)
     return run_ours(args)
 
 

@@ -178,6 +178,7 @@ JLC_API int jlc_device_status(jlc_ctx* ctx);
 #define JLC_PHASE_FP64_GATED 7  /* FP64 kernel behind an Ozaki call (runs only on Inf/NaN input) */
 #define JLC_PHASE_H2D 8         /* host -> device operand copies */
 #define JLC_PHASE_D2H 9         /* device -> host copy of C */
+#define JLC_PHASE_REDUCE 11     /* adjoint reductions: d(alpha) / d(beta) dots and sums, scaled copies */
 /* Turn event-pair recording around each phase on (1) or off (0).  Records
  * accumulate (up to 4096) until collected. */
 JLC_API int jlc_set_profiling(jlc_ctx* ctx, int on);

@@ -849,9 +849,13 @@ int jlc_dgemm_adjoint_device(jlc_ctx* ctx, int64_t m, int64_t n, int64_t k, doub
             g.dot_ld = lda;
             g.dot_partials = parts_a;
             rc = run_device(ctx, g, precision, 0, &sub);
-            if (!rc) rc = launch_sum(parts_a, np, dalpha, st);
+            if (!rc) {
+                Phase ph(ctx, JLC_PHASE_REDUCE);
+                rc = launch_sum(parts_a, np, dalpha, st);
+            }
         } else {
             rc = run_device(ctx, g, precision, 0, &sub);
+            Phase ph(ctx, JLC_PHASE_REDUCE);
             if (!rc) rc = launch_dot2d(a, lda, da, ldda, m, k, parts_a, 2 * np, dalpha, st);
             if (!rc && alpha != 1.0) rc = launch_scale_copy(da, ldda, da, ldda, m, k, alpha, st);
         }
@@ -872,8 +876,11 @@ int jlc_dgemm_adjoint_device(jlc_ctx* ctx, int64_t m, int64_t n, int64_t k, doub
         if (rc) return rc;
     }
     // 3) dbeta = <dC, C_in>;  4) dC_in = beta * dC
-    rc = launch_dot2d(dc, lddc, c_in, ldc_in, m, n, parts_b, 2 * np, dbeta, st);
-    if (!rc && dc_in) rc = launch_scale_copy(dc_in, lddc_in, dc, lddc, m, n, beta, st);
+    {
+        Phase ph(ctx, JLC_PHASE_REDUCE);
+        rc = launch_dot2d(dc, lddc, c_in, ldc_in, m, n, parts_b, 2 * np, dbeta, st);
+        if (!rc && dc_in) rc = launch_scale_copy(dc_in, lddc_in, dc, lddc, m, n, beta, st);
+    }
     if (rc) return set_err(ctx, rc, "adjoint reduction launch failed");
     ctx->launches += 3;
     return JLC_OK;
