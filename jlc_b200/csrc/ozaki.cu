@@ -588,9 +588,9 @@ constexpr double kMagic = 0x1.8p52;  // adding it rounds |x| < 2^51 to an intege
 //                   rounding tie for odd m_t (m_t = 256 has an exact inverse),
 //                   so the digit never leaves [-128, 128]; +128 only arises for
 //                   m_t = 256, where the byte 0x80 is still congruent.
-//                   All steps are exact: x + kMagic, m_t * q and their
-//                   difference are integers below 2^53, and the low byte of
-//                   kMagic + digit is the digit's two's-complement byte.
+//                   x + kMagic and the fma are exact integers below 2^53 whose
+//                   low words are x and q_t modulo 2^32, and the digit (small)
+//                   is their 32-bit wrap-around combination exactly.
 template <bool CRT>
 __device__ __forceinline__ void encode4(double (&v)[4], int count, uint8_t* dst, size_t stride) {
     if constexpr (!CRT) {
@@ -609,26 +609,32 @@ __device__ __forceinline__ void encode4(double (&v)[4], int count, uint8_t* dst,
             }
         }
     } else {
-        double xm[4], x[4];
+        // x = rint(v) as a double, and x mod 2^32 from the low word of
+        // kMagic + x; q_t = rint(x / m_t) likewise from the low word of
+        // fma(x, inv_t, kMagic).  The digit x - m_t q_t is small, so the 32-bit
+        // wrap-around difference of the low words equals it exactly and its
+        // low byte is the stored INT8: one DFMA and one IMAD per digit.
+        double x[4];
+        uint32_t xl[4];
 #pragma unroll
         for (int u = 0; u < 4; ++u) {
-            xm[u] = v[u] + kMagic;  // kMagic + rint(v)
-            x[u] = xm[u] - kMagic;  // rint(v)
+            const double xm = v[u] + kMagic;
+            x[u] = xm - kMagic;
+            xl[u] = (uint32_t)__double2loint(xm);
         }
+        uint8_t* out = dst;
 #pragma unroll
         for (int t = 0; t < MAX_MODULI; ++t) {
             if (t < count) {
-                const double m = (double)kModuli[t];
+                const uint32_t m = (uint32_t)kModuli[t];
                 const double inv = kInvModuli[t];
                 uint32_t b[4];
 #pragma unroll
-                for (int u = 0; u < 4; ++u) {
-                    const double qd = fma(x[u], inv, kMagic) - kMagic;  // rint(x / m)
-                    b[u] = (uint32_t)__double2loint(fma(-m, qd, xm[u]));
-                }
-                *reinterpret_cast<uint32_t*>(dst + (size_t)t * stride) =
+                for (int u = 0; u < 4; ++u) b[u] = xl[u] - m * (uint32_t)__double2loint(fma(x[u], inv, kMagic));
+                *reinterpret_cast<uint32_t*>(out) =
                     __byte_perm(__byte_perm(b[0], b[1], 0x0040), __byte_perm(b[2], b[3], 0x0040), 0x5410);
             }
+            out += stride;
         }
     }
 }
@@ -689,15 +695,29 @@ __global__ void __launch_bounds__(SPLIT_THREADS) colmax_kernel(const double* src
     const int i = blockIdx.x * SPLIT_THREADS + threadIdx.x;
     if (i >= cols) return;
     const int p0 = blockIdx.y * kchunk, p1 = min(K, p0 + kchunk);
-    double mx = 0.0;
+    // eight independent loads in flight per thread (the pass is latency-bound)
+    double mx[8] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
     bool bad = false;
-    for (int pp = p0; pp < p1; ++pp) {
+    int pp = p0;
+    for (; pp + 8 <= p1; pp += 8) {
+        double x[8];
+#pragma unroll
+        for (int u = 0; u < 8; ++u) x[u] = src[(long long)(pp + u) * ld + i];
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+            bad |= !isfinite(x[u]);
+            mx[u] = fmax(mx[u], fabs(x[u]));
+        }
+    }
+    for (; pp < p1; ++pp) {
         const double x = src[(long long)pp * ld + i];
         bad |= !isfinite(x);
-        mx = fmax(mx, fabs(x));
+        mx[0] = fmax(mx[0], fabs(x));
     }
+#pragma unroll
+    for (int u = 1; u < 8; ++u) mx[0] = fmax(mx[0], mx[u]);
     if (bad) atomicOr(nonfinite, 1);
-    atomicMax(&maxbits[i], (unsigned long long)__double_as_longlong(mx));
+    atomicMax(&maxbits[i], (unsigned long long)__double_as_longlong(mx[0]));
 }
 
 // Pass 2: 32 (i) x 128 (p) tiles through shared memory, written K-major.
