@@ -10,10 +10,13 @@
 // CUDA graph replay) in which persistent CTAs pull work items from an atomic
 // counter:
 //   * tile items: one 32x32 or 64x64 tile of C of one problem, FP64
-//     mma.sync (m16n8k8) over double-buffered cp.async stages of 16 k-values,
-//     with both operands stored K-major in swizzled shared memory (the layout
-//     and K permutation of the tiled DMMA kernel), alpha folded into the A
-//     fragments, beta fused in the epilogue;
+//     mma.sync (m16n8k8) over a 3-stage cp.async ring of 16 k-values; each
+//     operand is staged in the swizzled shared-memory layout that matches its
+//     global layout (K-major for row-major A / column-major B, MN-major
+//     otherwise), so the contiguous direction lands in 16-byte units and
+//     aligned operands move with 16-byte copies (8-byte copies otherwise,
+//     zero fill at ragged edges); alpha folded into the A fragments, beta
+//     fused in the epilogue;
 //   * tiny items: a batch of problems with m*n <= 64 and k <= 64 (the TINY
 //     and small SMALL shapes), one thread per output element running the
 //     reference's small-GEMM order (C <- beta*C, then an fma chain over p
@@ -50,7 +53,8 @@ constexpr int THREADS = 128;
 constexpr int GBK = 16;  // k-values per stage (one 128-byte swizzled row per tile row)
 constexpr int TINY_ELEMS = THREADS;
 constexpr int KIND_TINY = 0, KIND_T32 = 1, KIND_T64 = 2;
-constexpr int SMEM_BYTES = 2 * (64 + 64) * 128 + 128;
+constexpr int STAGES = 3;
+constexpr int SMEM_BYTES = STAGES * (64 + 64) * 128 + 128;
 
 struct Item {
     int prob;  // problem index, or first index into the tiny list
@@ -63,6 +67,12 @@ __device__ __forceinline__ void cp_async8(void* smem_dst, const void* src, bool 
     const uint32_t d = smem_u32(smem_dst);
     const int n = valid ? 8 : 0;  // 0: zero-fill without reading
     asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(d), "l"(src), "r"(n) : "memory");
+}
+// 16-byte copy of `bytes` (0, 8 or 16) valid bytes, the rest zero-filled;
+// src must be 16-byte aligned
+__device__ __forceinline__ void cp_async16(void* smem_dst, const void* src, int bytes) {
+    const uint32_t d = smem_u32(smem_dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 16, %2;" ::"r"(d), "l"(src), "r"(bytes) : "memory");
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 template <int N>
@@ -77,36 +87,55 @@ __device__ __forceinline__ double elem_b(const jlc_problem& P, long long p, long
     return P.layout_b == JLC_ROW_MAJOR ? P.b[p * P.ldb + j] : P.b[j * P.ldb + p];
 }
 
-// Stages one k-block of A (BM rows) and B (BN columns) into K-major swizzled
-// shared memory; threads walk the source's contiguous direction.
-template <int BM, int BN>
-__device__ __forceinline__ void load_stage(const jlc_problem& P, char* sA, char* sB, long long m0, long long n0,
-                                           long long k0) {
-    const int tid = threadIdx.x;
-    const bool a_row = P.layout_a == JLC_ROW_MAJOR;
-#pragma unroll 4
-    for (int e = tid; e < BM * GBK; e += THREADS) {
-        const int r = a_row ? e / GBK : e % BM;
-        const int c = a_row ? e % GBK : e / BM;
-        const long long gi = m0 + r, gk = k0 + c;
-        const bool ok = gi < P.m && gk < P.k;
-        const double* src = ok ? (a_row ? P.a + gi * P.lda + gk : P.a + gk * P.lda + gi) : P.a;
-        cp_async8(sA + dmma::kmajor_off(r, c), src, ok);
-    }
-    const bool b_row = P.layout_b == JLC_ROW_MAJOR;
-#pragma unroll 4
-    for (int e = tid; e < BN * GBK; e += THREADS) {
-        const int nn = b_row ? e % BN : e / GBK;
-        const int c = b_row ? e / BN : e % GBK;
-        const long long gj = n0 + nn, gk = k0 + c;
-        const bool ok = gj < P.n && gk < P.k;
-        const double* src = ok ? (b_row ? P.b + gk * P.ldb + gj : P.b + gj * P.ldb + gk) : P.b;
-        cp_async8(sB + dmma::kmajor_off(nn, c), src, ok);
-    }
-    cp_async_commit();
+// Byte offset of element (mn, k) of an operand tile: K-major (rows of 16 k)
+// or MN-major (16-wide mn chunks of 16 k rows), both 128B-swizzled.
+template <bool KMAJOR>
+__device__ __forceinline__ uint32_t op_off(int mn, int k) {
+    return KMAJOR ? dmma::kmajor_off(mn, k) : dmma::mnmajor_off(mn, k);
 }
 
-template <int BM, int BN>
+// Stages one k-block of one operand (ROWS rows of op(X) x GBK k) into its
+// shared-memory layout.  KMAJOR: X(i, p) = x[i * ld + p] (contiguous along
+// k); otherwise X(i, p) = x[p * ld + i] (contiguous along the rows).  Threads
+// walk the contiguous direction; with vec, pairs of doubles move as one
+// 16-byte copy (zero-filled past the problem's edge).
+template <int ROWS, bool KMAJOR>
+__device__ __forceinline__ void load_operand(const double* x, long long ld, long long nrows, long long nk, char* s,
+                                             long long r0, long long k0, bool vec) {
+    const int tid = threadIdx.x;
+    if (vec) {
+#pragma unroll 1
+        for (int e = tid; e < ROWS * GBK / 2; e += THREADS) {
+            int r, c;  // pair start: (r, c), (r, c+1) along k or (r, c), (r+1, c) along rows
+            if (KMAJOR) {
+                r = e / (GBK / 2);
+                c = 2 * (e % (GBK / 2));
+            } else {
+                c = e / (ROWS / 2);
+                r = 2 * (e % (ROWS / 2));
+            }
+            const long long gi = r0 + r, gk = k0 + c;
+            long long valid;
+            if (KMAJOR) valid = gi < nrows ? nk - gk : 0;
+            else valid = gk < nk ? nrows - gi : 0;
+            const int bytes = valid >= 2 ? 16 : (valid == 1 ? 8 : 0);
+            const double* src = bytes ? (KMAJOR ? x + gi * ld + gk : x + gk * ld + gi) : x;
+            cp_async16(s + op_off<KMAJOR>(r, c), src, bytes);
+        }
+    } else {
+#pragma unroll 1
+        for (int e = tid; e < ROWS * GBK; e += THREADS) {
+            const int r = KMAJOR ? e / GBK : e % ROWS;
+            const int c = KMAJOR ? e % GBK : e / ROWS;
+            const long long gi = r0 + r, gk = k0 + c;
+            const bool ok = gi < nrows && gk < nk;
+            const double* src = ok ? (KMAJOR ? x + gi * ld + gk : x + gk * ld + gi) : x;
+            cp_async8(s + op_off<KMAJOR>(r, c), src, ok);
+        }
+    }
+}
+
+template <int BM, int BN, bool AK, bool BK>
 __device__ void tile_item(const jlc_problem& P, int tm, int tn, char* smem) {
     constexpr int WM = BM / 2, WN = BN / 2;  // 2 x 2 warps
     constexpr int MT = WM / 16, NT = WN / 8;
@@ -118,6 +147,14 @@ __device__ void tile_item(const jlc_problem& P, int tm, int tn, char* smem) {
     constexpr int STAGE = (BM + BN) * 128;
     const int kblocks = P.alpha == 0.0 ? 0 : (int)((P.k + GBK - 1) / GBK);
     const bool scale_a = P.alpha != 1.0;
+    // 16-byte copies need 16-byte aligned rows (base and leading dimension)
+    const bool vec_a = ((reinterpret_cast<uintptr_t>(P.a) & 15) == 0) && ((P.lda & 1) == 0);
+    const bool vec_b = ((reinterpret_cast<uintptr_t>(P.b) & 15) == 0) && ((P.ldb & 1) == 0);
+    auto load = [&](int kb) {
+        char* sA = smem + (kb % STAGES) * STAGE;
+        load_operand<BM, AK>(P.a, P.lda, P.m, P.k, sA, m0, (long long)kb * GBK, vec_a);
+        load_operand<BN, BK>(P.b, P.ldb, P.n, P.k, sA + BM * 128, n0, (long long)kb * GBK, vec_b);
+    };
 
     double acc[MT][NT][4];
 #pragma unroll
@@ -127,19 +164,19 @@ __device__ void tile_item(const jlc_problem& P, int tm, int tn, char* smem) {
 #pragma unroll
             for (int e = 0; e < 4; ++e) acc[i][j][e] = 0.0;
 
-    if (kblocks > 0) load_stage<BM, BN>(P, smem, smem + BM * 128, m0, n0, 0);
+    // prologue: stages 0 .. STAGES-2 in flight (empty groups keep the count)
+#pragma unroll
+    for (int s = 0; s < STAGES - 1; ++s) {
+        if (s < kblocks) load(s);
+        cp_async_commit();
+    }
     for (int kb = 0; kb < kblocks; ++kb) {
-        const int cur = kb & 1;
-        const char* sA = smem + cur * STAGE;
+        cp_async_wait<STAGES - 2>();  // stage kb has landed
+        __syncthreads();              // ... for every thread, and stage kb-1 is no longer read
+        if (kb + STAGES - 1 < kblocks) load(kb + STAGES - 1);
+        cp_async_commit();
+        const char* sA = smem + (kb % STAGES) * STAGE;
         const char* sB = sA + BM * 128;
-        if (kb + 1 < kblocks) {
-            char* nA = smem + (cur ^ 1) * STAGE;
-            load_stage<BM, BN>(P, nA, nA + BM * 128, m0, n0, (long long)(kb + 1) * GBK);
-            cp_async_wait<1>();
-        } else {
-            cp_async_wait<0>();
-        }
-        __syncthreads();
 #pragma unroll
         for (int q = 0; q < GBK / 8; ++q) {
             double bf[NT][2];
@@ -147,14 +184,14 @@ __device__ void tile_item(const jlc_problem& P, int tm, int tn, char* smem) {
             for (int nt = 0; nt < NT; ++nt) {
                 const int c = warp_n * WN + nt * 8 + g;
 #pragma unroll
-                for (int j = 0; j < 2; ++j) bf[nt][j] = dmma::lds_b<true>(sB, dmma::phys_k<8>(q, t, j), c);
+                for (int j = 0; j < 2; ++j) bf[nt][j] = dmma::lds_b<BK>(sB, dmma::phys_k<8>(q, t, j), c);
             }
 #pragma unroll
             for (int mt = 0; mt < MT; ++mt) {
                 const int r = warp_m * WM + mt * 16 + g;
                 double af[4];
 #pragma unroll
-                for (int i = 0; i < 4; ++i) af[i] = dmma::lds_a<true>(sA, r + 8 * (i & 1), dmma::phys_k<8>(q, t, i >> 1));
+                for (int i = 0; i < 4; ++i) af[i] = dmma::lds_a<AK>(sA, r + 8 * (i & 1), dmma::phys_k<8>(q, t, i >> 1));
                 if (scale_a) {
 #pragma unroll
                     for (int i = 0; i < 4; ++i) af[i] *= P.alpha;
@@ -163,8 +200,9 @@ __device__ void tile_item(const jlc_problem& P, int tm, int tn, char* smem) {
                 for (int nt = 0; nt < NT; ++nt) dmma::mma_f64<8>(acc[mt][nt], af, bf[nt]);
             }
         }
-        __syncthreads();  // the stage is refilled two iterations later
     }
+    cp_async_wait<0>();
+    __syncthreads();  // the next item's prologue overwrites the stages
 
 #pragma unroll
     for (int mt = 0; mt < MT; ++mt)
@@ -184,6 +222,15 @@ __device__ void tile_item(const jlc_problem& P, int tm, int tn, char* smem) {
                     }
                 }
         }
+}
+
+template <int BM, int BN>
+__device__ void tile_dispatch(const jlc_problem& P, int tm, int tn, char* smem) {
+    const bool ak = P.layout_a == JLC_ROW_MAJOR, bk = P.layout_b == JLC_COL_MAJOR;
+    if (ak && !bk) tile_item<BM, BN, true, false>(P, tm, tn, smem);
+    else if (ak && bk) tile_item<BM, BN, true, true>(P, tm, tn, smem);
+    else if (!ak && !bk) tile_item<BM, BN, false, false>(P, tm, tn, smem);
+    else tile_item<BM, BN, false, true>(P, tm, tn, smem);
 }
 
 // A batch of tiny problems, one thread per output element.
@@ -222,8 +269,8 @@ __global__ void __launch_bounds__(THREADS, 3) grouped_kernel(const jlc_problem* 
             tiny_item(probs, tiny_ids, w.prob, w.tm);
         } else {
             const jlc_problem P = probs[w.prob];
-            if (w.kind == KIND_T64) tile_item<64, 64>(P, w.tm, w.tn, smem);
-            else tile_item<32, 32>(P, w.tm, w.tn, smem);
+            if (w.kind == KIND_T64) tile_dispatch<64, 64>(P, w.tm, w.tn, smem);
+            else tile_dispatch<32, 32>(P, w.tm, w.tn, smem);
         }
     }
 }
@@ -419,6 +466,7 @@ int upload(jlc_grouped_plan* pl, const std::vector<jlc_problem>& probs, const Wo
     }
     pl->nitems = (int)wl.items.size();
     int per_sm = 0;
+    cudaFuncSetAttribute(grouped_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, grouped_kernel, THREADS, SMEM_BYTES);
     if (per_sm < 1) per_sm = 1;
     pl->grid = std::max(1, std::min(pl->nitems, ctx->sm_count * per_sm));
