@@ -238,6 +238,7 @@ def run_ours(args):
     ctx.set_stream(stream.cuda_stream)
 
     peaks = ctx.measure_peaks()
+    int8_sustained = ctx.measure_int8_sustained(3.0)
     g = torch.Generator(device="cuda")
     g.manual_seed(20260604 + 7919 * rank)  # rank r owns row block r of the (world*size) x size product
     with torch.cuda.stream(stream):
@@ -383,11 +384,14 @@ def run_ours(args):
                          "gpu_launches": int(sl_launches)},
         "peaks_probed": {k: round(v, 2) for k, v in peaks.items()},
         "roofline": {"bound": "tensor", "kernel": "ozaki_gemm_kernel<CRT=true> (tcgen05 kind::i8)",
-                     "achieved": round(achieved_tops, 1), "peak": round(peaks["int8_tops"], 1),
-                     "unit": "TFLOP/s", "frac": round(achieved_tops / peaks["int8_tops"], 4),
+                     "achieved": round(achieved_tops, 1), "peak": round(int8_sustained, 1),
+                     "unit": "TFLOP/s", "frac": round(achieved_tops / int8_sustained, 4),
                      "traffic": traffic,
-                     "peak_source": "INT8 dense tcgen05 rate measured by the in-library probe in this run "
-                                    "(MEASURED_PEAKS.json has no INT8 figure)",
+                     "peak_source": "INT8 dense tcgen05 rate sustained over 3 s of back-to-back probe launches "
+                                    "(second half, at the power limit) in this run: the kernel is timed inside "
+                                    "a long step under sw_power_cap (MEASURED_PEAKS.json has no INT8 figure)",
+                     "peak_burst": round(peaks["int8_tops"], 1),
+                     "frac_of_burst": round(achieved_tops / peaks["int8_tops"], 4),
                      "bf16_probe_vs_measured_peaks": (round(peaks["bf16_tflops"] / mp["bf16_tflops"], 3)
                                                       if mp and mp.get("bf16_tflops") else None),
                      "ops_per_launch": int8_ops_per_launch},

@@ -205,6 +205,10 @@ JLC_API int jlc_check_fp64_bound_device(jlc_ctx* ctx, int layout_a, int layout_b
  * kernels: [0] FP64 on mma.sync .f64 (DMMA), [1] FP64 on DFMA, [2] INT8 on
  * tcgen05 (dense), [3] BF16 on tcgen05 (dense).  Takes about a second. */
 JLC_API int jlc_measure_peaks(jlc_ctx* ctx, double* out4);
+/* INT8 tcgen05 rate sustained over `seconds` of back-to-back probe launches
+ * (second half, after the power limiter settles), in TOP/s; new: the
+ * denominator for kernels timed inside long steps. */
+JLC_API int jlc_measure_int8_sustained(jlc_ctx* ctx, double seconds, double* tops);
 
 /* ---------------------------------------------------------------- adjoint */
 /* Reverse-mode derivative of C_out = alpha*A*B + beta*C_in (no reference

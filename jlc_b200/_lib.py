@@ -103,6 +103,7 @@ SIGNATURES = {
                                          _dp, _i64, _i64, _vp, _vp, ctypes.POINTER(_d), ctypes.POINTER(_d),
                                          ctypes.POINTER(_i64)]),
     "jlc_measure_peaks": (_i, [_vp, ctypes.POINTER(_d)]),
+    "jlc_measure_int8_sustained": (_i, [_vp, _d, ctypes.POINTER(_d)]),
     "jlc_dgemm_adjoint_device": (_i, [_vp, _i64, _i64, _i64, _d, _d, _dp, _i64, _dp, _i64, _dp, _i64, _dp, _i64,
                                       _dp, _i64, _dp, _i64, _dp, _dp, _dp, _i64, _i, _REP]),
     "jlc_grouped_plan_create": (_i, [_vp, _PROB, _i64, _i, _i, ctypes.POINTER(_vp)]),

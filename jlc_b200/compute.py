@@ -102,6 +102,13 @@ class Context:
         return {"fp64_dmma_tflops": out[0], "fp64_dfma_tflops": out[1], "int8_tops": out[2],
                 "bf16_tflops": out[3]}
 
+    def measure_int8_sustained(self, seconds: float = 3.0) -> float:
+        """INT8 tcgen05 TOP/s held over `seconds` of back-to-back probe launches
+        (rate over the second half, after the power limiter settles)."""
+        out = ctypes.c_double()
+        self.check(self.lib.jlc_measure_int8_sustained(self.h, float(seconds), ctypes.byref(out)))
+        return out.value
+
     def ozaki_crt_device(self, layout_a, layout_b, m, n, k, alpha, a_ptr, lda, b_ptr, ldb, beta, c_ptr, ldc,
                          moduli=0) -> dict:
         rep = L.Report()

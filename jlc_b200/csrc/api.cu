@@ -894,6 +894,15 @@ int jlc_measure_peaks(jlc_ctx* ctx, double* out4) {
     return finish_sync(ctx);
 }
 
+int jlc_measure_int8_sustained(jlc_ctx* ctx, double seconds, double* tops) {
+    if (!ctx || !tops || !(seconds > 0.0) || seconds > 60.0) return JLC_E_ARG;
+    cudaSetDevice(ctx->device);
+    int rc = measure_int8_sustained(ctx->sm_count, ctx->stream, ctx->d_status, seconds, tops, ctx->err,
+                                    sizeof(ctx->err));
+    if (rc) return rc;
+    return finish_sync(ctx);
+}
+
 int jlc_launch_count(jlc_ctx* ctx, int64_t* launches) {
     if (!ctx || !launches) return JLC_E_ARG;
     *launches = ctx->launches;

@@ -120,6 +120,8 @@ int launch_scale_copy(double* dst, long long ldd, const double* src, long long l
 
 // throughput probes (peaks.cu): out4 = {DMMA FP64, DFMA FP64, INT8 tcgen05, BF16 tcgen05} in T(FL)OP/s
 int measure_peaks(int sm_count, cudaStream_t st, int* status, double* out4, char* err, size_t errlen);
+int measure_int8_sustained(int sm_count, cudaStream_t st, int* status, double seconds, double* tops, char* err,
+                           size_t errlen);
 
 }  // namespace jlc
 

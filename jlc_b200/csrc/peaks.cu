@@ -160,4 +160,41 @@ int measure_peaks(int sm_count, cudaStream_t st, int* status, double* out4, char
     return JLC_OK;
 }
 
+// The INT8 tcgen05 rate held over `seconds` of back-to-back probe launches
+// (each ~45 ms): the rate over the second half, once the power limiter has
+// settled.  This is the denominator for kernels timed inside long steps.
+int measure_int8_sustained(int sm_count, cudaStream_t st, int* status, double seconds, double* tops, char* err,
+                           size_t errlen) {
+    const int smem = 48 * 1024 + 2048;
+    cudaFuncSetAttribute(umma_probe_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    const long long it_umma = 160000;
+    const double ops = (double)sm_count * it_umma * 4 * (2.0 * 128 * 256 * 32);
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    double total_ms = 0.0, late_ms = 0.0, late_ops = 0.0;
+    for (int i = 0; i < 1000 && total_ms < seconds * 1e3; ++i) {
+        cudaEventRecord(e0, st);
+        umma_probe_kernel<true><<<sm_count, 128, smem, st>>>(it_umma, status);
+        cudaEventRecord(e1, st);
+        cudaEventSynchronize(e1);
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        total_ms += ms;
+        if (total_ms > 0.5 * seconds * 1e3) {
+            late_ms += ms;
+            late_ops += ops;
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess || late_ms <= 0.0) {
+        snprintf(err, errlen, "sustained INT8 probe failed: %s", cudaGetErrorString(e));
+        return JLC_E_LAUNCH;
+    }
+    *tops = late_ops / (late_ms * 1e-3) / 1e12;
+    return JLC_OK;
+}
+
 }  // namespace jlc
