@@ -33,12 +33,15 @@ namespace jlc {
 namespace crt {
 
 constexpr int kMaxModuli = 15;
+// Accumulators handed to mod_pos satisfy |c| <= kAccBound (the GEMM caps the
+// k-length of one INT32 run so that sum |digit_a * digit_b| stays below it).
+constexpr int kAccBound = 1 << 28;
 
 struct Consts {
     int nmod, p, q, pad;
     int m[kMaxModuli];
-    uint32_t mu[kMaxModuli];    // floor(2^32 / m_l)
-    uint32_t off[kMaxModuli];   // 2^31 mod m_l
+    uint32_t mu[kMaxModuli];    // ceil(2^38 / m_l)
+    uint32_t bias[kMaxModuli];  // m_l * 2^21, a multiple of m_l above kAccBound
     uint32_t w[kMaxModuli][4];  // W_l, little-endian 32-bit limbs
     uint32_t M[4];              // M
     uint32_t halfM[4];          // floor(M / 2)
@@ -70,16 +73,18 @@ JLC_HD uint32_t mulhi32(uint32_t a, uint32_t b) {
 #endif
 }
 
-// c mod m in [0, m) with integer instructions only (the epilogue's reduction
-// of each INT32 accumulator): u = c + 2^31 is reduced by a Barrett step
-// (mu = floor(2^32 / m) underestimates u / m by less than one, so u - q m
-// lies in [0, 2m)), then off = 2^31 mod m is taken back off.
-JLC_HD int mod_pos(int c, uint32_t m, uint32_t mu, uint32_t off) {
-    const uint32_t u = (uint32_t)c ^ 0x80000000u;
-    uint32_t r = u - mulhi32(u, mu) * m;
-    r = r >= m ? r - m : r;
-    const int t = (int)r - (int)off;
-    return t < 0 ? t + (int)m : t;
+// c mod m in [0, m) for |c| <= kAccBound, with four integer instructions
+// (the epilogue's reduction of each INT32 accumulator).  u = c + bias is
+// non-negative and below 1.5 * 2^29 (bias = m * 2^21 <= 2^29, congruent to
+// 0).  With mu = ceil(2^38 / m) = (2^38 + e) / m, 0 <= e < m:
+//     u * mu / 2^38 = u / m + u * e / (m * 2^38),
+// and u * e < 2^30 * 2^8 = 2^38 keeps the excess below 1/m, so it never
+// carries the fractional part r/m <= (m-1)/m past the next integer:
+// floor(u * mu / 2^38) = floor(u / m) exactly, and u - q m is the residue.
+JLC_HD int mod_pos(int c, uint32_t m, uint32_t mu, uint32_t bias) {
+    const uint32_t u = (uint32_t)c + bias;
+    const uint32_t q = mulhi32(u, mu) >> 6;
+    return (int)(u - q * m);
 }
 
 // exact float of an integer below 2^23 (no conversion instruction)
@@ -245,8 +250,8 @@ inline void build_consts(int nmod, int p, int q, const int* moduli, Consts& c) {
     for (int l = 0; l < nmod; ++l) {
         const int m = moduli[l];
         c.m[l] = m;
-        c.mu[l] = (uint32_t)((1ull << 32) / (unsigned long long)m);
-        c.off[l] = (uint32_t)((1ull << 31) % (unsigned long long)m);
+        c.mu[l] = (uint32_t)(((1ull << 38) + (unsigned long long)m - 1) / (unsigned long long)m);
+        c.bias[l] = (uint32_t)m << 21;
         const u128 Ml = M / (u128)m;
         const int rem = (int)(Ml % (u128)m);
         int inv = 1;

@@ -82,7 +82,7 @@ constexpr int THREADS = 320;  // warp 0 TMA, warp 1 MMA, warps 2..9 epilogue
 constexpr int EPI_WARPS = 8;
 constexpr int TMEM_COLS = 512;
 constexpr int GROUP_CAP = 1040;      // k-blocks per INT32 run: 1040*128*127*127 < 2^31
-constexpr int GROUP_CAP_CRT = 1023;  // residues up to 128 in magnitude: 1023*128*128*128 < 2^31
+constexpr int GROUP_CAP_CRT = 128;  // residues up to 128 in magnitude: 128*128*128*128 = 2^28 (crt::kAccBound)
 constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024 + 256;
 constexpr int SCRATCH_DOUBLES = BM * BN;  // per CTA, slice scheme (FP64 running sums)
 constexpr int MAX_MODULI = 15;            // product of 15 moduli < 2^123 = three 41-bit digits
@@ -311,6 +311,9 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(THREADS, 1)
         const int row = quarter * 32 + lane;
         const bool c_vec = ((reinterpret_cast<uintptr_t>(p.C) & 15) == 0) && ((p.ldc & 1) == 0);
         const double out_scale = p.epi_scale == 1.0 ? p.alpha : p.alpha * p.epi_scale;
+        // decided once: FP64 issue is starved while the MMAs run, so the
+        // common alpha = 1, beta = 0 case issues no FP64 arithmetic at all
+        const bool do_scale = out_scale != 1.0, beta0 = p.beta == 0.0;
         double dot_acc = 0.0;
         uint32_t* crt_base = reinterpret_cast<uint32_t*>(p.scratch) + (size_t)blockIdx.x * 2 * MAX_MODULI * CRT_SLOT_WORDS;
         // writes 32 columns of row grow from tile column c0; out holds alpha-free values
@@ -323,14 +326,15 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(THREADS, 1)
                 for (int j = 0; j < 32; ++j)
                     if (j < ncols) dot_acc = fma(drow[j], p.alpha * out[j], dot_acc);
             }
+            if (do_scale)
 #pragma unroll
-            for (int j = 0; j < 32; ++j) out[j] *= out_scale;
+                for (int j = 0; j < 32; ++j) out[j] *= out_scale;
             if (c_vec && ncols == 32) {
                 double2* c2 = reinterpret_cast<double2*>(crow);
 #pragma unroll
                 for (int j = 0; j < 16; ++j) {
                     double2 v = make_double2(out[2 * j], out[2 * j + 1]);
-                    if (p.beta != 0.0) {
+                    if (!beta0) {
                         const double2 o = c2[j];
                         v.x = fma(p.beta, o.x, v.x);
                         v.y = fma(p.beta, o.y, v.y);
@@ -340,7 +344,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(THREADS, 1)
             } else {
 #pragma unroll
                 for (int j = 0; j < 32; ++j)
-                    if (j < ncols) crow[j] = (p.beta == 0.0) ? out[j] : fma(p.beta, crow[j], out[j]);
+                    if (j < ncols) crow[j] = beta0 ? out[j] : fma(p.beta, crow[j], out[j]);
             }
         };
         // writes 4 columns of row grow from tile column c; out holds alpha-free values
@@ -354,14 +358,15 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(THREADS, 1)
                 for (int j = 0; j < 4; ++j)
                     if (j < ncols) dot_acc = fma(drow[j], p.alpha * out[j], dot_acc);
             }
+            if (do_scale)
 #pragma unroll
-            for (int j = 0; j < 4; ++j) out[j] *= out_scale;
+                for (int j = 0; j < 4; ++j) out[j] *= out_scale;
             if (c_vec && ncols == 4) {
                 double2* c2 = reinterpret_cast<double2*>(crow);
 #pragma unroll
                 for (int j = 0; j < 2; ++j) {
                     double2 v = make_double2(out[2 * j], out[2 * j + 1]);
-                    if (p.beta != 0.0) {
+                    if (!beta0) {
                         const double2 o = c2[j];
                         v.x = fma(p.beta, o.x, v.x);
                         v.y = fma(p.beta, o.y, v.y);
@@ -371,7 +376,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(THREADS, 1)
             } else {
 #pragma unroll
                 for (int j = 0; j < 4; ++j)
-                    if (j < ncols) crow[j] = (p.beta == 0.0) ? out[j] : fma(p.beta, crow[j], out[j]);
+                    if (j < ncols) crow[j] = beta0 ? out[j] : fma(p.beta, crow[j], out[j]);
             }
         };
         // Residue scheme: a finished tile's Chinese remainder reconstruction is
@@ -481,11 +486,11 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(THREADS, 1)
                             // runs of the same modulus), one byte per element in
                             // slot d of the scratch, laid out [slot][col/4][row]
                             const int m = p.crt.m[d];
-                            const uint32_t mu = p.crt.mu[d], off = p.crt.off[d];
+                            const uint32_t mu = p.crt.mu[d], bias = p.crt.bias[d];
                             uint32_t* my = tile_slots + (size_t)d * CRT_SLOT_WORDS + (size_t)(c0 >> 2) * BM + row;
                             int res[32];
 #pragma unroll
-                            for (int j = 0; j < 32; ++j) res[j] = crt::mod_pos((int)r[j], (uint32_t)m, mu, off);
+                            for (int j = 0; j < 32; ++j) res[j] = crt::mod_pos((int)r[j], (uint32_t)m, mu, bias);
                             if (gi > 0) {
 #pragma unroll
                                 for (int w4 = 0; w4 < 8; ++w4) {

@@ -40,7 +40,7 @@ int crt_mod_batch(int l, int n, const int* c, int* out) {
     if (l < 0 || l > 14) return -1;
     jlc::crt::Consts k;
     jlc::crt::build_consts(15, 0, 0, kModuli, k);
-    for (int i = 0; i < n; ++i) out[i] = jlc::crt::mod_pos(c[i], (uint32_t)k.m[l], k.mu[l], k.off[l]);
+    for (int i = 0; i < n; ++i) out[i] = jlc::crt::mod_pos(c[i], (uint32_t)k.m[l], k.mu[l], k.bias[l]);
     return 0;
 }
 }

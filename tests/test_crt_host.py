@@ -7,7 +7,8 @@ against Python's arbitrary-precision integers:
   * reconstruct(residues of x) == the correctly rounded double of x * 2^s for
     |x| < M/2, every modulus count 2..15, values at 0, near +-M/2 and random;
   * the packed four-element path gives the same bits;
-  * the Barrett reduction of INT32 accumulators equals Python's c mod m.
+  * the reduction of INT32 accumulators (|c| <= 2^28, the bound the GEMM's
+    run length keeps) equals Python's c mod m.
 """
 import ctypes
 import math
@@ -116,8 +117,13 @@ def test_out_of_range_scales(harness):
 @pytest.mark.parametrize("l", list(range(15)))
 def test_barrett_reduction_of_accumulators(harness, l):
     rng = np.random.default_rng(l)
-    c = np.concatenate([rng.integers(-2**31, 2**31, 20000, dtype=np.int64),
-                        [-2**31, 2**31 - 1, 0, -1, 1, MODULI[l], -MODULI[l]]]).astype(np.int32)
+    bound = 2**28
+    m = MODULI[l]
+    edges = [-bound, bound, 0, -1, 1, m, -m, m - 1, -(m - 1), bound - 1, -(bound - 1)]
+    # the multiples of m and their neighbours near both ends of the range
+    for q in (bound // m, -(bound // m)):
+        edges += [q * m - 1, q * m, q * m + 1]
+    c = np.concatenate([rng.integers(-bound, bound + 1, 20000, dtype=np.int64), edges]).astype(np.int32)
     out = np.zeros_like(c)
     assert harness.crt_mod_batch(l, c.size, _ptr(c, ctypes.c_int), _ptr(out, ctypes.c_int)) == 0
     np.testing.assert_array_equal(out, np.mod(c.astype(np.int64), MODULI[l]))
