@@ -185,6 +185,11 @@ JLC_API int jlc_set_profiling(jlc_ctx* ctx, int on);
 /* Synchronises, then writes up to max (phase, milliseconds) records in launch
  * order, clears them and returns how many were written (or a JLC_E_* code). */
 JLC_API int jlc_profile_collect(jlc_ctx* ctx, int* phases, double* ms, int max);
+/* Same records as a timeline: start and end of each phase in milliseconds
+ * from the start of the first record (phases on the copy streams of the host
+ * entry included), then cleared like jlc_profile_collect.  New: no
+ * reference counterpart; used to read the host-entry pipeline's overlap. */
+JLC_API int jlc_profile_timeline(jlc_ctx* ctx, int* phases, double* start_ms, double* end_ms, int max);
 /* Number of kernels this context has launched since jlc_init. */
 JLC_API int jlc_launch_count(jlc_ctx* ctx, int64_t* launches);
 

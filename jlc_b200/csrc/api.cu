@@ -184,13 +184,22 @@ int run_device(jlc_ctx* ctx, const GemmDesc& g0, int precision, int slices, jlc_
         return launch_gemv(v, ctx->ws.ptr, ctx->stream, ctx->sm_count, ctx->err, sizeof(ctx->err));
     }
     // a row block of a pipelined product follows the whole product's choice
-    const bool ozaki = use_ozaki(precision, g.ws_m > g.m ? g.ws_m : g.m, g.n, g.k);
+    const long long whole_m = g.ws_m > g.m ? g.ws_m : g.m;
+    const bool ozaki = use_ozaki(precision, whole_m, g.n, g.k);
     // AUTO takes the residue scheme: fewer INT8 products for the same bound
     const bool crt = ozaki && precision != JLC_PREC_OZAKI;
+    // Small products split k across CTAs, partials in the workspace (after
+    // the Ozaki split data when the FP64 kernel is the gated fallback, so
+    // that its split choice, and with it its sums, match the native route).
+    const int ksplit = g.dot_mat ? 1 : dmma_splitk(whole_m, g.n, g.k, ctx->sm_count);
+    const size_t splitk_bytes = dmma_splitk_bytes(g.m, g.n, ksplit);
+    size_t splitk_off = 0;
     int rc = JLC_OK;
     if (ozaki) {
         const int s = slices > 0 ? slices : (crt ? ozaki_crt_auto_moduli(g.k) : auto_slices(g.k));
-        size_t need = ozaki_workspace_bytes(g.ws_m > g.m ? g.ws_m : g.m, g.n, g.k, s, ctx->sm_count, crt);
+        size_t need = ozaki_workspace_bytes(whole_m, g.n, g.k, s, ctx->sm_count, crt);
+        splitk_off = (need + 255) / 256 * 256;
+        if (splitk_bytes) need = splitk_off + splitk_bytes;
         rc = workspace_reserve(ctx->ws, need, ctx->err, sizeof(ctx->err));
         if (rc) return rc;
         {
@@ -241,12 +250,17 @@ int run_device(jlc_ctx* ctx, const GemmDesc& g0, int precision, int slices, jlc_
         g.ldb = ld;
     }
     if (!ozaki && rep) rep->kernel = JLC_KERNEL_DMMA;
+    if (!ozaki && splitk_bytes > 0) {
+        rc = workspace_reserve(ctx->ws, splitk_bytes, ctx->err, sizeof(ctx->err));
+        if (rc) return rc;
+    }
     // After an Ozaki launch the FP64 kernel is gated on the split's
     // non-finite flag: it only runs when Inf/NaN made slicing impossible.
     Phase ph(ctx, ozaki ? JLC_PHASE_FP64_GATED : JLC_PHASE_DMMA);
     ctx->launches += 1;
     return launch_dgemm_dmma(g, ctx->stream, ctx->sm_count, ctx->d_status, ozaki ? ctx->d_flags : nullptr,
-                             ctx->dmma_k, ctx->err, sizeof(ctx->err));
+                             ctx->dmma_k, ctx->err, sizeof(ctx->err), ksplit,
+                             splitk_bytes ? static_cast<char*>(ctx->ws.ptr) + splitk_off : nullptr, splitk_bytes);
 }
 
 int finish_sync(jlc_ctx* ctx) {
@@ -758,6 +772,25 @@ int jlc_profile_collect(jlc_ctx* ctx, int* phases, double* ms, int max) {
         if (e != cudaSuccess) return cuda_err(ctx, e, "profile event");
         phases[i] = ctx->rec_phase[i];
         ms[i] = t;
+    }
+    ctx->nrec = 0;
+    return n;
+}
+
+int jlc_profile_timeline(jlc_ctx* ctx, int* phases, double* start_ms, double* end_ms, int max) {
+    if (!ctx || max < 0 || (max > 0 && (!phases || !start_ms || !end_ms))) return JLC_E_ARG;
+    cudaSetDevice(ctx->device);
+    cudaError_t e = cudaDeviceSynchronize();  // records may sit on the copy streams
+    if (e != cudaSuccess) return cuda_err(ctx, e, "profile synchronize");
+    const int n = ctx->nrec < max ? ctx->nrec : max;
+    for (int i = 0; i < n; ++i) {
+        float t0 = 0.f, t1 = 0.f;
+        e = cudaEventElapsedTime(&t0, ctx->rec_ev[0], ctx->rec_ev[2 * i]);
+        if (e == cudaSuccess) e = cudaEventElapsedTime(&t1, ctx->rec_ev[0], ctx->rec_ev[2 * i + 1]);
+        if (e != cudaSuccess) return cuda_err(ctx, e, "profile event");
+        phases[i] = ctx->rec_phase[i];
+        start_ms[i] = t0;
+        end_ms[i] = t1;
     }
     ctx->nrec = 0;
     return n;

@@ -22,6 +22,12 @@
 // Register budget: the launch gives 384 threads x 168 = 64512 registers;
 // after the split 128 x 40 + 256 x 224 = 62464 are in use.
 //
+// Split-K (small products, fewer tiles than half the SMs): the k-blocks of a
+// tile are cut into ksplit contiguous parts, one work unit each.  A unit's
+// partial tile goes to workspace; the CTA whose unit arrives last at the
+// tile's counter sums the parts in index order (deterministic whatever the
+// arrival order) and runs the normal epilogue.  No CTA waits for another.
+//
 // K permutation: inside each k-step the logical k index of the mma fragment
 // layout is remapped to a physical column of the shared tile so that the four
 // rows a warp reads per fragment fall into different 64-byte halves of the
@@ -62,6 +68,9 @@ struct Params {
     double* C;
     long long ldc;
     int tiles_m, tiles_n, num_tiles, k_blocks;
+    int ksplit;         // k parts per tile (1: no split)
+    double* part;       // ksplit > 1: BM*BN partial sums per (tile, part)
+    int* counters;      // ksplit > 1: arrivals per tile, zero at launch
     int* status;
     const int* gate;  // when non-null the kernel runs only if gate[0] or gate[1] is set
 };
@@ -109,11 +118,15 @@ __global__ void __launch_bounds__(THREADS, 1)
             uint32_t phase = 0;
             uint32_t armed = 0, last_parity = 0;  // per-stage bit sets, for the drain
             bool ok = true;
-            for (int tile = blockIdx.x; tile < p.num_tiles && ok; tile += gridDim.x) {
+            const int num_units = p.num_tiles * p.ksplit;
+            for (int unit = blockIdx.x; unit < num_units && ok; unit += gridDim.x) {
+                const int tile = unit % p.num_tiles, part = unit / p.num_tiles;
                 int tm, tn;
                 tile_coords(tile, p.tiles_m, p.tiles_n, RASTER_GROUP, tm, tn);
                 const int m0 = tm * BM, n0 = tn * BN;
-                for (int kb = 0; kb < p.k_blocks; ++kb) {
+                const int kb0 = (int)((long long)part * p.k_blocks / p.ksplit);
+                const int kb1 = (int)((long long)(part + 1) * p.k_blocks / p.ksplit);
+                for (int kb = kb0; kb < kb1; ++kb) {
                     if (!mbar_wait(&empty[stage], phase ^ 1u, p.status)) {
                         ok = false;
                         break;
@@ -163,9 +176,16 @@ __global__ void __launch_bounds__(THREADS, 1)
     constexpr int BREG = MMA_K / 4;  // doubles of B per n8 tile per step
 
     bool failed = false;
-    for (int tile = blockIdx.x; tile < p.num_tiles && !failed; tile += gridDim.x) {
-        int tm, tn;
-        tile_coords(tile, p.tiles_m, p.tiles_n, RASTER_GROUP, tm, tn);
+    const int num_units = p.num_tiles * p.ksplit;
+    for (int unit = blockIdx.x; unit < num_units && !failed; unit += gridDim.x) {
+        // only unit and the k range stay live across the main loop; the tile
+        // coordinates are derived again for the epilogue
+        int kb0, kb1;
+        {
+            const int part = unit / p.num_tiles;
+            kb0 = (int)((long long)part * p.k_blocks / p.ksplit);
+            kb1 = (int)((long long)(part + 1) * p.k_blocks / p.ksplit);
+        }
         double acc[MT][NT][4];
 #pragma unroll
         for (int i = 0; i < MT; ++i)
@@ -174,7 +194,7 @@ __global__ void __launch_bounds__(THREADS, 1)
 #pragma unroll
                 for (int e = 0; e < 4; ++e) acc[i][j][e] = 0.0;
 
-        for (int kb = 0; kb < p.k_blocks; ++kb) {
+        for (int kb = kb0; kb < kb1; ++kb) {
             if (!mbar_wait(&full[stage], phase, p.status)) {
                 failed = true;  // status word reports it; still reach the reduction barrier below
                 break;
@@ -218,6 +238,49 @@ __global__ void __launch_bounds__(THREADS, 1)
         }
 
         if (failed) break;
+        const int tile = unit % p.num_tiles, part = unit / p.num_tiles;
+        int tm, tn;
+        tile_coords(tile, p.tiles_m, p.tiles_n, RASTER_GROUP, tm, tn);
+        if (p.ksplit > 1) {
+            // publish this part, count it; the last part of the tile to arrive
+            // sums all parts in index order and writes C
+            const int ct = threadIdx.x - PRODUCER_WARPS * 32;  // consumer thread 0..255
+            double* mine = p.part + (size_t)(tile * p.ksplit + part) * (BM * BN);
+#pragma unroll
+            for (int mt = 0; mt < MT; ++mt)
+#pragma unroll
+                for (int nt = 0; nt < NT; ++nt)
+#pragma unroll
+                    for (int e = 0; e < 4; ++e) mine[((mt * NT + nt) * 4 + e) * (MMA_WARPS * 32) + ct] = acc[mt][nt][e];
+            __threadfence();
+            int* last_flag = reinterpret_cast<int*>(empty + STAGES);
+            asm volatile("bar.sync 2, %0;" ::"n"(MMA_WARPS * 32) : "memory");
+            if (ct == 0) *last_flag = atomicAdd(&p.counters[tile], 1) == p.ksplit - 1;
+            asm volatile("bar.sync 2, %0;" ::"n"(MMA_WARPS * 32) : "memory");
+            // (the next unit's write of the flag comes after its first barrier,
+            // which every consumer reaches only after reading this one)
+            if (*last_flag == 0) continue;
+            __threadfence();
+            // parts 0, 1, ... summed in that order, every one (this CTA's
+            // included) read back from L2: the same additions whichever part
+            // arrived last
+            const double* base = p.part + (size_t)tile * p.ksplit * (BM * BN) + ct;
+#pragma unroll
+            for (int mt = 0; mt < MT; ++mt)
+#pragma unroll
+                for (int nt = 0; nt < NT; ++nt)
+#pragma unroll
+                    for (int e = 0; e < 4; ++e) acc[mt][nt][e] = __ldcg(base + ((mt * NT + nt) * 4 + e) * (MMA_WARPS * 32));
+            for (int q = 1; q < p.ksplit; ++q) {
+                const double* pq = base + (size_t)q * (BM * BN);
+#pragma unroll
+                for (int mt = 0; mt < MT; ++mt)
+#pragma unroll
+                    for (int nt = 0; nt < NT; ++nt)
+#pragma unroll
+                        for (int e = 0; e < 4; ++e) acc[mt][nt][e] += __ldcg(pq + ((mt * NT + nt) * 4 + e) * (MMA_WARPS * 32));
+            }
+        }
         // fused epilogue: C = epi_scale*acc + beta * C_old (C_old not read when
         // beta == 0); optional dot with dot_mat for the adjoint's d(alpha)
         const int row0 = tm * BM + warp_m * WM;
@@ -282,8 +345,42 @@ bool dmma_operand_ok(const void* ptr, long long ld) {
     return (reinterpret_cast<uintptr_t>(ptr) % 16 == 0) && ((ld * 8) % 16 == 0) && ld > 0;
 }
 
+// k parts per tile for an m x n x k product (1: no split).  A row block of a
+// pipelined product passes the whole product's m, so that every block sums
+// in the same order as the single-shot call.
+int dmma_splitk(long long m, long long n, long long k, int sm_count) {
+    using namespace dmma;
+    const long long tiles = ((m + BM - 1) / BM) * ((n + BN - 1) / BN);
+    const long long kbl = (k + BK - 1) / BK;
+    // wave balance of the persistent grid: units / (waves * SMs); a split must
+    // gain 5 % of it, keep >= 16 k-blocks (256 k) per part and <= 8 waves
+    auto balance = [&](long long units) {
+        const long long waves = (units + sm_count - 1) / sm_count;
+        return (double)units / (double)(waves * sm_count);
+    };
+    int best = 1;
+    double best_b = balance(tiles);
+    for (int s = 2; s <= 8; ++s) {
+        if (kbl / s < 16 || tiles * s > 8LL * sm_count) break;
+        const double b = balance(tiles * s);
+        if (b > best_b * 1.05) {
+            best = s;
+            best_b = b;
+        }
+    }
+    return best;
+}
+
+size_t dmma_splitk_bytes(long long m, long long n, int ksplit) {
+    using namespace dmma;
+    if (ksplit < 2) return 0;
+    const long long tiles = ((m + BM - 1) / BM) * ((n + BN - 1) / BN);
+    const int s = ksplit;
+    return (size_t)(tiles * s) * BM * BN * sizeof(double) + (size_t)tiles * sizeof(int);
+}
+
 int launch_dgemm_dmma(const GemmDesc& g, cudaStream_t st, int sm_count, int* status, const int* gate,
-                      int mma_k, char* err, size_t errlen) {
+                      int mma_k, char* err, size_t errlen, int ksplit, void* splitk_ws, size_t splitk_ws_bytes) {
     using namespace dmma;
     if (!dmma_operand_ok(g.a, g.lda) || !dmma_operand_ok(g.b, g.ldb)) {
         snprintf(err, errlen, "DMMA kernel needs 16-byte aligned A/B and even leading dimensions");
@@ -326,7 +423,27 @@ int launch_dgemm_dmma(const GemmDesc& g, cudaStream_t st, int sm_count, int* sta
     p.k_blocks = (int)((g.k + BK - 1) / BK);
     p.status = status;
     p.gate = gate;
-    const int grid = p.num_tiles < sm_count ? p.num_tiles : sm_count;
+    p.ksplit = 1;
+    p.part = nullptr;
+    p.counters = nullptr;
+    // split-K needs the caller's workspace; the adjoint's fused dot keeps one
+    // unit per tile (its per-CTA partial dots must not depend on arrival order)
+    if (ksplit > 1 && splitk_ws && !g.dot_mat) {
+        const int s = ksplit < p.k_blocks ? ksplit : p.k_blocks;
+        const size_t need = dmma_splitk_bytes(g.m, g.n, s);
+        if (s > 1 && need <= splitk_ws_bytes) {
+            p.ksplit = s;
+            p.part = static_cast<double*>(splitk_ws);
+            p.counters = reinterpret_cast<int*>(static_cast<char*>(splitk_ws) +
+                                                (size_t)p.num_tiles * s * BM * BN * sizeof(double));
+            if (cudaMemsetAsync(p.counters, 0, (size_t)p.num_tiles * sizeof(int), st) != cudaSuccess) {
+                snprintf(err, errlen, "split-K counters: %s", cudaGetErrorString(cudaGetLastError()));
+                return JLC_E_LAUNCH;
+            }
+        }
+    }
+    const int units = p.num_tiles * p.ksplit;
+    const int grid = units < sm_count ? units : sm_count;
 
 #define JLC_DMMA_DISPATCH(MK)                                                     \
     if (a_k && b_k) rc = launch_variant<true, true, MK>(ma, mb, p, grid, st);      \

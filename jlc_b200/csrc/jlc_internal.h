@@ -68,8 +68,13 @@ bool dmma_operand_ok(const void* ptr, long long ld);
 // FP64 DMMA tiled GEMM.  A/B must be 16-byte aligned with even leading
 // dimensions.  gate != nullptr: the kernel only runs if gate[0] or gate[1] is
 // nonzero (the Ozaki split's non-finite flags for A and B).
+// ksplit > 1 with splitk_ws of at least dmma_splitk_bytes(m, n, ksplit):
+// split-K over ksplit parts; otherwise every tile is one work unit.
 int launch_dgemm_dmma(const GemmDesc& g, cudaStream_t st, int sm_count, int* status, const int* gate, int mma_k,
-                      char* err, size_t errlen);
+                      char* err, size_t errlen, int ksplit = 1, void* splitk_ws = nullptr,
+                      size_t splitk_ws_bytes = 0);
+int dmma_splitk(long long m, long long n, long long k, int sm_count);
+size_t dmma_splitk_bytes(long long m, long long n, int ksplit);
 
 // y[i*incy] = alpha * sum_p M(i,p) x[p*incx] + beta * y[i*incy], M(i,p) = mat[i*rs + p*cs]
 // with rs == 1 or cs == 1.  scratch: ceil-split partial sums for the rs == 1 form.

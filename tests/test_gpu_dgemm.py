@@ -326,3 +326,35 @@ def test_device_entry_on_caller_stream(ctx, oracle):
     finally:
         ctx.set_stream(None)
     assert_fp64_bound("caller stream", C.cpu().numpy(), A.cpu().numpy(), B.cpu().numpy(), None, 1.0, 0.0)
+
+
+@pytest.mark.parametrize("m,n,k,alpha,beta", [
+    (1024, 1024, 1024, 1.5, 0.5),   # 64 tiles: two k parts
+    (300, 200, 3000, 1.0, 0.0),     # 6 tiles, ragged edges: eight k parts
+    (512, 768, 2000, -0.75, 2.0),   # 24 tiles, parts of uneven length
+    (128, 128, 4096, 1.0, -1.0),    # one tile
+])
+def test_split_k_small_products(ctx, oracle, m, n, k, alpha, beta):
+    """Products with fewer tiles than half the SMs split k across CTAs; the
+    last part to arrive sums the parts in index order: inside the FP64 bound,
+    and bitwise the same on every run (and through the host entry)."""
+    import torch
+    A = oracle.uniform((m, k), 71)
+    B = oracle.uniform((k, n), 72)
+    C = oracle.uniform((m, n), 73)
+    dA, dB = torch.from_numpy(A).cuda(), torch.from_numpy(B).cuda()
+    runs = []
+    for _ in range(3):
+        dC = torch.from_numpy(C.copy()).cuda()
+        rep = ctx.dgemm_device(0, 0, m, n, k, alpha, dA.data_ptr(), k, dB.data_ptr(), n, beta, dC.data_ptr(), n,
+                               precision=0)
+        ctx.synchronize()
+        assert rep["kernel"] == 1
+        runs.append(dC.cpu().numpy())
+    for r in runs[1:]:
+        np.testing.assert_array_equal(r, runs[0])
+    rows, cols = oracle.sample_entries(m, n, 2048, 5)
+    assert_fp64_bound(f"split-K {m}x{n}x{k}", runs[0], A, B, C, alpha, beta, rows=rows, cols=cols)
+    host = C.copy()
+    ctx.dgemm(0, 0, m, n, k, alpha, A, k, B, n, beta, host, n, precision=0)
+    np.testing.assert_array_equal(host, runs[0])
