@@ -98,6 +98,7 @@ SIGNATURES = {
     "jlc_device_status": (_i, [_vp]),
     "jlc_set_profiling": (_i, [_vp, _i]),
     "jlc_profile_collect": (_i, [_vp, ctypes.POINTER(_i), ctypes.POINTER(_d), _i]),
+    "jlc_profile_timeline": (_i, [_vp, ctypes.POINTER(_i), ctypes.POINTER(_d), ctypes.POINTER(_d), _i]),
     "jlc_launch_count": (_i, [_vp, ctypes.POINTER(_i64)]),
     "jlc_check_fp64_bound_device": (_i, [_vp, _i, _i, _i64, _i64, _i64, _d, _dp, _i64, _dp, _i64, _d, _dp, _i64,
                                          _dp, _i64, _i64, _vp, _vp, ctypes.POINTER(_d), ctypes.POINTER(_d),

@@ -83,6 +83,17 @@ class Context:
             self.check(n)
         return [(L.PHASES.get(phases[i], str(phases[i])), ms[i]) for i in range(n)]
 
+    def profile_timeline(self, max_records: int = 4096):
+        """[(phase name, start ms, end ms), ...] since the last collect, times
+        from the start of the first record (synchronises the device)."""
+        phases = (ctypes.c_int * max_records)()
+        t0 = (ctypes.c_double * max_records)()
+        t1 = (ctypes.c_double * max_records)()
+        n = self.lib.jlc_profile_timeline(self.h, phases, t0, t1, max_records)
+        if n < 0:
+            self.check(n)
+        return [(L.PHASES.get(phases[i], str(phases[i])), t0[i], t1[i]) for i in range(n)]
+
     def check_fp64_bound_device(self, layout_a, layout_b, m, n, k, alpha, a_ptr, lda, b_ptr, ldb, beta, cin_ptr,
                                 ldc_in, cout_ptr, ldc_out, rows, cols) -> dict:
         """Double-double check of sampled entries of a finished device GEMM."""
