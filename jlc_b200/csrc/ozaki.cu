@@ -389,27 +389,42 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(THREADS, 1)
         int local_tile = 0;
         const int runs_per_tile = CRT ? p.crt.nmod * ((p.KB + Runs<CRT>::cap - 1) / Runs<CRT>::cap) : 1;
         const int per_run = (RECON_GROUPS + runs_per_tile - 1) / runs_per_tile;
-        auto recon_group = [&](int g) {
-            if (!pend_row_ok) return;
+        // Reconstruction of groups [g0, g1) of the pending tile, software
+        // pipelined: the next group's residue words and column exponents are
+        // in flight while the current group is reconstructed.
+        auto recon_load = [&](int g, uint32_t(&w)[MAX_MODULI], int(&sc)[4]) {
             const CrtConsts& cc = p.crt;
             const int c = half * (BN / 2) + 4 * g;
             const uint32_t* gbase = pend_slots + (size_t)(c >> 2) * BM + row;
-            // every residue word of the group is requested before any is used
-            uint32_t cur[MAX_MODULI];
 #pragma unroll
-            for (int l = 0; l < MAX_MODULI; ++l) cur[l] = l < cc.nmod ? gbase[(size_t)l * CRT_SLOT_WORDS] : 0u;
-            int scale[4];
+            for (int l = 0; l < MAX_MODULI; ++l) w[l] = l < cc.nmod ? gbase[(size_t)l * CRT_SLOT_WORDS] : 0u;
 #pragma unroll
             for (int e = 0; e < 4; ++e) {
                 const int col = pend_n0 + c + e;
-                scale[e] = pend_ei + (col < p.N ? p.eb[col] : 0) - cc.p - cc.q;
+                sc[e] = pend_ei + (col < p.N ? p.eb[col] : 0) - cc.p - cc.q;
             }
-            double out[4];
-            crt::reconstruct4(cc, cur, scale, out);
+        };
+        auto recon_range = [&](int g0, int g1) {
+            if (!pend_row_ok || g0 >= g1) return;
+            uint32_t w[MAX_MODULI];
+            int sc[4];
+            recon_load(g0, w, sc);
+            for (int g = g0; g < g1; ++g) {
+                uint32_t cur[MAX_MODULI];
+                int scur[4];
 #pragma unroll
-            for (int e = 0; e < 4; ++e)
-                if (pend_n0 + c + e >= p.N) out[e] = 0.0;
-            write_out4(pend_grow, pend_n0, c, out);
+                for (int l = 0; l < MAX_MODULI; ++l) cur[l] = w[l];
+#pragma unroll
+                for (int e = 0; e < 4; ++e) scur[e] = sc[e];
+                if (g + 1 < g1) recon_load(g + 1, w, sc);
+                double out[4];
+                crt::reconstruct4(p.crt, cur, scur, out);
+                const int c = half * (BN / 2) + 4 * g;
+#pragma unroll
+                for (int e = 0; e < 4; ++e)
+                    if (pend_n0 + c + e >= p.N) out[e] = 0.0;
+                write_out4(pend_grow, pend_n0, c, out);
+            }
         };
         uint32_t gcount = 0;
         bool ok = true;
@@ -519,7 +534,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(THREADS, 1)
                         // that completes it within this tile's runs
                         if (ok) {
                             const int todo = min(pend_left, per_run);
-                            for (int i = 0; i < todo; ++i) recon_group(RECON_GROUPS - pend_left + i);
+                            recon_range(RECON_GROUPS - pend_left, RECON_GROUPS - pend_left + todo);
                             pend_left -= todo;
                         }
                         if (last) {
@@ -541,8 +556,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(THREADS, 1)
             ++local_tile;
         }
         if constexpr (CRT) {
-            if (ok)
-                for (; pend_left > 0; --pend_left) recon_group(RECON_GROUPS - pend_left);
+            if (ok) recon_range(RECON_GROUPS - pend_left, RECON_GROUPS);
         }
         if (p.dot_partials) {
             // deterministic CTA reduction over the epilogue warps (named barrier 1)
