@@ -253,8 +253,13 @@ typedef struct jlc_grouped_plan jlc_grouped_plan;
  * Hessenberg panel and trailing updates, HouseholderQR.java:167-210,
  * BlockedHessenbergQR.java:277-345) with one persistent launch.  The plan
  * copies the problem table to the device; later runs reuse the same device
- * pointers (update the data in place and run again).  precision must be
- * JLC_PREC_NATIVE or JLC_PREC_AUTO. */
+ * pointers (update the data in place and run again).  precision:
+ * JLC_PREC_NATIVE / JLC_PREC_AUTO run FP64 tiles; JLC_PREC_OZAKI_CRT (and
+ * JLC_PREC_OZAKI, served by the same residue scheme) run every problem on
+ * INT8 residues with the per-call route's moduli, scales and exact
+ * reconstruction, so each result is bitwise the per-call residue result;
+ * problems that route would compute in FP64 (Inf/NaN operands, alpha == 0,
+ * k == 0, m == 1 or n == 1, k < 32) run FP64 tiles. */
 JLC_API int jlc_grouped_plan_create(jlc_ctx* ctx, const jlc_problem* probs, int64_t count, int precision, int flags,
                                     jlc_grouped_plan** out);
 /* enqueue one run on the context stream (graph replay when captured) */

@@ -118,6 +118,17 @@ int auto_slices(long long k) {
     return 8;
 }
 
+// Whether the automatic slice / modulus count reaches the scheme's accuracy
+// target for this k.  For very short products neither scheme does (the
+// operand scales are capped by the split's exact integer range: 2^-51 of the
+// row/column maximum against a componentwise bound of 2 k u), so those run in
+// FP64 -- as calls whose operands hold Inf/NaN do.
+bool ozaki_reaches_bound(long long k, bool crt) {
+    if (crt) return ozaki_crt_est_ratio(ozaki_crt_auto_moduli(k), k) <= 1.0;
+    const int s = auto_slices(k);
+    return (s + 3) * std::ldexp(1.0, -7 * s) <= 2.0 * std::ldexp(1.0, -53) * (double)k / 16.0;
+}
+
 bool use_ozaki(int precision, long long m, long long n, long long k) {
     if (precision == JLC_PREC_OZAKI || precision == JLC_PREC_OZAKI_CRT) return true;
     if (precision == JLC_PREC_NATIVE) return false;
@@ -185,9 +196,11 @@ int run_device(jlc_ctx* ctx, const GemmDesc& g0, int precision, int slices, jlc_
     }
     // a row block of a pipelined product follows the whole product's choice
     const long long whole_m = g.ws_m > g.m ? g.ws_m : g.m;
-    const bool ozaki = use_ozaki(precision, whole_m, g.n, g.k);
-    // AUTO takes the residue scheme: fewer INT8 products for the same bound
-    const bool crt = ozaki && precision != JLC_PREC_OZAKI;
+    // AUTO takes the residue scheme: fewer INT8 products for the same bound;
+    // an automatic count that cannot reach the bound for this k means FP64
+    const bool crt_req = precision != JLC_PREC_OZAKI;
+    const bool ozaki = use_ozaki(precision, whole_m, g.n, g.k) && (slices > 0 || ozaki_reaches_bound(g.k, crt_req));
+    const bool crt = ozaki && crt_req;
     // Small products split k across CTAs, partials in the workspace (after
     // the Ozaki split data when the FP64 kernel is the gated fallback, so
     // that its split choice, and with it its sums, match the native route).

@@ -42,9 +42,11 @@
 
 #include <sys/stat.h>
 
+#include "jlc_crt.cuh"
 #include "jlc_device.cuh"
 #include "jlc_dmma.cuh"
 #include "jlc_internal.h"
+#include "jlc_residue.cuh"
 
 namespace jlc {
 namespace grp {
@@ -275,6 +277,201 @@ __global__ void __launch_bounds__(THREADS, 3) grouped_kernel(const jlc_problem* 
     }
 }
 
+// ------------------------------------------------------ grouped Ozaki (residues)
+// The residue scheme of ozaki.cu, per problem, inside the persistent launch:
+//   1. an exponent pass: E_i = exponent of max_p |op(A)(i, p)| per row, F_j
+//      per column of op(B), and a per-problem Inf/NaN flag (oz_exps_kernel);
+//   2. tile items of 32 x 32: every 32-deep k chunk of the tile's rows of
+//      op(A) and columns of op(B) is scaled by 2^(p - E_i) / 2^(q - F_j) and
+//      encoded into N INT8 residue planes in shared memory with the same
+//      encoder as the large path (jlc_residue.cuh), then one INT8 mma.sync
+//      (m16n8k32, INT32 accumulation) per modulus and 16 x 8 block; every
+//      16352 k the accumulators are folded back to their residues so that
+//      they stay inside the reduction's range;
+//   3. per element: residues -> exact CRT reconstruction (jlc_crt.cuh) ->
+//      x * 2^(E_i + F_j - p - q), then alpha and beta as the large path's
+//      epilogue applies them.
+// N, p and q follow the large path's choice for the problem's k, so every
+// problem's result is bitwise the one the per-call residue route gives.
+// Problems whose operands hold Inf/NaN (flagged by the exponent pass),
+// problems with alpha == 0 or k == 0, the matrix-vector shapes m == 1 or
+// n == 1 (which the per-call route sends to its GEMV kernel) and products too
+// short for the scheme to reach the FP64 bound (k < 32; the per-call route
+// computes those in FP64 as well) run the FP64 tile instead.
+constexpr int OZ_T = 32, OZ_KC = 32, OZ_ROWB = 48;  // tile, k chunk, bytes per smem row (32 + 16 pad)
+constexpr int OZ_PLANE = OZ_T * OZ_ROWB;           // one modulus of one operand
+constexpr int OZ_SMEM = 2 * res::MAX_MODULI * OZ_PLANE;
+constexpr int OZ_FOLD_CHUNKS = 511;                // 511 * 32 * 2^14 + 255 < 2^28 (crt::kAccBound)
+constexpr int KIND_OZ = 3;
+static_assert(OZ_SMEM <= SMEM_BYTES, "residue planes must fit the FP64 tile's shared memory");
+
+struct OzProb {
+    int ea_off, eb_off;  // offsets of the problem's exponents in the arena
+    int nmod, p, q;      // moduli count and operand scales (ozaki_crt_auto_moduli, crt_pq)
+    int active;          // 0: alpha == 0, k == 0 or empty (FP64 tile, no exponents)
+};
+
+// one warp: 32 rows of op(A) (which == 0) or 32 columns of op(B) of a problem
+struct ExpTask {
+    int prob, which, i0;
+};
+
+__constant__ crt::Consts c_crt[res::MAX_MODULI + 1];  // reconstruction constants by modulus count
+
+__global__ void __launch_bounds__(THREADS) oz_exps_kernel(const jlc_problem* probs, const OzProb* oz,
+                                                          const ExpTask* tasks, int ntasks, int* exps,
+                                                          int* nonfinite) {
+    const int t = (blockIdx.x * THREADS + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    if (t >= ntasks) return;
+    const ExpTask task = tasks[t];
+    const jlc_problem& P = probs[task.prob];
+    const long long idx = task.i0 + lane;
+    const long long lim = task.which == 0 ? P.m : P.n;
+    if (idx >= lim) return;
+    double mx = 0.0;
+    bool bad = false;
+    for (long long q = 0; q < P.k; ++q) {
+        const double x = task.which == 0 ? elem_a(P, idx, q) : elem_b(P, q, idx);
+        bad |= !isfinite(x);
+        mx = fmax(mx, fabs(x));
+    }
+    if (bad) atomicOr(&nonfinite[task.prob], 1);
+    const OzProb o = oz[task.prob];
+    exps[(task.which == 0 ? o.ea_off : o.eb_off) + idx] = bad ? 0 : res::frexp_exp(mx);
+}
+
+__device__ __forceinline__ void mma_s8(int (&c)[4], const uint32_t (&a)[4], uint32_t b0, uint32_t b1) {
+    asm volatile(
+        "mma.sync.aligned.m16n8k32.row.col.s32.s8.s8.s32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+        "{%0,%1,%2,%3};"
+        : "+r"(c[0]), "+r"(c[1]), "+r"(c[2]), "+r"(c[3])
+        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+
+// Encodes a 32 x 32 chunk of one operand: rows r of op(X) (rows of op(A) or
+// columns of op(B)), k values k0..k0+31, scaled by 2^(shift - e_r), as N
+// residue planes [modulus][row][k] (OZ_ROWB bytes per row).  Threads walk the
+// contiguous direction of the stored operand.
+template <bool A_OP>
+__device__ __forceinline__ void oz_encode_chunk(const jlc_problem& P, const int* ex, int shift, int nmod,
+                                                long long r0, long long k0, char* planes) {
+    const long long rows = A_OP ? P.m : P.n;
+    const bool kcontig = A_OP ? P.layout_a == JLC_ROW_MAJOR : P.layout_b == JLC_COL_MAJOR;
+#pragma unroll 1
+    for (int gi = threadIdx.x; gi < OZ_T * (OZ_KC / 4); gi += THREADS) {
+        const int r = kcontig ? gi / (OZ_KC / 4) : gi % OZ_T;
+        const int kg = kcontig ? gi % (OZ_KC / 4) : gi / OZ_T;
+        const long long row = r0 + r, kk = k0 + 4 * kg;
+        double v[4];
+        if (row < rows) {
+            const res::Pow2 sc = res::pow2_split(shift - ex[row]);
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                double x = 0.0;
+                if (kk + u < P.k) x = A_OP ? elem_a(P, row, kk + u) : elem_b(P, kk + u, row);
+                v[u] = x * sc.lo * sc.hi;
+            }
+        } else {
+#pragma unroll
+            for (int u = 0; u < 4; ++u) v[u] = 0.0;
+        }
+        res::encode4<true>(v, nmod, reinterpret_cast<uint8_t*>(planes + r * OZ_ROWB + 4 * kg), OZ_PLANE);
+    }
+}
+
+__device__ void oz_tile_item(const jlc_problem& P, const OzProb& o, const int* exps, int tm, int tn, char* smem) {
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int g = lane >> 2, t = lane & 3;
+    const int wm = warp >> 1, wn = warp & 1;  // 2 x 2 warps of 16 x 16
+    const long long m0 = (long long)tm * OZ_T, n0 = (long long)tn * OZ_T;
+    const int nmod = o.nmod;
+    const int* ea = exps + o.ea_off;
+    const int* eb = exps + o.eb_off;
+    char* sA = smem;
+    char* sB = smem + res::MAX_MODULI * OZ_PLANE;
+    int acc[res::MAX_MODULI][2][4];
+#pragma unroll
+    for (int l = 0; l < res::MAX_MODULI; ++l)
+#pragma unroll
+        for (int j = 0; j < 2; ++j)
+#pragma unroll
+            for (int e = 0; e < 4; ++e) acc[l][j][e] = 0;
+    const long long nchunks = (P.k + OZ_KC - 1) / OZ_KC;
+    for (long long ch = 0; ch < nchunks; ++ch) {
+        oz_encode_chunk<true>(P, ea, o.p, nmod, m0, ch * OZ_KC, sA);
+        oz_encode_chunk<false>(P, eb, o.q, nmod, n0, ch * OZ_KC, sB);
+        __syncthreads();
+#pragma unroll
+        for (int l = 0; l < res::MAX_MODULI; ++l) {
+            if (l < nmod) {
+                const char* pa = sA + l * OZ_PLANE + (wm * 16 + g) * OZ_ROWB + 4 * t;
+                const uint32_t a[4] = {*reinterpret_cast<const uint32_t*>(pa),
+                                       *reinterpret_cast<const uint32_t*>(pa + 8 * OZ_ROWB),
+                                       *reinterpret_cast<const uint32_t*>(pa + 16),
+                                       *reinterpret_cast<const uint32_t*>(pa + 8 * OZ_ROWB + 16)};
+#pragma unroll
+                for (int j = 0; j < 2; ++j) {
+                    const char* pb = sB + l * OZ_PLANE + (wn * 16 + 8 * j + g) * OZ_ROWB + 4 * t;
+                    mma_s8(acc[l][j], a, *reinterpret_cast<const uint32_t*>(pb),
+                           *reinterpret_cast<const uint32_t*>(pb + 16));
+                }
+            }
+        }
+        __syncthreads();  // the next chunk overwrites the planes
+        if ((ch + 1) % OZ_FOLD_CHUNKS == 0) {
+#pragma unroll
+            for (int l = 0; l < res::MAX_MODULI; ++l) {
+                if (l < nmod) {
+                    const crt::Consts& cc = c_crt[nmod];
+#pragma unroll
+                    for (int j = 0; j < 2; ++j)
+#pragma unroll
+                        for (int e = 0; e < 4; ++e)
+                            acc[l][j][e] = crt::mod_pos(acc[l][j][e], (uint32_t)cc.m[l], cc.mu[l], cc.bias[l]);
+                }
+            }
+        }
+    }
+    const crt::Consts& cc = c_crt[nmod];
+    const bool do_scale = P.alpha != 1.0, beta0 = P.beta == 0.0;
+#pragma unroll
+    for (int j = 0; j < 2; ++j)
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+            const long long row = m0 + wm * 16 + g + 8 * (e >> 1);
+            const long long col = n0 + wn * 16 + 8 * j + 2 * t + (e & 1);
+            if (row >= P.m || col >= P.n) continue;
+            uint32_t r[res::MAX_MODULI];
+#pragma unroll
+            for (int l = 0; l < res::MAX_MODULI; ++l)
+                r[l] = l < nmod ? (uint32_t)crt::mod_pos(acc[l][j][e], (uint32_t)cc.m[l], cc.mu[l], cc.bias[l]) : 0u;
+            double v = crt::reconstruct(cc, r, ea[row] + eb[col] - o.p - o.q);
+            if (do_scale) v *= P.alpha;
+            double* cp = P.c + row * P.ldc + col;
+            *cp = beta0 ? v : fma(P.beta, *cp, v);
+        }
+}
+
+__global__ void __launch_bounds__(THREADS, 3) grouped_oz_kernel(const jlc_problem* probs, const OzProb* oz,
+                                                             const Item* items, int nitems, const int* exps,
+                                                             const int* nonfinite, int* counter) {
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    char* smem = reinterpret_cast<char*>((reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~uintptr_t(127));
+    __shared__ int s_item;
+    for (;;) {
+        if (threadIdx.x == 0) s_item = atomicAdd(counter, 1);
+        __syncthreads();
+        const int it = s_item;
+        __syncthreads();
+        if (it >= nitems) return;
+        const Item w = items[it];
+        const jlc_problem P = probs[w.prob];
+        const OzProb o = oz[w.prob];
+        if (!o.active || nonfinite[w.prob]) tile_dispatch<32, 32>(P, w.tm, w.tn, smem);
+        else oz_tile_item(P, o, exps, w.tm, w.tn, smem);
+    }
+}
+
 // ------------------------------------------------------------------ host side
 bool is_tiny(const jlc_problem& p) { return p.m * p.n <= 64 && p.k <= 64; }
 int shape_class(const jlc_problem& p) { return std::max(p.m, p.n) <= 48 ? 0 : 1; }
@@ -386,6 +583,12 @@ void tune_store(const std::string& key, int value) {
 struct jlc_grouped_plan {
     jlc_ctx* ctx = nullptr;
     int64_t count = 0;
+    bool oz = false;  // Ozaki residue precision
+    jlc::grp::OzProb* d_oz = nullptr;
+    jlc::grp::ExpTask* d_tasks = nullptr;
+    int ntasks = 0;
+    int* d_exps = nullptr;
+    int* d_nonfinite = nullptr;
     jlc_problem* d_probs = nullptr;
     jlc::grp::Item* d_items = nullptr;
     int* d_tiny = nullptr;
@@ -438,6 +641,14 @@ void free_plan_buffers(jlc_grouped_plan* pl) {
     if (pl->d_items) cudaFree(pl->d_items);
     if (pl->d_tiny) cudaFree(pl->d_tiny);
     if (pl->d_counter) cudaFree(pl->d_counter);
+    if (pl->d_oz) cudaFree(pl->d_oz);
+    if (pl->d_tasks) cudaFree(pl->d_tasks);
+    if (pl->d_exps) cudaFree(pl->d_exps);
+    if (pl->d_nonfinite) cudaFree(pl->d_nonfinite);
+    pl->d_oz = nullptr;
+    pl->d_tasks = nullptr;
+    pl->d_exps = nullptr;
+    pl->d_nonfinite = nullptr;
     pl->exec = nullptr;
     pl->graph = nullptr;
     pl->d_probs = nullptr;
@@ -476,6 +687,16 @@ int upload(jlc_grouped_plan* pl, const std::vector<jlc_problem>& probs, const Wo
 int launch_plan(jlc_grouped_plan* pl, cudaStream_t st) {
     if (pl->nitems == 0) return JLC_OK;
     if (cudaMemsetAsync(pl->d_counter, 0, sizeof(int), st) != cudaSuccess) return JLC_E_CUDA;
+    if (pl->oz) {
+        if (cudaMemsetAsync(pl->d_nonfinite, 0, (size_t)pl->count * sizeof(int), st) != cudaSuccess)
+            return JLC_E_CUDA;
+        if (pl->ntasks > 0)
+            oz_exps_kernel<<<(pl->ntasks * 32 + THREADS - 1) / THREADS, THREADS, 0, st>>>(
+                pl->d_probs, pl->d_oz, pl->d_tasks, pl->ntasks, pl->d_exps, pl->d_nonfinite);
+        grouped_oz_kernel<<<pl->grid, THREADS, SMEM_BYTES, st>>>(pl->d_probs, pl->d_oz, pl->d_items, pl->nitems,
+                                                                pl->d_exps, pl->d_nonfinite, pl->d_counter);
+        return cudaGetLastError() == cudaSuccess ? JLC_OK : JLC_E_LAUNCH;
+    }
     grouped_kernel<<<pl->grid, THREADS, SMEM_BYTES, st>>>(pl->d_probs, pl->d_items, pl->nitems, pl->d_tiny,
                                                          pl->d_counter);
     return cudaGetLastError() == cudaSuccess ? JLC_OK : JLC_E_LAUNCH;
@@ -550,44 +771,92 @@ int autotune_class(jlc_ctx* ctx, const std::vector<jlc_problem>& probs, int cls)
     return best;
 }
 
-}  // namespace
+// Residue-scheme plan: per-problem N, p, q (the large path's choice for the
+// problem's k), exponent arena offsets, the exponent pass's tasks and one
+// 32 x 32 tile item per output tile of every problem, longest first.
+int build_oz_plan(jlc_grouped_plan* pl, const std::vector<jlc_problem>& probs) {
+    jlc_ctx* ctx = pl->ctx;
+    cudaStream_t st = ctx->stream;
+    std::vector<OzProb> oz(probs.size());
+    std::vector<ExpTask> tasks;
+    struct Costed {
+        Item it;
+        double cost;
+    };
+    std::vector<Costed> v;
+    long long arena = 0;
+    double flops = 0.0;
+    for (size_t i = 0; i < probs.size(); ++i) {
+        const jlc_problem& p = probs[i];
+        OzProb& o = oz[i];
+        o = OzProb{0, 0, 2, 0, 0, 0};
+        if (p.m == 0 || p.n == 0) continue;
+        // as on the per-call route: nothing to multiply (alpha == 0, k == 0),
+        // the matrix-vector shapes (m == 1, n == 1) and products too short for
+        // the residue scheme to reach the FP64 bound (k < 32) stay in FP64
+        const bool active = p.k > 0 && p.alpha != 0.0 && p.m > 1 && p.n > 1 &&
+                            ozaki_crt_est_ratio(ozaki_crt_auto_moduli(p.k), p.k) <= 1.0;
+        if (active) {
+            o.active = 1;
+            o.nmod = ozaki_crt_auto_moduli(p.k);
+            ozaki_crt_pq(o.nmod, p.k, &o.p, &o.q);
+            o.ea_off = (int)arena;
+            arena += p.m;
+            o.eb_off = (int)arena;
+            arena += p.n;
+            for (long long r = 0; r < p.m; r += 32) tasks.push_back(ExpTask{(int)i, 0, (int)r});
+            for (long long c = 0; c < p.n; c += 32) tasks.push_back(ExpTask{(int)i, 1, (int)c});
+            flops += 2.0 * p.m * p.n * p.k;
+        }
+        if (arena > (1LL << 30)) return gerr(ctx, JLC_E_UNSUPPORTED, "grouped: Ozaki exponent arena too large");
+        const int tmn = (int)((p.m + OZ_T - 1) / OZ_T), tnn = (int)((p.n + OZ_T - 1) / OZ_T);
+        const double cost = (double)OZ_T * OZ_T * ((active ? (double)p.k : 0.0) + 16.0) * (active ? o.nmod : 1);
+        for (int a = 0; a < tmn; ++a)
+            for (int b = 0; b < tnn; ++b) v.push_back({Item{(int)i, a, b, KIND_OZ}, cost});
+    }
+    std::stable_sort(v.begin(), v.end(), [](const Costed& x, const Costed& y) { return x.cost > y.cost; });
+    std::vector<Item> items;
+    items.reserve(v.size());
+    for (auto& c : v) items.push_back(c.it);
+    // reconstruction constants for every modulus count (p, q are per problem)
+    std::vector<crt::Consts> consts(res::MAX_MODULI + 1);
+    for (int nm = 2; nm <= res::MAX_MODULI; ++nm) crt::build_consts(nm, 0, 0, res::kModuliHost, consts[nm]);
+    auto alloc_copy = [&](void** dst, const void* src, size_t bytes) -> cudaError_t {
+        cudaError_t e = cudaMalloc(dst, bytes ? bytes : 16);
+        if (e != cudaSuccess) return e;
+        return bytes ? cudaMemcpyAsync(*dst, src, bytes, cudaMemcpyHostToDevice, st) : cudaSuccess;
+    };
+    cudaError_t e = alloc_copy((void**)&pl->d_probs, probs.data(), probs.size() * sizeof(jlc_problem));
+    if (e == cudaSuccess) e = alloc_copy((void**)&pl->d_oz, oz.data(), oz.size() * sizeof(OzProb));
+    if (e == cudaSuccess) e = alloc_copy((void**)&pl->d_items, items.data(), items.size() * sizeof(Item));
+    if (e == cudaSuccess) e = alloc_copy((void**)&pl->d_tasks, tasks.data(), tasks.size() * sizeof(ExpTask));
+    if (e == cudaSuccess) e = cudaMalloc((void**)&pl->d_exps, (size_t)(arena ? arena : 1) * sizeof(int));
+    if (e == cudaSuccess) e = cudaMalloc((void**)&pl->d_nonfinite, (size_t)(probs.empty() ? 1 : probs.size()) * 4);
+    if (e == cudaSuccess) e = cudaMalloc((void**)&pl->d_counter, sizeof(int));
+    if (e == cudaSuccess)
+        e = cudaMemcpyToSymbolAsync(c_crt, consts.data(), consts.size() * sizeof(crt::Consts), 0,
+                                    cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);  // host vectors are short-lived
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return gerr(ctx, e == cudaErrorMemoryAllocation ? JLC_E_OOM : JLC_E_CUDA, "grouped Ozaki plan: %s",
+                    cudaGetErrorString(e));
+    }
+    pl->nitems = (int)items.size();
+    pl->ntasks = (int)tasks.size();
+    pl->flops = flops;
+    int per_sm = 0;
+    cudaFuncSetAttribute(grouped_oz_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, grouped_oz_kernel, THREADS, SMEM_BYTES);
+    if (per_sm < 1) per_sm = 1;
+    pl->grid = std::max(1, std::min(pl->nitems, ctx->sm_count * per_sm));
+    return JLC_OK;
+}
 
-extern "C" {
-
-int jlc_grouped_plan_create(jlc_ctx* ctx, const jlc_problem* probs, int64_t count, int precision, int flags,
-                            jlc_grouped_plan** out) {
-    if (!ctx || !out) return JLC_E_ARG;
-    *out = nullptr;
-    if (count < 0 || (count > 0 && !probs)) return gerr(ctx, JLC_E_ARG, "grouped: bad problem table");
-    if (count > (1 << 28)) return gerr(ctx, JLC_E_UNSUPPORTED, "grouped: too many problems");
-    if (precision == JLC_PREC_OZAKI)
-        return gerr(ctx, JLC_E_UNSUPPORTED, "grouped: Ozaki precision is not available for grouped launches");
-    cudaSetDevice(ctx->device);
-    std::vector<jlc_problem> v(probs, probs + count);
-    for (int64_t i = 0; i < count; ++i) {
-        int rc = check_problem(ctx, v[i], i);
-        if (rc) return rc;
-    }
-    jlc_grouped_plan* pl = new (std::nothrow) jlc_grouped_plan();
-    if (!pl) return JLC_E_OOM;
-    pl->ctx = ctx;
-    pl->count = count;
-    for (int cls = 0; cls < 2; ++cls) {
-        const std::string key = tune_key(ctx->device, ctx->sm_count, cls);
-        int ts = (flags & JLC_GROUPED_AUTOTUNE) ? autotune_class(ctx, v, cls) : 0;
-        if (ts) tune_store(key, ts);
-        else ts = tune_lookup(key);
-        if (ts == 32 || ts == 64) pl->cfg[cls] = ts;
-    }
-    WorkList wl;
-    build_work(v, pl->cfg, -1, wl);
-    pl->flops = wl.flops;
-    int rc = upload(pl, v, wl);
-    if (rc) {
-        free_plan_buffers(pl);
-        delete pl;
-        return rc;
-    }
+// graph capture (when asked) and hand-over of a built plan
+int finish_plan(jlc_grouped_plan* pl, int flags, jlc_grouped_plan** out) {
+    jlc_ctx* ctx = pl->ctx;
+    int rc = JLC_OK;
     if (flags & JLC_GROUPED_GRAPH) {
         cudaError_t e = cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal);
         if (e == cudaSuccess) {
@@ -606,6 +875,62 @@ int jlc_grouped_plan_create(jlc_ctx* ctx, const jlc_problem* probs, int64_t coun
     *out = pl;
     return JLC_OK;
 }
+
+}  // namespace
+
+extern "C" {
+
+int jlc_grouped_plan_create(jlc_ctx* ctx, const jlc_problem* probs, int64_t count, int precision, int flags,
+                            jlc_grouped_plan** out) {
+    if (!ctx || !out) return JLC_E_ARG;
+    *out = nullptr;
+    if (count < 0 || (count > 0 && !probs)) return gerr(ctx, JLC_E_ARG, "grouped: bad problem table");
+    if (count > (1 << 28)) return gerr(ctx, JLC_E_UNSUPPORTED, "grouped: too many problems");
+    if (precision != JLC_PREC_NATIVE && precision != JLC_PREC_AUTO && precision != JLC_PREC_OZAKI &&
+        precision != JLC_PREC_OZAKI_CRT)
+        return gerr(ctx, JLC_E_ARG, "grouped: unknown precision %d", precision);
+    cudaSetDevice(ctx->device);
+    std::vector<jlc_problem> v(probs, probs + count);
+    for (int64_t i = 0; i < count; ++i) {
+        int rc = check_problem(ctx, v[i], i);
+        if (rc) return rc;
+    }
+    jlc_grouped_plan* pl = new (std::nothrow) jlc_grouped_plan();
+    if (!pl) return JLC_E_OOM;
+    pl->ctx = ctx;
+    pl->count = count;
+    if (precision == JLC_PREC_OZAKI || precision == JLC_PREC_OZAKI_CRT) {
+        // both Ozaki requests run the residue scheme (the slice scheme needs
+        // s(s+1)/2 products where the residues need N)
+        pl->oz = true;
+        int rc = build_oz_plan(pl, v);
+        if (rc) {
+            free_plan_buffers(pl);
+            delete pl;
+            return rc;
+        }
+        pl->cfg[0] = pl->cfg[1] = OZ_T;
+        return finish_plan(pl, flags, out);
+    }
+    for (int cls = 0; cls < 2; ++cls) {
+        const std::string key = tune_key(ctx->device, ctx->sm_count, cls);
+        int ts = (flags & JLC_GROUPED_AUTOTUNE) ? autotune_class(ctx, v, cls) : 0;
+        if (ts) tune_store(key, ts);
+        else ts = tune_lookup(key);
+        if (ts == 32 || ts == 64) pl->cfg[cls] = ts;
+    }
+    WorkList wl;
+    build_work(v, pl->cfg, -1, wl);
+    pl->flops = wl.flops;
+    int rc = upload(pl, v, wl);
+    if (rc) {
+        free_plan_buffers(pl);
+        delete pl;
+        return rc;
+    }
+    return finish_plan(pl, flags, out);
+}
+
 
 int jlc_grouped_plan_run(jlc_grouped_plan* plan) {
     if (!plan || !plan->ctx) return JLC_E_ARG;
@@ -654,7 +979,7 @@ int jlc_dgemm_grouped_device(jlc_ctx* ctx, const jlc_problem* probs, int64_t cou
     if (!rc && rep) {
         float ms = 0.f;
         cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
-        rep->precision = JLC_PREC_NATIVE;
+        rep->precision = pl->oz ? JLC_PREC_OZAKI_CRT : JLC_PREC_NATIVE;
         rep->kernel = JLC_KERNEL_GROUPED;
         rep->device_ms = ms;
     }

@@ -99,6 +99,8 @@ int launch_scale_c(double* c, long long ldc, long long m, long long n, double be
 // scheme, crt = true).
 size_t ozaki_workspace_bytes(long long m, long long n, long long k, int count, int sm_count, bool crt = false);
 int ozaki_crt_auto_moduli(long long k);
+// operand scales p (rows of op(A)) and q (columns of op(B)) of the residue scheme
+void ozaki_crt_pq(int nmod, long long k, int* p, int* q);
 double ozaki_crt_est_ratio(int nmod, long long k);
 // Phase 1: exponents + INT8 slices / residues of op(A) and op(B) into the
 // workspace; sets flags[0] when an operand holds Inf/NaN.  Phase 2: the

@@ -138,3 +138,132 @@ def test_grouped_rejects_bad_problem(ctx):
     bad = [dict(m=4, n=4, k=4, layout_a=0, layout_b=0, lda=2, ldb=4, ldc=4, alpha=1.0, beta=0.0, a=8, b=8, c=8)]
     with pytest.raises(IllegalArgumentException):
         ctx.dgemm_grouped_device(bad)
+
+
+def _per_problem_ozaki(ctx, probs, arena_before, base_ptr):
+    """Each problem through the per-call Ozaki residue route on a copy of the
+    arena as it was before the grouped run (problem pointers point into the
+    arena at base_ptr); returns that copy after all of them."""
+    import torch
+    from jlc_b200 import JLC_PREC_OZAKI_CRT
+    ref = arena_before.clone()
+    shift = ref.data_ptr() - base_ptr
+    for p in probs:
+        if p["m"] == 0 or p["n"] == 0:
+            continue
+        ctx.dgemm_device(p["layout_a"], p["layout_b"], p["m"], p["n"], p["k"], p["alpha"], p["a"] + shift,
+                         p["lda"], p["b"] + shift, p["ldb"], p["beta"], p["c"] + shift, p["ldc"],
+                         precision=JLC_PREC_OZAKI_CRT)
+    ctx.synchronize()
+    torch.cuda.synchronize()
+    return ref
+
+
+def _on_residues(p):
+    """Problems both routes compute with the residue scheme: the others (alpha
+    == 0, k == 0, matrix-vector shapes, k < 32 where no modulus count reaches
+    the FP64 bound) run FP64 kernels with different summation orders."""
+    return p["alpha"] != 0.0 and p["k"] >= 32 and p["m"] > 1 and p["n"] > 1
+
+
+def _assert_matches_per_call(probs, arena, want):
+    """Bitwise per residue-scheme problem (the rest are held to the FP64 bound
+    by check_batch)."""
+    got, ref = arena.cpu().numpy(), want.cpu().numpy()
+    exact = 0
+    for p in probs:
+        m, n = p["m"], p["n"]
+        if m == 0 or n == 0 or not _on_residues(p):
+            continue
+        o = (p["c"] - arena.data_ptr()) // 8
+        np.testing.assert_array_equal(got[o:o + m * n], ref[o:o + m * n], err_msg=f"{m}x{n}x{p['k']}")
+        exact += 1
+    assert exact > 0
+
+
+def test_grouped_ozaki_matches_per_call_route(ctx, oracle):
+    """Ozaki precision in a grouped launch: the residue scheme per problem,
+    bitwise equal to calling the residue route problem by problem (same
+    moduli, scales and exact reconstruction), and inside the FP64 bound."""
+    from jlc_b200 import JLC_PREC_OZAKI_CRT
+    rng = np.random.default_rng(21)
+    shapes = mixed_shapes(rng, 160) + [(1, 1, 1), (1, 150, 70), (150, 1, 70), (33, 65, 129), (64, 64, 600),
+                                       (0, 4, 4), (5, 6, 0)]
+    alphas = [float(x) for x in rng.uniform(-2, 2, size=len(shapes))]
+    betas = [float(x) for x in rng.uniform(-2, 2, size=len(shapes))]
+    alphas[3], betas[4], alphas[5] = 1.0, 0.0, 0.0
+    probs, host, arena = make_batch(oracle, shapes, 23, alphas=alphas, betas=betas)
+    before = arena.clone()
+    rep = ctx.dgemm_grouped_device(probs, precision=JLC_PREC_OZAKI_CRT)
+    assert rep["kernel"] == 4 and rep["precision"] == JLC_PREC_OZAKI_CRT
+    want = _per_problem_ozaki(ctx, probs, before, arena.data_ptr())
+    _assert_matches_per_call(probs, arena, want)
+    check_batch(oracle, probs, host, arena, "grouped ozaki")
+
+
+def test_grouped_ozaki_long_k_and_graph_replay(ctx, oracle):
+    """k beyond one INT32 run (the accumulators fold to residues every 16352
+    k) and a captured plan replayed on new data."""
+    import torch
+    from jlc_b200 import JLC_PREC_OZAKI
+    shapes = [(40, 36, 20000), (17, 70, 33000), (96, 96, 300), (3, 3, 3)]
+    probs, host, arena = make_batch(oracle, shapes, 29, betas=[0.0, 0.5, -1.0, 0.0])
+    before = arena.clone()
+    plan = ctx.grouped_plan(probs, precision=JLC_PREC_OZAKI, graph=True)
+    assert plan.info()["tile_small"] == 32
+    plan.run()
+    ctx.synchronize()
+    want = _per_problem_ozaki(ctx, probs, before, arena.data_ptr())
+    _assert_matches_per_call(probs, arena, want)
+    check_batch(oracle, probs, host, arena, "grouped ozaki long k")
+    # new B data in place, C restored: the replay recomputes every exponent
+    host2 = []
+    for p, (m, n, k, la, lb, alpha, beta, A, B, C) in zip(probs, host):
+        B2 = 0.001 * B
+        b_store = B2 if lb == 0 else np.ascontiguousarray(B2.T)
+        off = (p["b"] - arena.data_ptr()) // 8
+        arena[off:off + k * n] = torch.from_numpy(b_store.ravel())
+        offc = (p["c"] - arena.data_ptr()) // 8
+        arena[offc:offc + m * n] = torch.from_numpy(C.ravel())
+        host2.append((m, n, k, la, lb, alpha, beta, A, B2, C))
+    torch.cuda.synchronize()
+    before2 = arena.clone()
+    plan.run()
+    ctx.synchronize()
+    want2 = _per_problem_ozaki(ctx, probs, before2, arena.data_ptr())
+    _assert_matches_per_call(probs, arena, want2)
+    check_batch(oracle, probs, host2, arena, "grouped ozaki replay")
+    plan.close()
+
+
+def test_grouped_ozaki_nonfinite_problem_takes_fp64(ctx, oracle):
+    """A problem whose operands hold Inf/NaN runs the FP64 tile (IEEE
+    propagation as on the native route); the others stay on the residues."""
+    import torch
+    from jlc_b200 import JLC_PREC_OZAKI_CRT
+    shapes = [(20, 30, 40), (50, 20, 70), (8, 8, 48)]
+    probs, host, arena = make_batch(oracle, shapes, 31, betas=[0.0, 0.0, 0.0])
+    p1 = probs[1]
+    A1 = host[1][7].copy()
+    A1[3, 5] = np.nan
+    A1[10, 0] = np.inf
+    a_store = A1 if p1["layout_a"] == 0 else np.ascontiguousarray(A1.T)
+    off = (p1["a"] - arena.data_ptr()) // 8
+    arena[off:off + 50 * 70] = torch.from_numpy(a_store.ravel())
+    torch.cuda.synchronize()
+    before = arena.clone()
+    ctx.dgemm_grouped_device(probs, precision=JLC_PREC_OZAKI_CRT)
+    got = arena.cpu().numpy()
+    want = _per_problem_ozaki(ctx, probs, before, arena.data_ptr()).cpu().numpy()
+    flat_host = [(p, h) for p, h in zip(probs, host)]
+    for i, (p, h) in enumerate(flat_host):
+        m, n = p["m"], p["n"]
+        oc = (p["c"] - arena.data_ptr()) // 8
+        g, w = got[oc:oc + m * n], want[oc:oc + m * n]
+        if i == 1:
+            np.testing.assert_array_equal(np.isnan(g), np.isnan(w))
+            np.testing.assert_array_equal(np.isinf(g), np.isinf(w))
+            fin = np.isfinite(w)
+            np.testing.assert_allclose(g[fin], w[fin], rtol=0, atol=1e-12)
+        else:
+            np.testing.assert_array_equal(g, w)
