@@ -278,42 +278,51 @@ __global__ void __launch_bounds__(THREADS, 3) grouped_kernel(const jlc_problem* 
 }
 
 // ------------------------------------------------------ grouped Ozaki (residues)
-// The residue scheme of ozaki.cu, per problem, inside the persistent launch:
-//   1. an exponent pass: E_i = exponent of max_p |op(A)(i, p)| per row, F_j
-//      per column of op(B), and a per-problem Inf/NaN flag (oz_exps_kernel);
-//   2. tile items of 32 x 32: every 32-deep k chunk of the tile's rows of
-//      op(A) and columns of op(B) is scaled by 2^(p - E_i) / 2^(q - F_j) and
-//      encoded into N INT8 residue planes in shared memory with the same
-//      encoder as the large path (jlc_residue.cuh), then one INT8 mma.sync
-//      (m16n8k32, INT32 accumulation) per modulus and 16 x 8 block; every
-//      16352 k the accumulators are folded back to their residues so that
-//      they stay inside the reduction's range;
-//   3. per element: residues -> exact CRT reconstruction (jlc_crt.cuh) ->
-//      x * 2^(E_i + F_j - p - q), then alpha and beta as the large path's
-//      epilogue applies them.
-// N, p and q follow the large path's choice for the problem's k, so every
-// problem's result is bitwise the one the per-call residue route gives.
-// Problems whose operands hold Inf/NaN (flagged by the exponent pass),
-// problems with alpha == 0 or k == 0, the matrix-vector shapes m == 1 or
-// n == 1 (which the per-call route sends to its GEMV kernel) and products too
-// short for the scheme to reach the FP64 bound (k < 32; the per-call route
-// computes those in FP64 as well) run the FP64 tile instead.
-constexpr int OZ_T = 32, OZ_KC = 32, OZ_ROWB = 48;  // tile, k chunk, bytes per smem row (32 + 16 pad)
-constexpr int OZ_PLANE = OZ_T * OZ_ROWB;           // one modulus of one operand
-constexpr int OZ_SMEM = 2 * res::MAX_MODULI * OZ_PLANE;
-constexpr int OZ_FOLD_CHUNKS = 511;                // 511 * 32 * 2^14 + 255 < 2^28 (crt::kAccBound)
+// The residue scheme of ozaki.cu, per problem, in three launches:
+//   1. oz_exps_kernel: E_i = exponent of max_p |op(A)(i, p)| per row, F_j per
+//      column of op(B), and a per-problem Inf/NaN flag;
+//   2. oz_encode_kernel: every 32 x 32 block (rows x k) of op(A) scaled by
+//      2^(p - E_i), and of op(B)^T by 2^(q - F_j), encoded once into N INT8
+//      residue planes [modulus][row][Kp] of a residue arena (Kp = k rounded up
+//      to 32) with the same encoder as the large path (jlc_residue.cuh);
+//   3. grouped_oz_kernel: persistent 32 x 32 tile items; per 32-deep k chunk
+//      the tile's plane rows arrive by 16-byte cp.async (two stages), then one
+//      INT8 mma.sync (m16n8k32, INT32 accumulation) per modulus and 16 x 8
+//      block; every 16352 k the accumulators are folded back to residues so
+//      they stay inside the reduction's range; per element the residues are
+//      reconstructed exactly (jlc_crt.cuh) to x * 2^(E_i + F_j - p - q), and
+//      alpha and beta are applied as the large path's epilogue applies them.
+// N, p and q follow the per-call route's choice for the problem's k, so every
+// problem's result is bitwise the per-call residue result.  Problems whose
+// operands hold Inf/NaN (flagged by the exponent pass), problems with
+// alpha == 0 or k == 0, the matrix-vector shapes m == 1 or n == 1 (which the
+// per-call route sends to its GEMV kernel) and products too short for the
+// scheme to reach the FP64 bound (k < 32; the per-call route computes those
+// in FP64 as well) run the FP64 tile instead.
+constexpr int OZ_T = 32, OZ_KC = 32;                // tile, k chunk
+constexpr int OZ_PLANE = OZ_T * OZ_KC;              // one modulus of one operand in shared memory (1 KB)
+constexpr int OZ_STAGE = 2 * res::MAX_MODULI * OZ_PLANE;
+constexpr int OZ_SMEM = 2 * OZ_STAGE;               // two stages
+constexpr int OZ_FOLD_CHUNKS = 511;                 // 511 * 32 * 2^14 + 255 < 2^28 (crt::kAccBound)
 constexpr int KIND_OZ = 3;
-static_assert(OZ_SMEM <= SMEM_BYTES, "residue planes must fit the FP64 tile's shared memory");
+constexpr int OZ_LAUNCH_SMEM = (OZ_SMEM + 128 > SMEM_BYTES) ? OZ_SMEM + 128 : SMEM_BYTES;  // FP64 tiles fit too
 
 struct OzProb {
-    int ea_off, eb_off;  // offsets of the problem's exponents in the arena
-    int nmod, p, q;      // moduli count and operand scales (ozaki_crt_auto_moduli, crt_pq)
-    int active;          // 0: alpha == 0, k == 0 or empty (FP64 tile, no exponents)
+    long long ra, rb;    // byte offsets of op(A)'s and op(B)^T's residue planes in the residue arena
+    int ea_off, eb_off;  // offsets of the problem's exponents in the exponent arena
+    int nmod, p, q;      // moduli count and operand scales (ozaki_crt_auto_moduli, ozaki_crt_pq)
+    int kp;              // k rounded up to 32: bytes per plane row
+    int active;          // 0: computed by the FP64 tile (see above)
 };
 
 // one warp: 32 rows of op(A) (which == 0) or 32 columns of op(B) of a problem
 struct ExpTask {
     int prob, which, i0;
+};
+
+// one block: 32 rows of op(A) (which == 0) or of op(B)^T, all of k
+struct EncTask {
+    int prob, which, r0;
 };
 
 __constant__ crt::Consts c_crt[res::MAX_MODULI + 1];  // reconstruction constants by modulus count
@@ -340,6 +349,62 @@ __global__ void __launch_bounds__(THREADS) oz_exps_kernel(const jlc_problem* pro
     exps[(task.which == 0 ? o.ea_off : o.eb_off) + idx] = bad ? 0 : res::frexp_exp(mx);
 }
 
+// Encodes 32 rows of op(A) (which == 0) or of op(B)^T, all of k, into the
+// residue arena.  Each 32 x 32 block is read with the stored operand's
+// contiguous direction across the threads, scaled and staged in shared
+// memory, then encoded four k at a time per row, so every warp writes whole
+// 32-byte row segments of each plane.  k past the edge is encoded as zeros
+// (the tile kernel reads whole 32-k chunks); rows past the edge are skipped.
+__global__ void __launch_bounds__(THREADS) oz_encode_kernel(const jlc_problem* probs, const OzProb* oz,
+                                                            const EncTask* tasks, int ntasks, const int* exps,
+                                                            const int* nonfinite, uint8_t* arena) {
+    __shared__ double tile[OZ_T][OZ_KC + 1];  // [row][k], padded against bank conflicts
+    for (int t = blockIdx.x; t < ntasks; t += gridDim.x) {
+        const EncTask task = tasks[t];
+        if (nonfinite[task.prob]) continue;  // the FP64 tile computes this problem
+        const jlc_problem P = probs[task.prob];
+        const OzProb o = oz[task.prob];
+        const bool a_op = task.which == 0;
+        const long long rows = a_op ? P.m : P.n;
+        const bool kcontig = a_op ? P.layout_a == JLC_ROW_MAJOR : P.layout_b == JLC_COL_MAJOR;
+        const double* x = a_op ? P.a : P.b;
+        const long long ld = a_op ? P.lda : P.ldb;
+        const int* ex = exps + (a_op ? o.ea_off : o.eb_off);
+        const int shift = a_op ? o.p : o.q;
+        uint8_t* planes = arena + (a_op ? o.ra : o.rb);
+        const size_t plane = (size_t)rows * o.kp;
+        for (long long k0 = 0; k0 < P.k; k0 += OZ_KC) {
+            // stage: element (row r, k c) of op(X) is x[row * ld + k] when k is
+            // contiguous, x[k * ld + row] otherwise; threads walk the contiguous one
+#pragma unroll 1
+            for (int e = threadIdx.x; e < OZ_T * OZ_KC; e += THREADS) {
+                const int r = kcontig ? e / OZ_KC : e % OZ_T;
+                const int c = kcontig ? e % OZ_KC : e / OZ_T;
+                const long long row = task.r0 + r, kk = k0 + c;
+                double v = 0.0;
+                if (row < rows && kk < P.k) {
+                    const res::Pow2 sc = res::pow2_split(shift - ex[row]);
+                    v = (kcontig ? x[row * ld + kk] : x[kk * ld + row]) * sc.lo * sc.hi;
+                }
+                tile[r][c] = v;
+            }
+            __syncthreads();
+#pragma unroll 1
+            for (int gi = threadIdx.x; gi < OZ_T * (OZ_KC / 4); gi += THREADS) {
+                const int r = gi / (OZ_KC / 4), kg = gi % (OZ_KC / 4);
+                const long long row = task.r0 + r;
+                if (row < rows) {
+                    double v[4];
+#pragma unroll
+                    for (int u = 0; u < 4; ++u) v[u] = tile[r][4 * kg + u];
+                    res::encode4<true>(v, o.nmod, planes + (size_t)row * o.kp + k0 + 4 * kg, plane);
+                }
+            }
+            __syncthreads();  // the next block overwrites the stage
+        }
+    }
+}
+
 __device__ __forceinline__ void mma_s8(int (&c)[4], const uint32_t (&a)[4], uint32_t b0, uint32_t b1) {
     asm volatile(
         "mma.sync.aligned.m16n8k32.row.col.s32.s8.s8.s32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
@@ -348,47 +413,41 @@ __device__ __forceinline__ void mma_s8(int (&c)[4], const uint32_t (&a)[4], uint
         : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
 }
 
-// Encodes a 32 x 32 chunk of one operand: rows r of op(X) (rows of op(A) or
-// columns of op(B)), k values k0..k0+31, scaled by 2^(shift - e_r), as N
-// residue planes [modulus][row][k] (OZ_ROWB bytes per row).  Threads walk the
-// contiguous direction of the stored operand.
-template <bool A_OP>
-__device__ __forceinline__ void oz_encode_chunk(const jlc_problem& P, const int* ex, int shift, int nmod,
-                                                long long r0, long long k0, char* planes) {
-    const long long rows = A_OP ? P.m : P.n;
-    const bool kcontig = A_OP ? P.layout_a == JLC_ROW_MAJOR : P.layout_b == JLC_COL_MAJOR;
-#pragma unroll 1
-    for (int gi = threadIdx.x; gi < OZ_T * (OZ_KC / 4); gi += THREADS) {
-        const int r = kcontig ? gi / (OZ_KC / 4) : gi % OZ_T;
-        const int kg = kcontig ? gi % (OZ_KC / 4) : gi / OZ_T;
-        const long long row = r0 + r, kk = k0 + 4 * kg;
-        double v[4];
-        if (row < rows) {
-            const res::Pow2 sc = res::pow2_split(shift - ex[row]);
-#pragma unroll
-            for (int u = 0; u < 4; ++u) {
-                double x = 0.0;
-                if (kk + u < P.k) x = A_OP ? elem_a(P, row, kk + u) : elem_b(P, kk + u, row);
-                v[u] = x * sc.lo * sc.hi;
-            }
-        } else {
-#pragma unroll
-            for (int u = 0; u < 4; ++u) v[u] = 0.0;
-        }
-        res::encode4<true>(v, nmod, reinterpret_cast<uint8_t*>(planes + r * OZ_ROWB + 4 * kg), OZ_PLANE);
-    }
-}
+// Shared-memory byte offset of (row r, 16-byte half h) in a 32 x 32 plane:
+// 32 bytes per row, the halves swapped on rows with bit 2 set, which keeps
+// the fragment loads (8 rows x 4 words per instruction) on 32 distinct banks.
+__device__ __forceinline__ int oz_half_off(int r, int h) { return r * 32 + ((h ^ ((r >> 2) & 1)) << 4); }
 
-__device__ void oz_tile_item(const jlc_problem& P, const OzProb& o, const int* exps, int tm, int tn, char* smem) {
+__device__ void oz_tile_item(const jlc_problem& P, const OzProb& o, const int* exps, const uint8_t* arena, int tm,
+                             int tn, char* smem) {
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int g = lane >> 2, t = lane & 3;
     const int wm = warp >> 1, wn = warp & 1;  // 2 x 2 warps of 16 x 16
     const long long m0 = (long long)tm * OZ_T, n0 = (long long)tn * OZ_T;
     const int nmod = o.nmod;
-    const int* ea = exps + o.ea_off;
-    const int* eb = exps + o.eb_off;
-    char* sA = smem;
-    char* sB = smem + res::MAX_MODULI * OZ_PLANE;
+    // copies: thread -> (row lr, half lh) of planes c = c0, c0 + 2, ... where
+    // plane c < nmod is op(A)'s modulus c and c >= nmod op(B)^T's modulus c - nmod
+    const int lr = (threadIdx.x >> 1) & (OZ_T - 1), lh = threadIdx.x & 1, c0 = threadIdx.x >> 6;
+    const bool ok_a = m0 + lr < P.m, ok_b = n0 + lr < P.n;
+    const uint8_t* src_a = arena + o.ra + (size_t)(ok_a ? m0 + lr : 0) * o.kp + 16 * lh;
+    const uint8_t* src_b = arena + o.rb + (size_t)(ok_b ? n0 + lr : 0) * o.kp + 16 * lh;
+    const size_t plane_a = (size_t)P.m * o.kp, plane_b = (size_t)P.n * o.kp;
+    const int dst_off = oz_half_off(lr, lh);
+    auto load = [&](long long ch, int s) {
+        char* st = smem + s * OZ_STAGE + dst_off;
+#pragma unroll 1
+        for (int c = c0; c < 2 * nmod; c += 2) {
+            const bool b = c >= nmod;
+            const int l = b ? c - nmod : c;
+            const uint8_t* src = (b ? src_b + l * plane_b : src_a + l * plane_a) + ch * OZ_KC;
+            cp_async16(st + (b ? res::MAX_MODULI * OZ_PLANE : 0) + l * OZ_PLANE, src, (b ? ok_b : ok_a) ? 16 : 0);
+        }
+    };
+    // fragment offsets inside a plane (fixed for the item)
+    const int fa0 = oz_half_off(wm * 16 + g, 0) + 4 * t, fa1 = oz_half_off(wm * 16 + g + 8, 0) + 4 * t;
+    const int fa2 = oz_half_off(wm * 16 + g, 1) + 4 * t, fa3 = oz_half_off(wm * 16 + g + 8, 1) + 4 * t;
+    const int fb00 = oz_half_off(wn * 16 + g, 0) + 4 * t, fb01 = oz_half_off(wn * 16 + g, 1) + 4 * t;
+    const int fb10 = oz_half_off(wn * 16 + 8 + g, 0) + 4 * t, fb11 = oz_half_off(wn * 16 + 8 + g, 1) + 4 * t;
     int acc[res::MAX_MODULI][2][4];
 #pragma unroll
     for (int l = 0; l < res::MAX_MODULI; ++l)
@@ -396,33 +455,37 @@ __device__ void oz_tile_item(const jlc_problem& P, const OzProb& o, const int* e
         for (int j = 0; j < 2; ++j)
 #pragma unroll
             for (int e = 0; e < 4; ++e) acc[l][j][e] = 0;
-    const long long nchunks = (P.k + OZ_KC - 1) / OZ_KC;
+    const long long nchunks = o.kp / OZ_KC;
+    load(0, 0);
+    cp_async_commit();
     for (long long ch = 0; ch < nchunks; ++ch) {
-        oz_encode_chunk<true>(P, ea, o.p, nmod, m0, ch * OZ_KC, sA);
-        oz_encode_chunk<false>(P, eb, o.q, nmod, n0, ch * OZ_KC, sB);
+        if (ch + 1 < nchunks) load(ch + 1, (int)((ch + 1) & 1));
+        cp_async_commit();
+        cp_async_wait<1>();  // chunk ch has landed
         __syncthreads();
+        const char* sA = smem + (ch & 1) * OZ_STAGE;
+        const char* sB = sA + res::MAX_MODULI * OZ_PLANE;
 #pragma unroll
         for (int l = 0; l < res::MAX_MODULI; ++l) {
             if (l < nmod) {
-                const char* pa = sA + l * OZ_PLANE + (wm * 16 + g) * OZ_ROWB + 4 * t;
-                const uint32_t a[4] = {*reinterpret_cast<const uint32_t*>(pa),
-                                       *reinterpret_cast<const uint32_t*>(pa + 8 * OZ_ROWB),
-                                       *reinterpret_cast<const uint32_t*>(pa + 16),
-                                       *reinterpret_cast<const uint32_t*>(pa + 8 * OZ_ROWB + 16)};
-#pragma unroll
-                for (int j = 0; j < 2; ++j) {
-                    const char* pb = sB + l * OZ_PLANE + (wn * 16 + 8 * j + g) * OZ_ROWB + 4 * t;
-                    mma_s8(acc[l][j], a, *reinterpret_cast<const uint32_t*>(pb),
-                           *reinterpret_cast<const uint32_t*>(pb + 16));
-                }
+                const char* pa = sA + l * OZ_PLANE;
+                const char* pb = sB + l * OZ_PLANE;
+                const uint32_t a[4] = {*reinterpret_cast<const uint32_t*>(pa + fa0),
+                                       *reinterpret_cast<const uint32_t*>(pa + fa1),
+                                       *reinterpret_cast<const uint32_t*>(pa + fa2),
+                                       *reinterpret_cast<const uint32_t*>(pa + fa3)};
+                mma_s8(acc[l][0], a, *reinterpret_cast<const uint32_t*>(pb + fb00),
+                       *reinterpret_cast<const uint32_t*>(pb + fb01));
+                mma_s8(acc[l][1], a, *reinterpret_cast<const uint32_t*>(pb + fb10),
+                       *reinterpret_cast<const uint32_t*>(pb + fb11));
             }
         }
-        __syncthreads();  // the next chunk overwrites the planes
+        __syncthreads();  // the stage is refilled two chunks on
         if ((ch + 1) % OZ_FOLD_CHUNKS == 0) {
+            const crt::Consts& cc = c_crt[nmod];
 #pragma unroll
             for (int l = 0; l < res::MAX_MODULI; ++l) {
                 if (l < nmod) {
-                    const crt::Consts& cc = c_crt[nmod];
 #pragma unroll
                     for (int j = 0; j < 2; ++j)
 #pragma unroll
@@ -432,29 +495,53 @@ __device__ void oz_tile_item(const jlc_problem& P, const OzProb& o, const int* e
             }
         }
     }
+    cp_async_wait<0>();
+    // epilogue: the four elements of each 16 x 8 block this thread holds,
+    // (g, 2t), (g, 2t+1), (g+8, 2t), (g+8, 2t+1), go through the packed
+    // four-element reconstruction
+    const int* ea = exps + o.ea_off;
+    const int* eb = exps + o.eb_off;
     const crt::Consts& cc = c_crt[nmod];
     const bool do_scale = P.alpha != 1.0, beta0 = P.beta == 0.0;
 #pragma unroll
-    for (int j = 0; j < 2; ++j)
+    for (int j = 0; j < 2; ++j) {
+        uint32_t words[res::MAX_MODULI];
+#pragma unroll
+        for (int l = 0; l < res::MAX_MODULI; ++l) {
+            uint32_t w = 0u;
+            if (l < nmod) {
+#pragma unroll
+                for (int e = 0; e < 4; ++e)
+                    w |= (uint32_t)crt::mod_pos(acc[l][j][e], (uint32_t)cc.m[l], cc.mu[l], cc.bias[l]) << (8 * e);
+            }
+            words[l] = w;
+        }
+        long long row[4], col[4];
+        int scale[4];
 #pragma unroll
         for (int e = 0; e < 4; ++e) {
-            const long long row = m0 + wm * 16 + g + 8 * (e >> 1);
-            const long long col = n0 + wn * 16 + 8 * j + 2 * t + (e & 1);
-            if (row >= P.m || col >= P.n) continue;
-            uint32_t r[res::MAX_MODULI];
+            row[e] = m0 + wm * 16 + g + 8 * (e >> 1);
+            col[e] = n0 + wn * 16 + 8 * j + 2 * t + (e & 1);
+            scale[e] = (row[e] < P.m && col[e] < P.n) ? ea[row[e]] + eb[col[e]] - o.p - o.q : 0;
+        }
+        double out[4];
+        crt::reconstruct4(cc, words, scale, out);
 #pragma unroll
-            for (int l = 0; l < res::MAX_MODULI; ++l)
-                r[l] = l < nmod ? (uint32_t)crt::mod_pos(acc[l][j][e], (uint32_t)cc.m[l], cc.mu[l], cc.bias[l]) : 0u;
-            double v = crt::reconstruct(cc, r, ea[row] + eb[col] - o.p - o.q);
+        for (int e = 0; e < 4; ++e) {
+            if (row[e] >= P.m || col[e] >= P.n) continue;
+            double v = out[e];
             if (do_scale) v *= P.alpha;
-            double* cp = P.c + row * P.ldc + col;
+            double* cp = P.c + row[e] * P.ldc + col[e];
             *cp = beta0 ? v : fma(P.beta, *cp, v);
         }
+    }
+    __syncthreads();  // the next item's loads overwrite the stages
 }
 
 __global__ void __launch_bounds__(THREADS, 3) grouped_oz_kernel(const jlc_problem* probs, const OzProb* oz,
                                                              const Item* items, int nitems, const int* exps,
-                                                             const int* nonfinite, int* counter) {
+                                                             const uint8_t* arena, const int* nonfinite,
+                                                             int* counter) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
     char* smem = reinterpret_cast<char*>((reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~uintptr_t(127));
     __shared__ int s_item;
@@ -468,7 +555,7 @@ __global__ void __launch_bounds__(THREADS, 3) grouped_oz_kernel(const jlc_proble
         const jlc_problem P = probs[w.prob];
         const OzProb o = oz[w.prob];
         if (!o.active || nonfinite[w.prob]) tile_dispatch<32, 32>(P, w.tm, w.tn, smem);
-        else oz_tile_item(P, o, exps, w.tm, w.tn, smem);
+        else oz_tile_item(P, o, exps, arena, w.tm, w.tn, smem);
     }
 }
 
@@ -587,6 +674,9 @@ struct jlc_grouped_plan {
     jlc::grp::OzProb* d_oz = nullptr;
     jlc::grp::ExpTask* d_tasks = nullptr;
     int ntasks = 0;
+    jlc::grp::EncTask* d_enc = nullptr;
+    int nenc = 0;
+    uint8_t* d_res = nullptr;  // residue arena
     int* d_exps = nullptr;
     int* d_nonfinite = nullptr;
     jlc_problem* d_probs = nullptr;
@@ -645,6 +735,10 @@ void free_plan_buffers(jlc_grouped_plan* pl) {
     if (pl->d_tasks) cudaFree(pl->d_tasks);
     if (pl->d_exps) cudaFree(pl->d_exps);
     if (pl->d_nonfinite) cudaFree(pl->d_nonfinite);
+    if (pl->d_enc) cudaFree(pl->d_enc);
+    if (pl->d_res) cudaFree(pl->d_res);
+    pl->d_enc = nullptr;
+    pl->d_res = nullptr;
     pl->d_oz = nullptr;
     pl->d_tasks = nullptr;
     pl->d_exps = nullptr;
@@ -693,8 +787,12 @@ int launch_plan(jlc_grouped_plan* pl, cudaStream_t st) {
         if (pl->ntasks > 0)
             oz_exps_kernel<<<(pl->ntasks * 32 + THREADS - 1) / THREADS, THREADS, 0, st>>>(
                 pl->d_probs, pl->d_oz, pl->d_tasks, pl->ntasks, pl->d_exps, pl->d_nonfinite);
-        grouped_oz_kernel<<<pl->grid, THREADS, SMEM_BYTES, st>>>(pl->d_probs, pl->d_oz, pl->d_items, pl->nitems,
-                                                                pl->d_exps, pl->d_nonfinite, pl->d_counter);
+        if (pl->nenc > 0)
+            oz_encode_kernel<<<std::min(pl->nenc, pl->ctx->sm_count * 16), THREADS, 0, st>>>(
+                pl->d_probs, pl->d_oz, pl->d_enc, pl->nenc, pl->d_exps, pl->d_nonfinite, pl->d_res);
+        grouped_oz_kernel<<<pl->grid, THREADS, OZ_LAUNCH_SMEM, st>>>(pl->d_probs, pl->d_oz, pl->d_items,
+                                                                    pl->nitems, pl->d_exps, pl->d_res,
+                                                                    pl->d_nonfinite, pl->d_counter);
         return cudaGetLastError() == cudaSuccess ? JLC_OK : JLC_E_LAUNCH;
     }
     grouped_kernel<<<pl->grid, THREADS, SMEM_BYTES, st>>>(pl->d_probs, pl->d_items, pl->nitems, pl->d_tiny,
@@ -779,6 +877,8 @@ int build_oz_plan(jlc_grouped_plan* pl, const std::vector<jlc_problem>& probs) {
     cudaStream_t st = ctx->stream;
     std::vector<OzProb> oz(probs.size());
     std::vector<ExpTask> tasks;
+    std::vector<EncTask> enc;
+    size_t res_bytes = 0;
     struct Costed {
         Item it;
         double cost;
@@ -789,7 +889,7 @@ int build_oz_plan(jlc_grouped_plan* pl, const std::vector<jlc_problem>& probs) {
     for (size_t i = 0; i < probs.size(); ++i) {
         const jlc_problem& p = probs[i];
         OzProb& o = oz[i];
-        o = OzProb{0, 0, 2, 0, 0, 0};
+        o = OzProb{0, 0, 0, 0, 2, 0, 0, 0, 0};
         if (p.m == 0 || p.n == 0) continue;
         // as on the per-call route: nothing to multiply (alpha == 0, k == 0),
         // the matrix-vector shapes (m == 1, n == 1) and products too short for
@@ -806,9 +906,19 @@ int build_oz_plan(jlc_grouped_plan* pl, const std::vector<jlc_problem>& probs) {
             arena += p.n;
             for (long long r = 0; r < p.m; r += 32) tasks.push_back(ExpTask{(int)i, 0, (int)r});
             for (long long c = 0; c < p.n; c += 32) tasks.push_back(ExpTask{(int)i, 1, (int)c});
+            // residue planes: N x rows x Kp bytes per operand (Kp a multiple of 32,
+            // so every plane row and chunk starts 16-byte aligned)
+            o.kp = (int)((p.k + OZ_KC - 1) / OZ_KC * OZ_KC);
+            o.ra = (long long)res_bytes;
+            res_bytes += (size_t)o.nmod * p.m * o.kp;
+            o.rb = (long long)res_bytes;
+            res_bytes += (size_t)o.nmod * p.n * o.kp;
+            for (long long r = 0; r < p.m; r += OZ_T) enc.push_back(EncTask{(int)i, 0, (int)r});
+            for (long long c = 0; c < p.n; c += OZ_T) enc.push_back(EncTask{(int)i, 1, (int)c});
             flops += 2.0 * p.m * p.n * p.k;
         }
-        if (arena > (1LL << 30)) return gerr(ctx, JLC_E_UNSUPPORTED, "grouped: Ozaki exponent arena too large");
+        if (arena > (1LL << 30) || enc.size() > (size_t)(1 << 30))
+            return gerr(ctx, JLC_E_UNSUPPORTED, "grouped: Ozaki plan too large");
         const int tmn = (int)((p.m + OZ_T - 1) / OZ_T), tnn = (int)((p.n + OZ_T - 1) / OZ_T);
         const double cost = (double)OZ_T * OZ_T * ((active ? (double)p.k : 0.0) + 16.0) * (active ? o.nmod : 1);
         for (int a = 0; a < tmn; ++a)
@@ -830,6 +940,8 @@ int build_oz_plan(jlc_grouped_plan* pl, const std::vector<jlc_problem>& probs) {
     if (e == cudaSuccess) e = alloc_copy((void**)&pl->d_oz, oz.data(), oz.size() * sizeof(OzProb));
     if (e == cudaSuccess) e = alloc_copy((void**)&pl->d_items, items.data(), items.size() * sizeof(Item));
     if (e == cudaSuccess) e = alloc_copy((void**)&pl->d_tasks, tasks.data(), tasks.size() * sizeof(ExpTask));
+    if (e == cudaSuccess) e = alloc_copy((void**)&pl->d_enc, enc.data(), enc.size() * sizeof(EncTask));
+    if (e == cudaSuccess) e = cudaMalloc((void**)&pl->d_res, res_bytes ? res_bytes : 16);
     if (e == cudaSuccess) e = cudaMalloc((void**)&pl->d_exps, (size_t)(arena ? arena : 1) * sizeof(int));
     if (e == cudaSuccess) e = cudaMalloc((void**)&pl->d_nonfinite, (size_t)(probs.empty() ? 1 : probs.size()) * 4);
     if (e == cudaSuccess) e = cudaMalloc((void**)&pl->d_counter, sizeof(int));
@@ -844,10 +956,11 @@ int build_oz_plan(jlc_grouped_plan* pl, const std::vector<jlc_problem>& probs) {
     }
     pl->nitems = (int)items.size();
     pl->ntasks = (int)tasks.size();
+    pl->nenc = (int)enc.size();
     pl->flops = flops;
     int per_sm = 0;
-    cudaFuncSetAttribute(grouped_oz_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, grouped_oz_kernel, THREADS, SMEM_BYTES);
+    cudaFuncSetAttribute(grouped_oz_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, OZ_LAUNCH_SMEM);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, grouped_oz_kernel, THREADS, OZ_LAUNCH_SMEM);
     if (per_sm < 1) per_sm = 1;
     pl->grid = std::max(1, std::min(pl->nitems, ctx->sm_count * per_sm));
     return JLC_OK;
