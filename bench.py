@@ -44,6 +44,7 @@ def parse():
     p.add_argument("--workload", default="dgemm", choices=["dgemm", "grouped", "configs"],
                    help="dgemm: the 8192^3 headline; grouped: 20,000 uneven problems in one launch; "
                         "configs: one line per C1-C5 shape (rate and accuracy), one GPU")
+    p.add_argument("--count", type=int, default=20000, help="grouped workload: number of problems")
     return p.parse_args()
 
 
@@ -434,7 +435,7 @@ def run_grouped(args):
     ctx = jlc_b200.Context(local)
     stream = torch.cuda.Stream()
     ctx.set_stream(stream.cuda_stream)
-    shapes, ab = c4_shapes(seed=20260604 + rank)
+    shapes, ab = c4_shapes(count=args.count, seed=20260604 + rank)
     al = lambda x: (x + 1) // 2 * 2  # each matrix starts 16-byte aligned, as separate allocations would
     total = sum(al(m * k) + al(k * n) + al(m * n) for (m, n, k) in shapes)
     g = torch.Generator(device="cuda")
@@ -481,11 +482,11 @@ def run_grouped(args):
     e1.synchronize()
     oz_ms = e0.elapsed_time(e1) / args.steps
     oz_plan.close()
-    line = {"metric": "grouped FP64 GEMM GFLOP/s (20,000 uneven problems, one persistent launch)",
+    line = {"metric": f"grouped FP64 GEMM GFLOP/s ({args.count:,} uneven problems, one persistent launch)",
             "value": round(flops / (ms * 1e-3) / 1e9, 1), "unit": "GFLOP/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 4), "higher_is_better": True,
             "dtype": "f64", "data": "synthetic uniform[-1,1), 30% M=N=K in {2,3,4}, 70% M,N,K log-uniform [8,512]",
-            "config": {"workload": "20000 uneven DGEMMs, alpha/beta uniform[-2,2], row-major, 16-byte aligned "
+            "config": {"workload": f"{args.count} uneven DGEMMs, alpha/beta uniform[-2,2], row-major, 16-byte aligned "
                                    "matrices in one arena, CUDA-graph replay",
                        "work_items": info["work_items"], "tile_small": info["tile_small"],
                        "tile_large": info["tile_large"], "flops_per_step": flops,
