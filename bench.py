@@ -41,10 +41,15 @@ def parse():
     p.add_argument("--cpu-seconds", type=float, default=12.0, help="target length of one CPU baseline sample")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu-baseline", action="store_true")
-    p.add_argument("--workload", default="dgemm", choices=["dgemm", "grouped", "configs"],
+    p.add_argument("--workload", default="dgemm", choices=["dgemm", "grouped", "configs", "harness"],
                    help="dgemm: the 8192^3 headline; grouped: 20,000 uneven problems in one launch; "
                         "configs: one line per C1-C5 shape (rate and accuracy), one GPU")
     p.add_argument("--count", type=int, default=20000, help="grouped workload: number of problems")
+    p.add_argument("--sizes", default="128,256,512", help="harness workload: square sizes")
+    p.add_argument("--iters", type=int, default=25, help="harness workload: timed iterations per backend")
+    p.add_argument("--warmups", type=int, default=8, help="harness workload: warm-up iterations per backend")
+    p.add_argument("--report-dir", default=os.path.join("build", "reports", "gemm"),
+                   help="harness workload: where the CSV/JSON reports go")
     return p.parse_args()
 
 
@@ -622,6 +627,181 @@ def run_configs(args):
     return 0
 
 
+# ----------------------------------------------------------------------------- harness (report port)
+HARNESS_BACKENDS = ["blas3-naive", "blas3-simd-1t", "blas3-parallel", "opt-1t", "opt-parallel", "cuda",
+                    "cuda-ozaki"]
+HARNESS_COLUMNS = ["timestamp", "size", "m", "k", "n", "backend", "threads", "valid", "parity_status", "oracle_type",
+                   "reference_backend", "rel_residual", "max_abs_err", "warmups", "iters", "median_ms", "mean_ms",
+                   "stddev_ms", "min_ms", "p10_ms", "p25_ms", "p75_ms", "p90_ms", "gflops_median",
+                   "speedup_vs_baseline", "baseline_label", "checksum", "notes"]
+
+
+def _percentile(sorted_v, q):
+    """Linear interpolation between order statistics (GemmBackendComparison.TimingStats)."""
+    if not sorted_v:
+        return float("nan")
+    if len(sorted_v) == 1:
+        return sorted_v[0]
+    pos = q * (len(sorted_v) - 1)
+    lo, hi = int(pos // 1), int(-(-pos // 1))
+    if lo == hi:
+        return sorted_v[lo]
+    w = pos - lo
+    return sorted_v[lo] * (1.0 - w) + sorted_v[hi] * w
+
+
+def run_harness(args):
+    """The reference's parity-gated GEMM backend comparison
+    (GemmBackendComparison.java:48-400, report columns :509-545), rerun here:
+    square sizes with GemmReference.seededMatrix inputs (seed + 31*size + 11 /
+    + 29), alpha = 1, beta = 0; every backend's C checked against
+    GemmReference.gemm (independent oracle) with the reference's tolerances
+    (GemmReference.java:175-181: CPU 1e-9 / rel 1e-12, GPU 1e-8 / rel 1e-10,
+    scaled by max|C| and k/16) before it is timed; timing as the reference's:
+    warm-ups, then iterations of max(1, 20M/flops) back-to-back calls, median /
+    mean / stddev / percentiles per call; speed-up against opt-1t (the naive
+    backend is not restated).  Backends: opt-1t and opt-parallel are the C
+    restatement of OptimizedBLAS3 (the CPU baseline, run from the oracle);
+    cuda is this library's FP64 route and cuda-ozaki its Ozaki residue route,
+    both through the CudaGemm mirror on host arrays (copies included, as
+    CudaGemm's calls are).  The blas3-* backends are not restated: SKIPPED."""
+    import datetime
+    import platform
+    import numpy as np
+    from oracle import oracle as O
+    import jlc_b200
+    from jlc_b200 import JLC_PREC_NATIVE, JLC_PREC_OZAKI_CRT, Matrix
+    from jlc_b200.compute import CudaGemm
+    world, rank, local = dist_env()
+    if rank != 0:
+        return 0
+    import torch
+    torch.cuda.set_device(local)
+    jlc_b200.Context(local)  # the library loads and the device answers before anything is timed
+    threads = os.cpu_count() or 1
+    now = datetime.datetime.now(datetime.timezone.utc)
+    stamp_iso, stamp = now.strftime("%Y-%m-%dT%H:%M:%SZ"), now.strftime("%Y%m%dT%H%M%SZ")
+    sizes = [int(x) for x in args.sizes.split(",") if x.strip()]
+    seed = 20260604
+
+    def execute(backend, a, b, size):
+        c = np.zeros((size, size))
+        if backend in ("opt-1t", "opt-parallel"):
+            out, _ = O.opt_gemm(a, b, c, 1.0, 0.0, threads=1 if backend == "opt-1t" else threads)
+            return out
+        prec = JLC_PREC_NATIVE if backend == "cuda" else JLC_PREC_OZAKI_CRT
+        cm = Matrix.wrap(c.ravel(), size, size)
+        if not CudaGemm.gemm(Matrix.wrap(a.ravel(), size, size), Matrix.wrap(b.ravel(), size, size), cm, 1.0,
+                             0.0, precision=prec):
+            return None
+        return cm.to_numpy()
+
+    rows = []
+    for size in sizes:
+        a = O.seeded_matrix(size, size, seed + size * 31 + 11)
+        b = O.seeded_matrix(size, size, seed + size * 31 + 29)
+        ref = O.gemm_reference(a, b, np.zeros((size, size)), 1.0, 0.0).ravel()
+        ref_norm = float(np.sqrt(np.sum(ref * ref)))
+        maxref = float(np.max(np.abs(ref))) if ref.size else 0.0
+        for backend in HARNESS_BACKENDS:
+            gpu = backend.startswith("cuda")
+            row = dict.fromkeys(HARNESS_COLUMNS)
+            row.update(timestamp=stamp_iso, size=size, m=size, k=size, n=size, backend=backend,
+                       threads=threads if backend in ("opt-parallel", "blas3-parallel") else 1,
+                       oracle_type="independent", reference_backend="", warmups=args.warmups, iters=args.iters)
+            if backend.startswith("blas3"):
+                row.update(valid=False, parity_status="SKIPPED",
+                           notes="BLAS3Kernels paths are not restated here; OptimizedBLAS3 (opt-*) is.")
+                rows.append(row)
+                continue
+            out = execute(backend, a, b, size)
+            if out is None:
+                row.update(valid=False, parity_status="SKIPPED", notes="GPU route returned false.")
+                rows.append(row)
+                continue
+            diff = out.ravel() - ref
+            rel = 0.0 if ref_norm == 0.0 else float(np.sqrt(np.sum(diff * diff))) / ref_norm
+            mae = float(np.max(np.abs(diff))) if diff.size else 0.0
+            abs_tol = max(1e-12, (1e-8 if gpu else 1e-9) * max(1.0, maxref) * max(1.0, size / 16.0))
+            rel_tol = 1e-10 if gpu else 1e-12
+            row.update(rel_residual=rel, max_abs_err=mae)
+            if not (mae <= abs_tol and rel <= rel_tol):
+                row.update(valid=False, parity_status="FAIL",
+                           notes=f"Parity exceeded tolerances relTol={rel_tol:g} absTol={abs_tol:g}.")
+                rows.append(row)
+                continue
+            flops = 2 * size ** 3
+            inner = max(1, -(-20_000_000 // flops))
+            checksum = 0.0
+            weights = np.arange(1, size * size + 1, dtype=np.float64)
+            for _ in range(args.warmups):
+                for _ in range(inner):
+                    checksum += float(np.dot(execute(backend, a, b, size).ravel(), weights))
+            per_call = []
+            for _ in range(args.iters):
+                t0 = time.perf_counter_ns()
+                for _ in range(inner):
+                    o = execute(backend, a, b, size)
+                per_call.append((time.perf_counter_ns() - t0) / inner)
+                checksum += float(np.dot(o.ravel(), weights))
+            srt = sorted(per_call)
+            mean = sum(per_call) / len(per_call)
+            var = sum((x - mean) ** 2 for x in per_call) / (len(per_call) - 1) if len(per_call) > 1 else 0.0
+            med = _percentile(srt, 0.5)
+            row.update(valid=True, parity_status="PASS", median_ms=med / 1e6, mean_ms=mean / 1e6,
+                       stddev_ms=var ** 0.5 / 1e6, min_ms=srt[0] / 1e6, p10_ms=_percentile(srt, 0.1) / 1e6,
+                       p25_ms=_percentile(srt, 0.25) / 1e6, p75_ms=_percentile(srt, 0.75) / 1e6,
+                       p90_ms=_percentile(srt, 0.9) / 1e6, gflops_median=flops / med if med > 0 else None,
+                       checksum=checksum,
+                       notes={"opt-1t": "C restatement of OptimizedBLAS3, one thread.",
+                              "opt-parallel": "C restatement of OptimizedBLAS3 PARALLEL_MICRO, all host threads.",
+                              "cuda": "libjlcgpu FP64 route through CudaGemm (host arrays, copies included).",
+                              "cuda-ozaki": "libjlcgpu Ozaki residue route through CudaGemm (host arrays, copies "
+                                            "included)."}[backend])
+            rows.append(row)
+        base = next((r for r in rows if r["size"] == size and r["backend"] == "opt-1t" and r["valid"]), None)
+        if base and base["median_ms"]:
+            for r in rows:
+                if r["size"] == size and r["valid"] and r["median_ms"]:
+                    r["baseline_label"] = "opt-1t"
+                    r["speedup_vs_baseline"] = base["median_ms"] / r["median_ms"]
+
+    def csv_cell(col, v):
+        if col in ("timestamp", "backend", "parity_status", "oracle_type", "reference_backend", "baseline_label",
+                   "notes"):
+            return '"' + ("" if v is None else str(v)).replace('"', '""') + '"'
+        if isinstance(v, bool):
+            return "true" if v else "false"
+        if v is None or (isinstance(v, float) and (v != v or v in (float("inf"), float("-inf")))):
+            return ""
+        return repr(v) if isinstance(v, float) else str(v)
+
+    os.makedirs(args.report_dir, exist_ok=True)
+    stable = os.path.join(args.report_dir, "gemm-backend-comparison.csv")
+    stamped = os.path.join(args.report_dir, f"gemm-backend-comparison-{stamp}.csv")
+    js = os.path.join(args.report_dir, "gemm-backend-comparison.json")
+    lines = [",".join(HARNESS_COLUMNS)] + [",".join(csv_cell(c, r[c]) for c in HARNESS_COLUMNS) for r in rows]
+    for path in (stable, stamped):
+        with open(path, "w") as f:
+            f.write("\n".join(lines) + "\n")
+    meta = {"timestamp_utc": stamp_iso, "os": platform.platform(), "available_processors": threads,
+            "cpu_model": platform.processor(), "gpu": torch.cuda.get_device_name(local),
+            "library": "libjlcgpu", "warmups": args.warmups, "iterations": args.iters, "seed": seed}
+    with open(js, "w") as f:
+        json.dump({"metadata": meta, "artifacts": {"stable_csv": os.path.abspath(stable),
+                                                   "timestamped_csv": os.path.abspath(stamped),
+                                                   "json": os.path.abspath(js)},
+                   "rows": rows}, f, indent=2)
+    print(f"{'size':>6} {'backend':>14} {'parity':>8} {'median_ms':>11} {'GFLOP/s':>10} {'speedup':>9}")
+    for r in rows:
+        fmt = lambda v, spec: format(v, spec) if isinstance(v, (int, float)) and v is not None else "-"
+        print(f"{r['size']:>6} {r['backend']:>14} {r['parity_status']:>8} {fmt(r['median_ms'], '11.4f'):>11} "
+              f"{fmt(r['gflops_median'], '10.1f'):>10} {fmt(r['speedup_vs_baseline'], '9.2f'):>9}")
+    print(json.dumps({"harness_rows": len(rows), "fail": sum(r["parity_status"] == "FAIL" for r in rows),
+                      "artifacts": [stable, stamped, js]}), flush=True)
+    return 1 if any(r["parity_status"] == "FAIL" for r in rows) else 0
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -630,6 +810,8 @@ def main():
         return run_grouped(args)
     if args.workload == "configs":
         return run_configs(args)
+    if args.workload == "harness":
+        return run_harness(args)
     return run_ours(args)
 
 
