@@ -38,8 +38,7 @@ constexpr int kMaxModuli = 15;
 constexpr int kAccBound = 1 << 28;
 
 struct Consts {
-    int nmod, p, q;
-    int qlo;                    // first limb whose share of S / M the quotient estimate needs
+    int nmod, p, q, pad;
     int m[kMaxModuli];
     uint32_t mu[kMaxModuli];    // ceil(2^38 / m_l)
     uint32_t bias[kMaxModuli];  // m_l * 2^21, a multiple of m_l above kAccBound
@@ -182,8 +181,7 @@ JLC_HD double u128_signed_to_double(U128 x, int scale) {
 JLC_HD double finish(const Consts& c, const uint64_t (&a)[4], int scale) {
     float f = 0.0f;
 #pragma unroll
-    for (int j = 0; j < 4; ++j)
-        if (j >= c.qlo) f += small_u_to_float((uint32_t)(a[j] >> c.qsh[j])) * c.qc[j];
+    for (int j = 0; j < 4; ++j) f += small_u_to_float((uint32_t)(a[j] >> c.qsh[j])) * c.qc[j];
     const uint32_t qv = (uint32_t)small_rint(f);
     // x = S - q M modulo 2^128, limb by limb with signed carries
     uint32_t y[4];
@@ -278,17 +276,6 @@ inline void build_consts(int nmod, int p, int q, const int* moduli, Consts& c) {
         long double sc = 1.0L;
         for (int t = 0; t < 32 * j + c.qsh[j]; ++t) sc *= 2.0L;
         c.qc[j] = amax[j] ? (float)(sc / Md) : 0.0f;
-    }
-    // Low limbs whose largest contribution to S / M stays below 2^-12 are left
-    // out of the estimate: the estimate only has to land within one of
-    // round(S / M) (the range check repairs that), so x is unchanged.
-    c.qlo = 0;
-    long double share = 0.0L;
-    for (int j = 0; j < 4; ++j) {
-        long double sc = (long double)amax[j];
-        for (int t = 0; t < 32 * j; ++t) sc *= 2.0L;
-        share += sc / Md;
-        if (share < 0x1p-12L) c.qlo = j + 1;
     }
 }
 
