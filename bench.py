@@ -41,7 +41,7 @@ def parse():
     p.add_argument("--cpu-seconds", type=float, default=12.0, help="target length of one CPU baseline sample")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu-baseline", action="store_true")
-    p.add_argument("--workload", default="dgemm", choices=["dgemm", "grouped", "configs", "harness"],
+    p.add_argument("--workload", default="dgemm", choices=["dgemm", "grouped", "configs", "harness", "qr"],
                    help="dgemm: the 8192^3 headline; grouped: 20,000 uneven problems in one launch; "
                         "configs: one line per C1-C5 shape (rate and accuracy), one GPU")
     p.add_argument("--count", type=int, default=20000, help="grouped workload: number of problems")
@@ -627,6 +627,52 @@ def run_configs(args):
     return 0
 
 
+# ----------------------------------------------------------------------------- blocked QR (next row)
+def run_qr(args):
+    """Device-resident blocked Householder QR of a size x size uniform[-1,1)
+    matrix (the reference's HouseholderQR.factorizeBlocked, panels of 64):
+    device time of jlc_qr_factor_device per factorisation (the matrix is
+    restored, untimed, before each), FLOPs 2mn^2 - 2n^3/3, and the share of the
+    time in the panel kernels (phase records)."""
+    import statistics
+    import torch
+    import jlc_b200
+    world, rank, local = dist_env()
+    if rank != 0:
+        return 0
+    torch.cuda.set_device(local)
+    ctx = jlc_b200.Context(local)
+    n = args.size
+    g = torch.Generator(device="cuda")
+    g.manual_seed(20260604)
+    a0 = torch.rand((n, n), dtype=torch.float64, device="cuda", generator=g) * 2 - 1
+    a = torch.empty_like(a0)
+    tau = torch.empty(n, dtype=torch.float64, device="cuda")
+    flops = 2.0 * n * n * n - 2.0 * n ** 3 / 3.0
+    times, panel = [], []
+    for it in range(args.warmup + args.steps):
+        a.copy_(a0)
+        torch.cuda.synchronize()
+        ctx.set_profiling(it >= args.warmup)
+        rep = ctx.qr_factor_device(n, n, a.data_ptr(), n, tau.data_ptr())
+        if it >= args.warmup:
+            recs = ctx.profile_collect()
+            times.append(rep["device_ms"])
+            panel.append(sum(ms for name, ms in recs if name == "qr_panel"))
+    ctx.set_profiling(False)
+    ms = statistics.median(times)
+    line = {"metric": f"blocked Householder QR GFLOP/s ({n}x{n}, FP64, device-resident)",
+            "value": round(flops / (ms * 1e-3) / 1e9, 1), "unit": "GFLOP/s", "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(ms, 3), "higher_is_better": True, "dtype": "f64",
+            "data": "synthetic uniform[-1,1) (torch Philox, seed 20260604), device resident",
+            "config": {"workload": f"QR {n}x{n}, panels of 64, compact-WY trailing update on the DMMA route"},
+            "panel_ms": round(statistics.median(panel), 3),
+            "panel_share": round(statistics.median(panel) / ms, 3)}
+    print(json.dumps(line), flush=True)
+    ctx.close()
+    return 0
+
+
 # ----------------------------------------------------------------------------- harness (report port)
 HARNESS_BACKENDS = ["blas3-naive", "blas3-simd-1t", "blas3-parallel", "opt-1t", "opt-parallel", "cuda",
                     "cuda-ozaki"]
@@ -812,6 +858,8 @@ def main():
         return run_configs(args)
     if args.workload == "harness":
         return run_harness(args)
+    if args.workload == "qr":
+        return run_qr(args)
     return run_ours(args)
 
 

@@ -179,6 +179,7 @@ JLC_API int jlc_device_status(jlc_ctx* ctx);
 #define JLC_PHASE_H2D 8         /* host -> device operand copies */
 #define JLC_PHASE_D2H 9         /* device -> host copy of C */
 #define JLC_PHASE_REDUCE 11     /* adjoint reductions: d(alpha) / d(beta) dots and sums, scaled copies */
+#define JLC_PHASE_QR_PANEL 12   /* blocked QR: one panel's factorisation kernel */
 /* Turn event-pair recording around each phase on (1) or off (0).  Records
  * accumulate (up to 4096) until collected. */
 JLC_API int jlc_set_profiling(jlc_ctx* ctx, int on);
@@ -270,6 +271,24 @@ JLC_API void jlc_grouped_plan_destroy(jlc_grouped_plan* plan);
 /* one-shot: plan, run, synchronise, destroy */
 JLC_API int jlc_dgemm_grouped_device(jlc_ctx* ctx, const jlc_problem* probs, int64_t count, int precision,
                                      jlc_report* rep);
+
+/* ---------------------------------------------------------------- blocked QR (device) */
+/* Blocked Householder QR of the column-major m x n matrix A on the device,
+ * in place: the reference's factorisation (HouseholderQR.factorizeBlocked,
+ * HouseholderQR.java:133-210: panels of 64 columns, max-normalised
+ * reflectors, compact-WY trailing update W = V^T C, W = T^T W, C -= V W), kept
+ * on the device across panels.  On return R is on and above the diagonal, the
+ * reflectors' tails (unit leading entry implied) below it, and tau holds the
+ * min(m, n) reflector scales.  precision applies to the trailing-update GEMMs.
+ * New: the reference runs this on the CPU only. */
+JLC_API int jlc_qr_factor_device(jlc_ctx* ctx, int64_t m, int64_t n, double* a, int64_t lda, double* tau,
+                                 int precision, jlc_report* rep);
+/* Q (column-major m x qcols, qcols <= m) of a factorisation made by
+ * jlc_qr_factor_device (f, ldf, tau): the reflectors applied in reverse order
+ * to the first qcols columns of the identity (HouseholderQR.buildQ,
+ * HouseholderQR.java:387-441), blocked with the same WY form. */
+JLC_API int jlc_qr_build_q_device(jlc_ctx* ctx, int64_t m, int64_t n, int64_t qcols, const double* f, int64_t ldf,
+                                  const double* tau, double* q, int64_t ldq, int precision, jlc_report* rep);
 
 /* ---------------------------------------------------------------- allocation-free entry */
 /* Ozaki-INT8 DGEMM on DEVICE pointers that allocates nothing: no context, no

@@ -217,6 +217,22 @@ class Context:
         self.check(rc)
         return rep.as_dict()
 
+    def qr_factor_device(self, m, n, a_ptr, lda, tau_ptr, precision=L.JLC_PREC_NATIVE) -> dict:
+        """Blocked Householder QR of the column-major m x n matrix at a_ptr, in
+        place (R on and above the diagonal, reflector tails below); tau_ptr
+        receives min(m, n) doubles."""
+        rep = L.Report()
+        self.check(self.lib.jlc_qr_factor_device(self.h, m, n, a_ptr, lda, tau_ptr, int(precision),
+                                                 ctypes.byref(rep)))
+        return rep.as_dict()
+
+    def qr_build_q_device(self, m, n, qcols, f_ptr, ldf, tau_ptr, q_ptr, ldq, precision=L.JLC_PREC_NATIVE) -> dict:
+        """Q (column-major m x qcols) of a factorisation from qr_factor_device."""
+        rep = L.Report()
+        self.check(self.lib.jlc_qr_build_q_device(self.h, m, n, qcols, f_ptr, ldf, tau_ptr, q_ptr, ldq,
+                                                  int(precision), ctypes.byref(rep)))
+        return rep.as_dict()
+
     def ozaki_device(self, layout_a, layout_b, m, n, k, alpha, a_ptr, lda, b_ptr, ldb, beta, c_ptr, ldc,
                      slices=0) -> dict:
         rep = L.Report()

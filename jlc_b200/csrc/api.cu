@@ -563,6 +563,71 @@ int make_tmap_3d(CUtensorMap* map, CUtensorMapDataType dt, int elem_bytes, void*
 }  // namespace jlc
 
 // ======================================================================== C ABI
+namespace {
+
+constexpr int kQrPanel = 64;  // panel width (HouseholderQR.java BLOCK_SIZE)
+
+struct QrWork {
+    double *v, *g, *t, *w, *w2;
+    long long ldv, ldw;
+};
+
+int qr_work(jlc_ctx* ctx, long long m, long long cols, QrWork& q) {
+    q.ldv = round_up(m > 0 ? m : 1, 8);
+    q.ldw = round_up(cols > 0 ? cols : 1, 8);
+    const size_t doubles = (size_t)(q.ldv * kQrPanel + 2 * kQrPanel * kQrPanel + 2 * kQrPanel * q.ldw);
+    int rc = reserve(ctx, ctx->bufQ, doubles * sizeof(double), "QR workspace");
+    if (rc) return rc;
+    q.v = static_cast<double*>(ctx->bufQ.ptr);
+    q.g = q.v + q.ldv * kQrPanel;
+    q.t = q.g + kQrPanel * kQrPanel;
+    q.w = q.t + kQrPanel * kQrPanel;
+    q.w2 = q.w + kQrPanel * q.ldw;
+    return JLC_OK;
+}
+
+// V and T of panel [k0, k0+kb) of the factored column-major matrix f (rows
+// from k0 down): V packed, G = V^T V over those rows, then T.
+int qr_panel_vt(jlc_ctx* ctx, const double* f, long long ldf, long long m, long long k0, int kb, const double* tau,
+                const QrWork& q, int precision) {
+    cudaStream_t st = ctx->stream;
+    int rc = launch_qr_pack_v(f, ldf, (int)m, (int)k0, kb, q.v, q.ldv, st);
+    if (rc) return set_err(ctx, rc, "QR: V packing launch failed");
+    // G (64 x 64, row-major) = V(k0:, :)^T V(k0:, :): op(A) = V^T as a row-major
+    // 64 x (m-k0) view, op(B) = V column-major
+    const long long rows = m - k0;
+    GemmDesc g{JLC_ROW_MAJOR, JLC_COL_MAJOR, kQrPanel, kQrPanel, rows, 1.0, 0.0, q.v + k0, q.ldv, q.v + k0, q.ldv,
+               q.g, kQrPanel};
+    rc = run_device(ctx, g, JLC_PREC_NATIVE, 0, nullptr);
+    if (rc) return rc;
+    rc = launch_qr_build_t(q.g, tau + k0, kb, q.t, st);
+    return rc ? set_err(ctx, rc, "QR: T launch failed") : JLC_OK;
+}
+
+// C (rows k0.. of a column-major m x cols block, ld ldc) <- H C with
+// H = I - V T V^T (trans_t = false) or H^T = I - V T^T V^T (trans_t = true):
+// W = V^T C, W2 = op(T) W, C -= V W2, the last as C^T -= W2^T V^T so that the
+// column-major C is the GEMM's row-major output.
+int qr_apply_wy(jlc_ctx* ctx, long long m, long long k0, long long cols, double* c, long long ldc, bool trans_t,
+                const QrWork& q, int precision) {
+    if (cols <= 0) return JLC_OK;
+    const long long rows = m - k0;
+    GemmDesc w{JLC_ROW_MAJOR, JLC_COL_MAJOR, kQrPanel, cols, rows, 1.0, 0.0, q.v + k0, q.ldv, c + k0, ldc, q.w,
+               q.ldw};
+    int rc = run_device(ctx, w, precision, 0, nullptr);
+    if (rc) return rc;
+    // op(T): T is row-major, so T^T is the same array read column-major
+    GemmDesc t{trans_t ? JLC_COL_MAJOR : JLC_ROW_MAJOR, JLC_ROW_MAJOR, kQrPanel, cols, kQrPanel, 1.0, 0.0, q.t,
+               kQrPanel, q.w, q.ldw, q.w2, q.ldw};
+    rc = run_device(ctx, t, JLC_PREC_NATIVE, 0, nullptr);
+    if (rc) return rc;
+    GemmDesc u{JLC_COL_MAJOR, JLC_ROW_MAJOR, cols, rows, kQrPanel, -1.0, 1.0, q.w2, q.ldw, q.v + k0, q.ldv,
+               c + k0, ldc};
+    return run_device(ctx, u, precision, 0, nullptr);
+}
+
+}  // namespace
+
 extern "C" {
 
 int jlc_version(void) { return JLCGPU_VERSION; }
@@ -850,6 +915,86 @@ int jlc_check_fp64_bound_device(jlc_ctx* ctx, int layout_a, int layout_b, int64_
     *max_ratio = r;
     *max_abs = ab;
     *over = (int64_t)h[2];
+    return JLC_OK;
+}
+
+int jlc_qr_factor_device(jlc_ctx* ctx, int64_t m, int64_t n, double* a, int64_t lda, double* tau, int precision,
+                         jlc_report* rep) {
+    report_init(rep);
+    if (!ctx) return JLC_E_ARG;
+    if (m < 0 || n < 0) return set_err(ctx, JLC_E_ARG, "dimensions must be non-negative");
+    if (m == 0 || n == 0) return JLC_OK;
+    if (!a || !tau || lda < m) return set_err(ctx, JLC_E_ARG, "A and tau must not be null and lda must be >= m");
+    if (m > INT32_MAX / 2 || n > INT32_MAX / 2) return set_err(ctx, JLC_E_UNSUPPORTED, "dimension above 2^30");
+    cudaSetDevice(ctx->device);
+    ctx->err[0] = 0;
+    QrWork q;
+    int rc = qr_work(ctx, m, n, q);
+    if (rc) return rc;
+    cudaEventRecord(ctx->ev0, ctx->stream);
+    const long long kmax = m < n ? m : n;
+    for (long long k0 = 0; k0 < kmax; k0 += kQrPanel) {
+        const int kb = (int)(kmax - k0 < kQrPanel ? kmax - k0 : kQrPanel);
+        {
+            Phase ph(ctx, JLC_PHASE_QR_PANEL);
+            ctx->launches += 1;
+            rc = launch_qr_panel(a, lda, (int)m, (int)k0, kb, tau, ctx->stream);
+            if (rc) return set_err(ctx, rc, "QR: panel launch failed");
+        }
+        const long long trail = n - (k0 + kb);
+        if (trail <= 0) continue;
+        rc = qr_panel_vt(ctx, a, lda, m, k0, kb, tau, q, precision);
+        if (!rc) rc = qr_apply_wy(ctx, m, k0, trail, a + (k0 + kb) * lda, lda, true, q, precision);
+        if (rc) return rc;
+    }
+    cudaEventRecord(ctx->ev1, ctx->stream);
+    rc = finish_sync(ctx);
+    if (rc) return rc;
+    if (rep) {
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
+        rep->device_ms = ms;
+        rep->kernel = JLC_KERNEL_DMMA;
+    }
+    return JLC_OK;
+}
+
+int jlc_qr_build_q_device(jlc_ctx* ctx, int64_t m, int64_t n, int64_t qcols, const double* f, int64_t ldf,
+                          const double* tau, double* q_out, int64_t ldq, int precision, jlc_report* rep) {
+    report_init(rep);
+    if (!ctx) return JLC_E_ARG;
+    if (m < 0 || n < 0 || qcols < 0 || qcols > m) return set_err(ctx, JLC_E_ARG, "need 0 <= qcols <= m");
+    if (m == 0 || qcols == 0) return JLC_OK;
+    if (!q_out || ldq < m) return set_err(ctx, JLC_E_ARG, "Q must not be null and ldq must be >= m");
+    const long long kmax = m < n ? m : n;
+    if (kmax > 0 && (!f || !tau || ldf < m)) return set_err(ctx, JLC_E_ARG, "F and tau must not be null, ldf >= m");
+    if (m > INT32_MAX / 2 || n > INT32_MAX / 2) return set_err(ctx, JLC_E_UNSUPPORTED, "dimension above 2^30");
+    cudaSetDevice(ctx->device);
+    ctx->err[0] = 0;
+    QrWork q;
+    int rc = qr_work(ctx, m, qcols, q);
+    if (rc) return rc;
+    cudaEventRecord(ctx->ev0, ctx->stream);
+    // Q = I (first qcols columns), then the panels' H applied in reverse order;
+    // panel k0 changes only rows and columns from k0 on
+    rc = launch_set_identity(q_out, ldq, m, qcols, ctx->stream);
+    if (rc) return set_err(ctx, rc, "QR: identity launch failed");
+    for (long long k0 = (kmax - 1) / kQrPanel * kQrPanel; k0 >= 0 && kmax > 0; k0 -= kQrPanel) {
+        const int kb = (int)(kmax - k0 < kQrPanel ? kmax - k0 : kQrPanel);
+        if (k0 >= qcols) continue;
+        rc = qr_panel_vt(ctx, f, ldf, m, k0, kb, tau, q, precision);
+        if (!rc) rc = qr_apply_wy(ctx, m, k0, qcols - k0, q_out + k0 * ldq, ldq, false, q, precision);
+        if (rc) return rc;
+    }
+    cudaEventRecord(ctx->ev1, ctx->stream);
+    rc = finish_sync(ctx);
+    if (rc) return rc;
+    if (rep) {
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
+        rep->device_ms = ms;
+        rep->kernel = JLC_KERNEL_DMMA;
+    }
     return JLC_OK;
 }
 

@@ -70,6 +70,12 @@ bool dmma_operand_ok(const void* ptr, long long ld);
 // nonzero (the Ozaki split's non-finite flags for A and B).
 // ksplit > 1 with splitk_ws of at least dmma_splitk_bytes(m, n, ksplit):
 // split-K over ksplit parts; otherwise every tile is one work unit.
+// blocked Householder QR kernels (qr.cu)
+int launch_qr_panel(double* a, long long lda, int m, int k0, int kb, double* tau, cudaStream_t st);
+int launch_qr_pack_v(const double* a, long long lda, int m, int k0, int kb, double* v, long long ldv,
+                     cudaStream_t st);
+int launch_qr_build_t(const double* g, const double* tau, int kb, double* t, cudaStream_t st);
+int launch_set_identity(double* q, long long ldq, long long m, long long cols, cudaStream_t st);
 int launch_dgemm_dmma(const GemmDesc& g, cudaStream_t st, int sm_count, int* status, const int* gate, int mma_k,
                       char* err, size_t errlen, int ksplit = 1, void* splitk_ws = nullptr,
                       size_t splitk_ws_bytes = 0);
@@ -148,6 +154,7 @@ struct jlc_ctx {
     int* d_flags = nullptr;   // control flags (e.g. the Ozaki non-finite gate)
     DevBuf bufA, bufB, bufC;
     DevBuf bufR;  // reduction partials (adjoint)
+    DevBuf bufQ;  // blocked QR: V, G, T and the two W panels
     Workspace ws;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     // host-entry pipeline: copy-in and copy-out streams beside `stream`, and

@@ -228,3 +228,84 @@ def sample_entries(m: int, n: int, count: int, seed: int):
             extra_r.append(i)
             extra_c.append(j)
     return np.concatenate([r, np.array(extra_r, np.int64)]), np.concatenate([c, np.array(extra_c, np.int64)])
+
+
+# ------------------------------------------------------------- blocked Householder QR
+def householder_qr_blocked(a, block: int = 64):
+    """HouseholderQR.factorizeBlocked (HouseholderQR.java:133-210) restated on a
+    copy of the m x n array a: panels of `block` columns factored column by
+    column (computeHouseholder :219-292 with the max normalisation,
+    applyHouseholderToColumn :345-384 on the panel's later columns), then the
+    trailing columns updated with the compact-WY form (packV :445-471, buildT
+    :297-325, W = V^T C, W = T^T W, C -= V W :167-210; the reference's 128-column
+    blocking of C does not change the arithmetic of a full product).  Returns
+    (F, tau): F[:, k] is column k of the factored column-major matrix (R on and
+    above the diagonal, reflector tails below), tau the min(m, n) scales."""
+    import math
+    f = np.array(a, dtype=np.float64, copy=True)
+    m, n = f.shape
+    kmax = min(m, n)
+    tau = np.zeros(kmax)
+    tiny = np.finfo(np.float64).tiny
+    for k0 in range(0, kmax, block):
+        k1 = min(k0 + block, kmax)
+        for k in range(k0, k1):
+            col = f[:, k]
+            t = 0.0
+            if m - k > 1:
+                mx = float(np.max(np.abs(col[k:])))
+                if mx >= tiny:
+                    inv = 1.0 / mx
+                    x0 = col[k] * inv
+                    xnorm = math.sqrt(float(np.sum((col[k + 1:] * inv) ** 2)))
+                    if xnorm == 0.0:
+                        if x0 < 0.0:
+                            t = 2.0
+                            col[k] = -col[k]
+                    else:
+                        nb = -math.copysign(math.hypot(x0, xnorm), x0)
+                        t = (nb - x0) / nb
+                        col[k + 1:] *= 1.0 / ((x0 - nb) * mx)
+                        col[k] = nb * mx
+            tau[k] = t
+            for j in range(k + 1, k1):
+                cj = f[:, j]
+                dot = (cj[k] + float(np.dot(col[k + 1:], cj[k + 1:]))) * t
+                cj[k] -= dot
+                cj[k + 1:] -= dot * col[k + 1:]
+        if k1 < n:
+            kb = k1 - k0
+            v = np.zeros((m, block))
+            for i in range(kb):
+                k = k0 + i
+                v[k, i] = 1.0
+                v[k + 1:, i] = f[k + 1:, k]
+            tm = np.zeros((block, block))
+            for i in range(kb):
+                ti = tau[k0 + i]
+                tm[i, i] = ti
+                for r in range(i):
+                    tm[r, i] = -ti * float(np.dot(v[k0 + i:, r], v[k0 + i:, i]))
+                for r in range(i):  # in place, increasing r (reads entries not yet overwritten)
+                    tm[r, i] = sum(tm[r, c] * tm[c, i] for c in range(r, i))
+            c = f[:, k1:]
+            w = tm.T @ (v.T @ c)
+            f[:, k1:] = c - v @ w
+    return f, tau
+
+
+def householder_build_q(f, tau, qcols: int):
+    """HouseholderQR.buildQ (HouseholderQR.java:387-441): the reflectors of a
+    factorisation applied in reverse order to the first qcols columns of the
+    identity; returns Q (m x qcols)."""
+    m = f.shape[0]
+    q = np.eye(m, qcols)
+    for k in reversed(range(len(tau))):
+        t = tau[k]
+        if t == 0.0 or k >= qcols:
+            continue
+        v = f[k + 1:, k]
+        dots = (q[k, k:] + v @ q[k + 1:, k:]) * t
+        q[k, k:] -= dots
+        q[k + 1:, k:] -= np.outer(v, dots)
+    return q
