@@ -570,19 +570,22 @@ constexpr int kQrPanel = 64;  // panel width (HouseholderQR.java BLOCK_SIZE)
 struct QrWork {
     double *v, *g, *t, *w, *w2;
     long long ldv, ldw;
+    void* panel_scratch;  // multi-CTA panel: partials, row records, barrier counter
 };
 
 int qr_work(jlc_ctx* ctx, long long m, long long cols, QrWork& q) {
     q.ldv = round_up(m > 0 ? m : 1, 8);
     q.ldw = round_up(cols > 0 ? cols : 1, 8);
     const size_t doubles = (size_t)(q.ldv * kQrPanel + 2 * kQrPanel * kQrPanel + 2 * kQrPanel * q.ldw);
-    int rc = reserve(ctx, ctx->bufQ, doubles * sizeof(double), "QR workspace");
+    const size_t scratch = qr_panel_mp_scratch_bytes(ctx->sm_count > 0 ? ctx->sm_count : 1);
+    int rc = reserve(ctx, ctx->bufQ, doubles * sizeof(double) + scratch, "QR workspace");
     if (rc) return rc;
     q.v = static_cast<double*>(ctx->bufQ.ptr);
     q.g = q.v + q.ldv * kQrPanel;
     q.t = q.g + kQrPanel * kQrPanel;
     q.w = q.t + kQrPanel * kQrPanel;
     q.w2 = q.w + kQrPanel * q.ldw;
+    q.panel_scratch = q.w2 + kQrPanel * q.ldw;
     return JLC_OK;
 }
 
@@ -936,9 +939,17 @@ int jlc_qr_factor_device(jlc_ctx* ctx, int64_t m, int64_t n, double* a, int64_t 
     for (long long k0 = 0; k0 < kmax; k0 += kQrPanel) {
         const int kb = (int)(kmax - k0 < kQrPanel ? kmax - k0 : kQrPanel);
         {
+            // tall panels: rows split over up to one CTA per SM (>= 128 rows
+            // each) in one cooperative launch; short ones: one CTA
             Phase ph(ctx, JLC_PHASE_QR_PANEL);
             ctx->launches += 1;
-            rc = launch_qr_panel(a, lda, (int)m, (int)k0, kb, tau, ctx->stream);
+            long long ctas = (m - k0) / 128;
+            if (ctas > ctx->sm_count) ctas = ctx->sm_count;
+            if (ctas >= 2)
+                rc = launch_qr_panel_mp(a, lda, (int)m, (int)k0, kb, tau, (int)ctas, q.panel_scratch, ctx->d_status,
+                                        ctx->stream);
+            else
+                rc = launch_qr_panel(a, lda, (int)m, (int)k0, kb, tau, ctx->stream);
             if (rc) return set_err(ctx, rc, "QR: panel launch failed");
         }
         const long long trail = n - (k0 + kb);

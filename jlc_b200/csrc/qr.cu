@@ -15,6 +15,7 @@
 #include <cfloat>
 #include <cmath>
 
+#include "jlc_device.cuh"
 #include "jlc_internal.h"
 
 namespace jlc {
@@ -119,6 +120,207 @@ __global__ void __launch_bounds__(PANEL_THREADS) qr_panel_kernel(double* A, long
     }
 }
 
+// ------------------------------------------------------------ multi-CTA panel
+// The same factorisation with the panel's rows split over the CTAs of one
+// cooperative launch (CTA c owns rows [k0 + c R, k0 + (c+1) R)).  Per column
+// k, one pass per CTA over its rows gives the column's local max, its scaled
+// sum of squares (scale, ssq) and its dots with the panel's later columns
+// (with the column still unscaled); one grid barrier; every CTA combines the
+// CTAs' partials in CTA order (the same result everywhere, and the same bits
+// on every run), forms beta, tau and 1/(x0 - beta) as the reference does
+// (sigma = (scale/max)^2 ssq, dot_j = (a_kj + sum_i x_i a_ij / (x0 - beta))
+// tau), then scales and updates its own rows.  Row k's entries reach the
+// other CTAs through a row record written by its owner before the barrier;
+// partial and row records alternate between two buffers by column parity,
+// so one barrier per column is enough.
+constexpr int MP_THREADS = 256, MP_WARPS = MP_THREADS / 32;
+constexpr int MP_PART = 72;  // per CTA and column: max, scale, ssq, dots with up to 63 later columns
+
+__device__ __forceinline__ unsigned ld_acquire_u32(const unsigned* p) {
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+// All CTAs of the launch arrive, then wait until `target` arrivals are
+// counted.  Bounded: past kWaitTimeoutNs (or once another CTA has recorded an
+// error) it records JLC_DEV_TIMEOUT and returns false in every thread.
+__device__ bool grid_barrier(unsigned* counter, unsigned target, int* status, int* s_ok) {
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        atomicAdd(counter, 1u);
+        const uint64_t t0 = globaltimer_ns();
+        int ok = 1;
+        for (unsigned it = 0; ld_acquire_u32(counter) < target; ++it) {
+            if ((it & 63u) == 0u) {
+                if (*(volatile int*)status != 0) {
+                    ok = 0;
+                    break;
+                }
+                if (globaltimer_ns() - t0 > kWaitTimeoutNs) {
+                    atomicOr(status, JLC_DEV_TIMEOUT);
+                    ok = 0;
+                    break;
+                }
+            }
+        }
+        __threadfence();
+        *s_ok = ok;
+    }
+    __syncthreads();
+    return *s_ok != 0;
+}
+
+// (scale, ssq) pairs: sum of squares = scale^2 * ssq, combined without overflow
+__device__ __forceinline__ void ssq_add(double& scale, double& ssq, double x) {
+    const double a = fabs(x);
+    if (a == 0.0) return;
+    if (a > scale) {
+        const double r = scale / a;
+        ssq = 1.0 + ssq * r * r;
+        scale = a;
+    } else {
+        const double r = a / scale;
+        ssq += r * r;
+    }
+}
+__device__ __forceinline__ void ssq_merge(double& scale, double& ssq, double s2, double q2) {
+    if (s2 == 0.0) return;
+    if (s2 > scale) {
+        const double r = scale / s2;
+        ssq = q2 + ssq * r * r;
+        scale = s2;
+    } else {
+        const double r = s2 / scale;
+        ssq += q2 * r * r;
+    }
+}
+
+__global__ void __launch_bounds__(MP_THREADS) qr_panel_mp_kernel(double* A, long long lda, int m, int k0, int kb,
+                                                                 double* tau, double* part, double* rowrec,
+                                                                 unsigned* counter, int* status) {
+    __shared__ double fin[64];  // fin[0] = tau, fin[t] = dot_t for the later columns
+    __shared__ double fin_v0inv, fin_beta;
+    __shared__ int fin_mode;  // 0: no reflector, 1: reflector, 2: sign flip (tau = 2)
+    __shared__ int s_ok;
+    const int P = gridDim.x, cta = blockIdx.x;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int R = (m - k0 + P - 1) / P;
+    const int r0 = k0 + cta * R, r1 = min(m, r0 + R);
+    for (int kk = 0; kk < kb; ++kk) {
+        const int k = k0 + kk;
+        const int later = kb - kk - 1;  // columns k+1 .. k0+kb-1
+        const double* colk = A + (long long)k * lda;
+        double* pk = part + ((size_t)(kk & 1) * P + cta) * MP_PART;
+        double* rk = rowrec + (size_t)(kk & 1) * 64;
+        // Phase A: this CTA's rows -- task 0 the column's max and (scale, ssq)
+        // over rows > k, task t >= 1 the dot of column k with column k + t
+        const int lo = max(r0, k), lo1 = max(r0, k + 1);
+        for (int t = warp; t <= later; t += MP_WARPS) {
+            if (t == 0) {
+                double mx = 0.0, sc = 0.0, sq = 0.0;
+                for (int i = lo + lane; i < r1; i += 32) {
+                    const double x = colk[i];
+                    mx = fmax(mx, fabs(x));
+                    if (i > k) ssq_add(sc, sq, x);
+                }
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) {
+                    mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+                    const double s2 = __shfl_xor_sync(0xffffffffu, sc, o);
+                    const double q2 = __shfl_xor_sync(0xffffffffu, sq, o);
+                    // merge in a fixed orientation so both lanes of a pair hold the same result
+                    double a_s = (lane & o) ? s2 : sc, a_q = (lane & o) ? q2 : sq;
+                    const double b_s = (lane & o) ? sc : s2, b_q = (lane & o) ? sq : q2;
+                    ssq_merge(a_s, a_q, b_s, b_q);
+                    sc = a_s;
+                    sq = a_q;
+                }
+                if (lane == 0) {
+                    pk[0] = mx;
+                    pk[1] = sc;
+                    pk[2] = sq;
+                }
+            } else {
+                const double* cj = A + (long long)(k + t) * lda;
+                double d = 0.0;
+                for (int i = lo1 + lane; i < r1; i += 32) d = fma(colk[i], cj[i], d);
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) d += __shfl_xor_sync(0xffffffffu, d, o);
+                if (lane == 0) pk[2 + t] = d;
+            }
+        }
+        // row k (its owner): x0 and the later columns' entries on row k
+        if (k >= r0 && k < r1)
+            for (int t = tid; t <= later; t += MP_THREADS) rk[t] = A[(long long)(k + t) * lda + k];
+        if (!grid_barrier(counter, (unsigned)(kk + 1) * (unsigned)P, status, &s_ok)) return;
+        // Phase B: combine the CTAs' partials in CTA order
+        const double* pb = part + (size_t)(kk & 1) * P * MP_PART;
+        if (tid == 0) {
+            fin_mode = 0;
+            if (m - k > 1) {
+                double mx = 0.0, sc = 0.0, sq = 0.0;
+                for (int q = 0; q < P; ++q) {
+                    mx = fmax(mx, pb[q * MP_PART]);
+                    ssq_merge(sc, sq, pb[q * MP_PART + 1], pb[q * MP_PART + 2]);
+                }
+                if (mx >= DBL_MIN) {
+                    const double inv = 1.0 / mx;  // as the reference: x * (1/max)
+                    const double x0 = rk[0] * inv;
+                    const double r = sc * inv;
+                    const double xnorm = sqrt(r * r * sq);
+                    if (xnorm == 0.0) {
+                        if (x0 < 0.0) fin_mode = 2;
+                    } else {
+                        const double nb = -copysign(hypot(x0, xnorm), x0);
+                        fin_mode = 1;
+                        fin_beta = nb * mx;
+                        fin_v0inv = 1.0 / ((x0 - nb) * mx);
+                        fin[0] = (nb - x0) / nb;  // tau
+                    }
+                }
+            }
+        }
+        __syncthreads();
+        const int mode = fin_mode;
+        const double tk = mode == 1 ? fin[0] : (mode == 2 ? 2.0 : 0.0);
+        if (mode == 1) {
+            for (int t = 1 + tid; t <= later; t += MP_THREADS) {
+                double d = 0.0;
+                for (int q = 0; q < P; ++q) d += pb[q * MP_PART + 2 + t];
+                fin[t] = (rk[t] + d * fin_v0inv) * tk;
+            }
+        } else if (mode == 2) {
+            for (int t = 1 + tid; t <= later; t += MP_THREADS) fin[t] = rk[t] * 2.0;  // the tail is zero
+        }
+        if (cta == 0 && tid == 0) tau[k] = tk;
+        __syncthreads();
+        if (mode != 0) {
+            // Phase C: reflector tail on this CTA's rows, then the later columns
+            const int nrows = r1 - lo1;
+            if (mode == 1) {
+                double* ck = A + (long long)k * lda;
+                for (int i = lo1 + tid; i < r1; i += MP_THREADS) ck[i] *= fin_v0inv;
+            }
+            if (k >= r0 && k < r1 && tid == 0) {
+                double* ck = A + (long long)k * lda;
+                ck[k] = mode == 1 ? fin_beta : -ck[k];
+            }
+            __syncthreads();
+            if (nrows > 0) {
+                for (int e = tid; e < nrows * later; e += MP_THREADS) {
+                    const int i = lo1 + e % nrows, t = 1 + e / nrows;
+                    A[(long long)(k + t) * lda + i] -= fin[t] * colk[i];
+                }
+            }
+            if (k >= r0 && k < r1)
+                for (int t = 1 + tid; t <= later; t += MP_THREADS) A[(long long)(k + t) * lda + k] -= fin[t];
+        }
+        __syncthreads();
+    }
+}
+
 // V (ldv x 64, column-major): column i < kb holds reflector k0+i (zeros above
 // row k0+i, one on it, A's tail below); columns kb .. 63 are zero.
 __global__ void qr_pack_v_kernel(const double* A, long long lda, int m, int k0, int kb, double* V, long long ldv) {
@@ -172,6 +374,25 @@ __global__ void set_diag_kernel(double* q, long long ldq, long long d) {
 int launch_qr_panel(double* a, long long lda, int m, int k0, int kb, double* tau, cudaStream_t st) {
     qr::qr_panel_kernel<<<1, qr::PANEL_THREADS, 0, st>>>(a, lda, m, k0, kb, tau);
     return cudaGetLastError() == cudaSuccess ? JLC_OK : JLC_E_LAUNCH;
+}
+
+// Multi-CTA panel: P CTAs in one cooperative launch (all resident at once);
+// scratch holds 2 x P x MP_PART partials, 2 x 64 row entries and the barrier
+// counter (zeroed here before the launch).
+size_t qr_panel_mp_scratch_bytes(int P) {
+    return ((size_t)2 * P * qr::MP_PART + 128) * sizeof(double) + 256;
+}
+
+int launch_qr_panel_mp(double* a, long long lda, int m, int k0, int kb, double* tau, int P, void* scratch,
+                       int* status, cudaStream_t st) {
+    double* part = static_cast<double*>(scratch);
+    double* rowrec = part + (size_t)2 * P * qr::MP_PART;
+    unsigned* counter = reinterpret_cast<unsigned*>(rowrec + 128);
+    if (cudaMemsetAsync(counter, 0, sizeof(unsigned), st) != cudaSuccess) return JLC_E_LAUNCH;
+    void* args[] = {&a, &lda, &m, &k0, &kb, &tau, &part, &rowrec, &counter, &status};
+    cudaError_t e = cudaLaunchCooperativeKernel((const void*)qr::qr_panel_mp_kernel, dim3(P), dim3(qr::MP_THREADS),
+                                                args, 0, st);
+    return e == cudaSuccess ? JLC_OK : JLC_E_LAUNCH;
 }
 
 int launch_qr_pack_v(const double* a, long long lda, int m, int k0, int kb, double* v, long long ldv,
