@@ -144,12 +144,14 @@ __device__ __forceinline__ unsigned ld_acquire_u32(const unsigned* p) {
 
 // All CTAs of the launch arrive, then wait until `target` arrivals are
 // counted.  Bounded: past kWaitTimeoutNs (or once another CTA has recorded an
-// error) it records JLC_DEV_TIMEOUT and returns false in every thread.
+// error) it records JLC_DEV_TIMEOUT and returns false in every thread.  The
+// arrival is a release reduction and the poll an acquire load: with the CTA
+// barriers on either side, every write a CTA made before arriving is visible
+// to every thread of every CTA after the wait.
 __device__ bool grid_barrier(unsigned* counter, unsigned target, int* status, int* s_ok) {
     __syncthreads();
     if (threadIdx.x == 0) {
-        __threadfence();
-        atomicAdd(counter, 1u);
+        asm volatile("red.release.gpu.global.add.u32 [%0], %1;" ::"l"(counter), "r"(1u) : "memory");
         const uint64_t t0 = globaltimer_ns();
         int ok = 1;
         for (unsigned it = 0; ld_acquire_u32(counter) < target; ++it) {
@@ -165,7 +167,6 @@ __device__ bool grid_barrier(unsigned* counter, unsigned target, int* status, in
                 }
             }
         }
-        __threadfence();
         *s_ok = ok;
     }
     __syncthreads();
@@ -321,6 +322,210 @@ __global__ void __launch_bounds__(MP_THREADS) qr_panel_mp_kernel(double* A, long
     }
 }
 
+// The multi-CTA panel with each CTA's rows held in shared memory for the
+// whole panel (slab = kb columns x R rows, column-major, loaded once and
+// written back once), so the per-column passes touch no global memory but
+// the partials.  The column's sum of squares is kept as (e, s) with
+// sum = s * 4^e, e a power-of-two exponent taken from a maximum (clamped to
+// +-1000 so that 2^-e is a normal number): every rescaling is exact, and the
+// merge needs no division.  The partials are laid out by quantity
+// (part[q][cta]); warp lanes merge them in a fixed order (lane l takes CTAs
+// l, l+32, ..., then a butterfly), so every CTA derives the same bits.
+constexpr int SP_MAX_SLAB_BYTES = 200 * 1024;
+constexpr int SP_MAX_CTAS = 160;                    // partial loads: up to 5 per lane
+constexpr int SP_TASKS = 64 / MP_WARPS;             // later columns per warp
+constexpr double SP_EMPTY_EXP = -4096.0;            // exponent of an empty (e, s) pair
+
+// exponent e with 2^e <= x < 2^(e+1) for a positive normal x, clamped to [-1000, 1000]
+__device__ __forceinline__ int sp_exp(double x) {
+    const int ex = (int)((__double_as_longlong(x) >> 52) & 0x7ff);
+    return x > 0.0 && ex != 0x7ff ? min(1000, max(-1000, ex - 1023)) : 0;
+}
+__device__ __forceinline__ double sp_pow2(int e) {  // 2^e, -1022 <= e <= 1023
+    return __longlong_as_double((long long)(e + 1023) << 52);
+}
+// s * 2^d for d <= 0 (flushed to zero below d = -2044, where the term is negligible)
+__device__ __forceinline__ double sp_scale(double s, int d) {
+    if (d >= -1022) return s * sp_pow2(d);
+    if (d >= -2044) return (s * sp_pow2(-1022)) * sp_pow2(d + 1022);
+    return 0.0;
+}
+// (e, s) += (e2, s2), both sums of squares in units of 4^e
+__device__ __forceinline__ void sp_merge(double& e, double& s, double e2, double s2) {
+    const double E = fmax(e, e2);
+    s = sp_scale(s, 2 * (int)(e - E)) + sp_scale(s2, 2 * (int)(e2 - E));
+    e = E;
+}
+
+__global__ void __launch_bounds__(MP_THREADS) qr_panel_sm_kernel(double* A, long long lda, int m, int k0, int kb,
+                                                                 double* tau, double* part, double* rowrec,
+                                                                 unsigned* counter, int* status) {
+    extern __shared__ double slab[];  // slab[c * R + (i - r0)] = A[i, k0 + c]
+    __shared__ double fin[64];
+    __shared__ double fin_v0inv, fin_beta, fin_tau;
+    __shared__ int fin_mode;
+    __shared__ int s_ok;
+    const int P = gridDim.x, cta = blockIdx.x;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int R = (m - k0 + P - 1) / P;
+    const int r0 = k0 + cta * R, r1 = min(m, r0 + R);
+    const int rows = max(0, r1 - r0);
+    for (int e = tid; e < rows * kb; e += MP_THREADS) {
+        const int c = e / rows, i = e - c * rows;
+        slab[c * R + i] = A[(long long)(k0 + c) * lda + r0 + i];
+    }
+    __syncthreads();
+    for (int kk = 0; kk < kb; ++kk) {
+        const int k = k0 + kk;
+        const int later = kb - kk - 1;
+        double* ck = slab + kk * R;  // ck[i - r0] = A[i, k] for own rows i
+        double* pk = part + (size_t)(kk & 1) * MP_PART * P + cta;
+        double* rk = rowrec + (size_t)(kk & 1) * 64;
+        const int lo = max(r0, k), lo1 = max(r0, k + 1);
+        // Phase A: warp w the dots of column k with the later columns
+        // t = 1 + w + 8j (all j together); the last warp also the column's
+        // max over rows >= k and its sum of squares over rows > k
+        {
+            double d[SP_TASKS];
+#pragma unroll
+            for (int j = 0; j < SP_TASKS; ++j) d[j] = 0.0;
+            for (int i = lo1 + lane; i < r1; i += 32) {
+                const double x = ck[i - r0];
+#pragma unroll
+                for (int j = 0; j < SP_TASKS; ++j) {
+                    const int t = 1 + warp + j * MP_WARPS;
+                    if (t <= later) d[j] = fma(x, ck[t * R + (i - r0)], d[j]);
+                }
+            }
+#pragma unroll
+            for (int j = 0; j < SP_TASKS; ++j) {
+                const int t = 1 + warp + j * MP_WARPS;
+                if (t <= later) {  // warp-uniform
+                    const double v = warp_sum(d[j]);
+                    if (lane == 0) pk[(2 + t) * P] = v;
+                }
+            }
+            if (warp == MP_WARPS - 1) {
+                double mx = 0.0;
+                for (int i = lo + lane; i < r1; i += 32) mx = fmax(mx, fabs(ck[i - r0]));
+                mx = warp_max(mx);
+                const int e = sp_exp(mx);
+                const double sc = sp_pow2(-e);
+                double sq = 0.0;
+                for (int i = lo1 + lane; i < r1; i += 32) {
+                    const double y = ck[i - r0] * sc;
+                    sq = fma(y, y, sq);
+                }
+                sq = warp_sum(sq);
+                if (lane == 0) {
+                    pk[0] = mx;
+                    pk[P] = (double)e;
+                    pk[2 * P] = sq;
+                }
+            }
+        }
+        if (k >= r0 && k < r1)
+            for (int t = tid; t <= later; t += MP_THREADS) rk[t] = ck[t * R + (k - r0)];
+        if (!grid_barrier(counter, (unsigned)(kk + 1) * (unsigned)P, status, &s_ok)) return;
+        // Phase B: merge the CTAs' partials (every CTA the same way).  All
+        // loads are issued before any result is needed.
+        const double* pb = part + (size_t)(kk & 1) * MP_PART * P;
+        double dsum[SP_TASKS], rkv[SP_TASKS];
+#pragma unroll
+        for (int j = 0; j < SP_TASKS; ++j) {
+            const int t = 1 + warp + j * MP_WARPS;
+            dsum[j] = 0.0;
+            rkv[j] = t <= later ? rk[t] : 0.0;
+        }
+        const double x0raw = rk[0];
+#pragma unroll
+        for (int c = 0; c < SP_MAX_CTAS / 32; ++c) {
+            const int q = lane + 32 * c;
+            if (32 * c < P) {  // warp-uniform
+#pragma unroll
+                for (int j = 0; j < SP_TASKS; ++j) {
+                    const int t = 1 + warp + j * MP_WARPS;
+                    if (t <= later && q < P) dsum[j] += pb[(2 + t) * P + q];
+                }
+            }
+        }
+        if (warp == 0) {
+            double mx = 0.0, e = SP_EMPTY_EXP, sq = 0.0;
+#pragma unroll
+            for (int c = 0; c < SP_MAX_CTAS / 32; ++c) {
+                const int q = lane + 32 * c;
+                if (q < P) {
+                    mx = fmax(mx, pb[q]);
+                    sp_merge(e, sq, pb[P + q], pb[2 * P + q]);
+                }
+            }
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {  // the merge is symmetric: both lanes get the same bits
+                mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+                const double e2 = __shfl_xor_sync(0xffffffffu, e, o);
+                const double s2 = __shfl_xor_sync(0xffffffffu, sq, o);
+                sp_merge(e, sq, e2, s2);
+            }
+            if (lane == 0) {
+                int mode = 0;
+                if (m - k > 1 && mx >= DBL_MIN) {
+                    const double inv = 1.0 / mx;  // as the reference: x * (1/max)
+                    const double x0 = x0raw * inv;
+                    // sqrt(sum over rows > k of (x/max)^2) = sqrt(sq) 2^e / max, 2^e <= max
+                    const double xnorm = sq > 0.0 ? sqrt(sq) * (inv * sp_pow2((int)e)) : 0.0;
+                    if (xnorm == 0.0) {
+                        if (x0 < 0.0) mode = 2;
+                    } else {
+                        const double nb = -copysign(hypot(x0, xnorm), x0);
+                        mode = 1;
+                        fin_beta = nb * mx;
+                        fin_v0inv = 1.0 / ((x0 - nb) * mx);
+                        fin_tau = (nb - x0) / nb;
+                    }
+                }
+                fin_mode = mode;
+                if (cta == 0) tau[k] = mode == 1 ? fin_tau : (mode == 2 ? 2.0 : 0.0);
+            }
+        }
+        __syncthreads();
+        const int mode = fin_mode;
+        if (mode == 1) {
+            const double v0inv = fin_v0inv, tk = fin_tau;
+#pragma unroll
+            for (int j = 0; j < SP_TASKS; ++j) {
+                const int t = 1 + warp + j * MP_WARPS;
+                if (t <= later) {  // warp-uniform
+                    const double d = warp_sum(dsum[j]);
+                    if (lane == 0) fin[t] = (rkv[j] + d * v0inv) * tk;
+                }
+            }
+        } else if (mode == 2) {
+            for (int t = 1 + tid; t <= later; t += MP_THREADS) fin[t] = rk[t] * 2.0;  // the tail is zero
+        }
+        __syncthreads();
+        if (mode != 0) {
+            // Phase C: reflector tail on own rows, then the later columns
+            if (mode == 1) {
+                const double v0inv = fin_v0inv;
+                for (int i = lo1 + tid; i < r1; i += MP_THREADS) ck[i - r0] *= v0inv;
+            }
+            if (k >= r0 && k < r1 && tid == 0) ck[k - r0] = mode == 1 ? fin_beta : -ck[k - r0];
+            __syncthreads();
+            for (int t = 1 + warp; t <= later; t += MP_WARPS) {
+                double* cj = ck + t * R;
+                const double f = fin[t];
+                for (int i = lo1 + lane; i < r1; i += 32) cj[i - r0] -= f * ck[i - r0];
+                if (lane == 0 && k >= r0 && k < r1) cj[k - r0] -= f;
+            }
+        }
+        __syncthreads();
+    }
+    for (int e = tid; e < rows * kb; e += MP_THREADS) {
+        const int c = e / rows, i = e - c * rows;
+        A[(long long)(k0 + c) * lda + r0 + i] = slab[c * R + i];
+    }
+}
+
 // V (ldv x 64, column-major): column i < kb holds reflector k0+i (zeros above
 // row k0+i, one on it, A's tail below); columns kb .. 63 are zero.
 __global__ void qr_pack_v_kernel(const double* A, long long lda, int m, int k0, int kb, double* V, long long ldv) {
@@ -390,8 +595,20 @@ int launch_qr_panel_mp(double* a, long long lda, int m, int k0, int kb, double* 
     unsigned* counter = reinterpret_cast<unsigned*>(rowrec + 128);
     if (cudaMemsetAsync(counter, 0, sizeof(unsigned), st) != cudaSuccess) return JLC_E_LAUNCH;
     void* args[] = {&a, &lda, &m, &k0, &kb, &tau, &part, &rowrec, &counter, &status};
-    cudaError_t e = cudaLaunchCooperativeKernel((const void*)qr::qr_panel_mp_kernel, dim3(P), dim3(qr::MP_THREADS),
-                                                args, 0, st);
+    // each CTA's rows in shared memory when the slab fits, else in place
+    const int R = (m - k0 + P - 1) / P;
+    const size_t slab = (size_t)R * kb * sizeof(double);
+    cudaError_t e;
+    if (slab <= (size_t)qr::SP_MAX_SLAB_BYTES && P <= qr::SP_MAX_CTAS) {
+        e = cudaFuncSetAttribute((const void*)qr::qr_panel_sm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 qr::SP_MAX_SLAB_BYTES);
+        if (e != cudaSuccess) return JLC_E_LAUNCH;
+        e = cudaLaunchCooperativeKernel((const void*)qr::qr_panel_sm_kernel, dim3(P), dim3(qr::MP_THREADS), args,
+                                        slab, st);
+    } else {
+        e = cudaLaunchCooperativeKernel((const void*)qr::qr_panel_mp_kernel, dim3(P), dim3(qr::MP_THREADS), args, 0,
+                                        st);
+    }
     return e == cudaSuccess ? JLC_OK : JLC_E_LAUNCH;
 }
 

@@ -66,3 +66,20 @@ def test_qr_zero_column(ctx, oracle):
     f_ref, tau_ref = oracle.householder_qr_blocked(a)
     assert tau.cpu().numpy()[10] == 0.0 and tau_ref[10] == 0.0
     np.testing.assert_allclose(at[:, :90].cpu().numpy().T, f_ref, rtol=0, atol=1e-11)
+
+
+def test_qr_tall_panel(ctx, oracle):
+    """60000 rows: the first panel's per-CTA rows (406 x 64 doubles) exceed the
+    shared-memory slab and are factored in place, the second panel's (6
+    columns) in shared memory; both against the restatement, and R against
+    the Gram matrix (R^T R = A^T A)."""
+    m, n = 60000, 70
+    a = oracle.uniform((m, n), 77)
+    at, tau = _factor(ctx, a)
+    f = at[:, :m].cpu().numpy().T
+    f_ref, tau_ref = oracle.householder_qr_blocked(a)
+    np.testing.assert_allclose(tau.cpu().numpy()[:n], tau_ref, rtol=0, atol=1e-12)
+    np.testing.assert_allclose(f, f_ref, rtol=0, atol=1e-11 * max(1.0, np.abs(f_ref).max()))
+    r = np.triu(f[:n, :])
+    g = a.T @ a
+    assert np.abs(r.T @ r - g).max() <= 1e-12 * np.abs(g).max()
