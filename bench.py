@@ -633,7 +633,8 @@ def run_qr(args):
     matrix (the reference's HouseholderQR.factorizeBlocked, panels of 64):
     device time of jlc_qr_factor_device per factorisation (the matrix is
     restored, untimed, before each), FLOPs 2mn^2 - 2n^3/3, and the share of the
-    time in the panel kernels (phase records)."""
+    time in the panel kernels and the device time of every phase (phase
+    records: qr_panel, qr_vt, and dmma for the Gram and trailing-update GEMMs)."""
     import statistics
     import torch
     import jlc_b200
@@ -649,7 +650,7 @@ def run_qr(args):
     a = torch.empty_like(a0)
     tau = torch.empty(n, dtype=torch.float64, device="cuda")
     flops = 2.0 * n * n * n - 2.0 * n ** 3 / 3.0
-    times, panel = [], []
+    times, panel, phases = [], [], []
     for it in range(args.warmup + args.steps):
         a.copy_(a0)
         torch.cuda.synchronize()
@@ -659,6 +660,10 @@ def run_qr(args):
             recs = ctx.profile_collect()
             times.append(rep["device_ms"])
             panel.append(sum(ms for name, ms in recs if name == "qr_panel"))
+            per = {}
+            for name, t in recs:
+                per[name] = per.get(name, 0.0) + t
+            phases.append(per)
     ctx.set_profiling(False)
     ms = statistics.median(times)
     line = {"metric": f"blocked Householder QR GFLOP/s ({n}x{n}, FP64, device-resident)",
@@ -667,7 +672,9 @@ def run_qr(args):
             "data": "synthetic uniform[-1,1) (torch Philox, seed 20260604), device resident",
             "config": {"workload": f"QR {n}x{n}, panels of 64, compact-WY trailing update on the DMMA route"},
             "panel_ms": round(statistics.median(panel), 3),
-            "panel_share": round(statistics.median(panel) / ms, 3)}
+            "panel_share": round(statistics.median(panel) / ms, 3),
+            "phase_ms": {name: round(statistics.median(p.get(name, 0.0) for p in phases), 3)
+                         for name in sorted({n for p in phases for n in p})}}
     print(json.dumps(line), flush=True)
     ctx.close()
     return 0

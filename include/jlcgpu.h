@@ -180,6 +180,7 @@ JLC_API int jlc_device_status(jlc_ctx* ctx);
 #define JLC_PHASE_D2H 9         /* device -> host copy of C */
 #define JLC_PHASE_REDUCE 11     /* adjoint reductions: d(alpha) / d(beta) dots and sums, scaled copies */
 #define JLC_PHASE_QR_PANEL 12   /* blocked QR: one panel's factorisation kernel */
+#define JLC_PHASE_QR_VT 13      /* blocked QR: V packing and the T factor (the Gram GEMM is a dmma phase) */
 /* Turn event-pair recording around each phase on (1) or off (0).  Records
  * accumulate (up to 4096) until collected. */
 JLC_API int jlc_set_profiling(jlc_ctx* ctx, int on);

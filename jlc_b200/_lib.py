@@ -120,7 +120,7 @@ SIGNATURES = {
 }
 
 PHASES = {1: "dmma", 2: "gemv", 3: "ozaki_gemm", 4: "grouped", 5: "ozaki_split", 6: "scale", 7: "fp64_gated", 8: "h2d",
-          9: "d2h", 11: "reduce", 12: "qr_panel"}
+          9: "d2h", 11: "reduce", 12: "qr_panel", 13: "qr_vt"}
 
 _lib = None
 

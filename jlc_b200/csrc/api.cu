@@ -594,7 +594,11 @@ int qr_work(jlc_ctx* ctx, long long m, long long cols, QrWork& q) {
 int qr_panel_vt(jlc_ctx* ctx, const double* f, long long ldf, long long m, long long k0, int kb, const double* tau,
                 const QrWork& q, int precision) {
     cudaStream_t st = ctx->stream;
-    int rc = launch_qr_pack_v(f, ldf, (int)m, (int)k0, kb, q.v, q.ldv, st);
+    int rc;
+    {
+        Phase ph(ctx, JLC_PHASE_QR_VT);
+        rc = launch_qr_pack_v(f, ldf, (int)m, (int)k0, kb, q.v, q.ldv, st);
+    }
     if (rc) return set_err(ctx, rc, "QR: V packing launch failed");
     // G (64 x 64, row-major) = V(k0:, :)^T V(k0:, :): op(A) = V^T as a row-major
     // 64 x (m-k0) view, op(B) = V column-major
@@ -603,7 +607,10 @@ int qr_panel_vt(jlc_ctx* ctx, const double* f, long long ldf, long long m, long 
                q.g, kQrPanel};
     rc = run_device(ctx, g, JLC_PREC_NATIVE, 0, nullptr);
     if (rc) return rc;
-    rc = launch_qr_build_t(q.g, tau + k0, kb, q.t, st);
+    {
+        Phase ph(ctx, JLC_PHASE_QR_VT);
+        rc = launch_qr_build_t(q.g, tau + k0, kb, q.t, st);
+    }
     return rc ? set_err(ctx, rc, "QR: T launch failed") : JLC_OK;
 }
 
@@ -939,15 +946,17 @@ int jlc_qr_factor_device(jlc_ctx* ctx, int64_t m, int64_t n, double* a, int64_t 
     for (long long k0 = 0; k0 < kmax; k0 += kQrPanel) {
         const int kb = (int)(kmax - k0 < kQrPanel ? kmax - k0 : kQrPanel);
         {
-            // tall panels: rows split over up to one CTA per SM (>= 128 rows
-            // each) in one cooperative launch; short ones: one CTA
+            // tall panels: rows split over CTAs of >= 128 rows each, one
+            // cluster while the slabs fit its shared memory, else up to one
+            // CTA per SM in one cooperative launch; short ones: one CTA
             Phase ph(ctx, JLC_PHASE_QR_PANEL);
             ctx->launches += 1;
             long long ctas = (m - k0) / 128;
             if (ctas > ctx->sm_count) ctas = ctx->sm_count;
+            if (ctas >= 2 && ctx->qr_cluster_max == 0) ctx->qr_cluster_max = qr_panel_cluster_max();
             if (ctas >= 2)
-                rc = launch_qr_panel_mp(a, lda, (int)m, (int)k0, kb, tau, (int)ctas, q.panel_scratch, ctx->d_status,
-                                        ctx->stream);
+                rc = launch_qr_panel_mp(a, lda, (int)m, (int)k0, kb, tau, (int)ctas, ctx->qr_cluster_max,
+                                        q.panel_scratch, ctx->d_status, ctx->stream);
             else
                 rc = launch_qr_panel(a, lda, (int)m, (int)k0, kb, tau, ctx->stream);
             if (rc) return set_err(ctx, rc, "QR: panel launch failed");

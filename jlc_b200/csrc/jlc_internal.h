@@ -73,8 +73,9 @@ bool dmma_operand_ok(const void* ptr, long long ld);
 // blocked Householder QR kernels (qr.cu)
 int launch_qr_panel(double* a, long long lda, int m, int k0, int kb, double* tau, cudaStream_t st);
 size_t qr_panel_mp_scratch_bytes(int P);
-int launch_qr_panel_mp(double* a, long long lda, int m, int k0, int kb, double* tau, int P, void* scratch,
-                       int* status, cudaStream_t st);
+int qr_panel_cluster_max();
+int launch_qr_panel_mp(double* a, long long lda, int m, int k0, int kb, double* tau, int P, int cluster_max,
+                       void* scratch, int* status, cudaStream_t st);
 int launch_qr_pack_v(const double* a, long long lda, int m, int k0, int kb, double* v, long long ldv,
                      cudaStream_t st);
 int launch_qr_build_t(const double* g, const double* tau, int kb, double* t, cudaStream_t st);
@@ -166,6 +167,7 @@ struct jlc_ctx {
     cudaStream_t cin = nullptr, cout = nullptr;
     cudaEvent_t pev[2 * kPipeMaxBlocks + 1] = {};
     int dmma_k = 8;
+    int qr_cluster_max = 0;  // largest QR panel cluster on this device (0: not queried yet)
     // profiler: event pairs around phases, reused from a pool
     bool profiling = false;
     static constexpr int kMaxRec = 4096;

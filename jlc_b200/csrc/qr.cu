@@ -15,6 +15,8 @@
 #include <cfloat>
 #include <cmath>
 
+#include <cooperative_groups.h>
+
 #include "jlc_device.cuh"
 #include "jlc_internal.h"
 
@@ -526,6 +528,184 @@ __global__ void __launch_bounds__(MP_THREADS) qr_panel_sm_kernel(double* A, long
     }
 }
 
+// The panel on one thread-block cluster (2..16 CTAs, one slab of rows each in
+// shared memory).  Each CTA stores its partials (and the CTA holding row k
+// the row record) straight into every CTA's shared memory, lane r to CTA r;
+// the stores complete under the cluster barrier's release, so after it every
+// CTA merges from its own shared memory.  The barrier is the hardware cluster
+// barrier (release/acquire), so nothing spins on memory.  Partials and row
+// records alternate between two buffers by column parity: a CTA writes
+// column k+1's while a slower one may still read column k's, and overwrites
+// column k's only after the next barrier.
+namespace cg = cooperative_groups;
+constexpr int CL_THREADS = 512, CL_WARPS = CL_THREADS / 32;
+constexpr int CL_TASKS = 64 / CL_WARPS;  // later columns per warp
+constexpr int CL_MAX = 16;
+constexpr int CL_MAX_SLAB_BYTES = 200 * 1024;
+
+__global__ void __launch_bounds__(CL_THREADS, 1) qr_panel_cl_kernel(double* A, long long lda, int m, int k0, int kb,
+                                                                 double* tau) {
+    extern __shared__ double slab[];          // slab[c * R + (i - r0)] = A[i, k0 + c]
+    __shared__ double part[2][CL_MAX][MP_PART];  // from CTA q: 0 max, 1 exponent, 2 sum of squares, 2 + t dot
+    __shared__ double rrec[2][64];            // row k of columns k .. k0 + kb - 1
+    __shared__ double fin[64];
+    __shared__ double fin_v0inv, fin_beta, fin_tau;
+    __shared__ int fin_mode;
+    cg::cluster_group cluster = cg::this_cluster();
+    const int P = (int)cluster.num_blocks(), cta = (int)cluster.block_rank();
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int R = (m - k0 + P - 1) / P;
+    const int r0 = k0 + cta * R, r1 = min(m, r0 + R);
+    const int rows = max(0, r1 - r0);
+    for (int e = tid; e < rows * kb; e += CL_THREADS) {
+        const int c = e / rows, i = e - c * rows;
+        slab[c * R + i] = A[(long long)(k0 + c) * lda + r0 + i];
+    }
+    __syncthreads();
+    for (int kk = 0; kk < kb; ++kk) {
+        const int k = k0 + kk;
+        const int later = kb - kk - 1;
+        const int owner = kk / R;  // the CTA holding row k
+        double* ck = slab + kk * R;
+        // this CTA's partials in CTA `lane`'s shared memory (lanes >= P unused)
+        double* pk = cluster.map_shared_rank(&part[kk & 1][cta][0], lane < P ? lane : 0);
+        const int lo = max(r0, k), lo1 = max(r0, k + 1);
+        // Phase A (own rows): warp w the dots with columns t = 1 + w + 16j,
+        // the last warp also the max and the (e, s) sum of squares
+        {
+            double d[CL_TASKS];
+#pragma unroll
+            for (int j = 0; j < CL_TASKS; ++j) d[j] = 0.0;
+            for (int i = lo1 + lane; i < r1; i += 32) {
+                const double x = ck[i - r0];
+#pragma unroll
+                for (int j = 0; j < CL_TASKS; ++j) {
+                    const int t = 1 + warp + j * CL_WARPS;
+                    if (t <= later) d[j] = fma(x, ck[t * R + (i - r0)], d[j]);
+                }
+            }
+#pragma unroll
+            for (int j = 0; j < CL_TASKS; ++j) {
+                const int t = 1 + warp + j * CL_WARPS;
+                if (t <= later) {  // warp-uniform
+                    const double v = warp_sum(d[j]);  // every lane holds the sum
+                    if (lane < P) pk[2 + t] = v;
+                }
+            }
+            if (warp == CL_WARPS - 1) {
+                double mx = 0.0;
+                for (int i = lo + lane; i < r1; i += 32) mx = fmax(mx, fabs(ck[i - r0]));
+                mx = warp_max(mx);
+                const int e = sp_exp(mx);
+                const double sc = sp_pow2(-e);
+                double sq = 0.0;
+                for (int i = lo1 + lane; i < r1; i += 32) {
+                    const double y = ck[i - r0] * sc;
+                    sq = fma(y, y, sq);
+                }
+                sq = warp_sum(sq);
+                if (lane < P) {
+                    pk[0] = mx;
+                    pk[1] = (double)e;
+                    pk[2] = sq;
+                }
+            }
+            if (cta == owner)
+                for (int e = tid; e < (later + 1) * P; e += CL_THREADS) {
+                    const int t = e / P, r = e - t * P;
+                    *cluster.map_shared_rank(&rrec[kk & 1][t], r) = ck[t * R + (k - r0)];
+                }
+        }
+        cluster.sync();
+        // Phase B: every CTA merges the partials of CTAs 0 .. P-1 in the same order
+        const double* orow = rrec[kk & 1];
+        double dsum[CL_TASKS], rkv[CL_TASKS];
+        const double* rp = part[kk & 1][lane < P ? lane : 0];
+#pragma unroll
+        for (int j = 0; j < CL_TASKS; ++j) {
+            const int t = 1 + warp + j * CL_WARPS;
+            rkv[j] = t <= later ? orow[t] : 0.0;
+            dsum[j] = t <= later && lane < P ? rp[2 + t] : 0.0;
+        }
+        if (warp == 0) {
+            const double x0raw = orow[0];
+            double mx = 0.0, e = SP_EMPTY_EXP, sq = 0.0;
+            if (lane < P) {
+                mx = rp[0];
+                e = rp[1];
+                sq = rp[2];
+            }
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {  // symmetric merge: every lane gets the same bits
+                mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+                const double e2 = __shfl_xor_sync(0xffffffffu, e, o);
+                const double s2 = __shfl_xor_sync(0xffffffffu, sq, o);
+                sp_merge(e, sq, e2, s2);
+            }
+            if (lane == 0) {
+                int mode = 0;
+                if (m - k > 1 && mx >= DBL_MIN) {
+                    const double inv = 1.0 / mx;  // as the reference: x * (1/max)
+                    const double x0 = x0raw * inv;
+                    const double xnorm = sq > 0.0 ? sqrt(sq) * (inv * sp_pow2((int)e)) : 0.0;
+                    if (xnorm == 0.0) {
+                        if (x0 < 0.0) mode = 2;
+                    } else {
+                        const double nb = -copysign(hypot(x0, xnorm), x0);
+                        mode = 1;
+                        fin_beta = nb * mx;
+                        fin_v0inv = 1.0 / ((x0 - nb) * mx);
+                        fin_tau = (nb - x0) / nb;
+                    }
+                }
+                fin_mode = mode;
+                if (cta == 0) tau[k] = mode == 1 ? fin_tau : (mode == 2 ? 2.0 : 0.0);
+            }
+        }
+        __syncthreads();
+        const int mode = fin_mode;
+        if (mode == 1) {
+            const double v0inv = fin_v0inv, tk = fin_tau;
+#pragma unroll
+            for (int j = 0; j < CL_TASKS; ++j) {
+                const int t = 1 + warp + j * CL_WARPS;
+                if (t <= later) {  // warp-uniform
+                    const double d = warp_sum(dsum[j]);
+                    if (lane == 0) fin[t] = (rkv[j] + d * v0inv) * tk;
+                }
+            }
+        } else if (mode == 2) {
+#pragma unroll
+            for (int j = 0; j < CL_TASKS; ++j) {
+                const int t = 1 + warp + j * CL_WARPS;
+                if (t <= later && lane == 0) fin[t] = rkv[j] * 2.0;  // the tail is zero
+            }
+        }
+        __syncthreads();
+        if (mode != 0) {
+            // Phase C: reflector tail on own rows, then the later columns
+            if (mode == 1) {
+                const double v0inv = fin_v0inv;
+                for (int i = lo1 + tid; i < r1; i += CL_THREADS) ck[i - r0] *= v0inv;
+            }
+            if (k >= r0 && k < r1 && tid == 0) ck[k - r0] = mode == 1 ? fin_beta : -ck[k - r0];
+            __syncthreads();
+            for (int t = 1 + warp; t <= later; t += CL_WARPS) {
+                double* cj = ck + t * R;
+                const double f = fin[t];
+                for (int i = lo1 + lane; i < r1; i += 32) cj[i - r0] -= f * ck[i - r0];
+                if (lane == 0 && k >= r0 && k < r1) cj[k - r0] -= f;
+            }
+        }
+        __syncthreads();
+    }
+    cluster.sync();  // no CTA leaves while another may still read its shared memory
+    for (int e = tid; e < rows * kb; e += CL_THREADS) {
+        const int c = e / rows, i = e - c * rows;
+        A[(long long)(k0 + c) * lda + r0 + i] = slab[c * R + i];
+    }
+}
+
 // V (ldv x 64, column-major): column i < kb holds reflector k0+i (zeros above
 // row k0+i, one on it, A's tail below); columns kb .. 63 are zero.
 __global__ void qr_pack_v_kernel(const double* A, long long lda, int m, int k0, int kb, double* V, long long ldv) {
@@ -588,8 +768,61 @@ size_t qr_panel_mp_scratch_bytes(int P) {
     return ((size_t)2 * P * qr::MP_PART + 128) * sizeof(double) + 256;
 }
 
-int launch_qr_panel_mp(double* a, long long lda, int m, int k0, int kb, double* tau, int P, void* scratch,
-                       int* status, cudaStream_t st) {
+// Largest cluster of the cluster panel kernel that can be resident with a
+// full slab on this device (16, else 8), or 1 when none can.
+int qr_panel_cluster_max() {
+    const void* kern = (const void*)qr::qr_panel_cl_kernel;
+    if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, qr::CL_MAX_SLAB_BYTES) !=
+            cudaSuccess ||
+        cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess) {
+        cudaGetLastError();
+        return 1;
+    }
+    for (int c = qr::CL_MAX; c >= 8; c /= 2) {
+        cudaLaunchConfig_t cfg = {};
+        cudaLaunchAttribute at[1];
+        cfg.gridDim = dim3(c);
+        cfg.blockDim = dim3(qr::CL_THREADS);
+        cfg.dynamicSmemBytes = qr::CL_MAX_SLAB_BYTES;
+        at[0].id = cudaLaunchAttributeClusterDimension;
+        at[0].val.clusterDim.x = c;
+        at[0].val.clusterDim.y = 1;
+        at[0].val.clusterDim.z = 1;
+        cfg.attrs = at;
+        cfg.numAttrs = 1;
+        int n = 0;
+        if (cudaOccupancyMaxActiveClusters(&n, kern, &cfg) == cudaSuccess && n > 0) return c;
+        cudaGetLastError();
+    }
+    return 1;
+}
+
+int launch_qr_panel_mp(double* a, long long lda, int m, int k0, int kb, double* tau, int P, int cluster_max,
+                       void* scratch, int* status, cudaStream_t st) {
+    // one cluster when its slabs fit in shared memory
+    const int cl = min((m - k0) / 128, min(cluster_max, qr::CL_MAX));
+    if (cl >= 2 && (size_t)((m - k0 + cl - 1) / cl) * kb * sizeof(double) <= (size_t)qr::CL_MAX_SLAB_BYTES) {
+        const void* kern = (const void*)qr::qr_panel_cl_kernel;
+        if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, qr::CL_MAX_SLAB_BYTES) !=
+                cudaSuccess ||
+            cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess)
+            return JLC_E_LAUNCH;
+        cudaLaunchConfig_t cfg = {};
+        cudaLaunchAttribute at[1];
+        cfg.gridDim = dim3(cl);
+        cfg.blockDim = dim3(qr::CL_THREADS);
+        cfg.dynamicSmemBytes = (size_t)((m - k0 + cl - 1) / cl) * kb * sizeof(double);
+        cfg.stream = st;
+        at[0].id = cudaLaunchAttributeClusterDimension;
+        at[0].val.clusterDim.x = cl;
+        at[0].val.clusterDim.y = 1;
+        at[0].val.clusterDim.z = 1;
+        cfg.attrs = at;
+        cfg.numAttrs = 1;
+        return cudaLaunchKernelEx(&cfg, qr::qr_panel_cl_kernel, a, lda, m, k0, kb, tau) == cudaSuccess
+                   ? JLC_OK
+                   : JLC_E_LAUNCH;
+    }
     double* part = static_cast<double*>(scratch);
     double* rowrec = part + (size_t)2 * P * qr::MP_PART;
     unsigned* counter = reinterpret_cast<unsigned*>(rowrec + 128);

@@ -68,12 +68,15 @@ def test_qr_zero_column(ctx, oracle):
     np.testing.assert_allclose(at[:, :90].cpu().numpy().T, f_ref, rtol=0, atol=1e-11)
 
 
-def test_qr_tall_panel(ctx, oracle):
-    """60000 rows: the first panel's per-CTA rows (406 x 64 doubles) exceed the
-    shared-memory slab and are factored in place, the second panel's (6
-    columns) in shared memory; both against the restatement, and R against
-    the Gram matrix (R^T R = A^T A)."""
-    m, n = 60000, 70
+@pytest.mark.parametrize("m,n", [(60000, 70), (8000, 130)])
+def test_qr_tall_panel(ctx, oracle, m, n):
+    """Tall panels, against the restatement and R against the Gram matrix
+    (R^T R = A^T A).  60000 x 70: the first panel's rows per CTA (406 x 64
+    doubles, one CTA per SM) exceed the shared-memory slab and are factored in
+    place, the second panel (6 columns) runs on one cluster.  8000 x 130: the
+    first two panels' slabs do not fit a 16-CTA cluster (500 x 64 doubles) and
+    run as a cooperative grid with slabs in shared memory, the third on a
+    cluster."""
     a = oracle.uniform((m, n), 77)
     at, tau = _factor(ctx, a)
     f = at[:, :m].cpu().numpy().T
