@@ -628,6 +628,23 @@ def run_configs(args):
 
 
 # ----------------------------------------------------------------------------- blocked QR (next row)
+def qr_cpu_baseline(n):
+    """The oracle's restatement of HouseholderQR.factorizeBlocked (panels of 64,
+    per-column reflectors in Python, the compact-WY update through numpy's
+    BLAS) on an n x n uniform[-1,1) matrix, timed on this host."""
+    import numpy as np
+    from oracle import oracle as O
+    a = np.random.default_rng(20260604).uniform(-1.0, 1.0, (n, n))
+    t0 = time.perf_counter()
+    O.householder_qr_blocked(a)
+    dt = time.perf_counter() - t0
+    cores = os.cpu_count() or 1
+    return {"value": round((2.0 * n ** 3 - 2.0 * n ** 3 / 3.0) / dt / 1e9, 2), "unit": "GFLOP/s", "cores": cores,
+            "kind": "port",
+            "sample": f"one {n}x{n} factorisation through the restatement of factorizeBlocked (numpy, up to "
+                      f"{cores} BLAS threads), {dt:.1f} s"}
+
+
 def run_qr(args):
     """Device-resident blocked Householder QR of a size x size uniform[-1,1)
     matrix (the reference's HouseholderQR.factorizeBlocked, panels of 64):
@@ -666,6 +683,7 @@ def run_qr(args):
             phases.append(per)
     ctx.set_profiling(False)
     ms = statistics.median(times)
+    cpu = None if args.no_cpu_baseline else qr_cpu_baseline(min(n, 1024))
     line = {"metric": f"blocked Householder QR GFLOP/s ({n}x{n}, FP64, device-resident)",
             "value": round(flops / (ms * 1e-3) / 1e9, 1), "unit": "GFLOP/s", "n_gpus": 1, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(ms, 3), "higher_is_better": True, "dtype": "f64",
@@ -674,7 +692,8 @@ def run_qr(args):
             "panel_ms": round(statistics.median(panel), 3),
             "panel_share": round(statistics.median(panel) / ms, 3),
             "phase_ms": {name: round(statistics.median(p.get(name, 0.0) for p in phases), 3)
-                         for name in sorted({n for p in phases for n in p})}}
+                         for name in sorted({n for p in phases for n in p})},
+            "cpu_baseline": cpu}
     print(json.dumps(line), flush=True)
     ctx.close()
     return 0

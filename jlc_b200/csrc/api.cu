@@ -946,19 +946,17 @@ int jlc_qr_factor_device(jlc_ctx* ctx, int64_t m, int64_t n, double* a, int64_t 
     for (long long k0 = 0; k0 < kmax; k0 += kQrPanel) {
         const int kb = (int)(kmax - k0 < kQrPanel ? kmax - k0 : kQrPanel);
         {
-            // tall panels: rows split over CTAs of >= 128 rows each, one
-            // cluster while the slabs fit its shared memory, else up to one
-            // CTA per SM in one cooperative launch; short ones: one CTA
+            // rows split over CTAs of >= 128 rows each: one cluster while
+            // the slabs fit its shared memory, else up to one CTA per SM in
+            // one cooperative launch
             Phase ph(ctx, JLC_PHASE_QR_PANEL);
             ctx->launches += 1;
             long long ctas = (m - k0) / 128;
             if (ctas > ctx->sm_count) ctas = ctx->sm_count;
-            if (ctas >= 2 && ctx->qr_cluster_max == 0) ctx->qr_cluster_max = qr_panel_cluster_max();
-            if (ctas >= 2)
-                rc = launch_qr_panel_mp(a, lda, (int)m, (int)k0, kb, tau, (int)ctas, ctx->qr_cluster_max,
-                                        q.panel_scratch, ctx->d_status, ctx->stream);
-            else
-                rc = launch_qr_panel(a, lda, (int)m, (int)k0, kb, tau, ctx->stream);
+            if (ctas < 1) ctas = 1;
+            if (ctx->qr_cluster_max == 0) ctx->qr_cluster_max = qr_panel_cluster_max();
+            rc = launch_qr_panel(a, lda, (int)m, (int)k0, kb, tau, (int)ctas, ctx->qr_cluster_max, q.panel_scratch,
+                                 ctx->d_status, ctx->stream);
             if (rc) return set_err(ctx, rc, "QR: panel launch failed");
         }
         const long long trail = n - (k0 + kb);

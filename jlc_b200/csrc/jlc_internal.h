@@ -71,11 +71,10 @@ bool dmma_operand_ok(const void* ptr, long long ld);
 // ksplit > 1 with splitk_ws of at least dmma_splitk_bytes(m, n, ksplit):
 // split-K over ksplit parts; otherwise every tile is one work unit.
 // blocked Householder QR kernels (qr.cu)
-int launch_qr_panel(double* a, long long lda, int m, int k0, int kb, double* tau, cudaStream_t st);
 size_t qr_panel_mp_scratch_bytes(int P);
 int qr_panel_cluster_max();
-int launch_qr_panel_mp(double* a, long long lda, int m, int k0, int kb, double* tau, int P, int cluster_max,
-                       void* scratch, int* status, cudaStream_t st);
+int launch_qr_panel(double* a, long long lda, int m, int k0, int kb, double* tau, int P, int cluster_max,
+                    void* scratch, int* status, cudaStream_t st);
 int launch_qr_pack_v(const double* a, long long lda, int m, int k0, int kb, double* v, long long ldv,
                      cudaStream_t st);
 int launch_qr_build_t(const double* g, const double* tau, int kb, double* t, cudaStream_t st);

@@ -5,9 +5,14 @@
 // to the panel's later columns), then the trailing columns are updated with
 // the compact-WY form Q^T C = C - V T^T V^T C as three GEMMs (api.cu).
 //
-//   qr_panel_kernel:   one CTA per panel; the column reductions (max, sum of
-//                      squares, dots) are block reductions in a fixed order,
-//                      so the factorisation is deterministic;
+//   qr_panel_cl_kernel: the panel on one thread-block cluster (1..16 CTAs,
+//                      each holding a slab of rows in shared memory), one
+//                      cluster barrier per column;
+//   qr_panel_sm_kernel / qr_panel_mp_kernel: taller panels on a cooperative
+//                      grid of up to one CTA per SM, slabs in shared memory
+//                      or (taller still) in place, one grid barrier per column;
+//                      all merge partials in a fixed order, so the
+//                      factorisation is deterministic;
 //   qr_pack_v_kernel:  V = the panel's reflectors with unit diagonal and zeros
 //                      above it (packV, HouseholderQR.java:445-471);
 //   qr_build_t_kernel: T from the Gram matrix G = V^T V and tau with the
@@ -23,9 +28,6 @@
 namespace jlc {
 namespace qr {
 
-constexpr int PANEL_THREADS = 1024;
-constexpr int WARPS = PANEL_THREADS / 32;
-
 __device__ __forceinline__ double warp_sum(double v) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
@@ -35,91 +37,6 @@ __device__ __forceinline__ double warp_max(double v) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
     return v;
-}
-
-// Block reduction in a fixed order (warps, then warp 0 over the warp
-// partials); every thread gets the result.
-template <bool MAX>
-__device__ double block_reduce(double v, double* red) {
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    v = MAX ? warp_max(v) : warp_sum(v);
-    if (lane == 0) red[warp] = v;
-    __syncthreads();
-    if (warp == 0) {
-        double w = lane < WARPS ? red[lane] : (MAX ? 0.0 : 0.0);
-        w = MAX ? warp_max(w) : warp_sum(w);
-        if (lane == 0) red[WARPS] = w;
-    }
-    __syncthreads();
-    const double r = red[WARPS];
-    __syncthreads();  // red is reused by the next reduction
-    return r;
-}
-
-// Factors columns k0 .. k0+kb-1 of the column-major m x n matrix A (rows from
-// the diagonal down), writing tau[k0 ..]; A's entries below the diagonal of
-// those columns become the reflectors' tails (v0 = 1 implied), the diagonal
-// the new R entries (computeHouseholder / applyHouseholderToColumn,
-// HouseholderQR.java:219-384).
-__global__ void __launch_bounds__(PANEL_THREADS) qr_panel_kernel(double* A, long long lda, int m, int k0, int kb,
-                                                                 double* tau) {
-    __shared__ double red[WARPS + 1];
-    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    for (int kk = 0; kk < kb; ++kk) {
-        const int k = k0 + kk;
-        double* col = A + (long long)k * lda;
-        double tk = 0.0;
-        if (m - k > 1) {
-            double mx = 0.0;
-            for (int i = k + tid; i < m; i += PANEL_THREADS) mx = fmax(mx, fabs(col[i]));
-            mx = block_reduce<true>(mx, red);
-            if (mx >= DBL_MIN) {
-                const double inv = 1.0 / mx;
-                const double x0 = col[k] * inv;
-                double s = 0.0;
-                for (int i = k + 1 + tid; i < m; i += PANEL_THREADS) {
-                    const double v = col[i] * inv;
-                    s += v * v;
-                }
-                const double xnorm = sqrt(block_reduce<false>(s, red));
-                if (xnorm == 0.0) {
-                    if (x0 < 0.0) {
-                        tk = 2.0;
-                        if (tid == 0) col[k] = -col[k];
-                    }
-                } else {
-                    const double nb = -copysign(hypot(x0, xnorm), x0);
-                    tk = (nb - x0) / nb;
-                    const double v0inv = 1.0 / ((x0 - nb) * mx);
-                    for (int i = k + 1 + tid; i < m; i += PANEL_THREADS) col[i] *= v0inv;
-                    if (tid == 0) col[k] = nb * mx;
-                }
-            }
-        }
-        if (tid == 0) tau[k] = tk;
-        __syncthreads();  // the reflector is complete
-        if (tk != 0.0) {
-            // H_k applied to the panel's later columns, one warp per column
-            for (int jj = warp; jj < kb - kk - 1; jj += WARPS) {
-                double* cj = A + (long long)(k + 1 + jj) * lda;
-                double d0 = 0.0, d1 = 0.0, d2 = 0.0, d3 = 0.0;
-                int i = k + 1 + lane;
-                for (; i + 96 < m; i += 128) {
-                    d0 = fma(col[i], cj[i], d0);
-                    d1 = fma(col[i + 32], cj[i + 32], d1);
-                    d2 = fma(col[i + 64], cj[i + 64], d2);
-                    d3 = fma(col[i + 96], cj[i + 96], d3);
-                }
-                for (; i < m; i += 32) d0 = fma(col[i], cj[i], d0);
-                double dot = warp_sum((d0 + d1) + (d2 + d3));
-                dot = (cj[k] + dot) * tk;  // v0 = 1
-                __syncwarp();
-                if (lane == 0) cj[k] -= dot;
-                for (int r = k + 1 + lane; r < m; r += 32) cj[r] -= dot * col[r];
-            }
-        }
-        __syncthreads();  // column k+1 is final before its reflector is formed
-    }
 }
 
 // ------------------------------------------------------------ multi-CTA panel
@@ -725,24 +642,34 @@ __global__ void qr_pack_v_kernel(const double* A, long long lda, int m, int k0, 
 // T[i][i] = tau_i; T[r][i] = -tau_i G[r][i] for r < i, then
 // T[r][i] = sum_{c=r}^{i-1} T[r][c] T[c][i] over the values before this
 // column's update (the reference overwrites in increasing r, which reads only
-// entries it has not yet overwritten).
+// entries it has not yet overwritten).  The starting values of every column
+// are staged at once (one coalesced pass over G); the sums run in four
+// interleaved partial sums.
 __global__ void __launch_bounds__(64) qr_build_t_kernel(const double* G, const double* tau, int kb, double* T) {
     __shared__ double t[64][65];
-    __shared__ double colv[64];
     const int r = threadIdx.x;
-    for (int c = 0; c < 64; ++c) t[r][c] = 0.0;
+#pragma unroll 16
+    for (int e = r; e < 64 * 64; e += 64) {
+        const int row = e >> 6, c = e & 63;
+        double v = 0.0;
+        if (c < kb) v = row < c ? -tau[c] * G[e] : (row == c ? tau[c] : 0.0);
+        t[row][c] = v;
+    }
     __syncthreads();
-    for (int i = 0; i < kb; ++i) {
-        const double ti = tau[i];
-        if (r == i) t[i][i] = ti;
-        if (r < i) colv[r] = -ti * G[r * 64 + i];
-        __syncthreads();
-        double s = 0.0;
+    for (int i = 1; i < kb; ++i) {
+        double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
         if (r < i) {
-            for (int c = r; c < i; ++c) s += t[r][c] * colv[c];
+            int c = r;
+            for (; c + 3 < i; c += 4) {
+                s0 = fma(t[r][c], t[c][i], s0);
+                s1 = fma(t[r][c + 1], t[c + 1][i], s1);
+                s2 = fma(t[r][c + 2], t[c + 2][i], s2);
+                s3 = fma(t[r][c + 3], t[c + 3][i], s3);
+            }
+            for (; c < i; ++c) s0 = fma(t[r][c], t[c][i], s0);
         }
-        __syncthreads();
-        if (r < i) t[r][i] = s;
+        __syncthreads();  // column i is read in full before it is overwritten
+        if (r < i) t[r][i] = (s0 + s1) + (s2 + s3);
         __syncthreads();
     }
     for (int c = 0; c < 64; ++c) T[r * 64 + c] = t[r][c];
@@ -755,11 +682,6 @@ __global__ void set_diag_kernel(double* q, long long ldq, long long d) {
 }
 
 }  // namespace qr
-
-int launch_qr_panel(double* a, long long lda, int m, int k0, int kb, double* tau, cudaStream_t st) {
-    qr::qr_panel_kernel<<<1, qr::PANEL_THREADS, 0, st>>>(a, lda, m, k0, kb, tau);
-    return cudaGetLastError() == cudaSuccess ? JLC_OK : JLC_E_LAUNCH;
-}
 
 // Multi-CTA panel: P CTAs in one cooperative launch (all resident at once);
 // scratch holds 2 x P x MP_PART partials, 2 x 64 row entries and the barrier
@@ -797,11 +719,17 @@ int qr_panel_cluster_max() {
     return 1;
 }
 
-int launch_qr_panel_mp(double* a, long long lda, int m, int k0, int kb, double* tau, int P, int cluster_max,
-                       void* scratch, int* status, cudaStream_t st) {
-    // one cluster when its slabs fit in shared memory
-    const int cl = min((m - k0) / 128, min(cluster_max, qr::CL_MAX));
-    if (cl >= 2 && (size_t)((m - k0 + cl - 1) / cl) * kb * sizeof(double) <= (size_t)qr::CL_MAX_SLAB_BYTES) {
+// Factors columns k0 .. k0+kb-1 of the column-major m x n matrix A (rows from
+// the diagonal down), writing tau[k0 ..]; A's entries below the diagonal of
+// those columns become the reflectors' tails (v0 = 1 implied), the diagonal
+// the new R entries (computeHouseholder / applyHouseholderToColumn,
+// HouseholderQR.java:219-384).  One cluster of CTAs with >= 128 rows each (a
+// single CTA below 256 rows) when their slabs fit in shared memory, else a
+// cooperative grid of P CTAs.
+int launch_qr_panel(double* a, long long lda, int m, int k0, int kb, double* tau, int P, int cluster_max,
+                    void* scratch, int* status, cudaStream_t st) {
+    const int cl = max(1, min((m - k0) / 128, min(cluster_max, qr::CL_MAX)));
+    if ((size_t)((m - k0 + cl - 1) / cl) * kb * sizeof(double) <= (size_t)qr::CL_MAX_SLAB_BYTES) {
         const void* kern = (const void*)qr::qr_panel_cl_kernel;
         if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, qr::CL_MAX_SLAB_BYTES) !=
                 cudaSuccess ||
