@@ -638,41 +638,70 @@ __global__ void qr_pack_v_kernel(const double* A, long long lda, int m, int k0, 
     V[e] = v;
 }
 
-// T (64 x 64, row-major, upper triangular) from G = V^T V (row-major) and tau:
-// T[i][i] = tau_i; T[r][i] = -tau_i G[r][i] for r < i, then
-// T[r][i] = sum_{c=r}^{i-1} T[r][c] T[c][i] over the values before this
-// column's update (the reference overwrites in increasing r, which reads only
-// entries it has not yet overwritten).  The starting values of every column
-// are staged at once (one coalesced pass over G); the sums run in four
-// interleaved partial sums.
-__global__ void __launch_bounds__(64) qr_build_t_kernel(const double* G, const double* tau, int kb, double* T) {
+// T (64 x 64, row-major, upper triangular) from G = V^T V (row-major) and tau,
+// the factor of H_0 H_1 ... H_63 = I - V T V^T.  The reference builds it
+// column by column: T[i][i] = tau_i, T[r][i] = sum_{c=r}^{i-1} T[r][c] t0[c][i]
+// with t0[c][i] = -tau_i G[c][i] (buildT).  Here that recurrence runs inside
+// the four 16 x 16 diagonal blocks at once, and the blocks are joined by the
+// same identity applied to blocks of reflectors, T_ab = -T_aa G_ab T_bb (two
+// 16-wide joins, then one 32-wide).  Equal to the column recurrence up to
+// rounding; columns from kb on are zero.
+constexpr int BT_THREADS = 256;
+
+__global__ void __launch_bounds__(BT_THREADS) qr_build_t_kernel(const double* G, const double* tau, int kb,
+                                                                double* T) {
     __shared__ double t[64][65];
-    const int r = threadIdx.x;
-#pragma unroll 16
-    for (int e = r; e < 64 * 64; e += 64) {
+    __shared__ double x[32][33];
+    const int tid = threadIdx.x;
+#pragma unroll 4
+    for (int e = tid; e < 64 * 64; e += BT_THREADS) {
         const int row = e >> 6, c = e & 63;
         double v = 0.0;
         if (c < kb) v = row < c ? -tau[c] * G[e] : (row == c ? tau[c] : 0.0);
         t[row][c] = v;
     }
     __syncthreads();
-    for (int i = 1; i < kb; ++i) {
-        double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
-        if (r < i) {
-            int c = r;
-            for (; c + 3 < i; c += 4) {
-                s0 = fma(t[r][c], t[c][i], s0);
-                s1 = fma(t[r][c + 1], t[c + 1][i], s1);
-                s2 = fma(t[r][c + 2], t[c + 2][i], s2);
-                s3 = fma(t[r][c + 3], t[c + 3][i], s3);
+    {
+        // diagonal blocks: 64 threads per block, rows r < 16
+        const int o = (tid >> 6) * 16, r = tid & 63;
+        for (int i = 1; i < 16; ++i) {
+            double s0 = 0.0, s1 = 0.0;
+            if (r < i) {
+                int c = r;
+                for (; c + 1 < i; c += 2) {
+                    s0 = fma(t[o + r][o + c], t[o + c][o + i], s0);
+                    s1 = fma(t[o + r][o + c + 1], t[o + c + 1][o + i], s1);
+                }
+                if (c < i) s0 = fma(t[o + r][o + c], t[o + c][o + i], s0);
             }
-            for (; c < i; ++c) s0 = fma(t[r][c], t[c][i], s0);
+            __syncthreads();  // column i of the block is read in full before it is overwritten
+            if (r < i) t[o + r][o + i] = s0 + s1;
+            __syncthreads();
         }
-        __syncthreads();  // column i is read in full before it is overwritten
-        if (r < i) t[r][i] = (s0 + s1) + (s2 + s3);
+    }
+    // joins: x = G_ab T_bb, then T_ab = -T_aa x (T_aa, T_bb upper triangular)
+    for (int level = 0; level < 2; ++level) {
+        const int w = level == 0 ? 16 : 32;
+        for (int e = tid; e < 2 * 16 * 16 * (1 - level) + 32 * 32 * level; e += BT_THREADS) {
+            const int p = level == 0 ? e >> 8 : 0, q = level == 0 ? e & 255 : e;
+            const int rr = q / w, j = q % w;
+            const int a0 = level == 0 ? 32 * p : 0, b0 = a0 + w;
+            double s = 0.0;
+            for (int c = 0; c <= j; ++c) s = fma(G[(a0 + rr) * 64 + b0 + c], t[b0 + c][b0 + j], s);
+            x[p * 16 + rr][j] = s;
+        }
+        __syncthreads();
+        for (int e = tid; e < 2 * 16 * 16 * (1 - level) + 32 * 32 * level; e += BT_THREADS) {
+            const int p = level == 0 ? e >> 8 : 0, q = level == 0 ? e & 255 : e;
+            const int rr = q / w, j = q % w;
+            const int a0 = level == 0 ? 32 * p : 0, b0 = a0 + w;
+            double s = 0.0;
+            for (int c = rr; c < w; ++c) s = fma(t[a0 + rr][a0 + c], x[p * 16 + c][j], s);
+            t[a0 + rr][b0 + j] = -s;
+        }
         __syncthreads();
     }
-    for (int c = 0; c < 64; ++c) T[r * 64 + c] = t[r][c];
+    for (int e = tid; e < 64 * 64; e += BT_THREADS) T[e] = t[e >> 6][e & 63];
 }
 
 // ones on the diagonal of a column-major matrix
@@ -790,7 +819,7 @@ int launch_set_identity(double* q, long long ldq, long long m, long long cols, c
 }
 
 int launch_qr_build_t(const double* g, const double* tau, int kb, double* t, cudaStream_t st) {
-    qr::qr_build_t_kernel<<<1, 64, 0, st>>>(g, tau, kb, t);
+    qr::qr_build_t_kernel<<<1, qr::BT_THREADS, 0, st>>>(g, tau, kb, t);
     return cudaGetLastError() == cudaSuccess ? JLC_OK : JLC_E_LAUNCH;
 }
 
