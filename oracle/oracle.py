@@ -14,6 +14,10 @@ reference file and lines it restates:
 * ``opt_gemm``          -- OptimizedBLAS3.gemm dispatch (OptimizedBLAS3.java:61-130)
 * ``gemm_packed_parallel`` -- PARALLEL_MICRO (OptimizedBLAS3.java:295-385)
 * ``gemm_dd``           -- double-double oracle + componentwise FP64 bound
+
+and restates in Python the blocked Householder QR (``householder_qr_blocked``,
+``householder_build_q``: HouseholderQR.java) and java.util.Random's generator
+(``java_random_doubles``, ``qr_test_matrices``) for the reference's QR tests.
 """
 from __future__ import annotations
 
@@ -100,6 +104,38 @@ def uniform(shape, seed: int) -> np.ndarray:
     """U[-1,1) i.i.d. from the SplitMix64 stream (no zeroed elements)."""
     n = int(np.prod(shape))
     return splittable_doubles(n, seed).reshape(shape)
+
+
+def java_random_doubles(seed: int, count: int) -> np.ndarray:
+    """``count`` successive ``new java.util.Random(seed).nextDouble()`` values:
+    the JDK's documented 48-bit linear congruential generator (initial
+    scramble seed ^ 0x5DEECE66D; seed' = seed * 0x5DEECE66D + 0xB mod 2^48;
+    next(b) = seed' >> (48 - b); nextDouble = (next(26) * 2^27 + next(27)) *
+    2^-53), so the reference's JUnit inputs can be regenerated exactly."""
+    mult, add, mask = 0x5DEECE66D, 0xB, (1 << 48) - 1
+    s = (int(seed) ^ mult) & mask
+    out = np.empty(count, dtype=np.float64)
+    for i in range(count):
+        s = (s * mult + add) & mask
+        hi = s >> 22
+        s = (s * mult + add) & mask
+        lo = s >> 21
+        out[i] = ((hi << 27) + lo) * (1.0 / (1 << 53))
+    return out
+
+
+def qr_test_matrices(seed: int, shapes):
+    """The reference QR stress test's inputs (HouseholderQRTest.randomMatrix /
+    randomMatrixRectangular, stress/HouseholderQRTest.java:122-139): one
+    java.util.Random(seed) stream consumed row by row, shape after shape,
+    each entry nextDouble() * 2.0 - 1.0."""
+    total = sum(m * n for m, n in shapes)
+    d = java_random_doubles(seed, total) * 2.0 - 1.0
+    out, o = [], 0
+    for m, n in shapes:
+        out.append(d[o:o + m * n].reshape(m, n).copy())
+        o += m * n
+    return out
 
 
 def normal(shape, seed: int) -> np.ndarray:

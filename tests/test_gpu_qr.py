@@ -86,3 +86,30 @@ def test_qr_tall_panel(ctx, oracle, m, n):
     r = np.triu(f[:n, :])
     g = a.T @ a
     assert np.abs(r.T @ r - g).max() <= 1e-12 * np.abs(g).max()
+
+
+# stress/HouseholderQRTest.java:14-120 replayed through the device route: the
+# same java.util.Random inputs, checks and tolerances
+REF_QR_SEED, REF_QR_SIZES, REF_QR_TOL = 12345, [1, 2, 3, 5, 10, 20, 50, 100], 1e-12
+
+
+@pytest.mark.parametrize("case", ["reconstruction", "orthogonality"])
+def test_reference_qr_cases(ctx, oracle, case):
+    seed = REF_QR_SEED + (0 if case == "reconstruction" else 1)
+    for a, n in zip(oracle.qr_test_matrices(seed, [(n, n) for n in REF_QR_SIZES]), REF_QR_SIZES):
+        at, tau = _factor(ctx, a)
+        q = _q(ctx, at, tau, n, n, n, n)
+        r = np.triu(at[:, :n].cpu().numpy().T)
+        if case == "reconstruction":
+            assert np.linalg.norm(q @ r - a) / np.linalg.norm(a) < REF_QR_TOL, n
+        else:
+            assert np.linalg.norm(q.T @ q - np.eye(n)) < REF_QR_TOL, n
+
+
+def test_reference_thin_qr_case(ctx, oracle):
+    (a,) = oracle.qr_test_matrices(REF_QR_SEED + 3, [(100, 40)])
+    at, tau = _factor(ctx, a)
+    q = _q(ctx, at, tau, 100, 40, 100, 40)
+    r = np.triu(at[:, :100].cpu().numpy().T)[:40, :]
+    assert np.linalg.norm(q @ r - a) / np.linalg.norm(a) < REF_QR_TOL
+    assert np.linalg.norm(q.T @ q - np.eye(40)) < REF_QR_TOL
