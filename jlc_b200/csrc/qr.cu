@@ -15,8 +15,9 @@
 //                      factorisation is deterministic;
 //   qr_pack_v_kernel:  V = the panel's reflectors with unit diagonal and zeros
 //                      above it (packV, HouseholderQR.java:445-471);
-//   qr_build_t_kernel: T from the Gram matrix G = V^T V and tau with the
-//                      reference's in-place recurrence (buildT, :300-325).
+//   qr_build_t_kernel: T from the Gram matrix G = V^T V and tau: the
+//                      reference's recurrence (buildT, :300-325) inside
+//                      16 x 16 diagonal blocks, joined blockwise.
 #include <cfloat>
 #include <cmath>
 
@@ -40,7 +41,8 @@ __device__ __forceinline__ double warp_max(double v) {
 }
 
 // ------------------------------------------------------------ multi-CTA panel
-// The same factorisation with the panel's rows split over the CTAs of one
+// The panel factorisation (computeHouseholder / applyHouseholderToColumn,
+// HouseholderQR.java:219-384) with the panel's rows split over the CTAs of one
 // cooperative launch (CTA c owns rows [k0 + c R, k0 + (c+1) R)).  Per column
 // k, one pass per CTA over its rows gives the column's local max, its scaled
 // sum of squares (scale, ssq) and its dots with the panel's later columns
@@ -445,7 +447,7 @@ __global__ void __launch_bounds__(MP_THREADS) qr_panel_sm_kernel(double* A, long
     }
 }
 
-// The panel on one thread-block cluster (2..16 CTAs, one slab of rows each in
+// The panel on one thread-block cluster (1..16 CTAs, one slab of rows each in
 // shared memory).  Each CTA stores its partials (and the CTA holding row k
 // the row record) straight into every CTA's shared memory, lane r to CTA r;
 // the stores complete under the cluster barrier's release, so after it every
