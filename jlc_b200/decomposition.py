@@ -1,0 +1,100 @@
+"""Host-side mirror of the reference's ``HouseholderQR`` on the device route.
+
+``HouseholderQR.decompose`` / ``decomposeThin`` / ``factorize``
+(decomposition/qr/HouseholderQR.java:26-92) with the same arguments, results
+and errors.  The matrix goes to the device once (column-major, the layout the
+reference factors in), ``jlc_qr_factor_device`` factors it there (panels,
+V/T and the compact-WY trailing updates all stay on the GPU),
+``jlc_qr_build_q_device`` forms Q there, and Q and R come back once.  Device
+memory is torch's; nothing here computes on the CPU.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+from . import _lib as L
+from .compute import IllegalArgumentException, Matrix, default_context
+
+
+class UnsupportedOperationException(RuntimeError):
+    """java.lang.UnsupportedOperationException."""
+
+
+class QRResult:
+    """decomposition/result/QRResult.java: the input, Q and R."""
+
+    def __init__(self, a: Matrix, q: Matrix, r: Matrix):
+        self._a, self._q, self._r = a, q, r
+
+    def getA(self) -> Matrix:
+        return self._a
+
+    def getQ(self) -> Matrix:
+        return self._q
+
+    def getR(self) -> Matrix:
+        return self._r
+
+
+def _check(a):
+    # HouseholderQR.java:57-58 (and :80-81 for factorize)
+    if a is None:
+        raise IllegalArgumentException("Matrix must not be null")
+    if a.getRawImagData() is not None:
+        raise UnsupportedOperationException("Householder QR requires real matrix")
+
+
+def _factor_on_device(a: Matrix, ctx, precision):
+    import torch
+    m, n = a.getRowCount(), a.getColumnCount()
+    dev = torch.device("cuda", ctx.device)
+    # column j of A is row j of `at` (column-major, leading dimension m)
+    at = torch.from_numpy(np.ascontiguousarray(a.to_numpy().T)).to(dev)
+    tau = torch.zeros(max(1, min(m, n)), dtype=torch.float64, device=dev)
+    ctx.qr_factor_device(m, n, at.data_ptr(), m, tau.data_ptr(), precision)
+    return at, tau
+
+
+def _decompose(a: Matrix, thin: bool, ctx, precision) -> QRResult:
+    _check(a)
+    m, n = a.getRowCount(), a.getColumnCount()
+    kmax = min(m, n)
+    q_cols = kmax if thin else m
+    r_rows = kmax if thin else m
+    if kmax == 0:
+        q = np.eye(m, q_cols)
+        r = np.zeros((r_rows, n))
+    else:
+        import torch
+        ctx = ctx or default_context()
+        at, tau = _factor_on_device(a, ctx, precision)
+        qt = torch.empty((q_cols, m), dtype=torch.float64, device=at.device)  # column-major m x q_cols
+        ctx.qr_build_q_device(m, n, q_cols, at.data_ptr(), m, tau.data_ptr(), qt.data_ptr(), m, precision)
+        q = qt.cpu().numpy().T
+        r = np.triu(at.cpu().numpy().T[:r_rows, :])  # extractR (HouseholderQR.java:552-572)
+    return QRResult(a, Matrix.wrap(np.ascontiguousarray(q).ravel(), m, q_cols),
+                    Matrix.wrap(np.ascontiguousarray(r).ravel(), r_rows, n))
+
+
+class HouseholderQR:
+    """decomposition/qr/HouseholderQR.java's public entry points.  ``ctx`` (a
+    ``jlc_b200.Context``; default: this thread's) and ``precision`` (the
+    route of the trailing-update GEMMs, as ``jlc_dgemm`` takes it) are the
+    additions; the policy argument is accepted and ignored, as the reference
+    ignores it (HouseholderQR.java:37-40)."""
+
+    @staticmethod
+    def decompose(a: Matrix, policy=None, ctx=None, precision: int = L.JLC_PREC_NATIVE) -> QRResult:
+        return _decompose(a, False, ctx, precision)
+
+    @staticmethod
+    def decomposeThin(a: Matrix, ctx=None, precision: int = L.JLC_PREC_NATIVE) -> QRResult:
+        return _decompose(a, True, ctx, precision)
+
+    @staticmethod
+    def factorize(a: Matrix, ctx=None, precision: int = L.JLC_PREC_NATIVE) -> None:
+        """Factors a copy and discards it, as the reference's benchmarking
+        entry does (factorizeOnly, HouseholderQR.java:79-92)."""
+        _check(a)
+        if min(a.getRowCount(), a.getColumnCount()) > 0:
+            _factor_on_device(a, ctx or default_context(), precision)

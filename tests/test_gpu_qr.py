@@ -113,3 +113,47 @@ def test_reference_thin_qr_case(ctx, oracle):
     r = np.triu(at[:, :100].cpu().numpy().T)[:40, :]
     assert np.linalg.norm(q @ r - a) / np.linalg.norm(a) < REF_QR_TOL
     assert np.linalg.norm(q.T @ q - np.eye(40)) < REF_QR_TOL
+
+
+def _ref_matrix(a):
+    import jlc_b200
+    return jlc_b200.Matrix.wrap(np.ascontiguousarray(a).ravel(), *a.shape)
+
+
+def _np(mat):
+    return mat.to_numpy()
+
+
+def test_reference_qr_test_file_through_mirror(ctx, oracle):
+    """stress/HouseholderQRTest.java's four tests, written against the
+    HouseholderQR mirror as the Java test is written against HouseholderQR."""
+    from jlc_b200 import HouseholderQR
+    for seed, case in ((REF_QR_SEED, "reconstruction"), (REF_QR_SEED + 1, "orthogonality"),
+                       (REF_QR_SEED + 2, "upper")):
+        for a, n in zip(oracle.qr_test_matrices(seed, [(n, n) for n in REF_QR_SIZES]), REF_QR_SIZES):
+            qr = HouseholderQR.decompose(_ref_matrix(a), ctx=ctx)
+            q, r = _np(qr.getQ()), _np(qr.getR())
+            assert q.shape == (n, n) and r.shape == (n, n)
+            if case == "reconstruction":
+                assert np.linalg.norm(q @ r - a) / np.linalg.norm(a) < REF_QR_TOL, n
+            elif case == "orthogonality":
+                assert np.linalg.norm(q.T @ q - np.eye(n)) < REF_QR_TOL, n
+            else:
+                assert np.abs(np.tril(r, -1)).max(initial=0.0) < 1e-12, n
+    (a,) = oracle.qr_test_matrices(REF_QR_SEED + 3, [(100, 40)])
+    qr = HouseholderQR.decomposeThin(_ref_matrix(a), ctx=ctx)
+    q, r = _np(qr.getQ()), _np(qr.getR())
+    assert q.shape == (100, 40) and r.shape == (40, 40)
+    assert np.linalg.norm(q @ r - a) / np.linalg.norm(a) < REF_QR_TOL
+    assert np.linalg.norm(q.T @ q - np.eye(40)) < REF_QR_TOL
+
+
+def test_mirror_shapes_and_factorize(ctx, oracle):
+    from jlc_b200 import HouseholderQR
+    a = oracle.uniform((70, 90), 4)           # wide: R is m x n, thin Q is m x m
+    qr = HouseholderQR.decompose(_ref_matrix(a), ctx=ctx)
+    assert _np(qr.getQ()).shape == (70, 70) and _np(qr.getR()).shape == (70, 90)
+    assert np.linalg.norm(_np(qr.getQ()) @ _np(qr.getR()) - a) <= 1e-13 * np.linalg.norm(a)
+    before = a.copy()
+    HouseholderQR.factorize(_ref_matrix(a), ctx=ctx)  # factors a copy
+    np.testing.assert_array_equal(a, before)

@@ -68,3 +68,18 @@ def test_reference_thin_qr_case_on_restatement():
     r = np.triu(f)[:40, :]
     assert np.linalg.norm(q @ r - a) / np.linalg.norm(a) < REF_QR_TOL
     assert np.linalg.norm(q.T @ q - np.eye(40)) < REF_QR_TOL
+
+
+def test_mirror_argument_errors():
+    """HouseholderQR.java:57-58: null and complex inputs are refused before
+    any device work."""
+    import jlc_b200
+    from jlc_b200 import HouseholderQR, IllegalArgumentException, UnsupportedOperationException
+    with pytest.raises(IllegalArgumentException, match="must not be null"):
+        HouseholderQR.decompose(None)
+    m = jlc_b200.Matrix(3, 3)
+    m.imag = np.zeros(9)
+    with pytest.raises(UnsupportedOperationException, match="real matrix"):
+        HouseholderQR.decomposeThin(m)
+    with pytest.raises(UnsupportedOperationException):
+        HouseholderQR.factorize(m)
