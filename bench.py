@@ -683,6 +683,8 @@ def run_qr(args):
             phases.append(per)
     ctx.set_profiling(False)
     ms = statistics.median(times)
+    peaks = ctx.measure_peaks()  # after the timed factorisations
+    tflops = flops / (ms * 1e-3) / 1e12
     cpu = None if args.no_cpu_baseline else qr_cpu_baseline(min(n, 1024))
     line = {"metric": f"blocked Householder QR GFLOP/s ({n}x{n}, FP64, device-resident)",
             "value": round(flops / (ms * 1e-3) / 1e9, 1), "unit": "GFLOP/s", "n_gpus": 1, "steps": args.steps,
@@ -693,6 +695,13 @@ def run_qr(args):
             "panel_share": round(statistics.median(panel) / ms, 3),
             "phase_ms": {name: round(statistics.median(p.get(name, 0.0) for p in phases), 3)
                          for name in sorted({n for p in phases for n in p})},
+            "roofline": {"bound": "tensor", "kernel": "whole factorisation (panel kernels + FP64 DMMA GEMMs)",
+                         "achieved": round(tflops, 3), "peak": round(peaks["fp64_dmma_tflops"], 2),
+                         "unit": "TFLOP/s", "frac": round(tflops / peaks["fp64_dmma_tflops"], 4), "traffic": None,
+                         "peak_source": "FP64 DMMA probe (jlc_measure_peaks) in this run; MEASURED_PEAKS.json has "
+                                        "no FP64 figure",
+                         "note": "the panel kernels, the largest share, are latency-bound (one barrier per "
+                                 "column), not tensor-bound"},
             "cpu_baseline": cpu}
     print(json.dumps(line), flush=True)
     ctx.close()
