@@ -119,11 +119,39 @@ __device__ __forceinline__ void ssq_merge(double& scale, double& ssq, double s2,
     }
 }
 
+// Power-of-two scaling shared by the panels: a column's values are scaled by
+// 2^-e, e the exponent of a maximum, before squares and dots are formed, so
+// nothing overflows or underflows whatever the input's range; sums carried in
+// units of 2^e (dots) or 4^e (squares) are rescaled exactly.
+constexpr double SP_EMPTY_EXP = -4096.0;  // exponent of an empty partial
+
+// exponent e with 2^e <= x < 2^(e+1) for a positive normal x, clamped to [-1000, 1000]
+__device__ __forceinline__ int sp_exp(double x) {
+    const int ex = (int)((__double_as_longlong(x) >> 52) & 0x7ff);
+    return x > 0.0 && ex != 0x7ff ? min(1000, max(-1000, ex - 1023)) : 0;
+}
+__device__ __forceinline__ double sp_pow2(int e) {  // 2^e, -1022 <= e <= 1023
+    return __longlong_as_double((long long)(e + 1023) << 52);
+}
+// s * 2^d for d <= 0 (flushed to zero below d = -2044, where the term is negligible)
+__device__ __forceinline__ double sp_scale(double s, int d) {
+    if (d >= -1022) return s * sp_pow2(d);
+    if (d >= -2044) return (s * sp_pow2(-1022)) * sp_pow2(d + 1022);
+    return 0.0;
+}
+// (e, s) += (e2, s2), both sums of squares in units of 4^e
+__device__ __forceinline__ void sp_merge(double& e, double& s, double e2, double s2) {
+    const double E = fmax(e, e2);
+    s = sp_scale(s, 2 * (int)(e - E)) + sp_scale(s2, 2 * (int)(e2 - E));
+    e = E;
+}
+
 __global__ void __launch_bounds__(MP_THREADS) qr_panel_mp_kernel(double* A, long long lda, int m, int k0, int kb,
                                                                  double* tau, double* part, double* rowrec,
                                                                  unsigned* counter, int* status) {
     __shared__ double fin[64];  // fin[0] = tau, fin[t] = dot_t for the later columns
-    __shared__ double fin_v0inv, fin_beta;
+    __shared__ double fin_v0inv, fin_v0s, fin_beta;
+    __shared__ int fin_e;
     __shared__ int fin_mode;  // 0: no reflector, 1: reflector, 2: sign flip (tau = 2)
     __shared__ int s_ok;
     const int P = gridDim.x, cta = blockIdx.x;
@@ -139,6 +167,12 @@ __global__ void __launch_bounds__(MP_THREADS) qr_panel_mp_kernel(double* A, long
         // Phase A: this CTA's rows -- task 0 the column's max and (scale, ssq)
         // over rows > k, task t >= 1 the dot of column k with column k + t
         const int lo = max(r0, k), lo1 = max(r0, k + 1);
+        // the dots use x 2^-e, e the exponent of this CTA's max of column k
+        // (every warp finds the same max)
+        double cmx = 0.0;
+        for (int i = lo + lane; i < r1; i += 32) cmx = fmax(cmx, fabs(colk[i]));
+        cmx = warp_max(cmx);
+        const double csc = sp_pow2(-sp_exp(cmx));
         for (int t = warp; t <= later; t += MP_WARPS) {
             if (t == 0) {
                 double mx = 0.0, sc = 0.0, sq = 0.0;
@@ -167,7 +201,7 @@ __global__ void __launch_bounds__(MP_THREADS) qr_panel_mp_kernel(double* A, long
             } else {
                 const double* cj = A + (long long)(k + t) * lda;
                 double d = 0.0;
-                for (int i = lo1 + lane; i < r1; i += 32) d = fma(colk[i], cj[i], d);
+                for (int i = lo1 + lane; i < r1; i += 32) d = fma(colk[i] * csc, cj[i], d);
 #pragma unroll
                 for (int o = 16; o > 0; o >>= 1) d += __shfl_xor_sync(0xffffffffu, d, o);
                 if (lane == 0) pk[2 + t] = d;
@@ -199,6 +233,8 @@ __global__ void __launch_bounds__(MP_THREADS) qr_panel_mp_kernel(double* A, long
                         fin_mode = 1;
                         fin_beta = nb * mx;
                         fin_v0inv = 1.0 / ((x0 - nb) * mx);
+                        fin_e = sp_exp(mx);
+                        fin_v0s = (inv * sp_pow2(fin_e)) / (x0 - nb);  // 2^E / ((x0 - beta) max), O(1)
                         fin[0] = (nb - x0) / nb;  // tau
                     }
                 }
@@ -208,10 +244,14 @@ __global__ void __launch_bounds__(MP_THREADS) qr_panel_mp_kernel(double* A, long
         const int mode = fin_mode;
         const double tk = mode == 1 ? fin[0] : (mode == 2 ? 2.0 : 0.0);
         if (mode == 1) {
+            const int E = fin_e;
             for (int t = 1 + tid; t <= later; t += MP_THREADS) {
-                double d = 0.0;
-                for (int q = 0; q < P; ++q) d += pb[q * MP_PART + 2 + t];
-                fin[t] = (rk[t] + d * fin_v0inv) * tk;
+                double d = 0.0;  // CTA q's dot is in units of 2^e_q, brought to 2^E
+                for (int q = 0; q < P; ++q) {
+                    const double mq = pb[q * MP_PART];
+                    if (mq > 0.0) d += sp_scale(pb[q * MP_PART + 2 + t], sp_exp(mq) - E);
+                }
+                fin[t] = (rk[t] + d * fin_v0s) * tk;
             }
         } else if (mode == 2) {
             for (int t = 1 + tid; t <= later; t += MP_THREADS) fin[t] = rk[t] * 2.0;  // the tail is zero
@@ -255,35 +295,13 @@ __global__ void __launch_bounds__(MP_THREADS) qr_panel_mp_kernel(double* A, long
 constexpr int SP_MAX_SLAB_BYTES = 200 * 1024;
 constexpr int SP_MAX_CTAS = 160;                    // partial loads: up to 5 per lane
 constexpr int SP_TASKS = 64 / MP_WARPS;             // later columns per warp
-constexpr double SP_EMPTY_EXP = -4096.0;            // exponent of an empty (e, s) pair
-
-// exponent e with 2^e <= x < 2^(e+1) for a positive normal x, clamped to [-1000, 1000]
-__device__ __forceinline__ int sp_exp(double x) {
-    const int ex = (int)((__double_as_longlong(x) >> 52) & 0x7ff);
-    return x > 0.0 && ex != 0x7ff ? min(1000, max(-1000, ex - 1023)) : 0;
-}
-__device__ __forceinline__ double sp_pow2(int e) {  // 2^e, -1022 <= e <= 1023
-    return __longlong_as_double((long long)(e + 1023) << 52);
-}
-// s * 2^d for d <= 0 (flushed to zero below d = -2044, where the term is negligible)
-__device__ __forceinline__ double sp_scale(double s, int d) {
-    if (d >= -1022) return s * sp_pow2(d);
-    if (d >= -2044) return (s * sp_pow2(-1022)) * sp_pow2(d + 1022);
-    return 0.0;
-}
-// (e, s) += (e2, s2), both sums of squares in units of 4^e
-__device__ __forceinline__ void sp_merge(double& e, double& s, double e2, double s2) {
-    const double E = fmax(e, e2);
-    s = sp_scale(s, 2 * (int)(e - E)) + sp_scale(s2, 2 * (int)(e2 - E));
-    e = E;
-}
 
 __global__ void __launch_bounds__(MP_THREADS) qr_panel_sm_kernel(double* A, long long lda, int m, int k0, int kb,
                                                                  double* tau, double* part, double* rowrec,
                                                                  unsigned* counter, int* status) {
     extern __shared__ double slab[];  // slab[c * R + (i - r0)] = A[i, k0 + c]
     __shared__ double fin[64];
-    __shared__ double fin_v0inv, fin_beta, fin_tau;
+    __shared__ double fin_v0inv, fin_v0s, fin_beta, fin_tau;
     __shared__ int fin_mode;
     __shared__ int s_ok;
     const int P = gridDim.x, cta = blockIdx.x;
@@ -303,15 +321,21 @@ __global__ void __launch_bounds__(MP_THREADS) qr_panel_sm_kernel(double* A, long
         double* pk = part + (size_t)(kk & 1) * MP_PART * P + cta;
         double* rk = rowrec + (size_t)(kk & 1) * 64;
         const int lo = max(r0, k), lo1 = max(r0, k + 1);
-        // Phase A: warp w the dots of column k with the later columns
-        // t = 1 + w + 8j (all j together); the last warp also the column's
-        // max over rows >= k and its sum of squares over rows > k
+        // Phase A: every warp the max of column k over own rows >= k and its
+        // exponent e; warp w the dots of x 2^-e with the later columns
+        // t = 1 + w + 8j (all j together); the last warp also the sum of
+        // squares over rows > k
         {
+            double mx = 0.0;
+            for (int i = lo + lane; i < r1; i += 32) mx = fmax(mx, fabs(ck[i - r0]));
+            mx = warp_max(mx);
+            const int e = sp_exp(mx);
+            const double sc = sp_pow2(-e);
             double d[SP_TASKS];
 #pragma unroll
             for (int j = 0; j < SP_TASKS; ++j) d[j] = 0.0;
             for (int i = lo1 + lane; i < r1; i += 32) {
-                const double x = ck[i - r0];
+                const double x = ck[i - r0] * sc;
 #pragma unroll
                 for (int j = 0; j < SP_TASKS; ++j) {
                     const int t = 1 + warp + j * MP_WARPS;
@@ -327,11 +351,6 @@ __global__ void __launch_bounds__(MP_THREADS) qr_panel_sm_kernel(double* A, long
                 }
             }
             if (warp == MP_WARPS - 1) {
-                double mx = 0.0;
-                for (int i = lo + lane; i < r1; i += 32) mx = fmax(mx, fabs(ck[i - r0]));
-                mx = warp_max(mx);
-                const int e = sp_exp(mx);
-                const double sc = sp_pow2(-e);
                 double sq = 0.0;
                 for (int i = lo1 + lane; i < r1; i += 32) {
                     const double y = ck[i - r0] * sc;
@@ -340,7 +359,7 @@ __global__ void __launch_bounds__(MP_THREADS) qr_panel_sm_kernel(double* A, long
                 sq = warp_sum(sq);
                 if (lane == 0) {
                     pk[0] = mx;
-                    pk[P] = (double)e;
+                    pk[P] = mx > 0.0 ? (double)e : SP_EMPTY_EXP;
                     pk[2 * P] = sq;
                 }
             }
@@ -359,6 +378,16 @@ __global__ void __launch_bounds__(MP_THREADS) qr_panel_sm_kernel(double* A, long
             rkv[j] = t <= later ? rk[t] : 0.0;
         }
         const double x0raw = rk[0];
+        // CTA q's dots are in units of 2^e_q: each is brought to 2^E, E = max e_q
+        double eqv[SP_MAX_CTAS / 32];
+        double emax = SP_EMPTY_EXP;
+#pragma unroll
+        for (int c = 0; c < SP_MAX_CTAS / 32; ++c) {
+            const int q = lane + 32 * c;
+            eqv[c] = q < P ? pb[P + q] : SP_EMPTY_EXP;
+            emax = fmax(emax, eqv[c]);
+        }
+        emax = warp_max(emax);
 #pragma unroll
         for (int c = 0; c < SP_MAX_CTAS / 32; ++c) {
             const int q = lane + 32 * c;
@@ -366,7 +395,7 @@ __global__ void __launch_bounds__(MP_THREADS) qr_panel_sm_kernel(double* A, long
 #pragma unroll
                 for (int j = 0; j < SP_TASKS; ++j) {
                     const int t = 1 + warp + j * MP_WARPS;
-                    if (t <= later && q < P) dsum[j] += pb[(2 + t) * P + q];
+                    if (t <= later && q < P) dsum[j] += sp_scale(pb[(2 + t) * P + q], (int)(eqv[c] - emax));
                 }
             }
         }
@@ -401,6 +430,7 @@ __global__ void __launch_bounds__(MP_THREADS) qr_panel_sm_kernel(double* A, long
                         mode = 1;
                         fin_beta = nb * mx;
                         fin_v0inv = 1.0 / ((x0 - nb) * mx);
+                        fin_v0s = (inv * sp_pow2((int)e)) / (x0 - nb);  // 2^E / ((x0 - beta) max), O(1)
                         fin_tau = (nb - x0) / nb;
                     }
                 }
@@ -411,13 +441,13 @@ __global__ void __launch_bounds__(MP_THREADS) qr_panel_sm_kernel(double* A, long
         __syncthreads();
         const int mode = fin_mode;
         if (mode == 1) {
-            const double v0inv = fin_v0inv, tk = fin_tau;
+            const double v0s = fin_v0s, tk = fin_tau;
 #pragma unroll
             for (int j = 0; j < SP_TASKS; ++j) {
                 const int t = 1 + warp + j * MP_WARPS;
                 if (t <= later) {  // warp-uniform
                     const double d = warp_sum(dsum[j]);
-                    if (lane == 0) fin[t] = (rkv[j] + d * v0inv) * tk;
+                    if (lane == 0) fin[t] = (rkv[j] + d * v0s) * tk;
                 }
             }
         } else if (mode == 2) {
@@ -468,7 +498,7 @@ __global__ void __launch_bounds__(CL_THREADS, 1) qr_panel_cl_kernel(double* A, l
     __shared__ double part[2][CL_MAX][MP_PART];  // from CTA q: 0 max, 1 exponent, 2 sum of squares, 2 + t dot
     __shared__ double rrec[2][64];            // row k of columns k .. k0 + kb - 1
     __shared__ double fin[64];
-    __shared__ double fin_v0inv, fin_beta, fin_tau;
+    __shared__ double fin_v0inv, fin_v0s, fin_beta, fin_tau;
     __shared__ int fin_mode;
     cg::cluster_group cluster = cg::this_cluster();
     const int P = (int)cluster.num_blocks(), cta = (int)cluster.block_rank();
@@ -489,14 +519,23 @@ __global__ void __launch_bounds__(CL_THREADS, 1) qr_panel_cl_kernel(double* A, l
         // this CTA's partials in CTA `lane`'s shared memory (lanes >= P unused)
         double* pk = cluster.map_shared_rank(&part[kk & 1][cta][0], lane < P ? lane : 0);
         const int lo = max(r0, k), lo1 = max(r0, k + 1);
-        // Phase A (own rows): warp w the dots with columns t = 1 + w + 16j,
-        // the last warp also the max and the (e, s) sum of squares
+        // Phase A (own rows): every warp the max of column k over rows >= k
+        // and its exponent e (the same in every warp); warp w the dots of
+        // x 2^-e with columns t = 1 + w + 16j; the last warp also the (e, s)
+        // sum of squares.  Scaling x by 2^-e keeps the dots finite and exact
+        // to rounding for any input range, as the reference's dots with the
+        // normalised reflector are.
         {
+            double mx = 0.0;
+            for (int i = lo + lane; i < r1; i += 32) mx = fmax(mx, fabs(ck[i - r0]));
+            mx = warp_max(mx);
+            const int e = sp_exp(mx);
+            const double sc = sp_pow2(-e);
             double d[CL_TASKS];
 #pragma unroll
             for (int j = 0; j < CL_TASKS; ++j) d[j] = 0.0;
             for (int i = lo1 + lane; i < r1; i += 32) {
-                const double x = ck[i - r0];
+                const double x = ck[i - r0] * sc;
 #pragma unroll
                 for (int j = 0; j < CL_TASKS; ++j) {
                     const int t = 1 + warp + j * CL_WARPS;
@@ -512,11 +551,6 @@ __global__ void __launch_bounds__(CL_THREADS, 1) qr_panel_cl_kernel(double* A, l
                 }
             }
             if (warp == CL_WARPS - 1) {
-                double mx = 0.0;
-                for (int i = lo + lane; i < r1; i += 32) mx = fmax(mx, fabs(ck[i - r0]));
-                mx = warp_max(mx);
-                const int e = sp_exp(mx);
-                const double sc = sp_pow2(-e);
                 double sq = 0.0;
                 for (int i = lo1 + lane; i < r1; i += 32) {
                     const double y = ck[i - r0] * sc;
@@ -525,7 +559,7 @@ __global__ void __launch_bounds__(CL_THREADS, 1) qr_panel_cl_kernel(double* A, l
                 sq = warp_sum(sq);
                 if (lane < P) {
                     pk[0] = mx;
-                    pk[1] = (double)e;
+                    pk[1] = mx > 0.0 ? (double)e : SP_EMPTY_EXP;
                     pk[2] = sq;
                 }
             }
@@ -540,11 +574,18 @@ __global__ void __launch_bounds__(CL_THREADS, 1) qr_panel_cl_kernel(double* A, l
         const double* orow = rrec[kk & 1];
         double dsum[CL_TASKS], rkv[CL_TASKS];
         const double* rp = part[kk & 1][lane < P ? lane : 0];
+        const double eq = lane < P ? rp[1] : SP_EMPTY_EXP;
 #pragma unroll
         for (int j = 0; j < CL_TASKS; ++j) {
             const int t = 1 + warp + j * CL_WARPS;
             rkv[j] = t <= later ? orow[t] : 0.0;
             dsum[j] = t <= later && lane < P ? rp[2 + t] : 0.0;
+        }
+        {
+            // CTA q's dots are in units of 2^e_q: bring them to 2^E, E = max e_q
+            const double emax = warp_max(eq);
+#pragma unroll
+            for (int j = 0; j < CL_TASKS; ++j) dsum[j] = sp_scale(dsum[j], (int)(eq - emax));
         }
         if (warp == 0) {
             const double x0raw = orow[0];
@@ -574,6 +615,7 @@ __global__ void __launch_bounds__(CL_THREADS, 1) qr_panel_cl_kernel(double* A, l
                         mode = 1;
                         fin_beta = nb * mx;
                         fin_v0inv = 1.0 / ((x0 - nb) * mx);
+                        fin_v0s = (inv * sp_pow2((int)e)) / (x0 - nb);  // 2^E / ((x0 - beta) max), O(1)
                         fin_tau = (nb - x0) / nb;
                     }
                 }
@@ -584,13 +626,13 @@ __global__ void __launch_bounds__(CL_THREADS, 1) qr_panel_cl_kernel(double* A, l
         __syncthreads();
         const int mode = fin_mode;
         if (mode == 1) {
-            const double v0inv = fin_v0inv, tk = fin_tau;
+            const double v0s = fin_v0s, tk = fin_tau;
 #pragma unroll
             for (int j = 0; j < CL_TASKS; ++j) {
                 const int t = 1 + warp + j * CL_WARPS;
                 if (t <= later) {  // warp-uniform
                     const double d = warp_sum(dsum[j]);
-                    if (lane == 0) fin[t] = (rkv[j] + d * v0inv) * tk;
+                    if (lane == 0) fin[t] = (rkv[j] + d * v0s) * tk;
                 }
             }
         } else if (mode == 2) {

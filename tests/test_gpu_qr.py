@@ -157,3 +157,25 @@ def test_mirror_shapes_and_factorize(ctx, oracle):
     before = a.copy()
     HouseholderQR.factorize(_ref_matrix(a), ctx=ctx)  # factors a copy
     np.testing.assert_array_equal(a, before)
+
+
+@pytest.mark.parametrize("m,n", [(2000, 130), (8000, 130), (60000, 70)])
+def test_qr_extreme_column_scales(ctx, oracle, m, n):
+    """Columns scaled by 2^900, 2^-900 and 1: products of two such entries
+    overflow or underflow, so the panel must scale before it forms squares
+    and dots, as the reference's normalised reflector does.  With power-of-two
+    scales S, QR(A S) has QR(A)'s reflectors and tau and R S (exactly, on the
+    restatement), so the device result is checked against the restatement of
+    the unscaled A.  One shape per panel kernel: one cluster, a grid with
+    slabs in shared memory, a grid in place."""
+    a = oracle.uniform((m, n), 5 + m)
+    s = np.array([2.0 ** 900 if j % 3 == 0 else (2.0 ** -900 if j % 3 == 1 else 1.0) for j in range(n)])
+    at, tau = _factor(ctx, a * s)
+    f = at[:, :m].cpu().numpy().T
+    f_ref, tau_ref = oracle.householder_qr_blocked(a)
+    assert np.isfinite(f).all()
+    np.testing.assert_allclose(tau.cpu().numpy()[:n], tau_ref, rtol=0, atol=1e-12)
+    up = np.triu(np.ones((m, n), bool))
+    tol = 1e-11 * max(1.0, np.abs(f_ref).max())
+    np.testing.assert_allclose(np.where(up, f / s, 0.0), np.where(up, f_ref, 0.0), rtol=0, atol=tol)
+    np.testing.assert_allclose(np.where(up, 0.0, f), np.where(up, 0.0, f_ref), rtol=0, atol=tol)
