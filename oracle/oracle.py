@@ -16,12 +16,15 @@ reference file and lines it restates:
 * ``gemm_dd``           -- double-double oracle + componentwise FP64 bound
 
 and restates in Python the blocked Householder QR (``householder_qr_blocked``,
-``householder_build_q``: HouseholderQR.java) and java.util.Random's generator
-(``java_random_doubles``, ``qr_test_matrices``) for the reference's QR tests.
+``householder_build_q``: HouseholderQR.java), the blocked Hessenberg reduction
+(``blocked_hessenberg``: BlockedHessenbergQR.java) and java.util.Random's
+generator (``java_random_doubles``, ``qr_test_matrices``, ``java_random_matrix``)
+for the reference's decomposition tests.
 """
 from __future__ import annotations
 
 import ctypes
+import math
 import os
 import subprocess
 
@@ -136,6 +139,104 @@ def qr_test_matrices(seed: int, shapes):
         out.append(d[o:o + m * n].reshape(m, n).copy())
         o += m * n
     return out
+
+
+def java_random_matrix(seed: int, rows: int, cols: int) -> np.ndarray:
+    """A rows x cols matrix filled row by row with new java.util.Random(seed)
+    .nextDouble() * 2 - 1, the reference tests' randomMatrix(n, seed)
+    (decomposition/DecompositionTests.java:81-104)."""
+    return (java_random_doubles(seed, rows * cols) * 2.0 - 1.0).reshape(rows, cols)
+
+
+# ------------------------------------------------------------- blocked Hessenberg reduction
+HESS_EPS = 1e-12  # BlockedHessenbergQR.EPS (eigen/qr/BlockedHessenbergQR.java:45)
+
+
+def _hess_panel(work, n, k, pw):
+    """factorPanelUnblocked (BlockedHessenbergQR.java:150-244): column by
+    column on a working copy, each reflector applied to the copy from the left
+    (columns col+1..) and from the right (all rows); returns V (m x pw, unit
+    entry at row j of column j, zeros above) and tau."""
+    m = n - (k + 1)
+    V = np.zeros((m, pw))
+    tau = np.zeros(pw)
+    for j in range(pw):
+        col = k + j
+        row_start = col + 1
+        length = n - row_start
+        if length <= 0:
+            continue
+        x0 = work[row_start, col]
+        tail = work[row_start + 1:, col]
+        sigma = float(np.cumsum(tail * tail)[-1]) if length > 1 else 0.0  # the reference's serial sum
+        if sigma <= HESS_EPS:
+            continue
+        mu = math.sqrt(x0 * x0 + sigma)
+        beta = -math.copysign(mu, x0)
+        v0 = x0 - beta
+        v0sq = v0 * v0
+        if v0sq <= HESS_EPS:
+            continue
+        t = 2.0 * v0sq / (sigma + v0sq)
+        tau[j] = t
+        v = np.zeros(m)
+        v[j] = 1.0
+        v[j + 1:j + length] = tail / v0
+        V[:, j] = v
+        vt = v[j:j + length]  # the reflector on rows row_start .. n-1
+        # from the left, columns col+1 .. n-1
+        dots = (vt @ work[row_start:, col + 1:]) * t
+        work[row_start:, col + 1:] -= np.outer(vt, dots)
+        # from the right, all rows, columns col+1 .. n-1
+        dots = (work[:, col + 1:col + 1 + length] @ vt) * t
+        work[:, col + 1:col + 1 + length] -= np.outer(dots, vt)
+        work[row_start, col] = beta
+        work[row_start + 1:, col] = 0.0
+    return V, tau
+
+
+def _hess_build_t(V, tau):
+    """buildT (BlockedHessenbergQR.java:246-275): T[j][i] = sum_{l=j}^{i-1}
+    T[j][l] (-tau_i V_l . V_i), T[i][i] = tau_i (a zero column when tau_i = 0)."""
+    pw = len(tau)
+    T = np.zeros((pw, pw))
+    for i in range(pw):
+        if tau[i] == 0.0:
+            continue
+        w = -tau[i] * (V[:, :i].T @ V[:, i])
+        for j in range(i):
+            T[j, i] = float(T[j, j:i] @ w[j:i])
+        T[i, i] = tau[i]
+    return T
+
+
+def blocked_hessenberg(a, block: int = 32):
+    """BlockedHessenbergQR.decompose (eigen/qr/BlockedHessenbergQR.java:99-146)
+    restated: panels of `block` columns factored on a copy of H, then H <-
+    (I - V T^T V^T) H (applyBlockLeft :277-307: W = V^T H, W = T^T W,
+    H -= V W), H <- H (I - V T V^T) and Q <- Q (I - V T V^T) (applyBlockRight
+    :309-345: W = H V, W = W T, H -= W V^T), and fill-in below the first
+    subdiagonal cleared.  Returns (H, Q) with A = Q H Q^T."""
+    h = np.array(a, dtype=np.float64, copy=True)
+    n = h.shape[0]
+    q = np.eye(n)
+    if n <= 2:
+        return h, q
+    for k in range(0, n - 2, block):
+        pw = min(block, (n - 2) - k)
+        m = n - (k + 1)
+        if pw <= 0 or m <= 0:
+            break
+        V, tau = _hess_panel(h.copy(), n, k, pw)
+        T = _hess_build_t(V, tau)
+        sub = h[k + 1:, k:]                      # applyBlockLeft, colStart = k
+        sub -= V @ (T.T @ (V.T @ sub))
+        for mat in (h, q):                       # applyBlockRight, colStart = k + 1
+            blk = mat[:, k + 1:]
+            blk -= ((blk @ V) @ T) @ V.T
+    for col in range(n - 2):
+        h[col + 2:, col] = 0.0
+    return h, q
 
 
 def normal(shape, seed: int) -> np.ndarray:
