@@ -75,7 +75,7 @@ typedef struct jlc_report {
     int32_t kernel;        /* JLC_KERNEL_* */
     int32_t slices;        /* Ozaki slice count s, or number of moduli N (0 for native) */
     int32_t products;      /* INT8 products run: s(s+1)/2 slice pairs, or N residue products */
-    double est_err_ratio;  /* Ozaki a-priori error estimate / FP64 bound (0 for native) */
+    double est_err_ratio;  /* Ozaki: certified bound of max |err| / FP64 bound (see below); 0 for native */
     double device_ms;      /* device time of the call, CUDA events (host entries only) */
     int64_t h2d_bytes;     /* bytes copied host -> device by this call */
     int64_t d2h_bytes;     /* bytes copied device -> host by this call */
@@ -167,6 +167,33 @@ JLC_API int jlc_dgemm_ozaki_crt_device(jlc_ctx* ctx, int layout_a, int layout_b,
  * JLC_OK, or JLC_E_TIMEOUT if a kernel gave up on a bounded wait. */
 JLC_API int jlc_device_status(jlc_ctx* ctx);
 
+/* Limit of every bounded device wait (mbarrier, grid barrier) of this
+ * context's kernels, in seconds (0: the default of 4 s; at most 600).  A wait
+ * that runs out records JLC_DEV_TIMEOUT, the kernel unwinds (in-flight copies
+ * drained, tensor memory freed) and the call reports JLC_E_TIMEOUT; the
+ * context stays usable.  New: the reference has no device waits. */
+JLC_API int jlc_set_wait_limit(jlc_ctx* ctx, double seconds);
+
+/* Test hook for the failure paths (new; no reference counterpart).  The
+ * (after + 1)-th operation of `kind` on this context fails once:
+ *   JLC_FAULT_ALLOC   a device buffer request reports JLC_E_OOM (nothing allocated)
+ *   JLC_FAULT_LAUNCH  a GEMM dispatch reports JLC_E_LAUNCH before launching
+ *   JLC_FAULT_COPY    a host<->device copy of a host entry reports JLC_E_CUDA
+ *   JLC_FAULT_WAIT    the next FP64 GEMM kernel leaves one stage unloaded, so
+ *                     one of its bounded waits runs out (JLC_E_TIMEOUT)
+ * JLC_FAULT_NONE clears it.  All faults are made on the host or by a wait
+ * that nothing satisfies; none faults the GPU.  The environment variable
+ * JLCGPU_FAULT=alloc|launch|copy|wait[:after] arms one at jlc_init.  A host
+ * entry that fails before it copies C back leaves C unchanged, as
+ * CudaGemm.gemm's contract expects (CudaGemm.java:114-115); after
+ * JLC_E_TIMEOUT the contents of C are not valid. */
+#define JLC_FAULT_NONE 0
+#define JLC_FAULT_ALLOC 1
+#define JLC_FAULT_LAUNCH 2
+#define JLC_FAULT_COPY 3
+#define JLC_FAULT_WAIT 4
+JLC_API int jlc_inject_fault(jlc_ctx* ctx, int kind, int after);
+
 /* ---------------------------------------------------------------- measurement */
 /* phases the profiler records (one CUDA event pair per phase and call) */
 #define JLC_PHASE_DMMA 1        /* FP64 DMMA GEMM kernel */
@@ -175,12 +202,16 @@ JLC_API int jlc_device_status(jlc_ctx* ctx);
 #define JLC_PHASE_GROUPED 4     /* persistent grouped launch */
 #define JLC_PHASE_OZAKI_SPLIT 5 /* exponent scaling + INT8 slicing of A and B */
 #define JLC_PHASE_SCALE 6       /* beta-only update of C */
-#define JLC_PHASE_FP64_GATED 7  /* FP64 kernel behind an Ozaki call (runs only on Inf/NaN input) */
+#define JLC_PHASE_FP64_GATED 7  /* FP64 kernel behind an Ozaki call (runs only on Inf/NaN input or when
+                                   the accuracy certificate fails at every count) */
 #define JLC_PHASE_H2D 8         /* host -> device operand copies */
 #define JLC_PHASE_D2H 9         /* device -> host copy of C */
 #define JLC_PHASE_REDUCE 11     /* adjoint reductions: d(alpha) / d(beta) dots and sums, scaled copies */
 #define JLC_PHASE_QR_PANEL 12   /* blocked QR: one panel's factorisation kernel */
 #define JLC_PHASE_QR_VT 13      /* blocked QR: V packing and the T factor (the Gram GEMM is a dmma phase) */
+#define JLC_PHASE_OZAKI_CERT 14     /* Ozaki accuracy certificate (magnitude product, route decision) */
+#define JLC_PHASE_OZAKI_SPLIT_HI 15 /* split at the higher count (runs only when the certificate picks it) */
+#define JLC_PHASE_OZAKI_GEMM_HI 16  /* INT8 GEMM at the higher count (likewise) */
 /* Turn event-pair recording around each phase on (1) or off (0).  Records
  * accumulate (up to 4096) until collected. */
 JLC_API int jlc_set_profiling(jlc_ctx* ctx, int on);
@@ -300,16 +331,21 @@ JLC_API int jlc_qr_build_q_device(jlc_ctx* ctx, int64_t m, int64_t n, int64_t qc
  * cudaFree may synchronise the device, embedders that forbid driver
  * allocations after start-up.  Scratch comes from a 64 MiB array compiled into
  * the library (held by every GPU that loads it until exit); problems whose
- * INT8 slices, s*(m+n)*roundup(k,16) bytes plus at least one 256 KB FP64 tile,
- * do not fit return JLC_E_ARG with a message.  Same arguments and semantics as
- * jlc_dgemm_ozaki_device, plus:
+ * INT8 slices and certificate plane, (s+1)*(m+n)*roundup(k,16) bytes plus at
+ * least one 256 KB FP64 tile, do not fit return JLC_E_ARG with a message.
+ * Same arguments and semantics as jlc_dgemm_ozaki_device (the automatic
+ * slice count is certified on the device and falls back to FP64 likewise;
+ * m == 1 or n == 1 runs the matrix-vector kernel), plus:
  *   cuda_stream  stream the work is enqueued on (NULL: legacy default stream);
- *   dev_status   optional DEVICE int that receives JLC_DEV_* bits if a bounded
- *                wait times out (NULL: kept inside the library's array);
+ *   dev_status   optional DEVICE int that receives the call's JLC_DEV_* bits
+ *                (copied from the library's array at the end of the call;
+ *                non-zero when a bounded wait timed out);
  *   err, errlen  optional HOST buffer for an error message.
  * A and B must have 16-byte aligned bases and even leading dimensions.
  * The first call on each device looks up the array's device address (with
- * that device current) and should come before any stream capture.  All calls
+ * that device current) and should come before any stream capture; the
+ * address is cached for the device's primary context (do not call this
+ * entry after resetting the device or under another driver context).  All calls
  * on a device share the array: calls that overlap on the GPU race and must be
  * serialised by the caller.  Returns when the work is enqueued. */
 JLC_API int jlc_dgemm_ozaki_static(int layout_a, int layout_b, int64_t m, int64_t n, int64_t k, double alpha,

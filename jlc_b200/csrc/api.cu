@@ -35,6 +35,7 @@ int cuda_err(jlc_ctx* ctx, cudaError_t e, const char* what) {
 }
 
 int reserve(jlc_ctx* ctx, DevBuf& b, size_t bytes, const char* what) {
+    if (fault_hit(ctx, JLC_FAULT_ALLOC)) return set_err(ctx, JLC_E_OOM, "%s: injected allocation failure", what);
     if (bytes <= b.bytes) return JLC_OK;
     if (b.ptr) cudaFree(b.ptr);
     b.ptr = nullptr;
@@ -56,6 +57,28 @@ int reserve(jlc_ctx* ctx, DevBuf& b, size_t bytes, const char* what) {
 }
 
 inline long long round_up(long long v, long long m) { return (v + m - 1) / m * m; }
+
+// the context workspace, grown on demand (and the allocation test hook)
+int ws_reserve(jlc_ctx* ctx, size_t bytes) {
+    if (fault_hit(ctx, JLC_FAULT_ALLOC)) return set_err(ctx, JLC_E_OOM, "workspace: injected allocation failure");
+    return workspace_reserve(ctx->ws, bytes, ctx->err, sizeof(ctx->err));
+}
+
+// a failed copy of the single-shot host entry: the stream is drained so the
+// context is idle when the error returns
+int copy_failed(jlc_ctx* ctx, cudaError_t e, const char* what) {
+    const int rc = cuda_err(ctx, e, what);
+    cudaStreamSynchronize(ctx->stream);
+    cudaGetLastError();
+    return rc;
+}
+
+// a host <-> device copy of a host entry (and the copy test hook)
+cudaError_t copy2d(jlc_ctx* ctx, void* dst, size_t dpitch, const void* src, size_t spitch, size_t width,
+                   size_t height, cudaMemcpyKind kind, cudaStream_t st) {
+    if (fault_hit(ctx, JLC_FAULT_COPY)) return cudaErrorUnknown;
+    return cudaMemcpy2DAsync(dst, dpitch, src, spitch, width, height, kind, st);
+}
 
 // Phase markers for the profiler: begin() records the start event of a new
 // record, end() its stop event.  Both are no-ops when profiling is off or the
@@ -104,30 +127,48 @@ void report_init(jlc_report* rep) {
     if (rep) memset(rep, 0, sizeof(*rep));
 }
 
-// Ozaki slice count from the a-priori model (see ozaki.cu): the smallest s in
-// [5,8] whose worst-case error estimate stays inside the FP64 bound for
-// inputs whose |A||B| is not far below rowmax*colmax*k.
-int auto_slices(long long k) {
-    // (s+3) * 2^-7s <= 2u * k * rho^2 with rho = 1/4 (uniform-like rows/cols)
-    const double u = std::ldexp(1.0, -53);
-    for (int s = 5; s <= 8; ++s) {
-        const double lhs = (s + 3) * std::ldexp(1.0, -7 * s);
-        const double rhs = 2.0 * u * (double)k / 16.0;
-        if (lhs <= rhs) return s;
-    }
-    return 8;
-}
+}  // namespace
 
-// Whether the automatic slice / modulus count reaches the scheme's accuracy
-// target for this k.  For very short products neither scheme does (the
-// operand scales are capped by the split's exact integer range: 2^-51 of the
-// row/column maximum against a componentwise bound of 2 k u), so those run in
-// FP64 -- as calls whose operands hold Inf/NaN do.
-bool ozaki_reaches_bound(long long k, bool crt) {
-    if (crt) return ozaki_crt_est_ratio(ozaki_crt_auto_moduli(k), k) <= 1.0;
-    const int s = auto_slices(k);
-    return (s + 3) * std::ldexp(1.0, -7 * s) <= 2.0 * std::ldexp(1.0, -53) * (double)k / 16.0;
+namespace jlc {
+// The matrix-vector form of a GEMM with n == 1 or m == 1.
+GemvDesc gemv_desc(const GemmDesc& g) {
+    GemvDesc v;
+    if (g.n == 1) {
+        // y = C(:,0), rows of op(A) dotted with x = B(:,0)
+        v.rows = g.m;
+        v.cols = g.k;
+        v.mat = g.a;
+        v.rs = g.layout_a == JLC_ROW_MAJOR ? g.lda : 1;
+        v.cs = g.layout_a == JLC_ROW_MAJOR ? 1 : g.lda;
+        v.x = g.b;
+        v.incx = g.layout_b == JLC_ROW_MAJOR ? g.ldb : 1;
+        v.y = g.c;
+        v.incy = g.ldc;
+    } else {
+        // y^T = C(0,:) = A(0,:) * B  ->  y = B^T x with x = A(0,:)
+        v.rows = g.n;
+        v.cols = g.k;
+        v.mat = g.b;
+        v.rs = g.layout_b == JLC_ROW_MAJOR ? 1 : g.ldb;
+        v.cs = g.layout_b == JLC_ROW_MAJOR ? g.ldb : 1;
+        v.x = g.a;
+        v.incx = g.layout_a == JLC_ROW_MAJOR ? 1 : g.lda;
+        v.y = g.c;
+        v.incy = 1;
+    }
+    v.alpha = g.alpha;
+    v.beta = g.beta;
+    if (v.cs != 1 && v.rs != 1) {
+        // single row/column with both strides > 1 cannot happen for a
+        // matrix operand; k == 1 makes either stride irrelevant
+        if (v.cols == 1) v.cs = 1;
+        else if (v.rows == 1) v.rs = 1;
+    }
+    return v;
 }
+}  // namespace jlc
+
+namespace {
 
 bool use_ozaki(int precision, long long m, long long n, long long k) {
     if (precision == JLC_PREC_OZAKI || precision == JLC_PREC_OZAKI_CRT) return true;
@@ -138,11 +179,13 @@ bool use_ozaki(int precision, long long m, long long n, long long k) {
 // Device dispatch on already-validated device operands.
 int run_device(jlc_ctx* ctx, const GemmDesc& g0, int precision, int slices, jlc_report* rep) {
     GemmDesc g = g0;
+    ctx->cert_pending = false;
     if (rep) rep->precision = JLC_PREC_NATIVE;
     if (g.m == 0 || g.n == 0) {
         if (rep) rep->kernel = JLC_KERNEL_NONE;
         return JLC_OK;
     }
+    if (fault_hit(ctx, JLC_FAULT_LAUNCH)) return set_err(ctx, JLC_E_LAUNCH, "injected kernel launch failure");
     if (g.alpha == 0.0 || g.k == 0) {
         if (rep) rep->kernel = JLC_KERNEL_NONE;
         if (g.beta == 1.0) return JLC_OK;
@@ -152,41 +195,10 @@ int run_device(jlc_ctx* ctx, const GemmDesc& g0, int precision, int slices, jlc_
         return rc ? set_err(ctx, rc, "scale kernel launch failed") : JLC_OK;
     }
     if (g.n == 1 || g.m == 1) {
-        GemvDesc v;
-        if (g.n == 1) {
-            // y = C(:,0), rows of op(A) dotted with x = B(:,0)
-            v.rows = g.m;
-            v.cols = g.k;
-            v.mat = g.a;
-            v.rs = g.layout_a == JLC_ROW_MAJOR ? g.lda : 1;
-            v.cs = g.layout_a == JLC_ROW_MAJOR ? 1 : g.lda;
-            v.x = g.b;
-            v.incx = g.layout_b == JLC_ROW_MAJOR ? g.ldb : 1;
-            v.y = g.c;
-            v.incy = g.ldc;
-        } else {
-            // y^T = C(0,:) = A(0,:) * B  ->  y = B^T x with x = A(0,:)
-            v.rows = g.n;
-            v.cols = g.k;
-            v.mat = g.b;
-            v.rs = g.layout_b == JLC_ROW_MAJOR ? 1 : g.ldb;
-            v.cs = g.layout_b == JLC_ROW_MAJOR ? g.ldb : 1;
-            v.x = g.a;
-            v.incx = g.layout_a == JLC_ROW_MAJOR ? 1 : g.lda;
-            v.y = g.c;
-            v.incy = 1;
-        }
-        v.alpha = g.alpha;
-        v.beta = g.beta;
-        if (v.cs != 1 && v.rs != 1) {
-            // single row/column with both strides > 1 cannot happen for a
-            // matrix operand; k == 1 makes either stride irrelevant
-            if (v.cols == 1) v.cs = 1;
-            else if (v.rows == 1) v.rs = 1;
-        }
+        const GemvDesc v = gemv_desc(g);
         size_t need = gemv_scratch_bytes(v, ctx->sm_count);
         if (need) {
-            int rc = workspace_reserve(ctx->ws, need, ctx->err, sizeof(ctx->err));
+            int rc = ws_reserve(ctx, need);
             if (rc) return rc;
         }
         if (rep) rep->kernel = JLC_KERNEL_GEMV;
@@ -209,34 +221,62 @@ int run_device(jlc_ctx* ctx, const GemmDesc& g0, int precision, int slices, jlc_
     size_t splitk_off = 0;
     int rc = JLC_OK;
     if (ozaki) {
-        const int s = slices > 0 ? slices : (crt ? ozaki_crt_auto_moduli(g.k) : auto_slices(g.k));
-        size_t need = ozaki_workspace_bytes(whole_m, g.n, g.k, s, ctx->sm_count, crt);
+        // The higher count re-splits op(B): not for row blocks that share
+        // one split of it (they fall back to FP64 instead).
+        const OzakiPlan pl = ozaki_plan(g.k, crt, slices, whole_m == g.m);
+        size_t need = ozaki_workspace_bytes(whole_m, g.n, g.k, pl, ctx->sm_count);
         splitk_off = (need + 255) / 256 * 256;
         if (splitk_bytes) need = splitk_off + splitk_bytes;
-        rc = workspace_reserve(ctx->ws, need, ctx->err, sizeof(ctx->err));
+        rc = ws_reserve(ctx, need);
         if (rc) return rc;
+        void* ws = ctx->ws.ptr;
+        const size_t wsb = ctx->ws.bytes;
+        int nl = 0;
         {
             Phase ph(ctx, JLC_PHASE_OZAKI_SPLIT);
-            ctx->launches += (g.layout_a == JLC_ROW_MAJOR ? 1 : 2) + (g.layout_b == JLC_COL_MAJOR ? 1 : 2);
-            rc = launch_ozaki_split(g, s, ctx->ws.ptr, ctx->ws.bytes, ctx->stream, ctx->sm_count, ctx->d_flags,
-                                    ctx->err, sizeof(ctx->err), crt);
+            rc = launch_ozaki_split(g, pl, 0, ws, wsb, ctx->stream, ctx->sm_count, ctx->d_flags, ctx->err,
+                                    sizeof(ctx->err), &nl);
         }
-        if (rc) return rc;
-        {
+        if (!rc) {
+            Phase ph(ctx, JLC_PHASE_OZAKI_CERT);
+            nl += 1;
+            rc = launch_ozaki_cert(g, pl, ws, wsb, ctx->stream, ctx->sm_count, ctx->d_status, ctx->d_flags, ctx->err,
+                                   sizeof(ctx->err));
+        }
+        if (!rc) {
             Phase ph(ctx, JLC_PHASE_OZAKI_GEMM);
-            ctx->launches += 1;
-            rc = launch_ozaki_gemm(g, s, ctx->ws.ptr, ctx->ws.bytes, ctx->stream, ctx->sm_count, ctx->d_status,
-                                   ctx->d_flags, ctx->err, sizeof(ctx->err), crt);
+            nl += 1;
+            rc = launch_ozaki_gemm(g, pl, 0, ws, wsb, ctx->stream, ctx->sm_count, ctx->d_status, ctx->d_flags,
+                                   ctx->err, sizeof(ctx->err));
         }
+        if (!rc && pl.hi > 0) {
+            {
+                Phase ph(ctx, JLC_PHASE_OZAKI_SPLIT_HI);
+                rc = launch_ozaki_split(g, pl, 1, ws, wsb, ctx->stream, ctx->sm_count, ctx->d_flags, ctx->err,
+                                        sizeof(ctx->err), &nl);
+            }
+            if (!rc) {
+                Phase ph(ctx, JLC_PHASE_OZAKI_GEMM_HI);
+                nl += 1;
+                rc = launch_ozaki_gemm(g, pl, 1, ws, wsb, ctx->stream, ctx->sm_count, ctx->d_status, ctx->d_flags,
+                                       ctx->err, sizeof(ctx->err));
+            }
+        }
+        ctx->launches += nl;
         if (rc) return rc;
+        ctx->cert_rec = reinterpret_cast<CertRecord*>(static_cast<char*>(ws) +
+                                                      ozaki_cert_offset(whole_m, g.n, g.k, pl));
+        ctx->cert_plan = pl;
+        ctx->cert_pending = true;
         if (rep) {
+            // a-priori figures; replaced by the certificate's when the caller reads it
             rep->precision = crt ? JLC_PREC_OZAKI_CRT : JLC_PREC_OZAKI;
             rep->kernel = JLC_KERNEL_OZAKI;
-            rep->slices = s;
-            rep->products = crt ? s : s * (s + 1) / 2;
+            rep->slices = pl.lo;
+            rep->products = crt ? pl.lo : pl.lo * (pl.lo + 1) / 2;
             const double u = std::ldexp(1.0, -53);
-            rep->est_err_ratio = crt ? ozaki_crt_est_ratio(s, g.k)
-                                     : (s + 3) * std::ldexp(1.0, -7 * s) / (2.0 * u * (double)g.k / 16.0);
+            rep->est_err_ratio = crt ? ozaki_crt_est_ratio(pl.lo, g.k)
+                                     : (pl.lo + 3) * std::ldexp(1.0, -7 * pl.lo) / (2.0 * u * (double)g.k / 16.0);
         }
     }
     // the DMMA kernel reads A/B through TMA: 16-byte aligned bases, even lds
@@ -263,8 +303,9 @@ int run_device(jlc_ctx* ctx, const GemmDesc& g0, int precision, int slices, jlc_
         g.ldb = ld;
     }
     if (!ozaki && rep) rep->kernel = JLC_KERNEL_DMMA;
+    if (!ozaki && fault_hit(ctx, JLC_FAULT_WAIT)) g.withhold_stage = true;
     if (!ozaki && splitk_bytes > 0) {
-        rc = workspace_reserve(ctx->ws, splitk_bytes, ctx->err, sizeof(ctx->err));
+        rc = ws_reserve(ctx, splitk_bytes);
         if (rc) return rc;
     }
     // After an Ozaki launch the FP64 kernel is gated on the split's
@@ -287,6 +328,44 @@ int finish_sync(jlc_ctx* ctx) {
         if (st & JLC_DEV_TIMEOUT) return set_err(ctx, JLC_E_TIMEOUT, "a device wait timed out (status 0x%x)", st);
         return set_err(ctx, JLC_E_CUDA, "device status 0x%x", st);
     }
+    return JLC_OK;
+}
+
+// Fills rep from the certificate record of the Ozaki call just enqueued
+// (waits for the device).  Not while the stream is being captured: the
+// a-priori figures stay.
+int read_cert(jlc_ctx* ctx, jlc_report* rep) {
+    if (!ctx->cert_pending) return JLC_OK;
+    ctx->cert_pending = false;
+    if (!rep) return JLC_OK;
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(ctx->stream, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone)
+        return JLC_OK;
+    CertRecord r;
+    cudaError_t e = cudaMemcpyAsync(&r, ctx->cert_rec, sizeof(r), cudaMemcpyDeviceToHost, ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    if (e != cudaSuccess) return cuda_err(ctx, e, "certificate read");
+    const OzakiPlan& pl = ctx->cert_plan;
+    auto as_double = [](unsigned long long b) {
+        double d;
+        memcpy(&d, &b, 8);
+        return d;
+    };
+    if (r.blocks == 0 || r.fb_blocks == r.blocks) {
+        // Inf/NaN operands (no certificate) or every block certified only in FP64
+        rep->precision = JLC_PREC_NATIVE;
+        rep->kernel = JLC_KERNEL_DMMA;
+        rep->slices = 0;
+        rep->products = 0;
+        rep->est_err_ratio = r.blocks == 0 ? 0.0 : as_double(r.fb_est_bits);
+        return JLC_OK;
+    }
+    const int used = r.hi_blocks > 0 ? pl.hi : pl.lo;
+    rep->precision = pl.crt ? JLC_PREC_OZAKI_CRT : JLC_PREC_OZAKI;
+    rep->kernel = JLC_KERNEL_OZAKI;
+    rep->slices = used;
+    rep->products = pl.crt ? used : used * (used + 1) / 2;
+    rep->est_err_ratio = as_double(r.oz_est_bits);
     return JLC_OK;
 }
 
@@ -340,7 +419,7 @@ int run_host_pipelined(jlc_ctx* ctx, int la, int lb, long long m, long long n, l
     if (e != cudaSuccess) return cuda_err(ctx, e, "pipeline start");
     {
         Phase ph(ctx, JLC_PHASE_H2D, ci);
-        e = cudaMemcpy2DAsync(ctx->bufB.ptr, dldb * 8, b, ldb * 8, b_cols * 8, b_rows, cudaMemcpyHostToDevice, ci);
+        e = copy2d(ctx, ctx->bufB.ptr, dldb * 8, b, ldb * 8, b_cols * 8, b_rows, cudaMemcpyHostToDevice, ci);
     }
     if (e != cudaSuccess) {
         drain();
@@ -349,22 +428,31 @@ int run_host_pipelined(jlc_ctx* ctx, int la, int lb, long long m, long long n, l
     h2d += b_rows * b_cols * 8;
     double* dA = static_cast<double*>(ctx->bufA.ptr);
     double* dC = static_cast<double*>(ctx->bufC.ptr);
+    auto block_rows = [&](int i, long long& r0, long long& mr) {
+        r0 = (long long)i * rb;
+        mr = (m - r0 < rb) ? m - r0 : rb;
+    };
+    // Every block's inputs and GEMM are enqueued before any block's rows of C
+    // are: a call that fails while enqueueing leaves the caller's C as it was.
+    // (Enqueueing takes microseconds; block 0's GEMM is still running when its
+    // copy-out is queued, so the overlap is unchanged.)
     for (int i = 0; i < nb; ++i) {
-        const long long r0 = (long long)i * rb, mr = (m - r0 < rb) ? m - r0 : rb;
+        long long r0, mr;
+        block_rows(i, r0, mr);
         const double* blk_a;
         {
             Phase ph(ctx, JLC_PHASE_H2D, ci);
             if (la == JLC_ROW_MAJOR) {
-                e = cudaMemcpy2DAsync(dA + r0 * dlda, dlda * 8, a + r0 * lda, lda * 8, k * 8, mr,
-                                      cudaMemcpyHostToDevice, ci);
+                e = copy2d(ctx, dA + r0 * dlda, dlda * 8, a + r0 * lda, lda * 8, k * 8, mr, cudaMemcpyHostToDevice,
+                           ci);
                 blk_a = dA + r0 * dlda;
             } else {
-                e = cudaMemcpy2DAsync(dA + r0, dlda * 8, a + r0, lda * 8, mr * 8, k, cudaMemcpyHostToDevice, ci);
+                e = copy2d(ctx, dA + r0, dlda * 8, a + r0, lda * 8, mr * 8, k, cudaMemcpyHostToDevice, ci);
                 blk_a = dA + r0;
             }
             if (e == cudaSuccess && beta != 0.0)
-                e = cudaMemcpy2DAsync(dC + r0 * dldc, dldc * 8, c + r0 * ldc, ldc * 8, n * 8, mr,
-                                      cudaMemcpyHostToDevice, ci);
+                e = copy2d(ctx, dC + r0 * dldc, dldc * 8, c + r0 * ldc, ldc * 8, n * 8, mr, cudaMemcpyHostToDevice,
+                           ci);
         }
         if (e == cudaSuccess) e = cudaEventRecord(ctx->pev[i], ci);
         if (e == cudaSuccess) e = cudaStreamWaitEvent(cs, ctx->pev[i], 0);
@@ -383,11 +471,18 @@ int run_host_pipelined(jlc_ctx* ctx, int la, int lb, long long m, long long n, l
             return rc;
         }
         e = cudaEventRecord(ctx->pev[maxb + i], cs);
-        if (e == cudaSuccess) e = cudaStreamWaitEvent(co, ctx->pev[maxb + i], 0);
+        if (e != cudaSuccess) {
+            drain();
+            return cuda_err(ctx, e, "pipeline event");
+        }
+    }
+    for (int i = 0; i < nb; ++i) {
+        long long r0, mr;
+        block_rows(i, r0, mr);
+        e = cudaStreamWaitEvent(co, ctx->pev[maxb + i], 0);
         if (e == cudaSuccess) {
             Phase ph(ctx, JLC_PHASE_D2H, co);
-            e = cudaMemcpy2DAsync(c + r0 * ldc, ldc * 8, dC + r0 * dldc, dldc * 8, n * 8, mr,
-                                  cudaMemcpyDeviceToHost, co);
+            e = copy2d(ctx, c + r0 * ldc, ldc * 8, dC + r0 * dldc, dldc * 8, n * 8, mr, cudaMemcpyDeviceToHost, co);
         }
         if (e != cudaSuccess) {
             drain();
@@ -429,6 +524,7 @@ int run_host(jlc_ctx* ctx, int la, int lb, long long m, long long n, long long k
         if (rc) return rc;
         cudaEventRecord(ctx->ev1, ctx->stream);
         rc = finish_sync(ctx);
+        if (!rc) rc = read_cert(ctx, rep);
         if (rc) return rc;
         if (rep) {
             float ms = 0.f;
@@ -443,17 +539,17 @@ int run_host(jlc_ctx* ctx, int la, int lb, long long m, long long n, long long k
     {
     Phase ph(ctx, JLC_PHASE_H2D);
     if (need_ab) {
-        e = cudaMemcpy2DAsync(ctx->bufA.ptr, dlda * 8, a, lda * 8, a_cols * 8, a_rows, cudaMemcpyHostToDevice,
+        e = copy2d(ctx, ctx->bufA.ptr, dlda * 8, a, lda * 8, a_cols * 8, a_rows, cudaMemcpyHostToDevice,
                               ctx->stream);
-        if (e != cudaSuccess) return cuda_err(ctx, e, "copy A to device");
-        e = cudaMemcpy2DAsync(ctx->bufB.ptr, dldb * 8, b, ldb * 8, b_cols * 8, b_rows, cudaMemcpyHostToDevice,
+        if (e != cudaSuccess) return copy_failed(ctx, e, "copy A to device");
+        e = copy2d(ctx, ctx->bufB.ptr, dldb * 8, b, ldb * 8, b_cols * 8, b_rows, cudaMemcpyHostToDevice,
                               ctx->stream);
-        if (e != cudaSuccess) return cuda_err(ctx, e, "copy B to device");
+        if (e != cudaSuccess) return copy_failed(ctx, e, "copy B to device");
         h2d += (a_rows * a_cols + b_rows * b_cols) * 8;
     }
     if (beta != 0.0) {
-        e = cudaMemcpy2DAsync(ctx->bufC.ptr, dldc * 8, c, ldc * 8, n * 8, m, cudaMemcpyHostToDevice, ctx->stream);
-        if (e != cudaSuccess) return cuda_err(ctx, e, "copy C to device");
+        e = copy2d(ctx, ctx->bufC.ptr, dldc * 8, c, ldc * 8, n * 8, m, cudaMemcpyHostToDevice, ctx->stream);
+        if (e != cudaSuccess) return copy_failed(ctx, e, "copy C to device");
         h2d += m * n * 8;
     }
     }
@@ -466,12 +562,13 @@ int run_host(jlc_ctx* ctx, int la, int lb, long long m, long long n, long long k
     }
     {
         Phase ph(ctx, JLC_PHASE_D2H);
-        e = cudaMemcpy2DAsync(c, ldc * 8, ctx->bufC.ptr, dldc * 8, n * 8, m, cudaMemcpyDeviceToHost, ctx->stream);
+        e = copy2d(ctx, c, ldc * 8, ctx->bufC.ptr, dldc * 8, n * 8, m, cudaMemcpyDeviceToHost, ctx->stream);
     }
-    if (e != cudaSuccess) return cuda_err(ctx, e, "copy C to host");
+    if (e != cudaSuccess) return copy_failed(ctx, e, "copy C to host");
     d2h += m * n * 8;
     cudaEventRecord(ctx->ev1, ctx->stream);
     rc = finish_sync(ctx);
+    if (!rc) rc = read_cert(ctx, rep);
     if (rc) return rc;
     if (rep) {
         float ms = 0.f;
@@ -682,10 +779,10 @@ int jlc_init(int device, jlc_ctx** out) {
         if (v == 4 || v == 8 || v == 16) ctx->dmma_k = v;
     }
     bool ok = cudaStreamCreateWithFlags(&ctx->own_stream, cudaStreamNonBlocking) == cudaSuccess &&
-              cudaMalloc(&ctx->d_status, 2 * sizeof(int)) == cudaSuccess &&
+              cudaMalloc(&ctx->d_status, 4 * sizeof(int)) == cudaSuccess &&
               cudaMalloc(&ctx->d_flags, 4 * sizeof(int)) == cudaSuccess &&
               cudaEventCreate(&ctx->ev0) == cudaSuccess && cudaEventCreate(&ctx->ev1) == cudaSuccess;
-    if (ok) ok = cudaMemset(ctx->d_status, 0, 2 * sizeof(int)) == cudaSuccess &&
+    if (ok) ok = cudaMemset(ctx->d_status, 0, 4 * sizeof(int)) == cudaSuccess &&
                  cudaMemset(ctx->d_flags, 0, 4 * sizeof(int)) == cudaSuccess;
     if (!ok) {
         cudaGetLastError();
@@ -693,7 +790,38 @@ int jlc_init(int device, jlc_ctx** out) {
         return JLC_E_CUDA;
     }
     ctx->stream = ctx->own_stream;
+    // JLCGPU_FAULT=alloc|launch|copy|wait[:after] arms the failure test hook
+    if (const char* f = getenv("JLCGPU_FAULT")) {
+        static const char* names[] = {"none", "alloc", "launch", "copy", "wait"};
+        for (int kind = 1; kind <= 4; ++kind) {
+            const size_t len = strlen(names[kind]);
+            if (strncmp(f, names[kind], len) == 0 && (f[len] == 0 || f[len] == ':')) {
+                ctx->fault_kind = kind;
+                ctx->fault_after = f[len] == ':' ? atoi(f + len + 1) : 0;
+            }
+        }
+    }
     *out = ctx;
+    return JLC_OK;
+}
+
+int jlc_set_wait_limit(jlc_ctx* ctx, double seconds) {
+    if (!ctx) return JLC_E_ARG;
+    if (!(seconds >= 0.0) || seconds > 600.0) return set_err(ctx, JLC_E_ARG, "wait limit must be in [0, 600] s");
+    cudaSetDevice(ctx->device);
+    const unsigned long long ns = (unsigned long long)(seconds * 1e9);
+    // the limit sits beside the status bits (byte 8 of the status block)
+    cudaError_t e = cudaMemcpyAsync(ctx->d_status + 2, &ns, sizeof(ns), cudaMemcpyHostToDevice, ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    return e == cudaSuccess ? JLC_OK : cuda_err(ctx, e, "wait limit");
+}
+
+int jlc_inject_fault(jlc_ctx* ctx, int kind, int after) {
+    if (!ctx) return JLC_E_ARG;
+    if (kind < JLC_FAULT_NONE || kind > JLC_FAULT_WAIT || after < 0)
+        return set_err(ctx, JLC_E_ARG, "fault kind must be JLC_FAULT_* and after >= 0");
+    ctx->fault_kind = kind;
+    ctx->fault_after = after;
     return JLC_OK;
 }
 
@@ -815,7 +943,8 @@ int jlc_dgemm_device(jlc_ctx* ctx, int layout_a, int layout_b, int64_t m, int64_
     if (rc) return rc;
     cudaSetDevice(ctx->device);
     GemmDesc g{layout_a, layout_b, m, n, k, alpha, beta, a, lda, b, ldb, c, ldc};
-    return run_device(ctx, g, precision, 0, rep);
+    rc = run_device(ctx, g, precision, 0, rep);
+    return rc ? rc : read_cert(ctx, rep);
 }
 
 int jlc_dgemm_ozaki_crt_device(jlc_ctx* ctx, int layout_a, int layout_b, int64_t m, int64_t n, int64_t k,
@@ -827,7 +956,8 @@ int jlc_dgemm_ozaki_crt_device(jlc_ctx* ctx, int layout_a, int layout_b, int64_t
     if (moduli != 0 && (moduli < 2 || moduli > 15)) return set_err(ctx, JLC_E_ARG, "moduli must be 0 or in [2,15]");
     cudaSetDevice(ctx->device);
     GemmDesc g{layout_a, layout_b, m, n, k, alpha, beta, a, lda, b, ldb, c, ldc};
-    return run_device(ctx, g, JLC_PREC_OZAKI_CRT, moduli, rep);
+    rc = run_device(ctx, g, JLC_PREC_OZAKI_CRT, moduli, rep);
+    return rc ? rc : read_cert(ctx, rep);
 }
 
 int jlc_dgemm_ozaki_device(jlc_ctx* ctx, int layout_a, int layout_b, int64_t m, int64_t n, int64_t k,
@@ -839,7 +969,8 @@ int jlc_dgemm_ozaki_device(jlc_ctx* ctx, int layout_a, int layout_b, int64_t m, 
     if (slices != 0 && (slices < 3 || slices > 8)) return set_err(ctx, JLC_E_ARG, "slices must be 0 or in [3,8]");
     cudaSetDevice(ctx->device);
     GemmDesc g{layout_a, layout_b, m, n, k, alpha, beta, a, lda, b, ldb, c, ldc};
-    return run_device(ctx, g, JLC_PREC_OZAKI, slices, rep);
+    rc = run_device(ctx, g, JLC_PREC_OZAKI, slices, rep);
+    return rc ? rc : read_cert(ctx, rep);
 }
 
 int jlc_set_profiling(jlc_ctx* ctx, int on) {

@@ -72,7 +72,8 @@ struct Params {
     double* part;       // ksplit > 1: BM*BN partial sums per (tile, part)
     int* counters;      // ksplit > 1: arrivals per tile, zero at launch
     int* status;
-    const int* gate;  // when non-null the kernel runs only if gate[0] or gate[1] is set
+    const int* gate;  // when non-null the kernel runs only if an Ozaki call's flags ask for FP64
+    int withhold;     // test hook: CTA 0 leaves its first stage unloaded, so a bounded wait runs out
 };
 
 // Bounded wait used only while draining: ignores errors recorded by others
@@ -80,8 +81,9 @@ struct Params {
 __device__ __forceinline__ void drain_wait(uint64_t* bar, uint32_t parity, int* status) {
     const uint32_t b = smem_u32(bar);
     const uint64_t t0 = globaltimer_ns();
+    const uint64_t limit = wait_limit_ns(status);
     while (!mbar_try_wait(b, parity)) {
-        if (globaltimer_ns() - t0 > kWaitTimeoutNs) {
+        if (globaltimer_ns() - t0 > limit) {
             atomicOr(status, JLC_DEV_TIMEOUT);
             return;
         }
@@ -92,7 +94,7 @@ template <bool A_KMAJOR, bool B_KMAJOR, int MMA_K>
 __global__ void __launch_bounds__(THREADS, 1)
     dgemm_dmma_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB,
                       const Params p) {
-    if (p.gate != nullptr && (p.gate[0] | p.gate[1]) == 0) return;
+    if (p.gate != nullptr && (p.gate[kFlagNonfiniteA] | p.gate[kFlagFallback] | p.gate[kFlagNonfiniteB]) == 0) return;
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     char* smem = reinterpret_cast<char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
     uint64_t* full = reinterpret_cast<uint64_t*>(smem + STAGES * STAGE_BYTES);
@@ -130,6 +132,15 @@ __global__ void __launch_bounds__(THREADS, 1)
                     if (!mbar_wait(&empty[stage], phase ^ 1u, p.status)) {
                         ok = false;
                         break;
+                    }
+                    if (p.withhold && blockIdx.x == 0 && unit == 0 && kb == kb0) {
+                        // nothing is loaded into this stage and nothing arms it:
+                        // its consumers' wait runs out (no copy to drain here)
+                        if (++stage == STAGES) {
+                            stage = 0;
+                            phase ^= 1u;
+                        }
+                        continue;
                     }
                     char* sA = smem + stage * STAGE_BYTES;
                     char* sB = sA + A_STAGE;
@@ -237,7 +248,23 @@ __global__ void __launch_bounds__(THREADS, 1)
             }
         }
 
-        if (failed) break;
+        if (p.ksplit > 1) {
+            // The split-K exchange below meets on a named barrier, so the
+            // consumer warps agree first (an OR over all of them on barrier 2)
+            // and leave together when any one gave up on a wait.
+            uint32_t any;
+            asm volatile(
+                "{\n\t.reg .pred f;\n\t"
+                "setp.ne.u32 f, %1, 0;\n\t"
+                "bar.red.or.pred f, 2, %2, f;\n\t"
+                "selp.u32 %0, 1, 0, f;\n\t}"
+                : "=r"(any)
+                : "r"((uint32_t)failed), "n"(MMA_WARPS * 32)
+                : "memory");
+            if (any) break;
+        } else if (failed) {
+            break;
+        }
         const int tile = unit % p.num_tiles, part = unit / p.num_tiles;
         int tm, tn;
         tile_coords(tile, p.tiles_m, p.tiles_n, RASTER_GROUP, tm, tn);
@@ -423,6 +450,7 @@ int launch_dgemm_dmma(const GemmDesc& g, cudaStream_t st, int sm_count, int* sta
     p.k_blocks = (int)((g.k + BK - 1) / BK);
     p.status = status;
     p.gate = gate;
+    p.withhold = g.withhold_stage ? 1 : 0;
     p.ksplit = 1;
     p.part = nullptr;
     p.counters = nullptr;

@@ -15,7 +15,17 @@ namespace jlc {
 
 // A wait that has not completed after this many nanoseconds is treated as a
 // hang: the kernel records JLC_DEV_TIMEOUT in its status word and unwinds.
+// This is the default; a context can set its own limit.
 constexpr uint64_t kWaitTimeoutNs = 4000000000ull;
+
+// The status block every kernel receives (16 bytes, 8-byte aligned): int 0
+// holds the JLC_DEV_* bits, the 64-bit word at byte 8 the bounded waits'
+// limit in nanoseconds (0: kWaitTimeoutNs).  A wait reads the limit only
+// once it has not completed at the first try.
+__device__ __forceinline__ uint64_t wait_limit_ns(const int* status) {
+    const uint64_t v = *reinterpret_cast<const volatile uint64_t*>(status + 2);
+    return v ? v : kWaitTimeoutNs;
+}
 
 __device__ __forceinline__ uint64_t globaltimer_ns() {
     uint64_t t;
@@ -64,18 +74,19 @@ __device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity) {
 }
 
 // Bounded wait on the phase with the given parity.  Returns false (and sets
-// JLC_DEV_TIMEOUT in *status) if the phase does not complete within
-// kWaitTimeoutNs, or false without waiting further once another thread has
+// JLC_DEV_TIMEOUT in *status) if the phase does not complete within the
+// status block's limit, or false without waiting further once another thread has
 // already recorded an error in *status.
 __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int* status) {
     const uint32_t b = smem_u32(bar);
     if (mbar_try_wait(b, parity)) return true;
     const uint64_t t0 = globaltimer_ns();
+    const uint64_t limit = wait_limit_ns(status);
     for (uint32_t it = 1;; ++it) {
         if (mbar_try_wait(b, parity)) return true;
         if ((it & 255u) == 0u) {
             if (*(volatile int*)status != 0) return false;
-            if (globaltimer_ns() - t0 > kWaitTimeoutNs) {
+            if (globaltimer_ns() - t0 > limit) {
                 atomicOr(status, JLC_DEV_TIMEOUT);
                 return false;
             }

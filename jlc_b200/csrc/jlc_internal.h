@@ -41,6 +41,9 @@ struct GemmDesc {
     const double* dot_mat = nullptr;
     long long dot_ld = 0;
     double* dot_partials = nullptr;
+    // test hook (jlc_inject_fault, JLC_FAULT_WAIT): the FP64 kernel leaves one
+    // stage unloaded so that a bounded wait runs out
+    bool withhold_stage = false;
 };
 
 // number of CTAs the DMMA / Ozaki GEMM kernels launch for this shape (the
@@ -66,8 +69,9 @@ int make_tmap_3d(CUtensorMap* map, CUtensorMapDataType dt, int elem_bytes, void*
 bool dmma_operand_ok(const void* ptr, long long ld);
 
 // FP64 DMMA tiled GEMM.  A/B must be 16-byte aligned with even leading
-// dimensions.  gate != nullptr: the kernel only runs if gate[0] or gate[1] is
-// nonzero (the Ozaki split's non-finite flags for A and B).
+// dimensions.  gate != nullptr: the kernel only runs if one of the Ozaki
+// call's flags gate[kFlagNonfiniteA], gate[kFlagFallback],
+// gate[kFlagNonfiniteB] is set.
 // ksplit > 1 with splitk_ws of at least dmma_splitk_bytes(m, n, ksplit):
 // split-K over ksplit parts; otherwise every tile is one work unit.
 // blocked Householder QR kernels (qr.cu)
@@ -98,27 +102,71 @@ struct GemvDesc {
     long long incy;
 };
 size_t gemv_scratch_bytes(const GemvDesc& g, int sm_count);
+// the matrix-vector form of a GEMM with n == 1 or m == 1
+GemvDesc gemv_desc(const GemmDesc& g);
 int launch_gemv(const GemvDesc& g, void* scratch, cudaStream_t st, int sm_count, char* err, size_t errlen);
 
 // C <- beta * C on the m x n window (beta == 0 writes zeros without reading).
 int launch_scale_c(double* c, long long ldc, long long m, long long n, double beta, cudaStream_t st);
 
-// Ozaki split-precision GEMM (INT8 on tcgen05, FP64 recombination).  count
-// is the slice count s (slice scheme) or the number of moduli N (residue
-// scheme, crt = true).
-size_t ozaki_workspace_bytes(long long m, long long n, long long k, int count, int sm_count, bool crt = false);
+// Control words of an Ozaki call (the context's d_flags, at least
+// kFlagWords ints): non-finite operands found by the split, the
+// certificate's FP64 fallback and its route (0: the call's count, 1: the
+// higher count, 2: FP64).  The FP64 kernel behind the call runs when
+// flags[kFlagNonfiniteA], flags[kFlagFallback] or flags[kFlagNonfiniteB] is set.
+constexpr int kFlagNonfiniteA = 0;
+constexpr int kFlagFallback = 1;
+constexpr int kFlagRoute = 2;
+constexpr int kFlagNonfiniteB = 3;
+constexpr int kFlagWords = 4;
+
+// Device record of the Ozaki accuracy certificate (in the Ozaki workspace).
+// The first kCertLaunchBytes are per certificate launch; the rest sums the
+// row blocks of one product (reset when op(B) is split).
+struct CertRecord {
+    unsigned int xbits, ybits, zbits;  // max ||b_j||/lb, ||a_i||/lb, 1/lb as float bits
+    unsigned int arrived;              // CTAs that have added their maxima
+    double est_lo, est_hi;             // certified error / bound at the two counts
+    int route, pad0, pad1, pad2;
+    unsigned long long oz_est_bits;    // max certified ratio of blocks that ran on INT8
+    unsigned long long fb_est_bits;    // max ratio of blocks that fell back to FP64
+    int blocks, hi_blocks, fb_blocks, pad3;
+};
+constexpr size_t kCertLaunchBytes = 48;
+
+// Ozaki split-precision GEMM (INT8 on tcgen05, FP64 recombination).  A plan
+// holds the scheme, the count the call runs with (lo: slices s or moduli N)
+// and, for an automatic count, a higher count the certificate may switch to
+// (hi, 0 = none).  A call runs: split at lo (with the certificate's
+// magnitude plane and row/column norms), the certificate, the GEMM at lo
+// (gated on route 0), the split and GEMM at hi (gated on route 1), and the
+// caller's FP64 kernel gated on the flags.
+struct OzakiPlan {
+    bool crt = true;
+    bool gate = true;  // automatic count: the certificate picks the route
+    int lo = 0, hi = 0;
+};
+int auto_slices(long long k);
 int ozaki_crt_auto_moduli(long long k);
+double ozaki_crt_est_ratio(int nmod, long long k);
+// whether the automatic count can reach the FP64 bound at all for this k
+// (very short products cannot: they run in FP64)
+bool ozaki_reaches_bound(long long k, bool crt);
+// count = 0: automatic; allow_hi: the certificate may switch to the higher
+// count (not for row blocks that share one split of op(B))
+OzakiPlan ozaki_plan(long long k, bool crt, int count, bool allow_hi);
+size_t ozaki_workspace_bytes(long long m, long long n, long long k, const OzakiPlan& pl, int sm_count);
+size_t ozaki_cert_offset(long long m, long long n, long long k, const OzakiPlan& pl);
 // operand scales p (rows of op(A)) and q (columns of op(B)) of the residue scheme
 void ozaki_crt_pq(int nmod, long long k, int* p, int* q);
-double ozaki_crt_est_ratio(int nmod, long long k);
-// Phase 1: exponents + INT8 slices / residues of op(A) and op(B) into the
-// workspace; sets flags[0] when an operand holds Inf/NaN.  Phase 2: the
-// tcgen05 GEMM with FP64 recombination into C (skipped on the device when
-// flags[0] is set).
-int launch_ozaki_split(const GemmDesc& g, int count, void* workspace, size_t ws_bytes, cudaStream_t st,
-                       int sm_count, int* flags, char* err, size_t errlen, bool crt = false);
-int launch_ozaki_gemm(const GemmDesc& g, int count, void* workspace, size_t ws_bytes, cudaStream_t st,
-                      int sm_count, int* status, int* flags, char* err, size_t errlen, bool crt = false);
+// level 0: split at lo (resets the flags and the certificate record);
+// level 1: split at hi, run on the device only when the route is 1
+int launch_ozaki_split(const GemmDesc& g, const OzakiPlan& pl, int level, void* workspace, size_t ws_bytes,
+                       cudaStream_t st, int sm_count, int* flags, char* err, size_t errlen, int* launches);
+int launch_ozaki_cert(const GemmDesc& g, const OzakiPlan& pl, void* workspace, size_t ws_bytes, cudaStream_t st,
+                      int sm_count, int* status, int* flags, char* err, size_t errlen);
+int launch_ozaki_gemm(const GemmDesc& g, const OzakiPlan& pl, int level, void* workspace, size_t ws_bytes,
+                      cudaStream_t st, int sm_count, int* status, int* flags, char* err, size_t errlen);
 
 // double-double accuracy check of sampled entries (verify.cu); d_out3 holds
 // [max ratio bits, max abs error bits, entries over the bound], zeroed by the caller
@@ -153,8 +201,8 @@ struct jlc_ctx {
     int sm_count = 0;
     cudaStream_t own_stream = nullptr;
     cudaStream_t stream = nullptr;
-    int* d_status = nullptr;  // status word written by kernels (JLC_DEV_* bits)
-    int* d_flags = nullptr;   // control flags (e.g. the Ozaki non-finite gate)
+    int* d_status = nullptr;  // status block: JLC_DEV_* bits written by kernels, wait limit at byte 8
+    int* d_flags = nullptr;   // control words of an Ozaki call (kFlag*)
     DevBuf bufA, bufB, bufC;
     DevBuf bufR;  // reduction partials (adjoint)
     DevBuf bufQ;  // blocked QR: V, G, T and the two W panels
@@ -174,7 +222,27 @@ struct jlc_ctx {
     int rec_phase[kMaxRec];
     cudaEvent_t rec_ev[2 * kMaxRec] = {};
     int64_t launches = 0;
+    // test hook (jlc_inject_fault): fail the next `fault_after + 1`-th
+    // operation of kind fault_kind once
+    int fault_kind = 0;
+    int fault_after = 0;
+    // the last Ozaki call's certificate record (read back when a report asks)
+    bool cert_pending = false;
+    jlc::CertRecord* cert_rec = nullptr;
+    jlc::OzakiPlan cert_plan;
     char err[512] = {0};
 };
+
+// The test hook of jlc_inject_fault: true once, for the operation of `kind`
+// that the countdown reaches.
+inline bool fault_hit(jlc_ctx* ctx, int kind) {
+    if (!ctx || ctx->fault_kind != kind) return false;
+    if (ctx->fault_after > 0) {
+        --ctx->fault_after;
+        return false;
+    }
+    ctx->fault_kind = JLC_FAULT_NONE;
+    return true;
+}
 
 

@@ -143,8 +143,9 @@ __device__ __forceinline__ void umma_commit_pair(uint64_t* bar) {
 __device__ __forceinline__ void drain_wait(uint64_t* bar, uint32_t parity, int* status) {
     const uint32_t b = smem_u32(bar);
     const uint64_t t0 = globaltimer_ns();
+    const uint64_t limit = wait_limit_ns(status);
     while (!mbar_try_wait(b, parity)) {
-        if (globaltimer_ns() - t0 > kWaitTimeoutNs) {
+        if (globaltimer_ns() - t0 > limit) {
             atomicOr(status, JLC_DEV_TIMEOUT);
             return;
         }

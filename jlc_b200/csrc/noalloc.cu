@@ -19,11 +19,16 @@
 // before any stream capture begins.
 //
 // All calls on a device share the array and it keeps the previous call's
-// contents: the parts that must start at zero (status word, non-finite flag,
-// column-max words) are cleared by every call, everything else is fully
-// rewritten before it is read.  Calls whose work overlaps on the GPU (two
-// streams, or two host threads) race on the array and must be serialised by
-// the caller.
+// contents: the parts that must start at zero (status word, control flags,
+// the accuracy certificate's record, column-max words and norms) are cleared
+// by every call, everything else is fully rewritten before it is read.  Calls
+// whose work overlaps on the GPU (two streams, or two host threads) race on
+// the array and must be serialised by the caller.
+//
+// The cached address belongs to the device's primary context, the one the
+// runtime API uses: a caller that makes another driver context current on
+// the device, or resets the device, must not call this entry afterwards in
+// the same process.
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -35,7 +40,9 @@ namespace jlc {
 namespace {
 
 constexpr size_t kStaticScratchBytes = size_t(64) << 20;
-constexpr size_t kHeadBytes = 256;  // [0] status word, [1] non-finite flag
+// the array's head: the status block (int 0: JLC_DEV_* bits, 64-bit word at
+// byte 8: the wait limit, 0 = default) and, from int 4, the control flags
+constexpr size_t kHeadBytes = 256;
 
 __device__ __align__(256) unsigned char g_static_scratch[kStaticScratchBytes];
 
@@ -115,10 +122,10 @@ int jlc_dgemm_ozaki_static(int layout_a, int layout_b, int64_t m, int64_t n, int
     int sms = 0;
     int rc = static_scratch(dev, &base, &sms, err, errlen);
     if (rc) return rc;
-    // kernels report bounded-wait timeouts into the caller's status word when
-    // one is given, else into the head of the static array
-    int* status = dev_status ? dev_status : static_cast<int*>(base);
-    int* flags = static_cast<int*>(base) + 1;
+    int* status = static_cast<int*>(base);
+    int* flags = static_cast<int*>(base) + 4;
+    void* ws = static_cast<char*>(base) + kHeadBytes;
+    const size_t avail = kStaticScratchBytes - kHeadBytes;
     if (alpha == 0.0 || k == 0) {
         rc = launch_scale_c(c, ldc, m, n, beta, st);
         if (rc) snprintf(err, errlen, "scale kernel launch failed");
@@ -129,47 +136,63 @@ int jlc_dgemm_ozaki_static(int layout_a, int layout_b, int64_t m, int64_t n, int
         snprintf(err, errlen, "A/B must not be null and their leading dimensions must cover the shape");
         return JLC_E_ARG;
     }
-    // the FP64 kernel that takes over for Inf/NaN inputs reads A/B by TMA
-    // and this entry has no buffer to repack them into
-    if (!dmma_operand_ok(a, lda) || !dmma_operand_ok(b, ldb)) {
-        snprintf(err, errlen, "A and B need 16-byte aligned bases and even leading dimensions");
-        return JLC_E_UNSUPPORTED;
-    }
     if (m > INT32_MAX / 2 || n > INT32_MAX / 2 || k > INT32_MAX / 2) {
         snprintf(err, errlen, "dimension above 2^30");
         return JLC_E_UNSUPPORTED;
     }
-    int s = slices;
-    if (s == 0) {
-        const double u = 0x1.0p-53;
-        s = 8;
-        for (int t = 5; t <= 8; ++t)
-            if ((t + 3) * ldexp(1.0, -7 * t) <= 2.0 * u * (double)k / 16.0) {
-                s = t;
-                break;
-            }
+    GemmDesc g{layout_a, layout_b, m, n, k, alpha, beta, a, lda, b, ldb, c, ldc};
+    // A single row or column of C is a matrix-vector product, as in the
+    // regular entry (its partial sums live in the array).
+    if (m == 1 || n == 1) {
+        const GemvDesc v = gemv_desc(g);
+        if (gemv_scratch_bytes(v, sms) > avail) {
+            snprintf(err, errlen, "matrix-vector partial sums exceed the %zu-byte static scratch", avail);
+            return JLC_E_ARG;
+        }
+        return launch_gemv(v, ws, st, sms, err, errlen);
     }
-    // Fit the per-CTA FP64 tiles into what the slices leave: fewer persistent
-    // CTAs when the array is tight (each CTA still covers all its tiles).
-    void* ws = static_cast<char*>(base) + kHeadBytes;
-    const size_t avail = kStaticScratchBytes - kHeadBytes;
-    int grid_cap = sms;
-    while (grid_cap > 0 && ozaki_workspace_bytes(m, n, k, s, grid_cap) > avail) grid_cap /= 2;
-    if (grid_cap < 1 || ozaki_workspace_bytes(m, n, k, s, grid_cap) > avail) {
-        snprintf(err, errlen,
-                 "problem too large for the %zu-byte static scratch (needs %zu bytes at one CTA; "
-                 "s*(m+n)*roundup(k,16) INT8 slice bytes dominate)",
-                 avail, ozaki_workspace_bytes(m, n, k, s, 1));
-        return JLC_E_ARG;
+    // the FP64 kernel (the route for short products, and the fallback for
+    // Inf/NaN inputs or a failed certificate) reads A/B by TMA and this
+    // entry has no buffer to repack them into
+    if (!dmma_operand_ok(a, lda) || !dmma_operand_ok(b, ldb)) {
+        snprintf(err, errlen, "A and B need 16-byte aligned bases and even leading dimensions");
+        return JLC_E_UNSUPPORTED;
     }
-    if (cudaMemsetAsync(status, 0, sizeof(int), st) != cudaSuccess) {
+    // the status bits and the wait limit (default) start at zero each call
+    if (cudaMemsetAsync(status, 0, 16, st) != cudaSuccess) {
         snprintf(err, errlen, "status reset failed");
         return JLC_E_CUDA;
     }
-    GemmDesc g{layout_a, layout_b, m, n, k, alpha, beta, a, lda, b, ldb, c, ldc};
-    rc = launch_ozaki_split(g, s, ws, avail, st, grid_cap, flags, err, errlen);
-    if (!rc) rc = launch_ozaki_gemm(g, s, ws, avail, st, grid_cap, status, flags, err, errlen);
-    if (!rc) rc = launch_dgemm_dmma(g, st, sms, status, flags, 8, err, errlen);
+    // Products too short for any slice count to reach the FP64 bound run in
+    // FP64, as in the regular entry (one work unit per tile: no scratch).
+    if (slices == 0 && !ozaki_reaches_bound(k, false)) {
+        rc = launch_dgemm_dmma(g, st, sms, status, nullptr, 8, err, errlen);
+    } else {
+        const OzakiPlan pl = ozaki_plan(k, false, slices, true);
+        // Fit the per-CTA scratch into what the slices leave: fewer persistent
+        // CTAs when the array is tight (each CTA still covers all its tiles).
+        int grid_cap = sms;
+        while (grid_cap > 0 && ozaki_workspace_bytes(m, n, k, pl, grid_cap) > avail) grid_cap /= 2;
+        if (grid_cap < 1 || ozaki_workspace_bytes(m, n, k, pl, grid_cap) > avail) {
+            snprintf(err, errlen,
+                     "problem too large for the %zu-byte static scratch (needs %zu bytes at one CTA; "
+                     "(s+1)*(m+n)*roundup(k,16) INT8 slice bytes dominate)",
+                     avail, ozaki_workspace_bytes(m, n, k, pl, 1));
+            return JLC_E_ARG;
+        }
+        int nl = 0;
+        rc = launch_ozaki_split(g, pl, 0, ws, avail, st, grid_cap, flags, err, errlen, &nl);
+        if (!rc) rc = launch_ozaki_cert(g, pl, ws, avail, st, grid_cap, status, flags, err, errlen);
+        if (!rc) rc = launch_ozaki_gemm(g, pl, 0, ws, avail, st, grid_cap, status, flags, err, errlen);
+        if (!rc) rc = launch_ozaki_split(g, pl, 1, ws, avail, st, grid_cap, flags, err, errlen, &nl);
+        if (!rc) rc = launch_ozaki_gemm(g, pl, 1, ws, avail, st, grid_cap, status, flags, err, errlen);
+        if (!rc) rc = launch_dgemm_dmma(g, st, sms, status, flags, 8, err, errlen);
+    }
+    // the caller's status word receives this call's JLC_DEV_* bits
+    if (!rc && dev_status && cudaMemcpyAsync(dev_status, status, sizeof(int), cudaMemcpyDeviceToDevice, st) != cudaSuccess) {
+        snprintf(err, errlen, "status copy failed");
+        rc = JLC_E_CUDA;
+    }
     return rc;
 }
 

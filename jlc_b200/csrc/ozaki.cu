@@ -102,6 +102,23 @@ using res::pow2_split;
 // three 41-bit digits (value = d0*2^82 + d1*2^41 + d2).
 using CrtConsts = crt::Consts;
 
+// What the kernel computes (template parameter MODE).
+constexpr int kModeSlices = 0;  // slice pairs, FP64 recombination
+constexpr int kModeCrt = 1;     // residues, exact CRT reconstruction
+constexpr int kModeCert = 2;    // accuracy certificate: one product of the magnitude planes
+
+// Route decision of the certificate (kModeCert), made by the CTA that
+// finishes last.  For a level (slice or modulus count) the certified ratio is
+//     est = c[0] * X + c[1] * Y + c[2] * Z + margin
+// with X = max_ij ||b_j||_1 / lb_ij, Y = max_ij ||a_i||_1 / lb_ij,
+// Z = max_ij 1 / lb_ij over the scaled operands (lb: the magnitude product).
+struct CertDecision {
+    double c_lo[3], c_hi[3];
+    double margin;
+    int have_hi;  // a higher level exists and may be chosen
+    int gate;     // 0: the count was given by the caller; report only
+};
+
 struct Params {
     int M, N, K, KB, s;
     int tiles_m, tiles_n, num_tiles;  // pair tiles (PM x BN)
@@ -111,13 +128,20 @@ struct Params {
     double* C;
     long long ldc;
     double* scratch;
+    long long scratch_stride;  // bytes of scratch per CTA
     int* status;
-    const int* nonfinite;
+    int* flags;       // kFlag* words (non-finite operands, fallback, route)
+    int route_want;   // run only when flags[kFlagRoute] equals it (-1: always)
     double epi_scale;
     const double* dot_mat;
     long long dot_ld;
     double* dot_partials;
     CrtConsts crt;  // residue scheme only (by value: read from the constant bank)
+    // certificate only
+    const double* l1a;  // ||a_i||_1 of the scaled rows of op(A)
+    const double* l1b;  // ||b_j||_1 of the scaled columns of op(B)
+    CertRecord* cert;
+    CertDecision dec;
 };
 
 // Instruction descriptor: kind::i8, D = S32, A = B = signed INT8, both K-major, 256 x 256 (pair).
@@ -127,15 +151,20 @@ constexpr uint32_t kIdescI8 = make_idesc(2u, 1u, PM, BN);
 // "diagonals"; diagonal di holds npairs(di) slice pairs whose INT8 products
 // accumulate into one INT32 accumulator (split into runs of at most cap
 // k-blocks).  Slice scheme: diagonals d = s-1 .. 0, pairs (t, d-t).
-// Residue scheme: diagonal l = modulus l, one pair (l, l).
-template <bool CRT>
+// Residue scheme: diagonal l = modulus l, one pair (l, l).  Certificate: one
+// diagonal, the magnitude planes (plane index `plane` of both operands).
+template <int MODE>
 struct Runs {
-    int ndiag, KB;
-    __device__ __forceinline__ int diag(int di) const { return CRT ? di : ndiag - 1 - di; }
-    __device__ __forceinline__ int npairs(int d) const { return CRT ? 1 : d + 1; }
-    __device__ __forceinline__ int slice_a(int d, int pr) const { return CRT ? d : pr; }
-    __device__ __forceinline__ int slice_b(int d, int pr) const { return CRT ? d : d - pr; }
-    static constexpr int cap = CRT ? GROUP_CAP_CRT : GROUP_CAP;
+    int ndiag, KB, plane;
+    __device__ __forceinline__ int diag(int di) const { return MODE == kModeSlices ? ndiag - 1 - di : di; }
+    __device__ __forceinline__ int npairs(int d) const { return MODE == kModeSlices ? d + 1 : 1; }
+    __device__ __forceinline__ int slice_a(int d, int pr) const {
+        return MODE == kModeSlices ? pr : (MODE == kModeCrt ? d : plane);
+    }
+    __device__ __forceinline__ int slice_b(int d, int pr) const {
+        return MODE == kModeSlices ? d - pr : (MODE == kModeCrt ? d : plane);
+    }
+    static constexpr int cap = MODE == kModeSlices ? GROUP_CAP : GROUP_CAP_CRT;
 };
 
 // v * 2^s for an integer-valued v: one exact multiply while 2^s is a normal
@@ -145,12 +174,45 @@ __device__ __forceinline__ double scale_pow2(double v, int s) {
     return ldexp(v, s);
 }
 
-template <bool CRT>
+// Route decision from the certificate's maxima (one thread, after every CTA
+// has added its maxima): level 0 when its certified ratio is at most 1, else
+// level 1 when it exists and is, else FP64 (the fallback flag gates the FP64
+// kernel behind the call).  Also folds the block into the product's totals.
+__device__ __forceinline__ void cert_decide(const Params& p) {
+    CertRecord* r = p.cert;
+    const double X = (double)__uint_as_float(atomicOr(&r->xbits, 0u));
+    const double Y = (double)__uint_as_float(atomicOr(&r->ybits, 0u));
+    const double Z = (double)__uint_as_float(atomicOr(&r->zbits, 0u));
+    const CertDecision& d = p.dec;
+    const double est_lo = d.c_lo[0] * X + d.c_lo[1] * Y + d.c_lo[2] * Z + d.margin;
+    const double est_hi = d.have_hi ? d.c_hi[0] * X + d.c_hi[1] * Y + d.c_hi[2] * Z + d.margin : est_lo;
+    int route = 0;
+    if (d.gate) route = est_lo <= 1.0 ? 0 : ((d.have_hi && est_hi <= 1.0) ? 1 : 2);
+    r->est_lo = est_lo;
+    r->est_hi = est_hi;
+    r->route = route;
+    p.flags[kFlagRoute] = route;
+    if (route == 2) p.flags[kFlagFallback] = 1;
+    atomicAdd(&r->blocks, 1);
+    if (route == 1) atomicAdd(&r->hi_blocks, 1);
+    if (route == 2) {
+        atomicAdd(&r->fb_blocks, 1);
+        atomicMax(&r->fb_est_bits, (unsigned long long)__double_as_longlong(est_hi));
+    } else {
+        atomicMax(&r->oz_est_bits, (unsigned long long)__double_as_longlong(route == 1 ? est_hi : est_lo));
+    }
+    __threadfence();
+}
+
+template <int MODE>
 __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(THREADS, 1)
     ozaki_gemm_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB,
                       const Params p) {
+    constexpr bool CRT = MODE == kModeCrt;
+    constexpr bool CERT = MODE == kModeCert;
     // both CTAs of a pair read the same flags, so both leave here or neither
-    if ((p.nonfinite[0] | p.nonfinite[1]) != 0) return;
+    if ((p.flags[kFlagNonfiniteA] | p.flags[kFlagNonfiniteB]) != 0) return;
+    if (p.route_want >= 0 && p.flags[kFlagRoute] != p.route_want) return;
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     char* smem = reinterpret_cast<char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
     uint64_t* full = reinterpret_cast<uint64_t*>(smem + STAGES * STAGE_BYTES);
@@ -160,7 +222,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(THREADS, 1)
     uint64_t* mma_done = acc_empty + 2;
     uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(mma_done + 1);
     double* red = reinterpret_cast<double*>(mma_done + 2);  // EPI_WARPS partial dots
-    const Runs<CRT> runs{p.s, p.KB};
+    const Runs<MODE> runs{CERT ? 1 : p.s, p.KB, p.s};
 
     const int warp = warp_id(), lane = lane_id();
     // Pair protocol.  full[s] of the leader (rank 0) collects both CTAs' TMA
@@ -250,8 +312,8 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(THREADS, 1)
             for (int tile = cluster; tile < p.num_tiles && ok; tile += nclusters) {
                 for (int di = 0; di < runs.ndiag && ok; ++di) {
                     const int nblk = runs.npairs(runs.diag(di)) * p.KB;
-                    for (int g0 = 0; g0 < nblk && ok; g0 += Runs<CRT>::cap) {
-                        const int g1 = min(nblk, g0 + Runs<CRT>::cap);
+                    for (int g0 = 0; g0 < nblk && ok; g0 += Runs<MODE>::cap) {
+                        const int g1 = min(nblk, g0 + Runs<MODE>::cap);
                         const uint32_t buf = gcount & 1u, accphase = (gcount >> 1) & 1u;
                         if (!mbar_wait(&acc_empty[buf], accphase ^ 1u, p.status)) {
                             ok = false;
@@ -374,7 +436,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(THREADS, 1)
         bool pend_row_ok = false;
         const uint32_t* pend_slots = crt_base;
         int local_tile = 0;
-        const int runs_per_tile = CRT ? p.crt.nmod * ((p.KB + Runs<CRT>::cap - 1) / Runs<CRT>::cap) : 1;
+        const int runs_per_tile = CRT ? p.crt.nmod * ((p.KB + Runs<MODE>::cap - 1) / Runs<MODE>::cap) : 1;
         const int per_run = (RECON_GROUPS + runs_per_tile - 1) / runs_per_tile;
         // Reconstruction of groups [g0, g1) of the pending tile, software
         // pipelined: the next group's residue words and column exponents are
@@ -415,6 +477,8 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(THREADS, 1)
         };
         uint32_t gcount = 0;
         bool ok = true;
+        // certificate: this thread's maxima of ||b_j|| / lb, ||a_i|| / lb, 1 / lb
+        float cx = 0.f, cy = 0.f, cz = 0.f;
         const uint32_t acc_empty_leader = mapa_shared(smem_u32(acc_empty), 0);
         for (int tile = cluster; tile < p.num_tiles && ok; tile += nclusters) {
             int tm, tn;
@@ -422,14 +486,17 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(THREADS, 1)
             const int m0 = tm * PM + (int)rank * BM, n0 = tn * BN;
             const int grow = m0 + row;
             const bool row_ok = grow < p.M;
-            const int ei = row_ok ? p.ea[grow] : 0;
+            const int ei = (row_ok && !CERT) ? p.ea[grow] : 0;
+            // certificate: ||a_i||_1 rounded up (0 for a zero row, whose products are exact)
+            const float arow = (CERT && row_ok) ? __double2float_ru(p.l1a[grow]) : 0.f;
+            float tz = 0.f;  // max 1 / lb over this row's columns of the tile
             // residue scheme: tiles alternate between two slot banks, so a finished
             // tile's residues stay intact while the next tile writes its own
             uint32_t* tile_slots = crt_base + (size_t)(local_tile & 1) * MAX_MODULI * CRT_SLOT_WORDS;
             for (int di = 0; di < runs.ndiag && ok; ++di) {
                 const int d = runs.diag(di);
                 const int nblk = runs.npairs(d) * p.KB;
-                const int ngroups = (nblk + Runs<CRT>::cap - 1) / Runs<CRT>::cap;
+                const int ngroups = (nblk + Runs<MODE>::cap - 1) / Runs<MODE>::cap;
                 for (int gi = 0; gi < ngroups; ++gi) {
                     const uint32_t buf = gcount & 1u, accphase = (gcount >> 1) & 1u;
                     if (!mbar_wait(&acc_full[buf], accphase, p.status)) {
@@ -445,7 +512,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(THREADS, 1)
                         uint32_t r[32];
                         tmem_ld32(taddr + ch * 32, r);
                         tmem_wait_ld();
-                        if constexpr (!CRT) {
+                        if constexpr (MODE == kModeSlices) {
                             double out[32];
                             // FP64 running sums, laid out [col/2][row][2] so a warp's
                             // 16-byte accesses for one column pair are contiguous
@@ -483,6 +550,37 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(THREADS, 1)
                                 out[2 * j + 1] = col0 + 1 < p.N ? ldexp(v.y, ei + p.eb[col0 + 1] - 14) : 0.0;
                             }
                             write_out(grow, n0, c0, out);
+                        } else if constexpr (CERT) {
+                            // lb = the magnitude product, a lower bound of (|A||B|)_ij
+                            // in units of 2^-14 of the scaled operands: converted and
+                            // summed over runs rounding down, so it stays a lower bound
+                            float* fs = reinterpret_cast<float*>(reinterpret_cast<char*>(p.scratch) +
+                                                                 (size_t)blockIdx.x * p.scratch_stride) +
+                                        (size_t)c0 * BM + row;
+                            float lb[32];
+#pragma unroll
+                            for (int j = 0; j < 32; ++j) lb[j] = __uint2float_rz(r[j]);
+                            if (gi > 0) {
+#pragma unroll
+                                for (int j = 0; j < 32; ++j) lb[j] = __fadd_rd(lb[j], fs[(size_t)j * BM]);
+                            }
+                            if (!last) {
+#pragma unroll
+                                for (int j = 0; j < 32; ++j) fs[(size_t)j * BM] = lb[j];
+                                continue;
+                            }
+                            if (!(arow > 0.f)) continue;
+#pragma unroll
+                            for (int j = 0; j < 32; ++j) {
+                                const int col = n0 + c0 + j;
+                                const float bj = col < p.N ? __double2float_ru(p.l1b[col]) : 0.f;
+                                if (bj > 0.f) {
+                                    // lb == 0 with both norms non-zero: nothing certifies this entry
+                                    const float rinv = lb[j] > 0.f ? __frcp_ru(lb[j]) : __int_as_float(0x7f800000);
+                                    tz = fmaxf(tz, rinv);
+                                    cx = fmaxf(cx, __fmul_ru(bj, rinv));
+                                }
+                            }
                         } else {
                             // residues: reduce this run mod m_d (adding the earlier
                             // runs of the same modulus), one byte per element in
@@ -540,10 +638,38 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(THREADS, 1)
                     }
                 }
             }
+            if constexpr (CERT) {
+                cy = fmaxf(cy, __fmul_ru(arow, tz));
+                cz = fmaxf(cz, tz);
+            }
             ++local_tile;
         }
         if constexpr (CRT) {
             if (ok) recon_range(RECON_GROUPS - pend_left, RECON_GROUPS);
+        }
+        if constexpr (CERT) {
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                cx = fmaxf(cx, __shfl_xor_sync(0xffffffffu, cx, o));
+                cy = fmaxf(cy, __shfl_xor_sync(0xffffffffu, cy, o));
+                cz = fmaxf(cz, __shfl_xor_sync(0xffffffffu, cz, o));
+            }
+            // non-negative floats order like their bit patterns (+Inf included)
+            if (lane == 0) {
+                atomicMax(&p.cert->xbits, __float_as_uint(cx));
+                atomicMax(&p.cert->ybits, __float_as_uint(cy));
+                atomicMax(&p.cert->zbits, __float_as_uint(cz));
+                __threadfence();
+            }
+            asm volatile("bar.sync 1, %0;" ::"n"(EPI_WARPS * 32) : "memory");
+            // the CTA that arrives last (no CTA waits for another) decides the route
+            if (warp == 2 && lane == 0) {
+                __threadfence();
+                if (atomicAdd(&p.cert->arrived, 1u) == gridDim.x - 1) {
+                    __threadfence();
+                    cert_decide(p);
+                }
+            }
         }
         if (p.dot_partials) {
             // deterministic CTA reduction over the epilogue warps (named barrier 1)
@@ -573,53 +699,97 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(THREADS, 1)
 // ------------------------------------------------------------- split kernels
 constexpr int SPLIT_THREADS = 256;
 
+// 2^e as a double for e in [-1022, 1023]
+__device__ __forceinline__ double pow2d(int e) { return __longlong_as_double((long long)(e + 1023) << 52); }
+
+// Magnitude byte of one scaled value for the accuracy certificate:
+// floor(|a| 2^-E * 128) in [0, 127], from v = a 2^(shift-E) (an exact
+// power-of-two rescale, then truncation), so byte / 128 <= |a| 2^-E.
+__device__ __forceinline__ uint32_t mag_byte(double v, double magsc) {
+    return (uint32_t)__double2int_rz(fabs(v) * magsc);
+}
 
 // K-major source: row r is src[r*ld + p], p < K.  One block per row.
+// mag / l1 (optional): the certificate's magnitude plane and the row's
+// ||a 2^-E||_1.  exps_in (optional): exponents of an earlier split of the
+// same operand, which skips the max pass.  run_if (optional): run only when
+// *run_if == 1 (the certificate chose the higher level).
 template <bool CRT>
 __global__ void __launch_bounds__(SPLIT_THREADS) split_rows_kernel(const double* src, long long ld, int rows, int K,
                                                                     int Kp, int count, int shift, uint8_t* out,
-                                                                    int* exps, int* nonfinite) {
+                                                                    int* exps, int* nonfinite, uint8_t* mag,
+                                                                    double* l1, const int* exps_in,
+                                                                    const int* run_if) {
+    if (run_if && *run_if != 1) return;
     __shared__ double red[SPLIT_THREADS / 32];
+    __shared__ double red_l1[SPLIT_THREADS / 32];
     __shared__ int bad_sh;
     const int r = blockIdx.x;
     if (r >= rows) return;
     const double* row = src + (long long)r * ld;
-    if (threadIdx.x == 0) bad_sh = 0;
-    double mx = 0.0;
-    bool bad = false;
-    for (int p = threadIdx.x; p < K; p += SPLIT_THREADS) {
-        const double x = row[p];
-        bad |= !isfinite(x);
-        mx = fmax(mx, fabs(x));
-    }
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
-    __syncthreads();
-    if (bad) atomicOr(&bad_sh, 1);
-    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = mx;
-    __syncthreads();
-    if (threadIdx.x < 32) {
-        double v = threadIdx.x < SPLIT_THREADS / 32 ? red[threadIdx.x] : 0.0;
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
-        if (threadIdx.x == 0) red[0] = v;
-    }
-    __syncthreads();
-    if (bad_sh) {
-        if (threadIdx.x == 0) {
-            atomicOr(nonfinite, 1);
-            exps[r] = 0;
+    int e;
+    if (exps_in) {
+        e = exps_in[r];
+    } else {
+        if (threadIdx.x == 0) bad_sh = 0;
+        double mx = 0.0;
+        bool bad = false;
+        for (int p = threadIdx.x; p < K; p += SPLIT_THREADS) {
+            const double x = row[p];
+            bad |= !isfinite(x);
+            mx = fmax(mx, fabs(x));
         }
-        return;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+        __syncthreads();
+        if (bad) atomicOr(&bad_sh, 1);
+        if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = mx;
+        __syncthreads();
+        if (threadIdx.x < 32) {
+            double v = threadIdx.x < SPLIT_THREADS / 32 ? red[threadIdx.x] : 0.0;
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+            if (threadIdx.x == 0) red[0] = v;
+        }
+        __syncthreads();
+        if (bad_sh) {
+            if (threadIdx.x == 0) {
+                atomicOr(nonfinite, 1);
+                exps[r] = 0;
+            }
+            return;
+        }
+        e = frexp_exp(red[0]);
+        if (threadIdx.x == 0) exps[r] = e;
     }
-    const int e = frexp_exp(red[0]);
-    if (threadIdx.x == 0) exps[r] = e;
     const Pow2 sc = pow2_split(shift - e);
+    const double magsc = pow2d(7 - shift);
+    double l1s = 0.0;
     for (int p4 = threadIdx.x * 4; p4 < K; p4 += SPLIT_THREADS * 4) {
         double v[4];
 #pragma unroll
         for (int u = 0; u < 4; ++u) v[u] = (p4 + u < K) ? row[p4 + u] * sc.lo * sc.hi : 0.0;
+        if (mag) {
+            uint32_t w = 0u;
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                l1s += fabs(v[u]);
+                w |= mag_byte(v[u], magsc) << (8 * u);
+            }
+            *reinterpret_cast<uint32_t*>(mag + (size_t)r * Kp + p4) = w;
+        }
         encode4<CRT>(v, count, out + (size_t)r * Kp + p4, (size_t)rows * Kp);
+    }
+    if (l1) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) l1s += __shfl_xor_sync(0xffffffffu, l1s, o);
+        if ((threadIdx.x & 31) == 0) red_l1[threadIdx.x >> 5] = l1s;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double t = 0.0;
+            for (int w = 0; w < SPLIT_THREADS / 32; ++w) t += red_l1[w];
+            l1[r] = t * pow2d(-shift);
+        }
     }
 }
 
@@ -656,13 +826,17 @@ __global__ void __launch_bounds__(SPLIT_THREADS) colmax_kernel(const double* src
 }
 
 // Pass 2: 32 (i) x 128 (p) tiles through shared memory, written K-major.
+// mag / l1 / exps_in / run_if as for split_rows_kernel (l1 accumulates with
+// atomics over the p tiles and must start at zero).
 constexpr int TR_I = 32, TR_P = 128;
 static_assert(TR_P / 4 <= TR_I && (TR_I & (TR_I - 1)) == 0, "swizzle needs p/4 < TR_I");
 template <bool CRT>
 __global__ void __launch_bounds__(SPLIT_THREADS, 4) split_cols_kernel(const double* src, long long ld, int cols, int K,
                                                                     int Kp, int count, int shift,
                                                                     const unsigned long long* maxbits, uint8_t* out,
-                                                                    int* exps) {
+                                                                    int* exps, uint8_t* mag, double* l1,
+                                                                    const int* exps_in, const int* run_if) {
+    if (run_if && *run_if != 1) return;
     // element (p, i) sits at column i ^ (p/4): the loads (lanes along i) and
     // the encoder's reads (lanes along p/4) both hit 32 distinct banks pairs
     __shared__ double tile[TR_P][TR_I];
@@ -683,77 +857,111 @@ __global__ void __launch_bounds__(SPLIT_THREADS, 4) split_cols_kernel(const doub
         tile[pi][ii ^ ((pi >> 2) & (TR_I - 1))] = ld_v[it];
     }
     __syncthreads();
+    const double magsc = pow2d(7 - shift);
+    // a warp's 32 items share one column ii (32 consecutive e), so the l1
+    // partial is a warp reduction
+    static_assert(TR_P / 4 == 32, "one warp per column of the tile");
     for (int e = threadIdx.x; e < TR_I * (TR_P / 4); e += SPLIT_THREADS) {
         const int ii = e / (TR_P / 4), q = e % (TR_P / 4);
         const int gi = i0 + ii, gp = p0 + 4 * q;
-        if (gi >= cols || gp >= K) continue;
-        const int ex = frexp_exp(__longlong_as_double((long long)maxbits[gi]));
-        if (blockIdx.y == 0 && q == 0) exps[gi] = ex;
-        const Pow2 sc = pow2_split(shift - ex);
-        double v[4];
+        double l1s = 0.0;
+        if (gi < cols && gp < K) {
+            const int ex = exps_in ? exps_in[gi] : frexp_exp(__longlong_as_double((long long)maxbits[gi]));
+            if (!exps_in && blockIdx.y == 0 && q == 0) exps[gi] = ex;
+            const Pow2 sc = pow2_split(shift - ex);
+            double v[4];
 #pragma unroll
-        for (int u = 0; u < 4; ++u) v[u] = tile[4 * q + u][ii ^ (q & (TR_I - 1))] * sc.lo * sc.hi;
-        encode4<CRT>(v, count, out + (size_t)gi * Kp + gp, (size_t)cols * Kp);
+            for (int u = 0; u < 4; ++u) v[u] = tile[4 * q + u][ii ^ (q & (TR_I - 1))] * sc.lo * sc.hi;
+            if (mag) {
+                uint32_t w = 0u;
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    l1s += fabs(v[u]);
+                    w |= mag_byte(v[u], magsc) << (8 * u);
+                }
+                *reinterpret_cast<uint32_t*>(mag + (size_t)gi * Kp + gp) = w;
+            }
+            encode4<CRT>(v, count, out + (size_t)gi * Kp + gp, (size_t)cols * Kp);
+        }
+        if (l1) {
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) l1s += __shfl_xor_sync(0xffffffffu, l1s, o);
+            if ((threadIdx.x & 31) == 0 && gi < cols) atomicAdd(&l1[gi], l1s * pow2d(-shift));
+        }
     }
 }
 
 struct Layout {
-    size_t sa, sb, ea, eb, maxb, scratch, total;
+    size_t sa, sb, ea, eb, maxb, l1a, l1b, cert, scratch, total, per_cta;
 };
 
 inline size_t up(size_t v, size_t a) { return (v + a - 1) / a * a; }
 
-// count: slices (slice scheme) or moduli (residue scheme)
-Layout plan_layout(long long m, long long n, long long k, int count, int grid, bool crt) {
+// planes: INT8 planes per operand (slices or residues, plus the
+// certificate's magnitude plane)
+Layout plan_layout(long long m, long long n, long long k, int planes, int grid, bool crt) {
     const size_t kp = up((size_t)k, 16);
     Layout L;
     size_t off = 0;
     L.sa = off;
-    off = up(off + (size_t)count * m * kp, 1024);
+    off = up(off + (size_t)planes * m * kp, 1024);
     L.sb = off;
-    off = up(off + (size_t)count * n * kp, 1024);
+    off = up(off + (size_t)planes * n * kp, 1024);
     L.ea = off;
     off = up(off + (size_t)m * 4, 256);
     L.eb = off;
     off = up(off + (size_t)n * 4, 256);
     L.maxb = off;
     off = up(off + (size_t)(m > n ? m : n) * 8, 256);
+    L.l1a = off;
+    off = up(off + (size_t)m * 8, 256);
+    L.l1b = off;
+    off = up(off + (size_t)n * 8, 256);
+    L.cert = off;
+    off = up(off + sizeof(CertRecord), 256);
     L.scratch = off;
     // residue scheme: two banks of slots per CTA (the tile being accumulated and
-    // the one being reconstructed)
-    const size_t per_cta = crt ? (size_t)2 * MAX_MODULI * CRT_SLOT_WORDS * 4 : (size_t)SCRATCH_DOUBLES * 8;
-    off = up(off + (size_t)grid * per_cta, 1024);
+    // the one being reconstructed); the certificate's float sums fit in either
+    L.per_cta = crt ? (size_t)2 * MAX_MODULI * CRT_SLOT_WORDS * 4 : (size_t)SCRATCH_DOUBLES * 8;
+    off = up(off + (size_t)grid * L.per_cta, 1024);
     L.total = off;
     return L;
 }
 
 // Split one operand given as K-major (rows contiguous along k) or MN-major.
 int split_operand(const double* src, long long ld, bool kmajor, int rows, int K, int Kp, int count, int shift,
-                  bool crt, uint8_t* out, int* exps, unsigned long long* maxbits, int* nonfinite, cudaStream_t st,
-                  int sm_count) {
+                  bool crt, uint8_t* out, int* exps, unsigned long long* maxbits, int* nonfinite, uint8_t* mag,
+                  double* l1, const int* exps_in, const int* run_if, cudaStream_t st, int sm_count, int* launches) {
     if (kmajor) {
         if (crt)
             split_rows_kernel<true><<<rows, SPLIT_THREADS, 0, st>>>(src, ld, rows, K, Kp, count, shift, out, exps,
-                                                                   nonfinite);
+                                                                   nonfinite, mag, l1, exps_in, run_if);
         else
             split_rows_kernel<false><<<rows, SPLIT_THREADS, 0, st>>>(src, ld, rows, K, Kp, count, 0, out, exps,
-                                                                    nonfinite);
+                                                                    nonfinite, mag, l1, exps_in, run_if);
+        *launches += 1;
     } else {
-        cudaMemsetAsync(maxbits, 0, (size_t)rows * 8, st);
-        const int cblocks = (rows + SPLIT_THREADS - 1) / SPLIT_THREADS;
-        int ksplit = (4 * sm_count + cblocks - 1) / cblocks;
-        if (ksplit < 1) ksplit = 1;
-        int kchunk = (K + ksplit - 1) / ksplit;
-        if (kchunk < 16) kchunk = 16;
-        ksplit = (K + kchunk - 1) / kchunk;
-        colmax_kernel<<<dim3(cblocks, ksplit), SPLIT_THREADS, 0, st>>>(src, ld, rows, K, kchunk, maxbits, nonfinite);
+        if (!exps_in) {
+            cudaMemsetAsync(maxbits, 0, (size_t)rows * 8, st);
+            const int cblocks = (rows + SPLIT_THREADS - 1) / SPLIT_THREADS;
+            int ksplit = (4 * sm_count + cblocks - 1) / cblocks;
+            if (ksplit < 1) ksplit = 1;
+            int kchunk = (K + ksplit - 1) / ksplit;
+            if (kchunk < 16) kchunk = 16;
+            ksplit = (K + kchunk - 1) / kchunk;
+            colmax_kernel<<<dim3(cblocks, ksplit), SPLIT_THREADS, 0, st>>>(src, ld, rows, K, kchunk, maxbits,
+                                                                          nonfinite);
+            *launches += 1;
+        }
+        if (l1) cudaMemsetAsync(l1, 0, (size_t)rows * 8, st);
         const dim3 grid((rows + TR_I - 1) / TR_I, (K + TR_P - 1) / TR_P);
         if (crt)
             split_cols_kernel<true><<<grid, SPLIT_THREADS, 0, st>>>(src, ld, rows, K, Kp, count, shift, maxbits, out,
-                                                                   exps);
+                                                                   exps, mag, l1, exps_in, run_if);
         else
             split_cols_kernel<false><<<grid, SPLIT_THREADS, 0, st>>>(src, ld, rows, K, Kp, count, 0, maxbits, out,
-                                                                    exps);
+                                                                    exps, mag, l1, exps_in, run_if);
+        *launches += 1;
     }
     return cudaGetLastError() == cudaSuccess ? JLC_OK : JLC_E_LAUNCH;
 }
@@ -787,6 +995,33 @@ void crt_constants(int nmod, long long k, CrtConsts& c) {
     crt::build_consts(nmod, p, q, kModuliHost, c);
 }
 
+// Coefficients of the certified error ratio at one level (see CertDecision).
+// In units of the scaled operands (|a 2^-E| < 1, |b 2^-F| < 1) the error of one
+// entry is at most
+//   residues (p, q):  h ||b_j|| + g ||a_i|| + k h g,  h = 2^-(p+1), g = 2^-(q+1)
+//                     (round to nearest of a 2^(p-E) and b 2^(q-F));
+//   slices (s):       2^-7s (||b_j|| + ||a_i|| + k s)
+//                     (truncation remainders below 2^-7s, plus the slice pairs
+//                     t + u > s + 1 that are not computed);
+// and the FP64 bound is 2 k u (|A||B|)_ij >= 2 k u 2^-14 lb_ij.
+void cert_coeffs(bool crt, int count, long long k, double (&c)[3]) {
+    const double two_ku = 2.0 * (double)k * 0x1p-53;
+    const double unit = 16384.0 / two_ku;  // 2^14 / (2 k u)
+    if (crt) {
+        int p, q;
+        crt_pq(count, k, p, q);
+        const double h = std::ldexp(1.0, -(p + 1)), g = std::ldexp(1.0, -(q + 1));
+        c[0] = h * unit;
+        c[1] = g * unit;
+        c[2] = (double)k * h * g * unit;
+    } else {
+        const double t = std::ldexp(1.0, -7 * count);
+        c[0] = t * unit;
+        c[1] = t * unit;
+        c[2] = (double)k * count * t * unit;
+    }
+}
+
 }  // namespace oz
 
 // CTAs of the persistent Ozaki GEMM: one pair per PM x BN tile, at most one
@@ -799,8 +1034,15 @@ int ozaki_grid(long long m, long long n, int sm_count) {
     return (int)(2 * pairs);
 }
 
-size_t ozaki_workspace_bytes(long long m, long long n, long long k, int count, int sm_count, bool crt) {
-    return oz::plan_layout(m, n, k, count, ozaki_grid(m, n, sm_count), crt).total;
+int auto_slices(long long k) {
+    // (s+3) * 2^-7s <= 2u * k * rho^2 with rho = 1/4 (uniform-like rows/cols)
+    const double u = std::ldexp(1.0, -53);
+    for (int s = 5; s <= 8; ++s) {
+        const double lhs = (s + 3) * std::ldexp(1.0, -7 * s);
+        const double rhs = 2.0 * u * (double)k / 16.0;
+        if (lhs <= rhs) return s;
+    }
+    return 8;
 }
 
 void ozaki_crt_pq(int nmod, long long k, int* p, int* q) { oz::crt_pq(nmod, k, *p, *q); }
@@ -823,24 +1065,51 @@ double ozaki_crt_est_ratio(int nmod, long long k) {
     return std::ldexp(1.0, -(p < q ? p : q)) / (2.0 * std::ldexp(1.0, -53) * (double)k / 16.0);
 }
 
+bool ozaki_reaches_bound(long long k, bool crt) {
+    if (crt) return ozaki_crt_est_ratio(ozaki_crt_auto_moduli(k), k) <= 1.0;
+    const int s = auto_slices(k);
+    return (s + 3) * std::ldexp(1.0, -7 * s) <= 2.0 * std::ldexp(1.0, -53) * (double)k / 16.0;
+}
+
+OzakiPlan ozaki_plan(long long k, bool crt, int count, bool allow_hi) {
+    OzakiPlan pl;
+    pl.crt = crt;
+    pl.gate = count == 0;
+    pl.lo = count > 0 ? count : (crt ? ozaki_crt_auto_moduli(k) : auto_slices(k));
+    const int top = crt ? oz::MAX_MODULI : 8;
+    pl.hi = (pl.gate && allow_hi && pl.lo < top) ? top : 0;
+    return pl;
+}
+
+static int plan_planes(const OzakiPlan& pl) { return pl.lo + 1 > pl.hi ? pl.lo + 1 : pl.hi; }
+
+size_t ozaki_workspace_bytes(long long m, long long n, long long k, const OzakiPlan& pl, int sm_count) {
+    return oz::plan_layout(m, n, k, plan_planes(pl), ozaki_grid(m, n, sm_count), pl.crt).total;
+}
+
+size_t ozaki_cert_offset(long long m, long long n, long long k, const OzakiPlan& pl) {
+    return oz::plan_layout(m, n, k, plan_planes(pl), 1, pl.crt).cert;
+}
+
 struct OzakiBufs {
     oz::Layout L;
     int Kp, grid;
     long long tiles_m, tiles_n;
 };
 
-static int ozaki_bufs(const GemmDesc& g, int count, size_t ws_bytes, int sm_count, bool crt, OzakiBufs& b,
-                      char* err, size_t errlen) {
+static int ozaki_bufs(const GemmDesc& g, const OzakiPlan& pl, size_t ws_bytes, int sm_count, OzakiBufs& b, char* err,
+                      size_t errlen) {
     using namespace oz;
-    if (count < 1 || count > (crt ? MAX_MODULI : 8)) {
-        snprintf(err, errlen, "%s count %d out of range", crt ? "modulus" : "slice", count);
+    const int top = pl.crt ? MAX_MODULI : 8;
+    if (pl.lo < 1 || pl.lo > top || pl.hi < 0 || pl.hi > top) {
+        snprintf(err, errlen, "%s count %d out of range", pl.crt ? "modulus" : "slice", pl.lo);
         return JLC_E_ARG;
     }
     b.tiles_m = (g.m + PM - 1) / PM;
     b.tiles_n = (g.n + BN - 1) / BN;
     b.grid = ozaki_grid(g.m, g.n, sm_count);
     const long long lm = g.ws_m > g.m ? g.ws_m : g.m;
-    b.L = plan_layout(lm, g.n, g.k, count, ozaki_grid(lm, g.n, sm_count), crt);
+    b.L = plan_layout(lm, g.n, g.k, plan_planes(pl), ozaki_grid(lm, g.n, sm_count), pl.crt);
     b.Kp = (int)up((size_t)g.k, 16);
     if (b.L.total > ws_bytes) {
         snprintf(err, errlen, "Ozaki workspace too small (%zu < %zu)", ws_bytes, b.L.total);
@@ -849,57 +1118,77 @@ static int ozaki_bufs(const GemmDesc& g, int count, size_t ws_bytes, int sm_coun
     return JLC_OK;
 }
 
-int launch_ozaki_split(const GemmDesc& g, int count, void* workspace, size_t ws_bytes, cudaStream_t st,
-                       int sm_count, int* flags, char* err, size_t errlen, bool crt) {
+int launch_ozaki_split(const GemmDesc& g, const OzakiPlan& pl, int level, void* workspace, size_t ws_bytes,
+                       cudaStream_t st, int sm_count, int* flags, char* err, size_t errlen, int* launches) {
     using namespace oz;
     OzakiBufs b;
-    int rc = ozaki_bufs(g, count, ws_bytes, sm_count, crt, b, err, errlen);
+    int rc = ozaki_bufs(g, pl, ws_bytes, sm_count, b, err, errlen);
     if (rc) return rc;
+    if (level == 1 && pl.hi == 0) return JLC_OK;
     char* ws = static_cast<char*>(workspace);
     auto* maxb = reinterpret_cast<unsigned long long*>(ws + b.L.maxb);
-    // flags[0]: A held Inf/NaN, flags[1]: B did (kept while B's split is reused)
+    const int count = level == 0 ? pl.lo : pl.hi;
     int p = 0, q = 0;
-    if (crt) crt_pq(count, g.k, p, q);
-    if (cudaMemsetAsync(flags, 0, (g.b_split_ready ? 1 : 2) * sizeof(int), st) != cudaSuccess) {
-        snprintf(err, errlen, "flag reset failed");
-        return JLC_E_CUDA;
+    if (pl.crt) crt_pq(count, g.k, p, q);
+    const int* ea = reinterpret_cast<const int*>(ws + b.L.ea);
+    const int* eb = reinterpret_cast<const int*>(ws + b.L.eb);
+    uint8_t* sa = reinterpret_cast<uint8_t*>(ws + b.L.sa);
+    uint8_t* sb = reinterpret_cast<uint8_t*>(ws + b.L.sb);
+    // the certificate's magnitude plane sits after the level-0 planes
+    uint8_t* maga = level == 0 ? sa + (size_t)pl.lo * g.m * b.Kp : nullptr;
+    uint8_t* magb = level == 0 ? sb + (size_t)pl.lo * g.n * b.Kp : nullptr;
+    double* l1a = level == 0 ? reinterpret_cast<double*>(ws + b.L.l1a) : nullptr;
+    double* l1b = level == 0 ? reinterpret_cast<double*>(ws + b.L.l1b) : nullptr;
+    const int* run_if = level == 1 ? flags + kFlagRoute : nullptr;
+    if (level == 0) {
+        // per call: non-finite A, fallback, route (and non-finite B when B is
+        // split here: a reused split keeps its flag); the certificate record's
+        // per-launch part, and its per-product totals with B's split
+        const size_t nflags = g.b_split_ready ? kFlagNonfiniteB : kFlagWords;
+        cudaError_t e = cudaMemsetAsync(flags, 0, nflags * sizeof(int), st);
+        if (e == cudaSuccess)
+            e = cudaMemsetAsync(ws + b.L.cert, 0, g.b_split_ready ? kCertLaunchBytes : sizeof(CertRecord), st);
+        if (e != cudaSuccess) {
+            snprintf(err, errlen, "Ozaki flag reset failed");
+            return JLC_E_CUDA;
+        }
     }
     // op(A) rows are contiguous along k when A is row-major; op(B) "rows"
     // (columns j of B) are contiguous along k when B is column-major.
-    rc = split_operand(g.a, g.lda, g.layout_a == JLC_ROW_MAJOR, (int)g.m, (int)g.k, b.Kp, count, p, crt,
-                       reinterpret_cast<uint8_t*>(ws + b.L.sa), reinterpret_cast<int*>(ws + b.L.ea), maxb,
-                       flags, st, sm_count);
-    if (!rc && !g.b_split_ready)
-        rc = split_operand(g.b, g.ldb, g.layout_b == JLC_COL_MAJOR, (int)g.n, (int)g.k, b.Kp, count, q, crt,
-                           reinterpret_cast<uint8_t*>(ws + b.L.sb), reinterpret_cast<int*>(ws + b.L.eb), maxb,
-                           flags + 1, st, sm_count);
+    rc = split_operand(g.a, g.lda, g.layout_a == JLC_ROW_MAJOR, (int)g.m, (int)g.k, b.Kp, count, p, pl.crt, sa,
+                       const_cast<int*>(ea), maxb, flags + kFlagNonfiniteA, maga, l1a, level == 1 ? ea : nullptr,
+                       run_if, st, sm_count, launches);
+    if (!rc && (!g.b_split_ready || level == 1))
+        rc = split_operand(g.b, g.ldb, g.layout_b == JLC_COL_MAJOR, (int)g.n, (int)g.k, b.Kp, count, q, pl.crt, sb,
+                           const_cast<int*>(eb), maxb, flags + kFlagNonfiniteB, magb, l1b,
+                           level == 1 ? eb : nullptr, run_if, st, sm_count, launches);
     if (rc) snprintf(err, errlen, "Ozaki split launch failed: %s", cudaGetErrorString(cudaGetLastError()));
     return rc;
 }
 
-int launch_ozaki_gemm(const GemmDesc& g, int count, void* workspace, size_t ws_bytes, cudaStream_t st,
-                      int sm_count, int* status, int* flags, char* err, size_t errlen, bool crt) {
+// one launch of the persistent kernel in `mode` (plane_dim: planes per
+// operand in the workspace; the certificate reads plane `count`)
+static int launch_mode(int mode, const GemmDesc& g, const OzakiBufs& b, int count, int plane_dim, char* ws,
+                       cudaStream_t st, int* status, int* flags, int route_want, const oz::CertDecision* dec,
+                       char* err, size_t errlen) {
     using namespace oz;
-    OzakiBufs b;
-    int rc = ozaki_bufs(g, count, ws_bytes, sm_count, crt, b, err, errlen);
-    if (rc) return rc;
-    char* ws = static_cast<char*>(workspace);
     CUtensorMap ma, mb;
-    rc = make_tmap_3d(&ma, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, ws + b.L.sa, (uint64_t)g.k, (uint64_t)g.m,
-                      (uint64_t)count, (uint64_t)b.Kp, (uint64_t)g.m * b.Kp, BKB, BM, 1, CU_TENSOR_MAP_SWIZZLE_128B,
-                      err, errlen);
+    int rc = make_tmap_3d(&ma, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, ws + b.L.sa, (uint64_t)g.k, (uint64_t)g.m,
+                          (uint64_t)plane_dim, (uint64_t)b.Kp, (uint64_t)g.m * b.Kp, BKB, BM, 1,
+                          CU_TENSOR_MAP_SWIZZLE_128B, err, errlen);
     if (rc) return rc;
     rc = make_tmap_3d(&mb, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, ws + b.L.sb, (uint64_t)g.k, (uint64_t)g.n,
-                      (uint64_t)count, (uint64_t)b.Kp, (uint64_t)g.n * b.Kp, BKB, BNH, 1, CU_TENSOR_MAP_SWIZZLE_128B,
-                      err, errlen);
+                      (uint64_t)plane_dim, (uint64_t)b.Kp, (uint64_t)g.n * b.Kp, BKB, BNH, 1,
+                      CU_TENSOR_MAP_SWIZZLE_128B, err, errlen);
     if (rc) return rc;
 
     Params p;
+    memset(&p, 0, sizeof(p));
     p.M = (int)g.m;
     p.N = (int)g.n;
     p.K = (int)g.k;
     p.KB = (int)((g.k + BKB - 1) / BKB);
-    p.s = count;
+    p.s = count;  // slices / moduli; the certificate: its plane index
     p.tiles_m = (int)b.tiles_m;
     p.tiles_n = (int)b.tiles_n;
     p.num_tiles = (int)(b.tiles_m * b.tiles_n);
@@ -910,15 +1199,25 @@ int launch_ozaki_gemm(const GemmDesc& g, int count, void* workspace, size_t ws_b
     p.C = g.c;
     p.ldc = g.ldc;
     p.scratch = reinterpret_cast<double*>(ws + b.L.scratch);
+    p.scratch_stride = (long long)b.L.per_cta;
     p.status = status;
-    p.nonfinite = flags;
+    p.flags = flags;
+    p.route_want = route_want;
     p.epi_scale = g.epi_scale;
-    p.dot_mat = g.dot_mat;
-    p.dot_ld = g.dot_ld;
-    p.dot_partials = g.dot_partials;
     p.crt = CrtConsts{};
-    if (crt) crt_constants(count, g.k, p.crt);
-    auto kern = crt ? ozaki_gemm_kernel<true> : ozaki_gemm_kernel<false>;
+    p.l1a = reinterpret_cast<const double*>(ws + b.L.l1a);
+    p.l1b = reinterpret_cast<const double*>(ws + b.L.l1b);
+    p.cert = reinterpret_cast<CertRecord*>(ws + b.L.cert);
+    if (mode == kModeCert) {
+        p.dec = *dec;
+    } else {
+        p.dot_mat = g.dot_mat;
+        p.dot_ld = g.dot_ld;
+        p.dot_partials = g.dot_partials;
+    }
+    if (mode == kModeCrt) crt_constants(count, g.k, p.crt);
+    auto kern = mode == kModeCrt ? ozaki_gemm_kernel<kModeCrt>
+                                 : (mode == kModeSlices ? ozaki_gemm_kernel<kModeSlices> : ozaki_gemm_kernel<kModeCert>);
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES);
     if (e != cudaSuccess) {
         snprintf(err, errlen, "Ozaki smem attribute: %s", cudaGetErrorString(e));
@@ -931,6 +1230,37 @@ int launch_ozaki_gemm(const GemmDesc& g, int count, void* workspace, size_t ws_b
         return JLC_E_LAUNCH;
     }
     return JLC_OK;
+}
+
+int launch_ozaki_cert(const GemmDesc& g, const OzakiPlan& pl, void* workspace, size_t ws_bytes, cudaStream_t st,
+                      int sm_count, int* status, int* flags, char* err, size_t errlen) {
+    using namespace oz;
+    OzakiBufs b;
+    int rc = ozaki_bufs(g, pl, ws_bytes, sm_count, b, err, errlen);
+    if (rc) return rc;
+    CertDecision dec;
+    memset(&dec, 0, sizeof(dec));
+    cert_coeffs(pl.crt, pl.lo, g.k, dec.c_lo);
+    if (pl.hi > 0) cert_coeffs(pl.crt, pl.hi, g.k, dec.c_hi);
+    // final roundings (reconstruction or FP64 recombination, alpha, beta):
+    // at most (s + 3) u |C| <= 11 u |C|, i.e. 5.5 / k of the bound
+    dec.margin = 6.0 / (double)g.k;
+    dec.have_hi = pl.hi > 0;
+    dec.gate = pl.gate;
+    return launch_mode(kModeCert, g, b, pl.lo, plan_planes(pl), static_cast<char*>(workspace), st, status, flags,
+                       -1, &dec, err, errlen);
+}
+
+int launch_ozaki_gemm(const GemmDesc& g, const OzakiPlan& pl, int level, void* workspace, size_t ws_bytes,
+                      cudaStream_t st, int sm_count, int* status, int* flags, char* err, size_t errlen) {
+    using namespace oz;
+    OzakiBufs b;
+    int rc = ozaki_bufs(g, pl, ws_bytes, sm_count, b, err, errlen);
+    if (rc) return rc;
+    if (level == 1 && pl.hi == 0) return JLC_OK;
+    const int count = level == 0 ? pl.lo : pl.hi;
+    return launch_mode(pl.crt ? kModeCrt : kModeSlices, g, b, count, plan_planes(pl), static_cast<char*>(workspace),
+                       st, status, flags, level, nullptr, err, errlen);
 }
 
 }  // namespace jlc

@@ -64,7 +64,7 @@ __device__ __forceinline__ unsigned ld_acquire_u32(const unsigned* p) {
 }
 
 // All CTAs of the launch arrive, then wait until `target` arrivals are
-// counted.  Bounded: past kWaitTimeoutNs (or once another CTA has recorded an
+// counted.  Bounded: past the status block's wait limit (or once another CTA has recorded an
 // error) it records JLC_DEV_TIMEOUT and returns false in every thread.  The
 // arrival is a release reduction and the poll an acquire load: with the CTA
 // barriers on either side, every write a CTA made before arriving is visible
@@ -74,6 +74,7 @@ __device__ bool grid_barrier(unsigned* counter, unsigned target, int* status, in
     if (threadIdx.x == 0) {
         asm volatile("red.release.gpu.global.add.u32 [%0], %1;" ::"l"(counter), "r"(1u) : "memory");
         const uint64_t t0 = globaltimer_ns();
+        const uint64_t limit = wait_limit_ns(status);
         int ok = 1;
         for (unsigned it = 0; ld_acquire_u32(counter) < target; ++it) {
             if ((it & 63u) == 0u) {
@@ -81,7 +82,7 @@ __device__ bool grid_barrier(unsigned* counter, unsigned target, int* status, in
                     ok = 0;
                     break;
                 }
-                if (globaltimer_ns() - t0 > kWaitTimeoutNs) {
+                if (globaltimer_ns() - t0 > limit) {
                     atomicOr(status, JLC_DEV_TIMEOUT);
                     ok = 0;
                     break;
