@@ -258,13 +258,16 @@ def run_ours(args):
         if world > 1:
             dist.barrier()
 
-    def step(prec, C):
+    def step(prec, C, report=False):
         return ctx.dgemm_device(0, 0, M, N, K, 1.0, A.data_ptr(), K, B.data_ptr(), N, 0.0, C.data_ptr(), N,
-                                precision=prec)
+                                precision=prec, report=report)
 
     def timed(prec, C, clocks=None):
-        for _ in range(args.warmup):
-            rep = step(prec, C)
+        # the first warm-up call reports (route, count, certified error ratio);
+        # the timed calls stay asynchronous
+        rep = step(prec, C, report=True)
+        for _ in range(args.warmup - 1):
+            step(prec, C)
         ctx.synchronize()
         ctx.profile_collect()
         ctx.set_profiling(True)
@@ -275,7 +278,7 @@ def run_ours(args):
         e1 = torch.cuda.Event(enable_timing=True)
         e0.record(stream)
         for _ in range(args.steps):
-            rep = step(prec, C)
+            step(prec, C)
         e1.record(stream)
         e1.synchronize()
         torch.cuda.synchronize()
@@ -568,12 +571,13 @@ def run_configs(args):
         C = C0.clone()
         lda = A.shape[1]
         ldb = B.shape[1]
-        ms, rep = timed(lambda: ctx.dgemm_device(la, lb, m, n, k, alpha, A.data_ptr(), lda, B.data_ptr(), ldb,
-                                                 beta, C.data_ptr(), n, precision=precision))
-        # accuracy of one fresh call on the original C
+        ms, _ = timed(lambda: ctx.dgemm_device(la, lb, m, n, k, alpha, A.data_ptr(), lda, B.data_ptr(), ldb,
+                                               beta, C.data_ptr(), n, precision=precision, report=False))
+        # accuracy of one fresh call on the original C (its report carries the
+        # route and, for the INT8 routes, the certified error ratio)
         C.copy_(C0)
-        ctx.dgemm_device(la, lb, m, n, k, alpha, A.data_ptr(), lda, B.data_ptr(), ldb, beta, C.data_ptr(), n,
-                         precision=precision)
+        rep = ctx.dgemm_device(la, lb, m, n, k, alpha, A.data_ptr(), lda, B.data_ptr(), ldb, beta, C.data_ptr(), n,
+                               precision=precision)
         ctx.synchronize()
         ratio = accuracy(la, lb, m, n, k, alpha, A, lda, B, ldb, beta, C0 if beta != 0.0 else None, C)
         flops = 2.0 * m * n * k
@@ -583,6 +587,8 @@ def run_configs(args):
                 else "row", "route": {0: "native", 1: "ozaki-slices", 3: "ozaki-crt"}.get(rep["precision"]),
                 "kernel": rep["kernel"], "ms": round(ms, 4), "gflops": round(flops / (ms * 1e-3) / 1e9, 1),
                 "gbs": round(nbytes / (ms * 1e-3) / 1e9, 1), "max_err_ratio": ratio}
+        if rep["kernel"] == 3:
+            line["certified_err_ratio"] = rep["est_err_ratio"]
         if scaled:
             line["inputs"] = "ill-scaled 2^e, e in [-20,20] per row of A / column of B"
         print(json.dumps(line), flush=True)

@@ -30,6 +30,12 @@ JLC_KERNEL_GEMV = 2
 JLC_KERNEL_OZAKI = 3
 JLC_KERNEL_GROUPED = 4
 
+JLC_FAULT_NONE = 0
+JLC_FAULT_ALLOC = 1
+JLC_FAULT_LAUNCH = 2
+JLC_FAULT_COPY = 3
+JLC_FAULT_WAIT = 4
+
 # every symbol include/jlcgpu.h declares, with (restype, argtypes)
 _i = ctypes.c_int
 _i64 = ctypes.c_int64
@@ -96,6 +102,8 @@ SIGNATURES = {
     "jlc_dgemm_ozaki_crt_device": (_i, [_vp, _i, _i, _i64, _i64, _i64, _d, _dp, _i64, _dp, _i64, _d, _dp, _i64,
                                         _i, _REP]),
     "jlc_device_status": (_i, [_vp]),
+    "jlc_set_wait_limit": (_i, [_vp, _d]),
+    "jlc_inject_fault": (_i, [_vp, _i, _i]),
     "jlc_set_profiling": (_i, [_vp, _i]),
     "jlc_profile_collect": (_i, [_vp, ctypes.POINTER(_i), ctypes.POINTER(_d), _i]),
     "jlc_profile_timeline": (_i, [_vp, ctypes.POINTER(_i), ctypes.POINTER(_d), ctypes.POINTER(_d), _i]),
@@ -120,7 +128,8 @@ SIGNATURES = {
 }
 
 PHASES = {1: "dmma", 2: "gemv", 3: "ozaki_gemm", 4: "grouped", 5: "ozaki_split", 6: "scale", 7: "fp64_gated", 8: "h2d",
-          9: "d2h", 11: "reduce", 12: "qr_panel", 13: "qr_vt"}
+          9: "d2h", 11: "reduce", 12: "qr_panel", 13: "qr_vt", 14: "ozaki_cert", 15: "ozaki_split_hi",
+          16: "ozaki_gemm_hi"}
 
 _lib = None
 

@@ -10,7 +10,8 @@ Same names, argument meaning and error behaviour as the reference's
 * ``Matrix`` / ``OffHeapMatrix``      -- Matrix.java:18-24,149-175,385;
   OffHeapMatrix.java:15-325 (row/column order, ld, offset, heap mirror)
 
-Every product runs on the GPU through the C ABI; there is no CPU path here.
+Every product runs on the GPU through the C ABI; there is no CPU path here
+(the reference's routing in front of it lives in ``dispatch``).
 Argument errors raise ``IllegalArgumentException`` (a ``ValueError``) with a
 non-empty message, as the reference throws IllegalArgumentException.
 """
@@ -22,6 +23,7 @@ import threading
 import numpy as np
 
 from . import _lib as L
+from .dispatch import DispatchPolicy
 
 
 class IllegalArgumentException(ValueError):
@@ -121,13 +123,24 @@ class Context:
         return out.value
 
     def ozaki_crt_device(self, layout_a, layout_b, m, n, k, alpha, a_ptr, lda, b_ptr, ldb, beta, c_ptr, ldc,
-                         moduli=0) -> dict:
-        rep = L.Report()
+                         moduli=0, report=True) -> dict | None:
+        """Residue-scheme Ozaki GEMM on device pointers.  With report=True the
+        call waits for the device and returns the accuracy certificate's
+        figures; report=False leaves it asynchronous and returns None."""
+        rep = L.Report() if report else None
         rc = self.lib.jlc_dgemm_ozaki_crt_device(self.h, int(layout_a), int(layout_b), m, n, k, float(alpha), a_ptr,
                                                  lda, b_ptr, ldb, float(beta), c_ptr, ldc, int(moduli),
-                                                 ctypes.byref(rep))
+                                                 ctypes.byref(rep) if report else None)
         self.check(rc)
-        return rep.as_dict()
+        return rep.as_dict() if report else None
+
+    def set_wait_limit(self, seconds: float):
+        """Limit of every bounded device wait of this context's kernels (0: default 4 s)."""
+        self.check(self.lib.jlc_set_wait_limit(self.h, float(seconds)))
+
+    def inject_fault(self, kind: int, after: int = 0):
+        """Test hook: the (after + 1)-th operation of `kind` (JLC_FAULT_*) fails once."""
+        self.check(self.lib.jlc_inject_fault(self.h, int(kind), int(after)))
 
     def adjoint_device(self, m, n, k, alpha, beta, a_ptr, lda, b_ptr, ldb, cin_ptr, ldc_in, dc_ptr, lddc,
                        da_ptr, ldda, db_ptr, lddb, dalpha_ptr, dbeta_ptr, dcin_ptr=None, lddc_in=0,
@@ -210,12 +223,16 @@ class Context:
 
     # -- device entries (raw device addresses, e.g. torch tensor.data_ptr()) --
     def dgemm_device(self, layout_a, layout_b, m, n, k, alpha, a_ptr, lda, b_ptr, ldb, beta, c_ptr, ldc,
-                     precision=L.JLC_PREC_NATIVE) -> dict:
-        rep = L.Report()
+                     precision=L.JLC_PREC_NATIVE, report=True) -> dict | None:
+        """jlc_dgemm_device.  An Ozaki route with report=True waits for the
+        device to read the accuracy certificate; report=False stays
+        asynchronous and returns None."""
+        rep = L.Report() if report else None
         rc = self.lib.jlc_dgemm_device(self.h, int(layout_a), int(layout_b), m, n, k, float(alpha), a_ptr, lda,
-                                       b_ptr, ldb, float(beta), c_ptr, ldc, int(precision), ctypes.byref(rep))
+                                       b_ptr, ldb, float(beta), c_ptr, ldc, int(precision),
+                                       ctypes.byref(rep) if report else None)
         self.check(rc)
-        return rep.as_dict()
+        return rep.as_dict() if report else None
 
     def qr_factor_device(self, m, n, a_ptr, lda, tau_ptr, precision=L.JLC_PREC_NATIVE) -> dict:
         """Blocked Householder QR of the column-major m x n matrix at a_ptr, in
@@ -234,13 +251,14 @@ class Context:
         return rep.as_dict()
 
     def ozaki_device(self, layout_a, layout_b, m, n, k, alpha, a_ptr, lda, b_ptr, ldb, beta, c_ptr, ldc,
-                     slices=0) -> dict:
-        rep = L.Report()
+                     slices=0, report=True) -> dict | None:
+        """Slice-scheme Ozaki GEMM on device pointers (report as for ozaki_crt_device)."""
+        rep = L.Report() if report else None
         rc = self.lib.jlc_dgemm_ozaki_device(self.h, int(layout_a), int(layout_b), m, n, k, float(alpha), a_ptr,
                                              lda, b_ptr, ldb, float(beta), c_ptr, ldc, int(slices),
-                                             ctypes.byref(rep))
+                                             ctypes.byref(rep) if report else None)
         self.check(rc)
-        return rep.as_dict()
+        return rep.as_dict() if report else None
 
 
 def _problem_array(problems):
@@ -480,28 +498,36 @@ class CudaGemm:
         return c if CudaGemm.gemm(a, b, c, 1.0, 0.0) else None
 
 
-class DispatchPolicy:
-    """The subset of DispatchPolicy (DispatchPolicy.java:58-679) the GPU route
-    reads: parallelism and the precision choice of the GPU path."""
-
-    def __init__(self, precision: int = L.JLC_PREC_NATIVE, parallelism: int = 1):
-        self.precision = precision
-        self.parallelism = parallelism
-
-    @staticmethod
-    def defaultPolicy() -> "DispatchPolicy":
-        return DispatchPolicy()
-
-    def getParallelism(self) -> int:
-        return self.parallelism
-
-
 class OptimizedBLAS3:
     @staticmethod
-    def gemm(a: Matrix, b: Matrix, c: Matrix, alpha: float, beta: float, policy: DispatchPolicy | None = None):
-        """OptimizedBLAS3.gemm (OptimizedBLAS3.java:61-130) on the GPU route."""
+    def gemm(a: Matrix, b: Matrix, c: Matrix, alpha: float, beta: float, policy: DispatchPolicy | None = None,
+             cpu=None):
+        """OptimizedBLAS3.gemm (OptimizedBLAS3.java:61-130).
+
+        Without ``cpu``: the GPU route for every size (what the reference's
+        CUDA branch runs).  With ``cpu``: the reference's own dispatch
+        (GemmDispatch.selectKernel against the persistent context, CUDA at
+        200M FLOPs and above), the CPU kernels being ``cpu(kernel_name, a, b, c,
+        alpha, beta, policy)``; a declined CUDA call runs MICROKERNEL there, as
+        OptimizedBLAS3.java:108-113 does.  Returns the kernel name run."""
         prec = policy.precision if policy is not None else L.JLC_PREC_NATIVE
-        return _gpu_gemm(a, b, c, alpha, beta, prec, None)
+        if cpu is None:
+            _gpu_gemm(a, b, c, alpha, beta, prec, None)
+            return "CUDA"
+        from .dispatch import GemmDispatch, select_optimized_kernel
+        m, k, n = _validate_gemm(a, b, c)
+        if a.getRawImagData() is not None or b.getRawImagData() is not None or c.getRawImagData() is not None:
+            cpu("NAIVE_COMPLEX", a, b, c, alpha, beta, policy)
+            return "NAIVE_COMPLEX"
+        kernel = select_optimized_kernel(m, n, k, policy)
+        if kernel == GemmDispatch.Kernel.CUDA:
+            if CudaGemm.gemm(a, b, c, alpha, beta, precision=prec):
+                return "CUDA"
+            kernel = GemmDispatch.Kernel.MICROKERNEL
+        cpu(kernel.value, a, b, c, alpha, beta, policy)
+        if isinstance(c, OffHeapMatrix):
+            c.syncToOffHeap()
+        return kernel.value
 
     @staticmethod
     def gemmStrided(a, aOffset, lda, b, bOffset, ldb, c, cOffset, ldc, m, k, n, alpha, beta,
@@ -514,9 +540,14 @@ class OptimizedBLAS3:
 class BLAS3Kernels:
     @staticmethod
     def gemm(a: Matrix, b: Matrix, c_or_policy=None, alpha: float = 1.0, beta: float = 0.0,
-             policy: DispatchPolicy | None = None):
+             policy: DispatchPolicy | None = None, cpu=None):
         """BLAS3Kernels.gemm: ``gemm(a, b[, policy]) -> Matrix`` (BLAS3Kernels.java:35-63) or
-        ``gemm(a, b, c, alpha, beta, policy)`` in place (BLAS3Kernels.java:75-139)."""
+        ``gemm(a, b, c, alpha, beta, policy)`` in place (BLAS3Kernels.java:75-139).
+
+        The in-place form without ``cpu`` is the GPU route for every size; with
+        ``cpu`` it routes as the reference does (the policy's CUDA thresholds,
+        CPU algorithms run as ``cpu(name, a, b, c, alpha, beta, policy)``) and
+        returns the algorithm name run."""
         if c_or_policy is None or isinstance(c_or_policy, DispatchPolicy):
             if a is None or b is None:
                 raise IllegalArgumentException("Matrices must not be null")
@@ -530,6 +561,19 @@ class BLAS3Kernels:
             _gpu_gemm(a, b, c, 1.0, 0.0, prec, None)
             return c
         prec = policy.precision if policy is not None else L.JLC_PREC_NATIVE
+        if cpu is not None:
+            # the reference's routing (BLAS3Kernels.java:91-101): CUDA when
+            # the policy offloads and CudaGemm accepts, else the CPU algorithm
+            c = c_or_policy
+            m, k, n = _validate_gemm(a, b, c)
+            active = policy or DispatchPolicy.defaultPolicy()
+            algorithm = active.selectForMultiply(m, n, k)
+            if algorithm == DispatchPolicy.Algorithm.CUDA:
+                if CudaGemm.gemm(a, b, c, alpha, beta, precision=active.precision):
+                    return "CUDA"
+                algorithm = active.selectCpuAlgorithm(m, n, k)
+            cpu(algorithm.value, a, b, c, alpha, beta, active)
+            return algorithm.value
         _gpu_gemm(a, b, c_or_policy, alpha, beta, prec, None)
         return None
 

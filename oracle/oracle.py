@@ -367,6 +367,91 @@ def sample_entries(m: int, n: int, count: int, seed: int):
     return np.concatenate([r, np.array(extra_r, np.int64)]), np.concatenate([c, np.array(extra_c, np.int64)])
 
 
+# ------------------------------------------------------------- Ozaki accuracy certificate
+# The reference has no split-precision route; this restates the library's own
+# certificate (a bound on the rounding error of the INT8 routes, jlc_b200/csrc/ozaki.cu)
+# so that the tests can check the figure the device reports.  Exact integer
+# and FP64 arithmetic here, where the device rounds its floats outward.
+MODULI = [256, 255, 253, 251, 247, 241, 239, 233, 229, 227, 223, 211, 199, 197, 193]
+
+
+def crt_pq(nmod: int, k: int):
+    """Operand scales (p, q) of the residue scheme for N moduli: p + q is the
+    largest integer with M > 2 k 2^(p+q), capped at 102."""
+    logm = sum(math.log2(x) for x in MODULI[:nmod])
+    b = int(math.floor(logm - math.log2(2.0 * max(k, 1)) - 1e-9))
+    b = min(b, 102)
+    return b // 2, b - b // 2
+
+
+def auto_moduli(k: int) -> int:
+    rhs = 2.0 * 2.0 ** -53 * k / 16.0
+    for nm in range(2, 16):
+        p, q = crt_pq(nm, k)
+        if 2.0 ** -min(p, q) <= rhs:
+            return nm
+    return 15
+
+
+def auto_slices(k: int) -> int:
+    rhs = 2.0 * 2.0 ** -53 * k / 16.0
+    for s in range(5, 9):
+        if (s + 3) * 2.0 ** (-7 * s) <= rhs:
+            return s
+    return 8
+
+
+def cert_coeffs(crt: bool, count: int, k: int):
+    """Per-level coefficients (c0, c1, c2) of est = c0 X + c1 Y + c2 Z + 6/k,
+    X, Y, Z in units of the 7-bit magnitude product."""
+    unit = 16384.0 / (2.0 * k * 2.0 ** -53)
+    if crt:
+        p, q = crt_pq(count, k)
+        h, g = 2.0 ** -(p + 1), 2.0 ** -(q + 1)
+        return h * unit, g * unit, k * h * g * unit
+    t = 2.0 ** (-7 * count)
+    return t * unit, t * unit, k * count * t * unit
+
+
+def _pow2_scale(x, axis):
+    mx = np.max(np.abs(x), axis=axis)
+    e = np.frexp(mx)[1].astype(np.int64)
+    e[mx == 0] = 0
+    return np.ldexp(x, -(e[:, None] if axis == 1 else e[None, :]))
+
+
+def ozaki_certificate(a_op, b_op, crt: bool, count: int):
+    """Certified ratio |err| / FP64 bound of the INT8 route at one count.
+
+    Rows of op(A) and columns of op(B) are scaled by the power of two of their
+    maximum; q = floor(|scaled| * 128) gives lb = q_A q_B <= 2^14 |A||B|
+    (scaled); with the scaled norms l1, X = max l1b_j / lb_ij, Y = max l1a_i /
+    lb_ij, Z = max 1 / lb_ij over rows and columns that are not all zero.
+    Returns (est, X, Y, Z)."""
+    a_op = np.asarray(a_op, dtype=np.float64)
+    b_op = np.asarray(b_op, dtype=np.float64)
+    k = a_op.shape[1]
+    ah = _pow2_scale(a_op, 1)
+    bh = _pow2_scale(b_op, 0)
+    qa = np.floor(np.abs(ah) * 128.0)
+    qb = np.floor(np.abs(bh) * 128.0)
+    lb = qa @ qb  # integers below 2^53: exact
+    l1a = np.sum(np.abs(ah), axis=1)
+    l1b = np.sum(np.abs(bh), axis=0)
+    valid = (l1a[:, None] > 0) & (l1b[None, :] > 0)
+    with np.errstate(divide="ignore"):
+        rinv = np.where(lb > 0, 1.0 / np.where(lb > 0, lb, 1.0), np.inf)
+    if not valid.any():
+        X = Y = Z = 0.0
+    else:
+        X = float(np.max(np.where(valid, l1b[None, :] * rinv, 0.0)))
+        Y = float(np.max(np.where(valid, l1a[:, None] * rinv, 0.0)))
+        Z = float(np.max(np.where(valid, rinv, 0.0)))
+    c = cert_coeffs(crt, count, k)
+    est = c[0] * X + c[1] * Y + c[2] * Z + 6.0 / k
+    return est, X, Y, Z
+
+
 # ------------------------------------------------------------- blocked Householder QR
 def householder_qr_blocked(a, block: int = 64):
     """HouseholderQR.factorizeBlocked (HouseholderQR.java:133-210) restated on a
