@@ -72,6 +72,64 @@ def test_static_entry_matches_regular_entry_on_two_calls(ctx, oracle):
         assert_fp64_bound(f"static entry {m}x{n}x{k}", got, A, B, C, alpha, beta)
 
 
+def _regular(ctx, la, lb, m, n, k, alpha, da, lda, db, ldb, beta, dc, slices):
+    ctx.ozaki_device(la, lb, m, n, k, alpha, da.data_ptr(), lda, db.data_ptr(), ldb, beta, dc.data_ptr(), n, slices)
+    ctx.synchronize()
+
+
+def test_static_entry_edge_routes(ctx, oracle):
+    """Routes the regular entry takes besides the INT8 one, through the static
+    entry: k = 4 (no slice count reaches the FP64 bound: the FP64 kernel),
+    single rows and columns of C (the matrix-vector kernel), a NaN operand
+    without a status word (the FP64 kernel behind the split, its flags in the
+    array) followed by a finite call (flags cleared), and a product that fits
+    only with fewer persistent CTAs."""
+    import torch
+    import jlc_b200
+    lib = jlc_b200.load()
+    stream = torch.cuda.current_stream()
+    cases = [
+        # (m, n, k, slices, seed, poison)
+        (96, 80, 4, 0, 31, False),
+        (1, 300, 77, 0, 33, False),
+        (300, 1, 77, 7, 35, False),
+        (130, 140, 150, 0, 37, True),
+        (130, 140, 150, 0, 39, False),
+        (1400, 1400, 1400, 7, 41, False),
+    ]
+    for (m, n, k, s, seed, poison) in cases:
+        A = oracle.uniform((m, k), seed)
+        B = oracle.uniform((k, n), seed + 1)
+        if poison:
+            A[3, 5] = np.nan
+        da = torch.from_numpy(A).cuda()
+        db = torch.from_numpy(B).cuda()
+        c_static = torch.zeros((m, n), dtype=torch.float64, device="cuda")
+        c_regular = torch.zeros((m, n), dtype=torch.float64, device="cuda")
+        err = ctypes.create_string_buffer(256)
+        rc = lib.jlc_dgemm_ozaki_static(0, 0, m, n, k, 1.0, da.data_ptr(), k, db.data_ptr(), n, 0.0,
+                                        c_static.data_ptr(), n, s, ctypes.c_void_p(stream.cuda_stream), None, err,
+                                        len(err))
+        assert rc == 0, err.value
+        stream.synchronize()
+        _regular(ctx, 0, 0, m, n, k, 1.0, da, k, db, n, 0.0, c_regular, s)
+        got, want = c_static.cpu().numpy(), c_regular.cpu().numpy()
+        if poison:
+            np.testing.assert_array_equal(np.isnan(got), np.isnan(want))
+            fin = np.isfinite(want)
+            np.testing.assert_array_equal(got[fin], want[fin])
+            continue
+        if m * n > 100000:
+            rows, cols = oracle.sample_entries(m, n, 3000, seed)
+            _, bound = oracle.gemm_dd(A, B, None, 1.0, 0.0, rows=rows, cols=cols)
+            assert np.all(np.abs(got[rows, cols] - want[rows, cols]) <= bound)
+            assert_fp64_bound(f"static {m}x{n}x{k}", got, A, B, None, 1.0, 0.0, rows=rows, cols=cols)
+        else:
+            _, bound = oracle.gemm_dd(A, B, None, 1.0, 0.0)
+            assert np.all(np.abs(got - want) <= bound), f"static vs regular {m}x{n}x{k}"
+            assert_fp64_bound(f"static {m}x{n}x{k}", got, A, B, None, 1.0, 0.0)
+
+
 def test_static_entry_rejects_problems_beyond_its_scratch(ctx):
     import torch
     import jlc_b200
