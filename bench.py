@@ -236,7 +236,12 @@ def run_ours(args):
         dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=torch.device("cuda", local))
     torch.cuda.set_device(local)
     size = args.size
-    M = N = K = size
+    # One product of world*size rows: rank r computes its row block of C from
+    # the same rows of A and all of B (no collective on the data path)
+    from jlc_b200 import shard
+    global_m = world * size
+    r0, r1 = shard.partition_rows(global_m, world)[rank]
+    M, N, K = r1 - r0, size, size
     flops = 2.0 * M * N * K
 
     ctx = jlc_b200.Context(local)
@@ -245,9 +250,12 @@ def run_ours(args):
 
     peaks = ctx.measure_peaks()  # burst rates, short probes on a cool GPU
     g = torch.Generator(device="cuda")
-    g.manual_seed(20260604 + 7919 * rank)  # rank r owns row block r of the (world*size) x size product
     with torch.cuda.stream(stream):
+        # rows [r0, r1) of the one global A (seeded by the block's first row)
+        # and the same B on every rank
+        g.manual_seed(shard.block_seed(20260604, r0))
         A = torch.rand((M, K), dtype=torch.float64, device="cuda", generator=g) * 2 - 1
+        g.manual_seed(20260605)
         B = torch.rand((K, N), dtype=torch.float64, device="cuda", generator=g) * 2 - 1
         Cn = torch.zeros((M, N), dtype=torch.float64, device="cuda")
         Cs = torch.zeros((M, N), dtype=torch.float64, device="cuda")
@@ -372,10 +380,11 @@ def run_ours(args):
         "scaling": "weak",
         "vs_baseline": None,
         "dtype": "f64 (INT8 residue products, INT32 accumulation, exact integer CRT reconstruction)",
-        "data": "synthetic uniform[-1,1) (torch Philox, seed 20260604 + 7919*rank), device resident",
+        "data": "synthetic uniform[-1,1) (torch Philox; one global A seeded per row block, one B), device resident",
         "config": {"workload": f"DGEMM M=N=K={size}, alpha=1, beta=0, row-major A/B/C, FP64-accurate "
                                f"(default policy: Ozaki-INT8 residue scheme, {oz_rep['slices']} moduli)",
-                   "global_M": world * M, "N": N, "K": K, "parallelism": f"dp{world} (row blocks of C)",
+                   "global_M": global_m, "N": N, "K": K,
+                   "parallelism": f"dp{world} (row blocks of one product, shard.partition_rows; no collective)",
                    "l2": "inputs 1.5 GiB > 126 MB L2, no flush"},
         "gpu_launches": int(oz_launches),
         "clocks": clocks,

@@ -25,6 +25,12 @@ def partition_rows(m: int, world: int, align: int = 128):
     return out
 
 
+def block_seed(base: int, r0: int) -> int:
+    """Seed of the row block of a sharded input that starts at global row r0:
+    the blocks of one global matrix get distinct, reproducible streams."""
+    return (base * 1_000_003 + r0) % (2 ** 63)
+
+
 def local_block(rank: int, world: int, m: int, align: int = 128):
     return partition_rows(m, world, align)[rank]
 
