@@ -280,6 +280,7 @@ typedef struct jlc_problem {
 typedef struct jlc_grouped_plan jlc_grouped_plan;
 #define JLC_GROUPED_GRAPH 1    /* capture the launch into a CUDA graph; run replays it */
 #define JLC_GROUPED_AUTOTUNE 2 /* time the tile shapes of each shape class now and cache the choice */
+#define JLC_GROUPED_RESIDUE 4  /* Ozaki precision: run eligible problems on INT8 residue tiles (see below) */
 
 /* Replaces the reference's per-call loop over many small GEMMs (the TINY and
  * SMALL dispatch classes, GemmDispatch.java:76-106, and the blocked QR /
@@ -287,18 +288,26 @@ typedef struct jlc_grouped_plan jlc_grouped_plan;
  * BlockedHessenbergQR.java:277-345) with one persistent launch.  The plan
  * copies the problem table to the device; later runs reuse the same device
  * pointers (update the data in place and run again).  precision:
- * JLC_PREC_NATIVE / JLC_PREC_AUTO run FP64 tiles; JLC_PREC_OZAKI_CRT (and
- * JLC_PREC_OZAKI, served by the same residue scheme) run every problem on
- * INT8 residues with the per-call route's moduli, scales and exact
- * reconstruction, so each result is bitwise the per-call residue result;
- * problems that route would compute in FP64 (Inf/NaN operands, alpha == 0,
- * k == 0, m == 1 or n == 1, k < 32) run FP64 tiles. */
+ * JLC_PREC_NATIVE / JLC_PREC_AUTO run FP64 tiles.  JLC_PREC_OZAKI_CRT and
+ * JLC_PREC_OZAKI run FP64 tiles too unless flags has JLC_GROUPED_RESIDUE: a
+ * grouped launch carries no per-problem accuracy certificate (the per-call
+ * route does), the FP64 tiles meet the FP64 bound by construction, and at
+ * batched sizes they are the faster route.  With JLC_GROUPED_RESIDUE every
+ * eligible problem runs on INT8 residues with the per-call route's moduli
+ * for its k, scales and exact reconstruction (bitwise the per-call residue
+ * result at that count); problems that route would compute in FP64 (Inf/NaN
+ * operands, alpha == 0, k == 0, m == 1 or n == 1, k < 32) run FP64 tiles.
+ * That opt-in is not certified per problem: use it for inputs whose rows
+ * and columns are not skewed. */
 JLC_API int jlc_grouped_plan_create(jlc_ctx* ctx, const jlc_problem* probs, int64_t count, int precision, int flags,
                                     jlc_grouped_plan** out);
 /* enqueue one run on the context stream (graph replay when captured) */
 JLC_API int jlc_grouped_plan_run(jlc_grouped_plan* plan);
 JLC_API int jlc_grouped_plan_info(const jlc_grouped_plan* plan, int64_t* work_items, double* flops, int* tile_small,
                                   int* tile_large);
+/* how many (non-empty) problems of the plan run on INT8 residue tiles and
+ * how many on FP64 tiles (new) */
+JLC_API int jlc_grouped_plan_routes(const jlc_grouped_plan* plan, int64_t* int8_problems, int64_t* fp64_problems);
 JLC_API void jlc_grouped_plan_destroy(jlc_grouped_plan* plan);
 /* one-shot: plan, run, synchronise, destroy */
 JLC_API int jlc_dgemm_grouped_device(jlc_ctx* ctx, const jlc_problem* probs, int64_t count, int precision,

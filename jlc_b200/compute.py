@@ -155,10 +155,12 @@ class Context:
         return rep.as_dict()
 
     # -- grouped batches ---------------------------------------------------
-    def grouped_plan(self, problems, precision=L.JLC_PREC_NATIVE, graph=False, autotune=False) -> "GroupedPlan":
+    def grouped_plan(self, problems, precision=L.JLC_PREC_NATIVE, graph=False, autotune=False,
+                     residue=False) -> "GroupedPlan":
         """Plan one persistent launch over a list of problems (dicts or
-        Problem structs with device pointers)."""
-        return GroupedPlan(self, problems, precision, graph, autotune)
+        Problem structs with device pointers).  residue=True opts Ozaki
+        precision into the INT8 residue tiles (JLC_GROUPED_RESIDUE)."""
+        return GroupedPlan(self, problems, precision, graph, autotune, residue)
 
     def dgemm_grouped_device(self, problems, precision=L.JLC_PREC_NATIVE) -> dict:
         arr = _problem_array(problems)
@@ -276,10 +278,11 @@ def _problem_array(problems):
 class GroupedPlan:
     """jlc_grouped_plan: a reusable persistent launch over a fixed problem table."""
 
-    def __init__(self, ctx: Context, problems, precision, graph, autotune):
+    def __init__(self, ctx: Context, problems, precision, graph, autotune, residue=False):
         self.ctx = ctx
         self.problems = _problem_array(problems)
-        flags = (L.JLC_GROUPED_GRAPH if graph else 0) | (L.JLC_GROUPED_AUTOTUNE if autotune else 0)
+        flags = (L.JLC_GROUPED_GRAPH if graph else 0) | (L.JLC_GROUPED_AUTOTUNE if autotune else 0) | \
+            (L.JLC_GROUPED_RESIDUE if residue else 0)
         h = ctypes.c_void_p()
         ctx.check(ctx.lib.jlc_grouped_plan_create(ctx.h, self.problems, len(self.problems), int(precision), flags,
                                                   ctypes.byref(h)))
@@ -293,7 +296,10 @@ class GroupedPlan:
         ts, tl = ctypes.c_int(), ctypes.c_int()
         self.ctx.check(self.ctx.lib.jlc_grouped_plan_info(self.h, ctypes.byref(items), ctypes.byref(flops),
                                                           ctypes.byref(ts), ctypes.byref(tl)))
-        return {"work_items": items.value, "flops": flops.value, "tile_small": ts.value, "tile_large": tl.value}
+        n8, n64 = ctypes.c_int64(), ctypes.c_int64()
+        self.ctx.check(self.ctx.lib.jlc_grouped_plan_routes(self.h, ctypes.byref(n8), ctypes.byref(n64)))
+        return {"work_items": items.value, "flops": flops.value, "tile_small": ts.value, "tile_large": tl.value,
+                "int8_problems": n8.value, "fp64_problems": n64.value}
 
     def close(self):
         if getattr(self, "h", None):

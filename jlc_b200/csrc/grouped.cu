@@ -686,6 +686,7 @@ struct jlc_grouped_plan {
     int nitems = 0;
     int grid = 0;
     double flops = 0.0;
+    int64_t n_int8 = 0, n_fp64 = 0;  // problems on residue tiles / on FP64 tiles
     int cfg[2] = {32, 64};
     bool use_graph = false;
     cudaGraph_t graph = nullptr;
@@ -896,6 +897,8 @@ int build_oz_plan(jlc_grouped_plan* pl, const std::vector<jlc_problem>& probs) {
         // the residue scheme to reach the FP64 bound (k < 32) stay in FP64
         const bool active = p.k > 0 && p.alpha != 0.0 && p.m > 1 && p.n > 1 &&
                             ozaki_crt_est_ratio(ozaki_crt_auto_moduli(p.k), p.k) <= 1.0;
+        if (active) ++pl->n_int8;
+        else ++pl->n_fp64;
         if (active) {
             o.active = 1;
             o.nmod = ozaki_crt_auto_moduli(p.k);
@@ -1012,7 +1015,11 @@ int jlc_grouped_plan_create(jlc_ctx* ctx, const jlc_problem* probs, int64_t coun
     if (!pl) return JLC_E_OOM;
     pl->ctx = ctx;
     pl->count = count;
-    if (precision == JLC_PREC_OZAKI || precision == JLC_PREC_OZAKI_CRT) {
+    // Ozaki precision runs the FP64 tiles unless the plan opts into the
+    // residue tiles: a grouped launch has no per-problem accuracy
+    // certificate, the FP64 tiles meet the FP64 bound by construction, and at
+    // the batched sizes (k in the hundreds) they are also the faster route.
+    if ((precision == JLC_PREC_OZAKI || precision == JLC_PREC_OZAKI_CRT) && (flags & JLC_GROUPED_RESIDUE)) {
         // both Ozaki requests run the residue scheme (the slice scheme needs
         // s(s+1)/2 products where the residues need N)
         pl->oz = true;
@@ -1035,6 +1042,7 @@ int jlc_grouped_plan_create(jlc_ctx* ctx, const jlc_problem* probs, int64_t coun
     WorkList wl;
     build_work(v, pl->cfg, -1, wl);
     pl->flops = wl.flops;
+    for (const jlc_problem& p : v) pl->n_fp64 += (p.m > 0 && p.n > 0) ? 1 : 0;
     int rc = upload(pl, v, wl);
     if (rc) {
         free_plan_buffers(pl);
@@ -1066,6 +1074,13 @@ int jlc_grouped_plan_info(const jlc_grouped_plan* plan, int64_t* work_items, dou
     if (flops) *flops = plan->flops;
     if (tile_small) *tile_small = plan->cfg[0];
     if (tile_large) *tile_large = plan->cfg[1];
+    return JLC_OK;
+}
+
+int jlc_grouped_plan_routes(const jlc_grouped_plan* plan, int64_t* int8_problems, int64_t* fp64_problems) {
+    if (!plan) return JLC_E_ARG;
+    if (int8_problems) *int8_problems = plan->n_int8;
+    if (fp64_problems) *fp64_problems = plan->n_fp64;
     return JLC_OK;
 }
 

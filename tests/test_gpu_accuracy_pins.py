@@ -98,8 +98,8 @@ def test_automatic_count_at_headline_depth(ctx, oracle, mode, m, n, k):
     assert ratio <= rep["est_err_ratio"] <= 1.0
 
 
-@pytest.mark.parametrize("precision", [0, 3])
-def test_c4_generator_first_2000(ctx, oracle, precision):
+@pytest.mark.parametrize("precision,residue", [(0, False), (3, False), (3, True)])
+def test_c4_generator_first_2000(ctx, oracle, precision, residue):
     """The benchmark's batch generator (30 % tiny M=N=K in {2,3,4}, the rest
     log-uniform on [8, 512], alpha and beta uniform on [-2, 2]): its first
     2,000 problems through one grouped launch, 24 sampled entries per problem
@@ -129,8 +129,10 @@ def test_c4_generator_first_2000(ctx, oracle, precision):
     probs = [dict(m=m, n=n, k=k, layout_a=0, layout_b=0, lda=k, ldb=n, ldc=n, alpha=alpha, beta=beta,
                   a=base + 8 * pa, b=base + 8 * pb, c=base + 8 * pc)
              for (m, n, k, alpha, beta, A, B, C), (pa, pb, pc) in zip(host, offs)]
-    rep = ctx.dgemm_grouped_device(probs, precision=precision)
-    assert rep["kernel"] == 4
+    plan = ctx.grouped_plan(probs, precision=precision, residue=residue)
+    plan.run()
+    ctx.synchronize()
+    plan.close()
     res = arena.cpu().numpy()
     rng = np.random.default_rng(1401)
     for (m, n, k, alpha, beta, A, B, C), (pa, pb, pc) in zip(host, offs):
@@ -142,4 +144,4 @@ def test_c4_generator_first_2000(ctx, oracle, precision):
             cols = rng.integers(0, n, 24, dtype=np.int64)
         ref, bound = oracle.gemm_dd(A, B, C, alpha, beta, rows=rows, cols=cols)
         ratio, _ = oracle.max_err_ratio(got[rows, cols], ref, bound)
-        assert ratio <= 1.0, f"C4 problem {m}x{n}x{k} precision {precision}: |err|/bound {ratio:.3g}"
+        assert ratio <= 1.0, f"C4 problem {m}x{n}x{k} precision {precision} residue {residue}: {ratio:.3g}"

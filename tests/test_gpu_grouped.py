@@ -194,8 +194,12 @@ def test_grouped_ozaki_matches_per_call_route(ctx, oracle):
     alphas[3], betas[4], alphas[5] = 1.0, 0.0, 0.0
     probs, host, arena = make_batch(oracle, shapes, 23, alphas=alphas, betas=betas)
     before = arena.clone()
-    rep = ctx.dgemm_grouped_device(probs, precision=JLC_PREC_OZAKI_CRT)
-    assert rep["kernel"] == 4 and rep["precision"] == JLC_PREC_OZAKI_CRT
+    plan = ctx.grouped_plan(probs, precision=JLC_PREC_OZAKI_CRT, residue=True)
+    info = plan.info()
+    assert info["int8_problems"] == sum(1 for p in probs if p["m"] and p["n"] and _on_residues(p))
+    plan.run()
+    ctx.synchronize()
+    plan.close()
     want = _per_problem_ozaki(ctx, probs, before, arena.data_ptr())
     _assert_matches_per_call(probs, arena, want)
     check_batch(oracle, probs, host, arena, "grouped ozaki")
@@ -209,7 +213,7 @@ def test_grouped_ozaki_long_k_and_graph_replay(ctx, oracle):
     shapes = [(40, 36, 20000), (17, 70, 33000), (96, 96, 300), (3, 3, 3)]
     probs, host, arena = make_batch(oracle, shapes, 29, betas=[0.0, 0.5, -1.0, 0.0])
     before = arena.clone()
-    plan = ctx.grouped_plan(probs, precision=JLC_PREC_OZAKI, graph=True)
+    plan = ctx.grouped_plan(probs, precision=JLC_PREC_OZAKI, graph=True, residue=True)
     assert plan.info()["tile_small"] == 32
     plan.run()
     ctx.synchronize()
@@ -252,7 +256,10 @@ def test_grouped_ozaki_nonfinite_problem_takes_fp64(ctx, oracle):
     arena[off:off + 50 * 70] = torch.from_numpy(a_store.ravel())
     torch.cuda.synchronize()
     before = arena.clone()
-    ctx.dgemm_grouped_device(probs, precision=JLC_PREC_OZAKI_CRT)
+    plan = ctx.grouped_plan(probs, precision=JLC_PREC_OZAKI_CRT, residue=True)
+    plan.run()
+    ctx.synchronize()
+    plan.close()
     got = arena.cpu().numpy()
     want = _per_problem_ozaki(ctx, probs, before, arena.data_ptr()).cpu().numpy()
     flat_host = [(p, h) for p, h in zip(probs, host)]
@@ -267,3 +274,30 @@ def test_grouped_ozaki_nonfinite_problem_takes_fp64(ctx, oracle):
             np.testing.assert_allclose(g[fin], w[fin], rtol=0, atol=1e-12)
         else:
             np.testing.assert_array_equal(g, w)
+
+
+def test_grouped_ozaki_default_runs_fp64_tiles(ctx, oracle):
+    """Without the residue opt-in, Ozaki precision runs every problem on the
+    FP64 tiles (no per-problem certificate exists in a grouped launch): the
+    results are bitwise the native plan's and the routes say so."""
+    from jlc_b200 import JLC_PREC_NATIVE, JLC_PREC_OZAKI_CRT
+    rng = np.random.default_rng(41)
+    shapes = mixed_shapes(rng, 120) + [(64, 64, 600), (40, 36, 2500)]
+    probs, host, arena = make_batch(oracle, shapes, 43)
+    before = arena.clone()
+    plan = ctx.grouped_plan(probs, precision=JLC_PREC_OZAKI_CRT)
+    info = plan.info()
+    nonempty = sum(1 for p in probs if p["m"] and p["n"])
+    assert info["int8_problems"] == 0 and info["fp64_problems"] == nonempty
+    plan.run()
+    ctx.synchronize()
+    plan.close()
+    got = arena.clone()
+    arena.copy_(before)
+    rep = ctx.dgemm_grouped_device(probs, precision=JLC_PREC_NATIVE)
+    assert rep["precision"] == JLC_PREC_NATIVE
+    np.testing.assert_array_equal(got.cpu().numpy(), arena.cpu().numpy())
+    check_batch(oracle, probs, host, arena, "grouped ozaki default")
+    arena.copy_(before)
+    rep = ctx.dgemm_grouped_device(probs, precision=JLC_PREC_OZAKI_CRT)
+    assert rep["precision"] == JLC_PREC_NATIVE  # the precision actually used
