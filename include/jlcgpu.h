@@ -163,6 +163,20 @@ JLC_API int jlc_dgemm_ozaki_crt_device(jlc_ctx* ctx, int layout_a, int layout_b,
                                        double alpha, const double* a, int64_t lda, const double* b, int64_t ldb,
                                        double beta, double* c, int64_t ldc, int moduli, jlc_report* rep);
 
+/* Split-K of the FP64 kernel per shape class (GemmDispatch.computeBlockSizes,
+ * GemmDispatch.java:118-149, picks CPU blocking; this picks how many k parts
+ * a product's tiles are split into).  jlc_autotune_splitk times every legal
+ * factor (1..8, at least 256 k per part, at most 8 waves of work) for the
+ * class of an m x n x k product -- its tile count and k to a power of two --
+ * on this context's device, stores the fastest in the tuning cache
+ * ($JLCGPU_TUNE_CACHE, default ~/.cache/jlcgpu/grouped_tune.txt, shared with
+ * the grouped tuner) and returns it; later products of the class use it (the
+ * wave-balance rule otherwise).  jlc_splitk_choice reports the factor a
+ * product would use now.  A different factor sums k in different groups:
+ * results stay inside the FP64 bound but may change in the last bits. */
+JLC_API int jlc_autotune_splitk(jlc_ctx* ctx, int64_t m, int64_t n, int64_t k, int* split);
+JLC_API int jlc_splitk_choice(jlc_ctx* ctx, int64_t m, int64_t n, int64_t k, int* split);
+
 /* Reads and clears the context's device status word after synchronising:
  * JLC_OK, or JLC_E_TIMEOUT if a kernel gave up on a bounded wait. */
 JLC_API int jlc_device_status(jlc_ctx* ctx);

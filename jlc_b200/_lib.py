@@ -104,6 +104,8 @@ SIGNATURES = {
                                         _i, _REP]),
     "jlc_device_status": (_i, [_vp]),
     "jlc_set_wait_limit": (_i, [_vp, _d]),
+    "jlc_autotune_splitk": (_i, [_vp, _i64, _i64, _i64, ctypes.POINTER(_i)]),
+    "jlc_splitk_choice": (_i, [_vp, _i64, _i64, _i64, ctypes.POINTER(_i)]),
     "jlc_inject_fault": (_i, [_vp, _i, _i]),
     "jlc_set_profiling": (_i, [_vp, _i]),
     "jlc_profile_collect": (_i, [_vp, ctypes.POINTER(_i), ctypes.POINTER(_d), _i]),

@@ -134,6 +134,18 @@ class Context:
         self.check(rc)
         return rep.as_dict() if report else None
 
+    def autotune_splitk(self, m: int, n: int, k: int) -> int:
+        """Time the FP64 kernel's split-K factors for the shape class of an
+        m x n x k product; the fastest is cached and used from now on."""
+        v = ctypes.c_int()
+        self.check(self.lib.jlc_autotune_splitk(self.h, m, n, k, ctypes.byref(v)))
+        return v.value
+
+    def splitk_choice(self, m: int, n: int, k: int) -> int:
+        v = ctypes.c_int()
+        self.check(self.lib.jlc_splitk_choice(self.h, m, n, k, ctypes.byref(v)))
+        return v.value
+
     def set_wait_limit(self, seconds: float):
         """Limit of every bounded device wait of this context's kernels (0: default 4 s)."""
         self.check(self.lib.jlc_set_wait_limit(self.h, float(seconds)))

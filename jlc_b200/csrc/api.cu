@@ -816,6 +816,61 @@ int jlc_set_wait_limit(jlc_ctx* ctx, double seconds) {
     return e == cudaSuccess ? JLC_OK : cuda_err(ctx, e, "wait limit");
 }
 
+int jlc_splitk_choice(jlc_ctx* ctx, int64_t m, int64_t n, int64_t k, int* split) {
+    if (!ctx || !split || m < 1 || n < 1 || k < 1) return set_err(ctx, JLC_E_ARG, "splitk_choice: bad arguments");
+    *split = dmma_splitk(m, n, k, ctx->sm_count);
+    return JLC_OK;
+}
+
+int jlc_autotune_splitk(jlc_ctx* ctx, int64_t m, int64_t n, int64_t k, int* split) {
+    if (!ctx || !split || m < 2 || n < 2 || k < 1 || m > (1 << 20) || n > (1 << 20) || k > (1 << 20))
+        return set_err(ctx, JLC_E_ARG, "autotune_splitk: bad arguments");
+    cudaSetDevice(ctx->device);
+    const long long tiles = ((m + 127) / 128) * ((n + 127) / 128), kbl = (k + 15) / 16;
+    const long long lda = round_up(k, 8), ldb = round_up(n, 8), ldc = n;
+    int rc = reserve(ctx, ctx->bufA, (size_t)(m * lda) * 8, "autotune A");
+    if (!rc) rc = reserve(ctx, ctx->bufB, (size_t)(k * ldb) * 8, "autotune B");
+    if (!rc) rc = reserve(ctx, ctx->bufC, (size_t)(m * ldc) * 8, "autotune C");
+    if (rc) return rc;
+    // the kernel's time does not depend on the values: zeros will do
+    cudaMemsetAsync(ctx->bufA.ptr, 0, (size_t)(m * lda) * 8, ctx->stream);
+    cudaMemsetAsync(ctx->bufB.ptr, 0, (size_t)(k * ldb) * 8, ctx->stream);
+    GemmDesc g{JLC_ROW_MAJOR, JLC_ROW_MAJOR, m, n, k, 1.0, 0.0, (const double*)ctx->bufA.ptr, lda,
+               (const double*)ctx->bufB.ptr, ldb, (double*)ctx->bufC.ptr, ldc};
+    int best = 1;
+    float best_ms = 0.f;
+    for (int s = 1; s <= 8; ++s) {
+        if (!dmma_splitk_legal(tiles, kbl, s, ctx->sm_count)) continue;
+        const size_t wsb = dmma_splitk_bytes(m, n, s);
+        if (wsb && (rc = ws_reserve(ctx, wsb))) return rc;
+        float ms_min = 0.f;
+        for (int rep = 0; rep < 4; ++rep) {  // one warm-up, three timed
+            cudaEventRecord(ctx->ev0, ctx->stream);
+            rc = launch_dgemm_dmma(g, ctx->stream, ctx->sm_count, ctx->d_status, nullptr, ctx->dmma_k, ctx->err,
+                                   sizeof(ctx->err), s, wsb ? ctx->ws.ptr : nullptr, wsb);
+            if (rc) return rc;
+            cudaEventRecord(ctx->ev1, ctx->stream);
+            cudaError_t e = cudaEventSynchronize(ctx->ev1);
+            if (e != cudaSuccess) return cuda_err(ctx, e, "autotune");
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
+            if (rep == 1 || (rep > 1 && ms < ms_min)) ms_min = ms;
+        }
+        ctx->launches += 4;
+        if (s == 1 || ms_min < best_ms) {
+            best = s;
+            best_ms = ms_min;
+        }
+    }
+    rc = finish_sync(ctx);
+    if (rc) return rc;
+    const std::string cls = dmma_splitk_class(ctx->sm_count, tiles, kbl);
+    grp::tune_store(cls, best);
+    dmma_splitk_remember(cls, best);
+    *split = best;
+    return JLC_OK;
+}
+
 int jlc_inject_fault(jlc_ctx* ctx, int kind, int after) {
     if (!ctx) return JLC_E_ARG;
     if (kind < JLC_FAULT_NONE || kind > JLC_FAULT_WAIT || after < 0)

@@ -34,9 +34,13 @@
 // 128B swizzle pattern; A and B use the same map, so the sum is unchanged and
 // every fragment load is bank-conflict free.
 #include <cstdio>
+#include <map>
+#include <mutex>
+#include <string>
 
 #include "jlc_device.cuh"
 #include "jlc_dmma.cuh"
+
 #include "jlc_internal.h"
 
 namespace jlc {
@@ -372,15 +376,52 @@ bool dmma_operand_ok(const void* ptr, long long ld) {
     return (reinterpret_cast<uintptr_t>(ptr) % 16 == 0) && ((ld * 8) % 16 == 0) && ld > 0;
 }
 
-// k parts per tile for an m x n x k product (1: no split).  A row block of a
-// pipelined product passes the whole product's m, so that every block sums
-// in the same order as the single-shot call.
+// Split factors a product may use: at least 16 k-blocks (256 k) per part and
+// at most 8 waves of work units over the persistent grid.
+bool dmma_splitk_legal(long long tiles, long long kbl, int s, int sm_count) {
+    return s == 1 || (s >= 2 && s <= 8 && kbl / s >= 16 && tiles * s <= 8LL * sm_count);
+}
+
+// Shape class of the split-K tuner: the exact tile count (what the wave
+// balance depends on) and the k-block count to a power of two.
+std::string dmma_splitk_class(int sm_count, long long tiles, long long kbl) {
+    int lg = 0;
+    while ((2LL << lg) <= kbl) ++lg;
+    return "sm" + std::to_string(sm_count) + "|v" + std::to_string(JLCGPU_VERSION) + "|dmma-splitk|t" +
+           std::to_string(tiles) + "|kb" + std::to_string(lg);
+}
+
+namespace {
+// tuned split factors by class, read from the tuning cache once per class
+std::mutex g_split_mu;
+std::map<std::string, int> g_split_table;
+}  // namespace
+
+void dmma_splitk_remember(const std::string& cls, int s) {
+    std::lock_guard<std::mutex> lock(g_split_mu);
+    g_split_table[cls] = s;
+}
+
+int dmma_splitk_tuned(int sm_count, long long tiles, long long kbl) {
+    const std::string cls = dmma_splitk_class(sm_count, tiles, kbl);
+    std::lock_guard<std::mutex> lock(g_split_mu);
+    auto it = g_split_table.find(cls);
+    if (it == g_split_table.end()) it = g_split_table.emplace(cls, grp::tune_lookup(cls)).first;
+    return it->second;
+}
+
+// k parts per tile for an m x n x k product (1: no split): the tuner's choice
+// for the shape class when one is cached, else the wave-balance rule.  A row
+// block of a pipelined product passes the whole product's m, so that every
+// block sums in the same order as the single-shot call.
 int dmma_splitk(long long m, long long n, long long k, int sm_count) {
     using namespace dmma;
     const long long tiles = ((m + BM - 1) / BM) * ((n + BN - 1) / BN);
     const long long kbl = (k + BK - 1) / BK;
+    const int tuned = dmma_splitk_tuned(sm_count, tiles, kbl);
+    if (tuned > 0 && dmma_splitk_legal(tiles, kbl, tuned, sm_count)) return tuned;
     // wave balance of the persistent grid: units / (waves * SMs); a split must
-    // gain 5 % of it, keep >= 16 k-blocks (256 k) per part and <= 8 waves
+    // gain 5 % of it
     auto balance = [&](long long units) {
         const long long waves = (units + sm_count - 1) / sm_count;
         return (double)units / (double)(waves * sm_count);
@@ -388,7 +429,7 @@ int dmma_splitk(long long m, long long n, long long k, int sm_count) {
     int best = 1;
     double best_b = balance(tiles);
     for (int s = 2; s <= 8; ++s) {
-        if (kbl / s < 16 || tiles * s > 8LL * sm_count) break;
+        if (!dmma_splitk_legal(tiles, kbl, s, sm_count)) break;
         const double b = balance(tiles * s);
         if (b > best_b * 1.05) {
             best = s;

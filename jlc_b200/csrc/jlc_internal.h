@@ -6,6 +6,7 @@
 
 #include <cstddef>
 #include <cstdint>
+#include <string>
 
 #include "jlc_errors.h"
 #include "jlcgpu.h"
@@ -87,6 +88,17 @@ int launch_dgemm_dmma(const GemmDesc& g, cudaStream_t st, int sm_count, int* sta
                       char* err, size_t errlen, int ksplit = 1, void* splitk_ws = nullptr,
                       size_t splitk_ws_bytes = 0);
 int dmma_splitk(long long m, long long n, long long k, int sm_count);
+// split-K tuning (dgemm_dmma.cu): legal factors, the shape class, and the
+// tuned factor of a class (0: none cached); remember() records a new choice
+bool dmma_splitk_legal(long long tiles, long long kbl, int s, int sm_count);
+std::string dmma_splitk_class(int sm_count, long long tiles, long long kbl);
+int dmma_splitk_tuned(int sm_count, long long tiles, long long kbl);
+void dmma_splitk_remember(const std::string& cls, int s);
+// the tuning cache file shared by the tuners ($JLCGPU_TUNE_CACHE)
+namespace grp {
+int tune_lookup(const std::string& key);
+void tune_store(const std::string& key, int value);
+}  // namespace grp
 size_t dmma_splitk_bytes(long long m, long long n, int ksplit);
 
 // y[i*incy] = alpha * sum_p M(i,p) x[p*incx] + beta * y[i*incy], M(i,p) = mat[i*rs + p*cs]

@@ -358,3 +358,31 @@ def test_split_k_small_products(ctx, oracle, m, n, k, alpha, beta):
     host = C.copy()
     ctx.dgemm(0, 0, m, n, k, alpha, A, k, B, n, beta, host, n, precision=0)
     np.testing.assert_array_equal(host, runs[0])
+
+
+def test_splitk_autotune_caches_and_is_used(ctx, oracle, tmp_path, monkeypatch):
+    """The split-K tuner (the per-shape-class counterpart of
+    GemmDispatch.computeBlockSizes, GemmDispatch.java:118-149): it times the
+    legal factors for a class, stores the fastest in the tuning cache, and
+    products of that class use it from then on, inside the FP64 bound and
+    bitwise repeatable."""
+    import torch
+    monkeypatch.setenv("JLCGPU_TUNE_CACHE", str(tmp_path / "tune.txt"))
+    m, n, k = 640, 512, 2048  # 20 tiles: split-K matters
+    s = ctx.autotune_splitk(m, n, k)
+    assert 1 <= s <= 8
+    text = (tmp_path / "tune.txt").read_text()
+    assert "dmma-splitk|t20|kb7" in text and text.strip().endswith(str(s))
+    assert ctx.splitk_choice(m, n, k) == s
+    assert ctx.splitk_choice(m, n, k + 100) == s  # same class (k to a power of two)
+    A = oracle.uniform((m, k), 1601)
+    B = oracle.uniform((k, n), 1602)
+    dA, dB = torch.from_numpy(A).cuda(), torch.from_numpy(B).cuda()
+    outs = []
+    for _ in range(2):
+        dC = torch.zeros((m, n), dtype=torch.float64, device="cuda")
+        ctx.dgemm_device(0, 0, m, n, k, 1.0, dA.data_ptr(), k, dB.data_ptr(), n, 0.0, dC.data_ptr(), n)
+        ctx.synchronize()
+        outs.append(dC.cpu().numpy())
+    np.testing.assert_array_equal(outs[0], outs[1])
+    assert_fp64_bound("tuned split-K", outs[0], A, B, None, 1.0, 0.0)
