@@ -41,10 +41,12 @@ def parse():
     p.add_argument("--cpu-seconds", type=float, default=12.0, help="target length of one CPU baseline sample")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu-baseline", action="store_true")
-    p.add_argument("--workload", default="dgemm", choices=["dgemm", "grouped", "configs", "harness", "qr"],
+    p.add_argument("--workload", default="dgemm", choices=["dgemm", "grouped", "configs", "harness", "qr", "shape"],
                    help="dgemm: the 8192^3 headline; grouped: 20,000 uneven problems in one launch; "
                         "configs: one line per C1-C5 shape (rate and accuracy), one GPU")
     p.add_argument("--count", type=int, default=20000, help="grouped workload: number of problems")
+    p.add_argument("--mnk", default="16384,1,16384", help="shape workload: m,n,k of one device product")
+    p.add_argument("--precision", type=int, default=0, help="shape workload: JLC_PREC_* of the product")
     p.add_argument("--sizes", default="128,256,512", help="harness workload: square sizes")
     p.add_argument("--iters", type=int, default=25, help="harness workload: timed iterations per backend")
     p.add_argument("--warmups", type=int, default=8, help="harness workload: warm-up iterations per backend")
@@ -363,6 +365,7 @@ def run_ours(args):
     P = oz_rep["products"]
     gemm_ms = statistics.mean(oz_phases.get("ozaki_gemm", [float("nan")]))
     split_ms = statistics.mean(oz_phases.get("ozaki_split", [float("nan")]))
+    cert_ms = statistics.mean(oz_phases.get("ozaki_cert", [float("nan")]))
     dmma_ms = statistics.mean(nat_phases.get("dmma", [float("nan")]))
     int8_ops_per_launch = 2.0 * M * N * K * P
     achieved_tops = int8_ops_per_launch / (gemm_ms * 1e-3) / 1e12
@@ -395,8 +398,8 @@ def run_ours(args):
                         "frac_of_dmma_peak": round(flops / (dmma_ms * 1e-3) / 1e12 / peaks["fp64_dmma_tflops"], 4),
                         "gpu_launches": int(nat_launches)},
         "ozaki": {"scheme": "residues (CRT)", "moduli": oz_rep["slices"], "products": P,
-                  "est_err_ratio": oz_rep["est_err_ratio"],
-                  "split_ms": round(split_ms, 3), "gemm_ms": round(gemm_ms, 3),
+                  "certified_err_ratio": oz_rep["est_err_ratio"],
+                  "split_ms": round(split_ms, 3), "cert_ms": round(cert_ms, 3), "gemm_ms": round(gemm_ms, 3),
                   "speedup_vs_native": round(oz_gflops / nat_gflops, 3)},
         "ozaki_slices": {"value": round(world * sl_gflops, 1), "unit": "GFLOP/s", "ms_per_step": round(sl_ms, 3),
                          "slices": sl_rep["slices"], "products": sl_rep["products"],
@@ -912,6 +915,48 @@ def run_harness(args):
     return 1 if any(r["parity_status"] == "FAIL" for r in rows) else 0
 
 
+def run_shape(args):
+    """One device product of the given shape and precision, timed (the case an
+    ncu capture of a single kernel runs: few launches before the timed ones)."""
+    import torch
+    import jlc_b200
+    m, n, k = (int(x) for x in args.mnk.split(","))
+    torch.cuda.set_device(0)
+    ctx = jlc_b200.Context(0)
+    stream = torch.cuda.Stream()
+    ctx.set_stream(stream.cuda_stream)
+    g = torch.Generator(device="cuda")
+    g.manual_seed(20260604)
+    with torch.cuda.stream(stream):
+        A = torch.rand((m, k), dtype=torch.float64, device="cuda", generator=g) * 2 - 1
+        B = torch.rand((k, n), dtype=torch.float64, device="cuda", generator=g) * 2 - 1
+        C = torch.zeros((m, n), dtype=torch.float64, device="cuda")
+    stream.synchronize()
+
+    def call(report=False):
+        return ctx.dgemm_device(0, 0, m, n, k, 1.0, A.data_ptr(), k, B.data_ptr(), n, 0.0, C.data_ptr(), n,
+                                precision=args.precision, report=report)
+
+    rep = call(report=True)
+    for _ in range(args.warmup - 1):
+        call()
+    ctx.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        call()
+    e1.record(stream)
+    e1.synchronize()
+    ms = e0.elapsed_time(e1) / args.steps
+    nbytes = 8.0 * (m * k + k * n + m * n)
+    print(json.dumps({"workload": "shape", "m": m, "n": n, "k": k, "precision": args.precision,
+                      "kernel": rep["kernel"], "ms": round(ms, 4),
+                      "gflops": round(2.0 * m * n * k / (ms * 1e-3) / 1e9, 1),
+                      "gbs_algorithmic": round(nbytes / (ms * 1e-3) / 1e9, 1)}), flush=True)
+    ctx.close()
+    return 0
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -922,6 +967,8 @@ def main():
         return run_configs(args)
     if args.workload == "harness":
         return run_harness(args)
+    if args.workload == "shape":
+        return run_shape(args)
     if args.workload == "qr":
         return run_qr(args)
     return run_ours(args)
