@@ -223,6 +223,7 @@ JLC_API int jlc_inject_fault(jlc_ctx* ctx, int kind, int after);
 #define JLC_PHASE_REDUCE 11     /* adjoint reductions: d(alpha) / d(beta) dots and sums, scaled copies */
 #define JLC_PHASE_QR_PANEL 12   /* blocked QR: one panel's factorisation kernel */
 #define JLC_PHASE_QR_VT 13      /* blocked QR: V packing and the T factor (the Gram GEMM is a dmma phase) */
+#define JLC_PHASE_HESS_PANEL 17     /* Hessenberg: one panel's reflectors (column, GEMV, Y updates) */
 #define JLC_PHASE_OZAKI_CERT 14     /* Ozaki accuracy certificate (magnitude product, route decision) */
 #define JLC_PHASE_OZAKI_SPLIT_HI 15 /* split at the higher count (runs only when the certificate picks it) */
 #define JLC_PHASE_OZAKI_GEMM_HI 16  /* INT8 GEMM at the higher count (likewise) */
@@ -344,6 +345,19 @@ JLC_API int jlc_qr_factor_device(jlc_ctx* ctx, int64_t m, int64_t n, double* a, 
  * HouseholderQR.java:387-441), blocked with the same WY form. */
 JLC_API int jlc_qr_build_q_device(jlc_ctx* ctx, int64_t m, int64_t n, int64_t qcols, const double* f, int64_t ldf,
                                   const double* tau, double* q, int64_t ldq, int precision, jlc_report* rep);
+
+/* ---------------------------------------------------------------- Hessenberg reduction (device) */
+/* Reduces the column-major n x n matrix A (lda >= n) on the device, in place,
+ * to upper Hessenberg form H with A = Q H Q^T, as
+ * BlockedHessenbergQR.decompose does (eigen/qr/BlockedHessenbergQR.java:99-146):
+ * panels of 32 columns, the reference's reflectors (its 1e-12 skips
+ * included), each panel's block reflector applied with W = V^T H, W = T^T W,
+ * H -= V W from the left and W = H V, W = W T, H -= W V^T from the right
+ * (:277-345) on the GEMM route, entries below the first subdiagonal cleared.
+ * q (column-major, ldq >= n), when not NULL, receives Q.  precision applies
+ * to the block-update GEMMs.  New: the reference runs this on the CPU only. */
+JLC_API int jlc_hessenberg_device(jlc_ctx* ctx, int64_t n, double* a, int64_t lda, double* q, int64_t ldq,
+                                  int precision, jlc_report* rep);
 
 /* ---------------------------------------------------------------- allocation-free entry */
 /* Ozaki-INT8 DGEMM on DEVICE pointers that allocates nothing: no context, no

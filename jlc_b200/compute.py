@@ -257,6 +257,14 @@ class Context:
                                                  ctypes.byref(rep)))
         return rep.as_dict()
 
+    def hessenberg_device(self, n, a_ptr, lda, q_ptr, ldq, precision=L.JLC_PREC_NATIVE) -> dict:
+        """Hessenberg reduction of the column-major n x n matrix at a_ptr, in
+        place; q_ptr (or None) receives Q with A = Q H Q^T."""
+        rep = L.Report()
+        self.check(self.lib.jlc_hessenberg_device(self.h, n, a_ptr, lda, q_ptr, ldq, int(precision),
+                                                  ctypes.byref(rep)))
+        return rep.as_dict()
+
     def qr_build_q_device(self, m, n, qcols, f_ptr, ldf, tau_ptr, q_ptr, ldq, precision=L.JLC_PREC_NATIVE) -> dict:
         """Q (column-major m x qcols) of a factorisation from qr_factor_device."""
         rep = L.Report()

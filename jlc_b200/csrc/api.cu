@@ -885,6 +885,7 @@ void jlc_destroy(jlc_ctx* ctx) {
     cudaSetDevice(ctx->device);
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
     if (ctx->bufA.ptr) cudaFree(ctx->bufA.ptr);
+    if (ctx->bufH.ptr) cudaFree(ctx->bufH.ptr);
     if (ctx->bufB.ptr) cudaFree(ctx->bufB.ptr);
     if (ctx->bufC.ptr) cudaFree(ctx->bufC.ptr);
     if (ctx->bufR.ptr) cudaFree(ctx->bufR.ptr);
@@ -1152,6 +1153,121 @@ int jlc_qr_factor_device(jlc_ctx* ctx, int64_t m, int64_t n, double* a, int64_t 
         if (rc) return rc;
     }
     cudaEventRecord(ctx->ev1, ctx->stream);
+    rc = finish_sync(ctx);
+    if (rc) return rc;
+    if (rep) {
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
+        rep->device_ms = ms;
+        rep->kernel = JLC_KERNEL_DMMA;
+    }
+    return JLC_OK;
+}
+
+// The block reflector of one Hessenberg panel applied as the reference does
+// (BlockedHessenbergQR.applyBlockLeft / applyBlockRight, :277-345), on
+// column-major matrices.  Left, rows r0.. and columns c0.. of h:
+// W = V^T C, W2 = T^T W, C -= V W2 (the last as C^T -= W2^T V^T).  Right,
+// columns r0.. (all rows) of mat: W = B V, W2 = W T, B -= W2 V^T (as
+// B^T -= V W2^T).
+constexpr int kHessPanel = 32;
+
+int hess_apply_left(jlc_ctx* ctx, double* h, long long ldh, long long n, long long k, int pw, const double* V,
+                    long long ldv, const double* T, double* W, double* W2, long long ldw, int precision) {
+    const long long m = n - k - 1, cols = n - k;
+    double* c = h + (k + 1) + k * ldh;
+    GemmDesc w{JLC_ROW_MAJOR, JLC_COL_MAJOR, pw, cols, m, 1.0, 0.0, V, ldv, c, ldh, W, ldw};
+    int rc = run_device(ctx, w, precision, 0, nullptr);
+    if (rc) return rc;
+    GemmDesc t{JLC_COL_MAJOR, JLC_ROW_MAJOR, pw, cols, pw, 1.0, 0.0, T, kHessPanel, W, ldw, W2, ldw};
+    rc = run_device(ctx, t, JLC_PREC_NATIVE, 0, nullptr);
+    if (rc) return rc;
+    GemmDesc u{JLC_COL_MAJOR, JLC_ROW_MAJOR, cols, m, pw, -1.0, 1.0, W2, ldw, V, ldv, c, ldh};
+    return run_device(ctx, u, precision, 0, nullptr);
+}
+
+int hess_apply_right(jlc_ctx* ctx, double* mat, long long ldm, long long n, long long k, int pw, const double* V,
+                     long long ldv, const double* T, double* W, double* W2, int precision) {
+    const long long m = n - k - 1;
+    double* b = mat + (k + 1) * ldm;
+    GemmDesc w{JLC_COL_MAJOR, JLC_COL_MAJOR, n, pw, m, 1.0, 0.0, b, ldm, V, ldv, W, kHessPanel};
+    int rc = run_device(ctx, w, precision, 0, nullptr);
+    if (rc) return rc;
+    GemmDesc t{JLC_ROW_MAJOR, JLC_ROW_MAJOR, n, pw, pw, 1.0, 0.0, W, kHessPanel, T, kHessPanel, W2, kHessPanel};
+    rc = run_device(ctx, t, JLC_PREC_NATIVE, 0, nullptr);
+    if (rc) return rc;
+    GemmDesc u{JLC_COL_MAJOR, JLC_COL_MAJOR, m, n, pw, -1.0, 1.0, V, ldv, W2, kHessPanel, b, ldm};
+    return run_device(ctx, u, precision, 0, nullptr);
+}
+
+int jlc_hessenberg_device(jlc_ctx* ctx, int64_t n, double* a, int64_t lda, double* q, int64_t ldq, int precision,
+                          jlc_report* rep) {
+    report_init(rep);
+    if (!ctx) return JLC_E_ARG;
+    if (n < 0) return set_err(ctx, JLC_E_ARG, "dimension must be non-negative");
+    if (n == 0) return JLC_OK;
+    if (!a || lda < n) return set_err(ctx, JLC_E_ARG, "A must not be null and lda must be >= n");
+    if (q && ldq < n) return set_err(ctx, JLC_E_ARG, "ldq must be >= n");
+    if (n > INT32_MAX / 4) return set_err(ctx, JLC_E_UNSUPPORTED, "dimension above 2^29");
+    cudaSetDevice(ctx->device);
+    ctx->err[0] = 0;
+    cudaStream_t st = ctx->stream;
+    cudaEventRecord(ctx->ev0, st);
+    int rc = JLC_OK;
+    if (q && (rc = launch_set_identity(q, ldq, n, n, st))) return set_err(ctx, rc, "Hessenberg: identity launch failed");
+    if (n > 2) {
+        const long long ldv = round_up(n, 8), ldw = ldv;
+        if ((rc = reserve(ctx, ctx->bufH, hess_work_doubles(n) * sizeof(double), "Hessenberg workspace"))) return rc;
+        double* V = static_cast<double*>(ctx->bufH.ptr);
+        double* Y = V + ldv * kHessPanel;
+        double* W = Y + ldv * kHessPanel;
+        double* W2 = W + ldv * kHessPanel;
+        double* T = W2 + ldv * kHessPanel;
+        double* tau = T + kHessPanel * kHessPanel;
+        double* sv = tau + kHessPanel;
+        double* wbuf = sv + kHessPanel;
+        // the GEMV's partial sums: at most 64 column chunks of at most n - 1
+        // rows for every trailing block (gemv.cu, axpy_split)
+        if ((rc = ws_reserve(ctx, (size_t)64 * (size_t)(n - 1) * sizeof(double)))) return rc;
+        for (long long k = 0; k < n - 2; k += kHessPanel) {
+            const int pw = (int)((n - 2 - k) < kHessPanel ? (n - 2 - k) : kHessPanel);
+            const long long m = n - k - 1, r0 = k + 1;
+            {
+                Phase ph(ctx, JLC_PHASE_HESS_PANEL);
+                if (cudaMemsetAsync(T, 0, kHessPanel * kHessPanel * sizeof(double), st) != cudaSuccess)
+                    return set_err(ctx, JLC_E_CUDA, "Hessenberg: T reset failed");
+                for (int j = 0; j < pw; ++j) {
+                    rc = launch_hess_reflector(a, lda, (int)n, (int)k, j, V, ldv, Y, T, tau, sv, wbuf, st);
+                    if (rc) return set_err(ctx, rc, "Hessenberg: reflector launch failed");
+                    // Y column j <- A[r0:, r0+j:] v_j[j:]
+                    GemvDesc v;
+                    v.rows = m;
+                    v.cols = m - j;
+                    v.mat = a + r0 + (r0 + j) * lda;
+                    v.rs = 1;
+                    v.cs = lda;
+                    v.x = V + j * ldv + j;
+                    v.incx = 1;
+                    v.y = Y + j * ldv;
+                    v.incy = 1;
+                    v.alpha = 1.0;
+                    v.beta = 0.0;
+                    rc = launch_gemv(v, ctx->ws.ptr, st, ctx->sm_count, ctx->err, sizeof(ctx->err));
+                    if (rc) return rc;
+                    rc = launch_hess_y_finish((int)m, j, Y, ldv, tau, sv, st);
+                    if (rc) return set_err(ctx, rc, "Hessenberg: Y launch failed");
+                    ctx->launches += 4;
+                }
+            }
+            rc = hess_apply_left(ctx, a, lda, n, k, pw, V, ldv, T, W, W2, ldw, precision);
+            if (!rc) rc = hess_apply_right(ctx, a, lda, n, k, pw, V, ldv, T, W, W2, precision);
+            if (!rc && q) rc = hess_apply_right(ctx, q, ldq, n, k, pw, V, ldv, T, W, W2, precision);
+            if (rc) return rc;
+        }
+        if ((rc = launch_hess_clear(a, lda, (int)n, st))) return set_err(ctx, rc, "Hessenberg: clear launch failed");
+        ctx->launches += 1;
+    }
+    cudaEventRecord(ctx->ev1, st);
     rc = finish_sync(ctx);
     if (rc) return rc;
     if (rep) {

@@ -84,6 +84,12 @@ int launch_qr_pack_v(const double* a, long long lda, int m, int k0, int kb, doub
                      cudaStream_t st);
 int launch_qr_build_t(const double* g, const double* tau, int kb, double* t, cudaStream_t st);
 int launch_set_identity(double* q, long long ldq, long long m, long long cols, cudaStream_t st);
+// blocked Hessenberg reduction kernels (hess.cu)
+size_t hess_work_doubles(long long n);
+int launch_hess_reflector(const double* h, long long ldh, int n, int k, int j, double* V, long long ldv,
+                          const double* Y, double* T, double* tau, double* s, double* wbuf, cudaStream_t st);
+int launch_hess_y_finish(int m, int j, double* Y, long long ldv, const double* tau, const double* s, cudaStream_t st);
+int launch_hess_clear(double* h, long long ldh, int n, cudaStream_t st);
 int launch_dgemm_dmma(const GemmDesc& g, cudaStream_t st, int sm_count, int* status, const int* gate, int mma_k,
                       char* err, size_t errlen, int ksplit = 1, void* splitk_ws = nullptr,
                       size_t splitk_ws_bytes = 0);
@@ -218,6 +224,7 @@ struct jlc_ctx {
     DevBuf bufA, bufB, bufC;
     DevBuf bufR;  // reduction partials (adjoint)
     DevBuf bufQ;  // blocked QR: V, G, T and the two W panels
+    DevBuf bufH;  // Hessenberg reduction: V, Y, T, tau, s, the column buffer and two W panels
     Workspace ws;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     // host-entry pipeline: copy-in and copy-out streams beside `stream`, and

@@ -1,4 +1,5 @@
-"""Host-side mirror of the reference's ``HouseholderQR`` on the device route.
+"""Host-side mirrors of the reference's ``HouseholderQR`` and
+``BlockedHessenbergQR`` on the device route.
 
 ``HouseholderQR.decompose`` / ``decomposeThin`` / ``factorize``
 (decomposition/qr/HouseholderQR.java:26-92) with the same arguments, results
@@ -98,3 +99,63 @@ class HouseholderQR:
         _check(a)
         if min(a.getRowCount(), a.getColumnCount()) > 0:
             _factor_on_device(a, ctx or default_context(), precision)
+
+
+class ArithmeticException(ArithmeticError):
+    """java.lang.ArithmeticException."""
+
+
+class HessenbergResult:
+    """decomposition/result/HessenbergResult.java: the input, H and Q with
+    A = Q H Q^T."""
+
+    def __init__(self, a: Matrix, h: Matrix, q: Matrix):
+        self._a, self._h, self._q = a, h, q
+
+    def getOriginal(self) -> Matrix:
+        return self._a
+
+    def getH(self) -> Matrix:
+        return self._h
+
+    def getQ(self) -> Matrix:
+        return self._q
+
+    def reconstruct(self) -> Matrix:
+        q, h = self._q.to_numpy(), self._h.to_numpy()
+        n = h.shape[0]
+        return Matrix.wrap(np.ascontiguousarray(q @ h @ q.T).ravel(), n, n)
+
+    def residualNorm(self) -> float:
+        a = self._a.to_numpy()
+        return float(np.linalg.norm(a - self.reconstruct().to_numpy()) / max(np.linalg.norm(a), 1e-300))
+
+
+class BlockedHessenbergQR:
+    """eigen/qr/BlockedHessenbergQR.java:99-146 on the device: the matrix goes
+    to the device once (column-major), jlc_hessenberg_device reduces it there
+    (panels, reflectors, block updates of H and Q), and H and Q come back."""
+
+    BLOCK_SIZE = 32
+
+    @staticmethod
+    def decompose(a: Matrix, ctx=None, precision: int = L.JLC_PREC_NATIVE) -> HessenbergResult:
+        if a is None:
+            raise IllegalArgumentException("Matrix must not be null")
+        if a.getRawImagData() is not None:
+            raise UnsupportedOperationException("Hessenberg reduction requires a real-valued matrix")
+        n = a.getRowCount()
+        if a.getColumnCount() != n:
+            raise ArithmeticException("Matrix must be square to compute Hessenberg form")
+        if n <= 2:
+            h = a.to_numpy().copy()
+            return HessenbergResult(a, Matrix.wrap(h.ravel(), n, n), Matrix.wrap(np.eye(n).ravel(), n, n))
+        import torch
+        ctx = ctx or default_context()
+        dev = torch.device("cuda", ctx.device)
+        ht = torch.from_numpy(np.ascontiguousarray(a.to_numpy().T)).to(dev)  # column-major H
+        qt = torch.empty((n, n), dtype=torch.float64, device=dev)
+        ctx.hessenberg_device(n, ht.data_ptr(), n, qt.data_ptr(), n, precision)
+        h = np.ascontiguousarray(ht.cpu().numpy().T)
+        q = np.ascontiguousarray(qt.cpu().numpy().T)
+        return HessenbergResult(a, Matrix.wrap(h.ravel(), n, n), Matrix.wrap(q.ravel(), n, n))
