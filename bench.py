@@ -41,7 +41,8 @@ def parse():
     p.add_argument("--cpu-seconds", type=float, default=12.0, help="target length of one CPU baseline sample")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu-baseline", action="store_true")
-    p.add_argument("--workload", default="dgemm", choices=["dgemm", "grouped", "configs", "harness", "qr", "shape"],
+    p.add_argument("--workload", default="dgemm",
+                   choices=["dgemm", "grouped", "configs", "harness", "qr", "shape", "hessenberg"],
                    help="dgemm: the 8192^3 headline; grouped: 20,000 uneven problems in one launch; "
                         "configs: one line per C1-C5 shape (rate and accuracy), one GPU")
     p.add_argument("--count", type=int, default=20000, help="grouped workload: number of problems")
@@ -740,6 +741,72 @@ def run_qr(args):
     return 0
 
 
+def hess_cpu_baseline(n):
+    """The oracle's restatement of BlockedHessenbergQR.decompose (panels of 32,
+    the reference's per-reflector updates of a working copy in numpy, the
+    block updates through numpy's BLAS) on an n x n uniform[-1,1) matrix."""
+    import numpy as np
+    from oracle import oracle as O
+    a = np.random.default_rng(20260604).uniform(-1.0, 1.0, (n, n))
+    t0 = time.perf_counter()
+    O.blocked_hessenberg(a)
+    dt = time.perf_counter() - t0
+    cores = os.cpu_count() or 1
+    return {"value": round(14.0 / 3.0 * n ** 3 / dt / 1e9, 2), "unit": "GFLOP/s", "cores": cores, "kind": "port",
+            "sample": f"one {n}x{n} reduction (H and Q) through the restatement of BlockedHessenbergQR.decompose "
+                      f"(numpy, up to {cores} BLAS threads), {dt:.1f} s"}
+
+
+def run_hessenberg(args):
+    """Device-resident blocked Hessenberg reduction of a size x size
+    uniform[-1,1) matrix with Q formed (BlockedHessenbergQR.decompose): device
+    time per reduction (the matrix restored, untimed, before each), FLOPs
+    10n^3/3 for H and 4n^3/3 for Q, and the device time of every phase."""
+    import statistics
+    import torch
+    import jlc_b200
+    world, rank, local = dist_env()
+    if rank != 0:
+        return 0
+    torch.cuda.set_device(local)
+    ctx = jlc_b200.Context(local)
+    n = args.size
+    g = torch.Generator(device="cuda")
+    g.manual_seed(20260604)
+    a0 = torch.rand((n, n), dtype=torch.float64, device="cuda", generator=g) * 2 - 1
+    a = torch.empty_like(a0)
+    q = torch.empty_like(a0)
+    flops = 14.0 / 3.0 * n ** 3
+    times, phases = [], []
+    for it in range(args.warmup + args.steps):
+        a.copy_(a0)
+        torch.cuda.synchronize()
+        ctx.set_profiling(it >= args.warmup)
+        rep = ctx.hessenberg_device(n, a.data_ptr(), n, q.data_ptr(), n)
+        if it >= args.warmup:
+            recs = ctx.profile_collect()
+            times.append(rep["device_ms"])
+            per = {}
+            for name, t in recs:
+                per[name] = per.get(name, 0.0) + t
+            phases.append(per)
+    ctx.set_profiling(False)
+    ms = statistics.median(times)
+    cpu = None if args.no_cpu_baseline else hess_cpu_baseline(min(n, 1024))
+    line = {"metric": f"blocked Hessenberg reduction GFLOP/s ({n}x{n}, FP64, H and Q, device-resident)",
+            "value": round(flops / (ms * 1e-3) / 1e9, 1), "unit": "GFLOP/s", "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(ms, 3), "higher_is_better": True, "dtype": "f64",
+            "data": "synthetic uniform[-1,1) (torch Philox, seed 20260604), device resident",
+            "config": {"workload": f"Hessenberg {n}x{n} with Q, panels of 32, one GEMV per reflector, block "
+                                   "updates on the DMMA route"},
+            "phase_ms": {name: round(statistics.median(p.get(name, 0.0) for p in phases), 3)
+                         for name in sorted({nm for p in phases for nm in p})},
+            "cpu_baseline": cpu}
+    print(json.dumps(line), flush=True)
+    ctx.close()
+    return 0
+
+
 # ----------------------------------------------------------------------------- harness (report port)
 HARNESS_BACKENDS = ["blas3-naive", "blas3-simd-1t", "blas3-parallel", "opt-1t", "opt-parallel", "cuda",
                     "cuda-ozaki"]
@@ -969,6 +1036,8 @@ def main():
         return run_harness(args)
     if args.workload == "shape":
         return run_shape(args)
+    if args.workload == "hessenberg":
+        return run_hessenberg(args)
     if args.workload == "qr":
         return run_qr(args)
     return run_ours(args)
