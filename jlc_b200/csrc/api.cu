@@ -1217,47 +1217,29 @@ int jlc_hessenberg_device(jlc_ctx* ctx, int64_t n, double* a, int64_t lda, doubl
     if (q && (rc = launch_set_identity(q, ldq, n, n, st))) return set_err(ctx, rc, "Hessenberg: identity launch failed");
     if (n > 2) {
         const long long ldv = round_up(n, 8), ldw = ldv;
-        if ((rc = reserve(ctx, ctx->bufH, hess_work_doubles(n) * sizeof(double), "Hessenberg workspace"))) return rc;
+        const size_t work_bytes = hess_work_doubles(n) * sizeof(double);
+        if ((rc = reserve(ctx, ctx->bufH, work_bytes + hess_panel_scratch_bytes(ctx->sm_count),
+                          "Hessenberg workspace")))
+            return rc;
         double* V = static_cast<double*>(ctx->bufH.ptr);
         double* Y = V + ldv * kHessPanel;
         double* W = Y + ldv * kHessPanel;
         double* W2 = W + ldv * kHessPanel;
         double* T = W2 + ldv * kHessPanel;
         double* tau = T + kHessPanel * kHessPanel;
-        double* sv = tau + kHessPanel;
-        double* wbuf = sv + kHessPanel;
-        // the GEMV's partial sums: at most 64 column chunks of at most n - 1
-        // rows for every trailing block (gemv.cu, axpy_split)
-        if ((rc = ws_reserve(ctx, (size_t)64 * (size_t)(n - 1) * sizeof(double)))) return rc;
+        double* wbuf = tau + 2 * kHessPanel;
+        void* panel_scratch = static_cast<char*>(ctx->bufH.ptr) + work_bytes;
         for (long long k = 0; k < n - 2; k += kHessPanel) {
             const int pw = (int)((n - 2 - k) < kHessPanel ? (n - 2 - k) : kHessPanel);
-            const long long m = n - k - 1, r0 = k + 1;
             {
+                // the panel's reflectors, V, T and Y in one cooperative launch
                 Phase ph(ctx, JLC_PHASE_HESS_PANEL);
                 if (cudaMemsetAsync(T, 0, kHessPanel * kHessPanel * sizeof(double), st) != cudaSuccess)
                     return set_err(ctx, JLC_E_CUDA, "Hessenberg: T reset failed");
-                for (int j = 0; j < pw; ++j) {
-                    rc = launch_hess_reflector(a, lda, (int)n, (int)k, j, V, ldv, Y, T, tau, sv, wbuf, st);
-                    if (rc) return set_err(ctx, rc, "Hessenberg: reflector launch failed");
-                    // Y column j <- A[r0:, r0+j:] v_j[j:]
-                    GemvDesc v;
-                    v.rows = m;
-                    v.cols = m - j;
-                    v.mat = a + r0 + (r0 + j) * lda;
-                    v.rs = 1;
-                    v.cs = lda;
-                    v.x = V + j * ldv + j;
-                    v.incx = 1;
-                    v.y = Y + j * ldv;
-                    v.incy = 1;
-                    v.alpha = 1.0;
-                    v.beta = 0.0;
-                    rc = launch_gemv(v, ctx->ws.ptr, st, ctx->sm_count, ctx->err, sizeof(ctx->err));
-                    if (rc) return rc;
-                    rc = launch_hess_y_finish((int)m, j, Y, ldv, tau, sv, st);
-                    if (rc) return set_err(ctx, rc, "Hessenberg: Y launch failed");
-                    ctx->launches += 4;
-                }
+                rc = launch_hess_panel(a, lda, (int)n, (int)k, pw, V, ldv, Y, T, tau, wbuf, panel_scratch,
+                                       ctx->sm_count, ctx->d_status, st);
+                if (rc) return set_err(ctx, rc, "Hessenberg: panel launch failed");
+                ctx->launches += 1;
             }
             rc = hess_apply_left(ctx, a, lda, n, k, pw, V, ldv, T, W, W2, ldw, precision);
             if (!rc) rc = hess_apply_right(ctx, a, lda, n, k, pw, V, ldv, T, W, W2, precision);

@@ -27,14 +27,13 @@
 // row r is global row k+1+r), T row-major 32 x 32.
 #include <cstdio>
 
+#include "jlc_device.cuh"
 #include "jlc_internal.h"
 
 namespace jlc {
 namespace hess {
 
-constexpr int PW = 32;         // panel width of the reference
-constexpr int THREADS = 256;   // one CTA per reflector
-constexpr int WARPS = THREADS / 32;
+constexpr int PW = 32;  // panel width of the reference
 
 __device__ __forceinline__ double warp_sum(double v) {
 #pragma unroll
@@ -42,9 +41,45 @@ __device__ __forceinline__ double warp_sum(double v) {
     return v;
 }
 
-// Sums each of the first `cnt` entries of part[] over the CTA into out[]
-// (red: WARPS x PW shared scratch).  All threads take part.
-__device__ void block_sum_vec(double (&part)[PW], int cnt, double (*red)[PW], double* out) {
+// Entries below the first subdiagonal set to zero (the reference clears the
+// fill-in its block updates leave there, BlockedHessenbergQR.java:137-141).
+__global__ void hess_clear_kernel(double* h, long long ldh, int n) {
+    for (int col = blockIdx.y; col < n - 2; col += gridDim.y)
+        for (int r = col + 2 + blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x)
+            h[r + (long long)col * ldh] = 0.0;
+}
+
+// ---------------------------------------------------------------------------
+// All reflectors of a panel in one cooperative launch.  The m rows (global
+// rows k+1..n-1) are split into slabs of `slab` rows (a multiple of 32), one
+// per CTA.  Per reflector j every CTA works on its own rows and three bounded
+// grid barriers join the reductions:
+//   1. w = A e_col - Y V^T e_col on its rows, its part of u = V^T w;
+//   2. u summed over the CTAs' parts in a fixed order (so every CTA gets the
+//      same bits), z = T^T u, w -= V z, its part of sigma (and x0 from the
+//      CTA that holds row j);
+//   3. sigma summed, the reflector (computed identically in every CTA), v_j
+//      on its rows, its part of s = V_{j-1}^T v_j;
+// then s summed, T's column j (CTA 0), and, with v_j complete, the GEMV
+// A_sub v_j over its rows (every column of the trailing block) and
+// y_j = tau_j (A_sub v_j - Y s) on its rows.  The next reflector reads only
+// its own rows of Y and row j of V, which every CTA wrote before barrier 3.
+constexpr int PT = 512;           // threads of the cooperative panel kernel
+constexpr int PWARPS = PT / 32;
+
+struct PanelArgs {
+    const double* h;
+    long long ldh;
+    int n, k, pw, m, slab;
+    double *V, *Y, *T, *tau, *wbuf;
+    long long ldv;
+    double *part_u, *part_s, *part_sig, *x0rec;  // [grid][PW], [grid][PW], [grid], [1]
+    unsigned* counter;                           // zero at launch
+    int* status;
+    double eps;
+};
+
+__device__ void block_sum_to(double (&part)[PW], int cnt, double (*red)[PW], double* out_row) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
     for (int i = 0; i < PW; ++i) {
@@ -56,141 +91,204 @@ __device__ void block_sum_vec(double (&part)[PW], int cnt, double (*red)[PW], do
     __syncthreads();
     if (threadIdx.x < cnt) {
         double s = 0.0;
-        for (int w = 0; w < WARPS; ++w) s += red[w][threadIdx.x];
-        out[threadIdx.x] = s;
+        for (int w = 0; w < PWARPS; ++w) s += red[w][threadIdx.x];
+        out_row[threadIdx.x] = s;
     }
-    __syncthreads();
 }
 
-// Reflector j of the panel starting at column k (one CTA): forms column
-// col = k + j of Q_j^T A Q_j on rows k+1.. into wbuf, then v_j (V column j),
-// tau_j, s = V_{j-1}^T v_j and T's column j.
-__global__ void __launch_bounds__(THREADS) hess_reflector_kernel(const double* h, long long ldh, int n, int k, int j,
-                                                                 double* V, long long ldv, const double* Y,
-                                                                 double* T, double* tau, double* s_out, double* wbuf,
-                                                                 double eps) {
+__global__ void __launch_bounds__(PT, 1) hess_panel_kernel(const PanelArgs p) {
     __shared__ double vrow[PW], u[PW], z[PW], s[PW];
-    __shared__ double red[WARPS][PW];
-    __shared__ double sc[4];  // x0, sigma, v0, t
-    const int m = n - k - 1, col = k + j, r0 = k + 1;
-    if (threadIdx.x < PW) vrow[threadIdx.x] = (j > 0 && threadIdx.x < j) ? V[(j - 1) + threadIdx.x * ldv] : 0.0;
-    __syncthreads();
-    // w = A e_col - Y V^T e_col (row j-1 of V holds V^T e_col), and V^T w
-    double part[PW];
+    __shared__ double red[PWARPS][PW];
+    __shared__ double sc[4];
+    __shared__ double ypart[PWARPS][32];
+    __shared__ int s_ok;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int ra = blockIdx.x * p.slab, rb = min(p.m, ra + p.slab);
+    const int r0 = p.k + 1, P = gridDim.x;
+    unsigned target = 0;
+    for (int j = 0; j < p.pw; ++j) {
+        const int col = p.k + j;
+        if (tid < PW) vrow[tid] = (tid < j) ? p.V[(j - 1) + (long long)tid * p.ldv] : 0.0;
+        __syncthreads();
+        // 1. w and this CTA's part of V^T w
+        double part[PW];
 #pragma unroll
-    for (int i = 0; i < PW; ++i) part[i] = 0.0;
-    for (int r = threadIdx.x; r < m; r += THREADS) {
-        double w = h[(long long)(r0 + r) + (long long)col * ldh];
-        for (int i = 0; i < j; ++i) w -= Y[r + i * ldv] * vrow[i];
-        wbuf[r] = w;
+        for (int i = 0; i < PW; ++i) part[i] = 0.0;
+        for (int r = ra + tid; r < rb; r += PT) {
+            double w = p.h[(long long)(r0 + r) + (long long)col * p.ldh];
+            for (int i = 0; i < j; ++i) w -= p.Y[r + (long long)i * p.ldv] * vrow[i];
+            p.wbuf[r] = w;
 #pragma unroll
-        for (int i = 0; i < PW; ++i)
-            if (i < j) part[i] += V[r + i * ldv] * w;
-    }
-    block_sum_vec(part, j, red, u);
-    // z = T^T u (T upper triangular)
-    if (threadIdx.x < j) {
-        double acc = 0.0;
-        for (int l = 0; l <= (int)threadIdx.x; ++l) acc += T[l * PW + threadIdx.x] * u[l];
-        z[threadIdx.x] = acc;
-    }
-    __syncthreads();
-    // w -= V z; x0 = w[j], sigma = |w[j+1..]|^2
-    double sig = 0.0;
-    for (int r = threadIdx.x; r < m; r += THREADS) {
-        double w = wbuf[r];
-        for (int i = 0; i < j; ++i) w -= V[r + i * ldv] * z[i];
-        wbuf[r] = w;
-        if (r == j) sc[0] = w;
-        else if (r > j) sig += w * w;
-    }
-    sig = warp_sum(sig);
-    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5][0] = sig;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        double sigma = 0.0;
-        for (int w = 0; w < WARPS; ++w) sigma += red[w][0];
-        const double x0 = j < m ? sc[0] : 0.0;
-        double t = 0.0, v0 = 0.0;
-        if (j < m && sigma > eps) {
-            const double mu = sqrt(x0 * x0 + sigma);
-            const double beta = -copysign(mu, x0);
-            v0 = x0 - beta;
-            const double v0sq = v0 * v0;
-            if (v0sq > eps) t = 2.0 * v0sq / (sigma + v0sq);
+            for (int i = 0; i < PW; ++i)
+                if (i < j) part[i] += p.V[r + (long long)i * p.ldv] * w;
         }
-        sc[2] = v0;
-        sc[3] = t;
-        tau[j] = t;
-    }
-    __syncthreads();
-    const double v0 = sc[2], t = sc[3];
-    // v_j (zero when there is no reflector) and s = V_{j-1}^T v_j
-#pragma unroll
-    for (int i = 0; i < PW; ++i) part[i] = 0.0;
-    double* vj = V + (long long)j * ldv;
-    for (int r = threadIdx.x; r < m; r += THREADS) {
-        double v = 0.0;
-        if (t != 0.0) v = r < j ? 0.0 : (r == j ? 1.0 : wbuf[r] / v0);
-        vj[r] = v;
-#pragma unroll
-        for (int i = 0; i < PW; ++i)
-            if (i < j) part[i] += V[r + i * ldv] * v;
-    }
-    block_sum_vec(part, j, red, s);
-    // T column j: T[i][j] = -t sum_{l=i}^{j-1} T[i][l] s_l, T[j][j] = t
-    if (threadIdx.x < PW) {
-        const int i = threadIdx.x;
-        double val = 0.0;
-        if (i < j) {
+        block_sum_to(part, j, red, p.part_u + (long long)blockIdx.x * PW);
+        target += P;
+        if (!grid_barrier(p.counter, target, p.status, &s_ok)) return;
+        // 2. u in a fixed order, z = T^T u, w -= V z, sigma part, x0
+        if (tid < j) {
             double acc = 0.0;
-            for (int l = i; l < j; ++l) acc += T[i * PW + l] * s[l];
-            val = -t * acc;
-        } else if (i == j) {
-            val = t;
+            for (int b = 0; b < P; ++b) acc += p.part_u[(long long)b * PW + tid];
+            u[tid] = acc;
         }
-        T[i * PW + j] = val;
-        s_out[i] = i < j ? s[i] : 0.0;
+        __syncthreads();
+        if (tid < j) {
+            double acc = 0.0;
+            for (int l = 0; l <= tid; ++l) acc += p.T[l * PW + tid] * u[l];
+            z[tid] = acc;
+        }
+        __syncthreads();
+        double sig = 0.0;
+        for (int r = ra + tid; r < rb; r += PT) {
+            double w = p.wbuf[r];
+            for (int i = 0; i < j; ++i) w -= p.V[r + (long long)i * p.ldv] * z[i];
+            p.wbuf[r] = w;
+            if (r == j) *p.x0rec = w;
+            else if (r > j) sig += w * w;
+        }
+        sig = warp_sum(sig);
+        if (lane == 0) red[warp][0] = sig;
+        __syncthreads();
+        if (tid == 0) {
+            double t = 0.0;
+            for (int w = 0; w < PWARPS; ++w) t += red[w][0];
+            p.part_sig[blockIdx.x] = t;
+        }
+        target += P;
+        if (!grid_barrier(p.counter, target, p.status, &s_ok)) return;
+        // 3. the reflector (the same bits in every CTA), v_j, part of V^T v_j
+        if (tid == 0) {
+            double sigma = 0.0;
+            for (int b = 0; b < P; ++b) sigma += p.part_sig[b];
+            const double x0 = *p.x0rec;
+            double t = 0.0, v0 = 0.0;
+            if (sigma > p.eps) {
+                const double mu = sqrt(x0 * x0 + sigma);
+                const double beta = -copysign(mu, x0);
+                v0 = x0 - beta;
+                const double v0sq = v0 * v0;
+                if (v0sq > p.eps) t = 2.0 * v0sq / (sigma + v0sq);
+            }
+            sc[2] = v0;
+            sc[3] = t;
+        }
+        __syncthreads();
+        const double v0 = sc[2], t = sc[3];
+#pragma unroll
+        for (int i = 0; i < PW; ++i) part[i] = 0.0;
+        double* vj = p.V + (long long)j * p.ldv;
+        for (int r = ra + tid; r < rb; r += PT) {
+            double v = 0.0;
+            if (t != 0.0) v = r < j ? 0.0 : (r == j ? 1.0 : p.wbuf[r] / v0);
+            vj[r] = v;
+#pragma unroll
+            for (int i = 0; i < PW; ++i)
+                if (i < j) part[i] += p.V[r + (long long)i * p.ldv] * v;
+        }
+        block_sum_to(part, j, red, p.part_s + (long long)blockIdx.x * PW);
+        target += P;
+        if (!grid_barrier(p.counter, target, p.status, &s_ok)) return;
+        // 4. s, T's column j, then y_j on this CTA's rows
+        if (tid < j) {
+            double acc = 0.0;
+            for (int b = 0; b < P; ++b) acc += p.part_s[(long long)b * PW + tid];
+            s[tid] = acc;
+        }
+        __syncthreads();
+        if (blockIdx.x == 0 && tid < PW) {
+            const int i = tid;
+            double val = 0.0;
+            if (i < j) {
+                double acc = 0.0;
+                for (int l = i; l < j; ++l) acc += p.T[i * PW + l] * s[l];
+                val = -t * acc;
+            } else if (i == j) {
+                val = t;
+            }
+            p.T[i * PW + j] = val;
+            if (i == 0) p.tau[j] = t;
+        }
+        // GEMV over the trailing block: lanes walk 32 rows, warps the columns
+        for (int c0 = ra; c0 < rb; c0 += 32) {
+            const int r = c0 + lane;
+            double acc = 0.0;
+            if (t != 0.0 && r < rb) {
+                const double* arow = p.h + (long long)(r0 + r) + (long long)r0 * p.ldh;
+                int c = j + warp;
+                for (; c + 3 * PWARPS < p.m; c += 4 * PWARPS) {
+                    const double a0 = arow[(long long)c * p.ldh];
+                    const double a1 = arow[(long long)(c + PWARPS) * p.ldh];
+                    const double a2 = arow[(long long)(c + 2 * PWARPS) * p.ldh];
+                    const double a3 = arow[(long long)(c + 3 * PWARPS) * p.ldh];
+                    acc += a0 * vj[c] + a1 * vj[c + PWARPS] + a2 * vj[c + 2 * PWARPS] + a3 * vj[c + 3 * PWARPS];
+                }
+                for (; c < p.m; c += PWARPS) acc += arow[(long long)c * p.ldh] * vj[c];
+            }
+            ypart[warp][lane] = acc;
+            __syncthreads();
+            if (warp == 0 && r < rb) {
+                double y = 0.0;
+                for (int w = 0; w < PWARPS; ++w) y += ypart[w][lane];
+                for (int i = 0; i < j; ++i) y -= p.Y[r + (long long)i * p.ldv] * s[i];
+                p.Y[r + (long long)j * p.ldv] = t * y;
+            }
+            __syncthreads();
+        }
     }
-}
-
-// Y column j = tau_j (Y column j - Y_{j-1} s), after the GEMV has left
-// A_sub v_j in Y column j.
-__global__ void __launch_bounds__(256) hess_y_finish_kernel(int m, int j, double* Y, long long ldv, const double* tau,
-                                                            const double* s) {
-    const int r = blockIdx.x * blockDim.x + threadIdx.x;
-    if (r >= m) return;
-    const double t = tau[j];
-    double y = Y[r + (long long)j * ldv];
-    for (int i = 0; i < j; ++i) y -= Y[r + (long long)i * ldv] * s[i];
-    Y[r + (long long)j * ldv] = t * y;
-}
-
-// Entries below the first subdiagonal set to zero (the reference clears the
-// fill-in its block updates leave there, BlockedHessenbergQR.java:137-141).
-__global__ void hess_clear_kernel(double* h, long long ldh, int n) {
-    for (int col = blockIdx.y; col < n - 2; col += gridDim.y)
-        for (int r = col + 2 + blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x)
-            h[r + (long long)col * ldh] = 0.0;
 }
 
 }  // namespace hess
 
+int hess_panel_grid(int m, int sm_count, int* slab) {
+    int P = (m + 31) / 32;
+    if (P > sm_count) P = sm_count;
+    if (P < 1) P = 1;
+    int sl = (m + P - 1) / P;
+    sl = (sl + 31) / 32 * 32;
+    P = (m + sl - 1) / sl;
+    *slab = sl;
+    return P;
+}
+
+size_t hess_panel_scratch_bytes(int sm_count) {
+    return (size_t)(2 * sm_count * hess::PW + sm_count + 8) * sizeof(double) + 256;
+}
+
+int launch_hess_panel(const double* h, long long ldh, int n, int k, int pw, double* V, long long ldv, double* Y,
+                      double* T, double* tau, double* wbuf, void* scratch, int sm_count, int* status,
+                      cudaStream_t st) {
+    using namespace hess;
+    PanelArgs a;
+    a.h = h;
+    a.ldh = ldh;
+    a.n = n;
+    a.k = k;
+    a.pw = pw;
+    a.m = n - k - 1;
+    const int P = hess_panel_grid(a.m, sm_count, &a.slab);
+    a.V = V;
+    a.Y = Y;
+    a.T = T;
+    a.tau = tau;
+    a.wbuf = wbuf;
+    a.ldv = ldv;
+    double* d = static_cast<double*>(scratch);
+    a.part_u = d;
+    a.part_s = d + (size_t)sm_count * PW;
+    a.part_sig = a.part_s + (size_t)sm_count * PW;
+    a.x0rec = a.part_sig + sm_count;
+    a.counter = reinterpret_cast<unsigned*>(a.x0rec + 8);
+    a.status = status;
+    a.eps = 1e-12;
+    if (cudaMemsetAsync(a.counter, 0, sizeof(unsigned), st) != cudaSuccess) return JLC_E_CUDA;
+    void* args[] = {&a};
+    cudaError_t e = cudaLaunchCooperativeKernel((const void*)hess_panel_kernel, dim3(P), dim3(PT), args, 0, st);
+    return e == cudaSuccess ? JLC_OK : JLC_E_LAUNCH;
+}
+
 size_t hess_work_doubles(long long n) {
     const long long ldv = (n + 7) / 8 * 8;
     return (size_t)(3 * ldv * hess::PW + 2 * hess::PW * hess::PW + 2 * hess::PW + 2 * ldv * hess::PW);
-}
-
-int launch_hess_reflector(const double* h, long long ldh, int n, int k, int j, double* V, long long ldv,
-                          const double* Y, double* T, double* tau, double* s, double* wbuf, cudaStream_t st) {
-    hess::hess_reflector_kernel<<<1, hess::THREADS, 0, st>>>(h, ldh, n, k, j, V, ldv, Y, T, tau, s, wbuf, 1e-12);
-    return cudaGetLastError() == cudaSuccess ? JLC_OK : JLC_E_LAUNCH;
-}
-
-int launch_hess_y_finish(int m, int j, double* Y, long long ldv, const double* tau, const double* s, cudaStream_t st) {
-    if (m <= 0) return JLC_OK;
-    hess::hess_y_finish_kernel<<<(m + 255) / 256, 256, 0, st>>>(m, j, Y, ldv, tau, s);
-    return cudaGetLastError() == cudaSuccess ? JLC_OK : JLC_E_LAUNCH;
 }
 
 int launch_hess_clear(double* h, long long ldh, int n, cudaStream_t st) {

@@ -86,10 +86,13 @@ int launch_qr_build_t(const double* g, const double* tau, int kb, double* t, cud
 int launch_set_identity(double* q, long long ldq, long long m, long long cols, cudaStream_t st);
 // blocked Hessenberg reduction kernels (hess.cu)
 size_t hess_work_doubles(long long n);
-int launch_hess_reflector(const double* h, long long ldh, int n, int k, int j, double* V, long long ldv,
-                          const double* Y, double* T, double* tau, double* s, double* wbuf, cudaStream_t st);
-int launch_hess_y_finish(int m, int j, double* Y, long long ldv, const double* tau, const double* s, cudaStream_t st);
 int launch_hess_clear(double* h, long long ldh, int n, cudaStream_t st);
+// all reflectors of one panel in one cooperative launch (rows in slabs over
+// up to sm_count CTAs); scratch of hess_panel_scratch_bytes
+size_t hess_panel_scratch_bytes(int sm_count);
+int launch_hess_panel(const double* h, long long ldh, int n, int k, int pw, double* V, long long ldv, double* Y,
+                      double* T, double* tau, double* wbuf, void* scratch, int sm_count, int* status,
+                      cudaStream_t st);
 int launch_dgemm_dmma(const GemmDesc& g, cudaStream_t st, int sm_count, int* status, const int* gate, int mma_k,
                       char* err, size_t errlen, int ksplit = 1, void* splitk_ws = nullptr,
                       size_t splitk_ws_bytes = 0);

@@ -57,43 +57,6 @@ __device__ __forceinline__ double warp_max(double v) {
 constexpr int MP_THREADS = 256, MP_WARPS = MP_THREADS / 32;
 constexpr int MP_PART = 72;  // per CTA and column: max, scale, ssq, dots with up to 63 later columns
 
-__device__ __forceinline__ unsigned ld_acquire_u32(const unsigned* p) {
-    unsigned v;
-    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
-    return v;
-}
-
-// All CTAs of the launch arrive, then wait until `target` arrivals are
-// counted.  Bounded: past the status block's wait limit (or once another CTA has recorded an
-// error) it records JLC_DEV_TIMEOUT and returns false in every thread.  The
-// arrival is a release reduction and the poll an acquire load: with the CTA
-// barriers on either side, every write a CTA made before arriving is visible
-// to every thread of every CTA after the wait.
-__device__ bool grid_barrier(unsigned* counter, unsigned target, int* status, int* s_ok) {
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        asm volatile("red.release.gpu.global.add.u32 [%0], %1;" ::"l"(counter), "r"(1u) : "memory");
-        const uint64_t t0 = globaltimer_ns();
-        const uint64_t limit = wait_limit_ns(status);
-        int ok = 1;
-        for (unsigned it = 0; ld_acquire_u32(counter) < target; ++it) {
-            if ((it & 63u) == 0u) {
-                if (*(volatile int*)status != 0) {
-                    ok = 0;
-                    break;
-                }
-                if (globaltimer_ns() - t0 > limit) {
-                    atomicOr(status, JLC_DEV_TIMEOUT);
-                    ok = 0;
-                    break;
-                }
-            }
-        }
-        *s_ok = ok;
-    }
-    __syncthreads();
-    return *s_ok != 0;
-}
 
 // (scale, ssq) pairs: sum of squares = scale^2 * ssq, combined without overflow
 __device__ __forceinline__ void ssq_add(double& scale, double& ssq, double x) {
