@@ -36,6 +36,10 @@
  *      MC x NC tiles over threads, B packed KC x roundUp(NC,NR), A packed in
  *      MR strips with alpha folded in, MR x NR register microkernel.  It is
  *      bit-identical to orc_gemm_fmachain and is what the CPU baseline times.
+ *  - orc_householder_qr_blocked:
+ *      HouseholderQR.factorizeBlocked (HouseholderQR.java:133-384): scalar
+ *      panels of 64 columns, compact-WY trailing updates per 128-column block
+ *      through the packed kernel above; the QR CPU baseline.
  *  - orc_gemm_dd:
  *      the double-double oracle (absent from the reference): Dot2 of
  *      Ogita, Rump and Oishi, "Accurate sum and dot product", SIAM J. Sci.
@@ -318,8 +322,8 @@ ORC_EXPORT int orc_opt_gemm(int64_t m, int64_t n, int64_t k, const double* a, co
 #define ORC_MC 2048
 
 typedef struct {
-    const double* a; int64_t lda;
-    const double* b; int64_t ldb;
+    const double* a; int64_t a_rs, a_cs;
+    const double* b; int64_t b_rs, b_cs;
     double* c; int64_t ldc;
     int64_t m, n, k;
     double alpha;
@@ -358,9 +362,9 @@ static void packed_tiles(void* vctx, int64_t lo, int64_t hi) {
         for (int64_t kk = 0; kk < g->k; kk += ORC_KC) {
             int64_t kb = kk + ORC_KC < g->k ? ORC_KC : g->k - kk;
             for (int64_t p = 0; p < kb; p++) {
-                const double* src = g->b + (kk + p) * g->ldb + c0;
+                const double* src = g->b + (kk + p) * g->b_rs + c0 * g->b_cs;
                 double* dst = bpack + p * packed_n;
-                for (int64_t j = 0; j < nb; j++) dst[j] = src[j];
+                for (int64_t j = 0; j < nb; j++) dst[j] = src[j * g->b_cs];
                 for (int64_t j = nb; j < packed_n; j++) dst[j] = 0.0;
             }
             for (int64_t i = r0; i < r1; i += ORC_MR) {
@@ -368,8 +372,8 @@ static void packed_tiles(void* vctx, int64_t lo, int64_t hi) {
                 for (int64_t r = 0; r < ORC_MR; r++)
                     for (int64_t p = 0; p < kb; p++)
                         apack[r * kb + p] = r < rows
-                            ? (g->alpha == 1.0 ? g->a[(i + r) * g->lda + kk + p]
-                                               : g->a[(i + r) * g->lda + kk + p] * g->alpha)
+                            ? (g->alpha == 1.0 ? g->a[(i + r) * g->a_rs + (kk + p) * g->a_cs]
+                                               : g->a[(i + r) * g->a_rs + (kk + p) * g->a_cs] * g->alpha)
                             : 0.0;
                 for (int64_t j = 0; j < nb; j += ORC_NR) {
                     int64_t cols = j + ORC_NR < nb ? ORC_NR : nb - j;
@@ -383,11 +387,15 @@ static void packed_tiles(void* vctx, int64_t lo, int64_t hi) {
     free(apack);
 }
 
-ORC_EXPORT void orc_gemm_packed_parallel(int64_t m, int64_t n, int64_t k,
-                                         const double* a, int64_t lda,
-                                         const double* b, int64_t ldb,
-                                         double* c, int64_t ldc,
-                                         double alpha, double beta, int nthreads) {
+/* The packed algorithm on operands addressed by (row stride, column stride):
+ * A_op(i,p) = a[i*a_rs + p*a_cs], B_op(p,j) = b[p*b_rs + j*b_cs]; packing
+ * absorbs the strides, so the transposed and column-major forms of
+ * BLAS3Kernels.gemmStrided* (BLAS3Kernels.java:244-303) run the same kernel. */
+ORC_EXPORT void orc_gemm_packed_strided(int64_t m, int64_t n, int64_t k,
+                                        const double* a, int64_t a_rs, int64_t a_cs,
+                                        const double* b, int64_t b_rs, int64_t b_cs,
+                                        double* c, int64_t ldc,
+                                        double alpha, double beta, int nthreads) {
     for (int64_t i = 0; i < m; i++)
         for (int64_t j = 0; j < n; j++) {
             double* p = &c[i * ldc + j];
@@ -395,9 +403,17 @@ ORC_EXPORT void orc_gemm_packed_parallel(int64_t m, int64_t n, int64_t k,
             else if (beta != 1.0) *p = *p * beta;
         }
     if (alpha == 0.0 || k == 0 || m == 0 || n == 0) return;
-    orc_packed_args g = {a, lda, b, ldb, c, ldc, m, n, k, alpha,
+    orc_packed_args g = {a, a_rs, a_cs, b, b_rs, b_cs, c, ldc, m, n, k, alpha,
                          (m + ORC_MC - 1) / ORC_MC, (n + ORC_NC - 1) / ORC_NC};
     orc_parallel_for(nthreads, g.tiles_m * g.tiles_n, packed_tiles, &g);
+}
+
+ORC_EXPORT void orc_gemm_packed_parallel(int64_t m, int64_t n, int64_t k,
+                                         const double* a, int64_t lda,
+                                         const double* b, int64_t ldb,
+                                         double* c, int64_t ldc,
+                                         double alpha, double beta, int nthreads) {
+    orc_gemm_packed_strided(m, n, k, a, lda, 1, b, ldb, 1, c, ldc, alpha, beta, nthreads);
 }
 
 /* ------------------------------------------------------------------ */
@@ -506,6 +522,248 @@ ORC_EXPORT double orc_max_err_ratio(int64_t count, const double* x, const double
     }
     if (max_abs) *max_abs = mabs;
     return worst;
+}
+
+/* ------------------------------------------------------------------ */
+/* HouseholderQR.factorizeBlocked restated (the QR CPU baseline)        */
+/* ------------------------------------------------------------------ */
+#define ORC_QR_PANEL 64      /* HouseholderQR.java:20 BLOCK_SIZE     */
+#define ORC_QR_TRAIL 128     /* HouseholderQR.java:22 TRAILING_BLOCK */
+
+/* computeHouseholder (HouseholderQR.java:219-292): max normalisation, the
+ * LAPACK-style beta, tail scaled by 1/((x0 - beta) * max).  at is column-major
+ * with m rows per column. */
+static void qr_householder(double* at, double* tau, int64_t m, int64_t k) {
+    double* col = at + k * m;
+    if (m - k <= 1) { tau[k] = 0.0; return; }
+    double mx = fabs(col[k]);
+    for (int64_t i = k + 1; i < m; i++) if (fabs(col[i]) > mx) mx = fabs(col[i]);
+    if (mx < 0x1.0p-1022) { tau[k] = 0.0; return; }
+    double inv = 1.0 / mx, x0 = col[k] * inv, sigma = 0.0;
+    for (int64_t i = k + 1; i < m; i++) { double v = col[i] * inv; sigma += v * v; }
+    double xnorm = sqrt(sigma);
+    if (xnorm == 0.0) {
+        if (x0 >= 0.0) { tau[k] = 0.0; }
+        else { tau[k] = 2.0; col[k] = -col[k]; }
+        return;
+    }
+    double nb = -copysign(hypot(x0, xnorm), x0);
+    double v0inv = 1.0 / ((x0 - nb) * mx);
+    for (int64_t i = k + 1; i < m; i++) col[i] *= v0inv;
+    tau[k] = (nb - x0) / nb;
+    col[k] = nb * mx;
+}
+
+/* applyHouseholderToColumn (HouseholderQR.java:345-384). */
+static void qr_apply_column(double* at, double t, int64_t m, int64_t k, int64_t j) {
+    const double* v = at + k * m;
+    double* c = at + j * m;
+    double dot = c[k];
+    for (int64_t i = k + 1; i < m; i++) dot += v[i] * c[i];
+    dot *= t;
+    c[k] -= dot;
+    for (int64_t i = k + 1; i < m; i++) c[i] -= dot * v[i];
+}
+
+typedef struct {
+    double* at; int64_t m, k_start, k_end, n;
+    const double* vpack; const double* vtpack; const double* t;
+} orc_qr_trail_args;
+
+/* One thread's share of updateTrailingMatrix (HouseholderQR.java:167-210):
+ * per 128-column block, packTrailingBlock, W = V^T C and C -= V W through the
+ * packed MR x NR kernel above, W = T^T W between them (applyTTranspose
+ * :326-338), unpackTrailingBlock.  The GEMMs run over all m rows, as the
+ * reference's do. */
+static void qr_trail_blocks(void* vctx, int64_t lo, int64_t hi) {
+    const orc_qr_trail_args* g = (const orc_qr_trail_args*)vctx;
+    const int64_t m = g->m, P = ORC_QR_PANEL, NB = ORC_QR_TRAIL;
+    double* cb = (double*)malloc(sizeof(double) * m * NB);
+    double* w = (double*)malloc(sizeof(double) * P * NB);
+    double* tw = (double*)malloc(sizeof(double) * P * NB);
+    for (int64_t blk = lo; blk < hi; blk++) {
+        int64_t c0 = g->k_end + blk * NB;
+        int64_t used = c0 + NB <= g->n ? NB : g->n - c0;
+        for (int64_t row = 0; row < m; row++)
+            for (int64_t j = 0; j < NB; j++) cb[row * NB + j] = j < used ? g->at[(c0 + j) * m + row] : 0.0;
+        orc_gemm_packed_parallel(P, NB, m, g->vtpack, m, cb, NB, w, NB, 1.0, 0.0, 1);
+        for (int64_t i = 0; i < P; i++)
+            for (int64_t j = 0; j < NB; j++) {
+                double s = 0.0;
+                for (int64_t q = 0; q <= i; q++) s = fma(g->t[q * P + i], w[q * NB + j], s);
+                tw[i * NB + j] = s;
+            }
+        orc_gemm_packed_parallel(m, NB, P, g->vpack, P, tw, NB, cb, NB, -1.0, 1.0, 1);
+        for (int64_t row = 0; row < m; row++)
+            for (int64_t j = 0; j < used; j++) g->at[(c0 + j) * m + row] = cb[row * NB + j];
+    }
+    free(tw);
+    free(w);
+    free(cb);
+}
+
+/* HouseholderQR.factorizeBlocked (HouseholderQR.java:133-146) on the
+ * column-major array at (n columns of m rows; the reference's AT): panels of
+ * 64 columns factored column by column (factorizePanel :151-162), then the
+ * trailing columns updated in the compact-WY form (packV :445-471 with a unit
+ * diagonal and zeros above it, buildT :297-325).  The panel work is scalar, as
+ * the reference's is; the trailing 128-column blocks are independent and are
+ * spread over nthreads threads, each running its GEMMs on one thread.  tau
+ * receives min(m, n) scales. */
+ORC_EXPORT void orc_householder_qr_blocked(double* at, double* tau, int64_t m, int64_t n, int nthreads) {
+    const int64_t P = ORC_QR_PANEL, kmax = m < n ? m : n;
+    double* vpack = (double*)malloc(sizeof(double) * m * P);
+    double* vtpack = (double*)malloc(sizeof(double) * m * P);
+    double* t = (double*)malloc(sizeof(double) * P * P);
+    for (int64_t ks = 0; ks < kmax; ks += P) {
+        int64_t ke = ks + P < kmax ? ks + P : kmax, pa = ke - ks;
+        for (int64_t k = ks; k < ke; k++) {
+            qr_householder(at, tau, m, k);
+            for (int64_t j = k + 1; j < ke; j++) qr_apply_column(at, tau[k], m, k, j);
+        }
+        if (ke >= n) continue;
+        for (int64_t i = 0; i < P; i++)
+            for (int64_t row = 0; row < m; row++) {
+                int64_t r = row - ks;
+                double val = (i >= pa || row < ks || r < i) ? 0.0 : (r == i ? 1.0 : at[(ks + i) * m + row]);
+                vpack[row * P + i] = val;
+                vtpack[i * m + row] = val;
+            }
+        memset(t, 0, sizeof(double) * P * P);
+        for (int64_t i = 0; i < pa; i++) {
+            double tk = tau[ks + i];
+            t[i * P + i] = tk;
+            for (int64_t r = 0; r < i; r++) {
+                double dot = 0.0;
+                for (int64_t row = ks + i; row < m; row++) dot += vpack[row * P + r] * vpack[row * P + i];
+                t[r * P + i] = -tk * dot;
+            }
+            for (int64_t r = 0; r < i; r++) {
+                double s = 0.0;
+                for (int64_t c = r; c < i; c++) s += t[r * P + c] * t[c * P + i];
+                t[r * P + i] = s;
+            }
+        }
+        orc_qr_trail_args g = {at, m, ks, ke, n, vpack, vtpack, t};
+        orc_parallel_for(nthreads, (n - ke + ORC_QR_TRAIL - 1) / ORC_QR_TRAIL, qr_trail_blocks, &g);
+    }
+    free(t);
+    free(vtpack);
+    free(vpack);
+}
+
+/* ------------------------------------------------------------------ */
+/* BlockedHessenbergQR.decompose restated (the Hessenberg CPU baseline) */
+/* ------------------------------------------------------------------ */
+#define ORC_HESS_EPS 1e-12   /* BlockedHessenbergQR.java:45 */
+
+/* factorPanelUnblocked (BlockedHessenbergQR.java:150-244) on the row-major
+ * working copy w: per column, the reflector from the serial sigma with the
+ * EPS skips, then applied to the whole copy from the left (columns col+1..)
+ * and from the right (all rows), in the reference's loop order.  V is m x pw
+ * row-major. */
+static void hess_panel_unblocked(double* w, int64_t n, int64_t k, int64_t pw, double* V, double* tau,
+                                 double* vw) {
+    const int64_t m = n - (k + 1);
+    for (int64_t j = 0; j < pw; j++) {
+        const int64_t col = k + j, rs = col + 1, len = n - rs;
+        tau[j] = 0.0;
+        if (len <= 0) continue;
+        const double x0 = w[rs * n + col];
+        double sigma = 0.0;
+        for (int64_t i = 1; i < len; i++) { double v = w[(rs + i) * n + col]; sigma += v * v; }
+        if (sigma <= ORC_HESS_EPS) continue;
+        const double mu = sqrt(x0 * x0 + sigma), beta = -copysign(mu, x0);
+        const double v0 = x0 - beta, v0sq = v0 * v0;
+        if (v0sq <= ORC_HESS_EPS) continue;
+        const double t = 2.0 * v0sq / (sigma + v0sq);
+        tau[j] = t;
+        const int64_t off = rs - (k + 1);
+        for (int64_t i = 0; i < m; i++) vw[i] = 0.0;
+        vw[off] = 1.0;
+        for (int64_t i = 1; i < len; i++) vw[off + i] = w[(rs + i) * n + col] / v0;
+        for (int64_t r = 0; r < m; r++) V[r * pw + j] = vw[r];
+        for (int64_t c2 = col + 1; c2 < n; c2++) {
+            double dot = w[rs * n + c2];
+            for (int64_t i = 1; i < len; i++) dot += vw[off + i] * w[(rs + i) * n + c2];
+            dot *= t;
+            w[rs * n + c2] -= dot;
+            for (int64_t i = 1; i < len; i++) w[(rs + i) * n + c2] -= dot * vw[off + i];
+        }
+        for (int64_t row = 0; row < n; row++) {
+            double* r = w + row * n + col + 1;
+            double dot = r[0];
+            for (int64_t i = 1; i < len; i++) dot += r[i] * vw[off + i];
+            dot *= t;
+            r[0] -= dot;
+            for (int64_t i = 1; i < len; i++) r[i] -= dot * vw[off + i];
+        }
+        w[rs * n + col] = beta;
+        for (int64_t i = 1; i < len; i++) w[(rs + i) * n + col] = 0.0;
+    }
+}
+
+/* buildT (BlockedHessenbergQR.java:246-275). */
+static void hess_build_t(const double* V, int64_t m, int64_t pw, const double* tau, double* T, double* wk) {
+    for (int64_t i = 0; i < pw * pw; i++) T[i] = 0.0;
+    for (int64_t i = 0; i < pw; i++) {
+        const double ti = tau[i];
+        if (ti == 0.0) continue;
+        for (int64_t j = 0; j < i; j++) {
+            double dot = 0.0;
+            for (int64_t r = 0; r < m; r++) dot += V[r * pw + j] * V[r * pw + i];
+            wk[j] = -ti * dot;
+        }
+        for (int64_t j = 0; j < i; j++) {
+            double s = 0.0;
+            for (int64_t l = j; l < i; l++) s += T[j * pw + l] * wk[l];
+            T[j * pw + i] = s;
+        }
+        T[i * pw + i] = ti;
+    }
+}
+
+/* BlockedHessenbergQR.decompose (BlockedHessenbergQR.java:99-146) on the
+ * row-major n x n array h, Q (row-major, n x n) formed beside it: per panel of
+ * 32 columns the working copy of H is factored (factorPanelUnblocked), then
+ * applyBlockLeft on H (:277-307: W = V^T H, W2 = T^T W, H -= V W2) and
+ * applyBlockRight on H and Q (:309-345: W = X V, W2 = W T, X -= W2 V^T)
+ * through the packed kernel above over nthreads threads, and the fill-in
+ * below the first subdiagonal cleared at the end. */
+ORC_EXPORT void orc_blocked_hessenberg(double* h, double* q, int64_t n, int nthreads) {
+    const int64_t PB = 32;
+    for (int64_t i = 0; i < n * n; i++) q[i] = 0.0;
+    for (int64_t i = 0; i < n; i++) q[i * n + i] = 1.0;
+    if (n <= 2) return;
+    double* w = (double*)malloc(sizeof(double) * n * n);
+    double* V = (double*)malloc(sizeof(double) * n * PB);
+    double* W = (double*)malloc(sizeof(double) * n * PB);
+    double* W2 = (double*)malloc(sizeof(double) * n * PB);
+    double* T = (double*)malloc(sizeof(double) * PB * PB);
+    double* tau = (double*)malloc(sizeof(double) * PB);
+    double* vw = (double*)malloc(sizeof(double) * n);
+    for (int64_t k = 0; k < n - 2; k += PB) {
+        const int64_t pw = PB < (n - 2) - k ? PB : (n - 2) - k, m = n - (k + 1);
+        memcpy(w, h, sizeof(double) * n * n);
+        hess_panel_unblocked(w, n, k, pw, V, tau, vw);
+        hess_build_t(V, m, pw, tau, T, vw);
+        /* applyBlockLeft, colStart = k: rows k+1.., columns k.. */
+        const int64_t nl = n - k;
+        double* hs = h + (k + 1) * n + k;
+        orc_gemm_packed_strided(pw, nl, m, V, 1, pw, hs, n, 1, W, nl, 1.0, 0.0, nthreads);
+        orc_gemm_packed_strided(pw, nl, pw, T, 1, pw, W, nl, 1, W2, nl, 1.0, 0.0, nthreads);
+        orc_gemm_packed_strided(m, nl, pw, V, pw, 1, W2, nl, 1, hs, n, -1.0, 1.0, nthreads);
+        /* applyBlockRight on H then Q, colStart = k+1: all rows */
+        for (int pass = 0; pass < 2; pass++) {
+            double* x = pass == 0 ? h : q;
+            orc_gemm_packed_strided(n, pw, m, x + k + 1, n, 1, V, pw, 1, W, pw, 1.0, 0.0, nthreads);
+            orc_gemm_packed_strided(n, pw, pw, W, pw, 1, T, pw, 1, W2, pw, 1.0, 0.0, nthreads);
+            orc_gemm_packed_strided(n, m, pw, W2, pw, 1, V, 1, pw, x + k + 1, n, -1.0, 1.0, nthreads);
+        }
+    }
+    for (int64_t col = 0; col < n - 2; col++)
+        for (int64_t row = col + 2; row < n; row++) h[row * n + col] = 0.0;
+    free(vw); free(tau); free(T); free(W2); free(W); free(V); free(w);
 }
 
 ORC_EXPORT int orc_version(void) { return 1; }

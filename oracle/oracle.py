@@ -72,6 +72,10 @@ def lib():
                                   _i64, _i64p, _i64p, _dp, _dp, ctypes.c_int]
         L.orc_max_err_ratio.argtypes = [_i64, _dp, _dp, _dp, _dp]
         L.orc_max_err_ratio.restype = ctypes.c_double
+        L.orc_householder_qr_blocked.argtypes = [_dp, _dp, _i64, _i64, ctypes.c_int]
+        L.orc_blocked_hessenberg.argtypes = [_dp, _dp, _i64, ctypes.c_int]
+        L.orc_gemm_packed_strided.argtypes = [_i64, _i64, _i64, _dp, _i64, _i64, _dp, _i64, _i64, _dp, _i64,
+                                              _d, _d, ctypes.c_int]
         _lib = L
     return _lib
 
@@ -236,6 +240,19 @@ def blocked_hessenberg(a, block: int = 32):
             blk -= ((blk @ V) @ T) @ V.T
     for col in range(n - 2):
         h[col + 2:, col] = 0.0
+    return h, q
+
+
+def blocked_hessenberg_c(a, threads: int = 0):
+    """The C restatement of BlockedHessenbergQR.decompose (liboracle's
+    orc_blocked_hessenberg): the reference's scalar factorPanelUnblocked on a
+    full working copy per panel, the six block-update GEMMs per panel through
+    the packed kernel over `threads` threads (0: all cores).  Returns (H, Q)
+    as blocked_hessenberg does."""
+    h = np.array(a, dtype=np.float64, copy=True, order="C")
+    n = h.shape[0]
+    q = np.empty_like(h)
+    lib().orc_blocked_hessenberg(_ptr(h), _ptr(q), n, threads or (os.cpu_count() or 1))
     return h, q
 
 
@@ -453,6 +470,21 @@ def ozaki_certificate(a_op, b_op, crt: bool, count: int):
 
 
 # ------------------------------------------------------------- blocked Householder QR
+def householder_qr_blocked_c(a, threads: int = 0):
+    """The C restatement of HouseholderQR.factorizeBlocked (HouseholderQR.java:
+    133-384, liboracle's orc_householder_qr_blocked) on a copy of the m x n
+    array a: scalar panels, the compact-WY trailing update per 128-column block
+    through the packed PARALLEL_MICRO kernel, the blocks spread over `threads`
+    threads (0: all cores).  Returns (F, tau) laid out as householder_qr_blocked
+    returns them."""
+    a = np.asarray(a, dtype=np.float64)
+    m, n = a.shape
+    at = np.ascontiguousarray(a.T)          # column k of A is row k of at
+    tau = np.zeros(max(min(m, n), 1))
+    lib().orc_householder_qr_blocked(_ptr(at), _ptr(tau), m, n, threads or (os.cpu_count() or 1))
+    return at.T.copy(), tau[:min(m, n)]
+
+
 def householder_qr_blocked(a, block: int = 64):
     """HouseholderQR.factorizeBlocked (HouseholderQR.java:133-210) restated on a
     copy of the m x n array a: panels of `block` columns factored column by

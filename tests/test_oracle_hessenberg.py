@@ -70,3 +70,18 @@ def test_hessenberg_panels_and_eigenvalues():
     ev_a = np.sort_complex(np.linalg.eigvals(a))
     ev_h = np.sort_complex(np.linalg.eigvals(h32))
     np.testing.assert_allclose(ev_h, ev_a, rtol=0, atol=1e-10)
+
+
+@pytest.mark.parametrize("n,seed", [(2, 702), (3, 703), (10, 710), (33, 933), (100, 1000), (130, 1130)])
+def test_c_restatement_matches_python(n, seed):
+    """The C port of decompose (the Hessenberg CPU baseline) against the numpy
+    restatement, and the reference's own acceptance check on its result; the
+    thread count does not change its arithmetic."""
+    a = O.java_random_matrix(seed, n, n)
+    h1, q1 = O.blocked_hessenberg(a)
+    h2, q2 = O.blocked_hessenberg_c(a, 4)
+    np.testing.assert_allclose(h2, h1, rtol=0, atol=1e-12 * max(1.0, np.abs(h1).max()))
+    np.testing.assert_allclose(q2, q1, rtol=0, atol=1e-12)
+    _check_hessenberg(a, h2, q2, _tolerance(n))
+    h3, q3 = O.blocked_hessenberg_c(a, 1)
+    assert np.array_equal(h3, h2) and np.array_equal(q3, q2)

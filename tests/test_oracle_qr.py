@@ -83,3 +83,34 @@ def test_mirror_argument_errors():
         HouseholderQR.decomposeThin(m)
     with pytest.raises(UnsupportedOperationException):
         HouseholderQR.factorize(m)
+
+
+@pytest.mark.parametrize("m,n", [(5, 3), (130, 70), (64, 300), (300, 129), (257, 257)])
+def test_c_restatement_matches_python(m, n):
+    """The C port of factorizeBlocked (the QR CPU baseline) against the numpy
+    restatement: same reflectors and R up to summation order."""
+    a = np.random.default_rng(m * 1000 + n).uniform(-1.0, 1.0, (m, n))
+    f1, t1 = O.householder_qr_blocked(a)
+    f2, t2 = O.householder_qr_blocked_c(a, 4)
+    assert np.allclose(f2, f1, rtol=0, atol=1e-12 * max(m, n))
+    assert np.allclose(t2, t1, rtol=0, atol=1e-13 * max(m, n))
+    # the thread count does not change the arithmetic
+    f3, t3 = O.householder_qr_blocked_c(a, 1)
+    assert np.array_equal(f3, f2) and np.array_equal(t3, t2)
+
+
+def test_packed_strided_is_the_fma_chain():
+    """The strided packed kernel under both baselines computes the
+    OptimizedBLAS3 fma chain bit for bit, for transposed and column-major
+    operands too."""
+    import ctypes
+    rng = np.random.default_rng(5)
+    for (m, n, k) in [(7, 9, 5), (70, 130, 129), (33, 8, 300)]:
+        a = rng.uniform(-1, 1, (k, m))       # A_op = a.T
+        b = rng.uniform(-1, 1, (n, k))       # B_op = b.T
+        c = rng.uniform(-1, 1, (m, n))
+        want = O.gemm_fmachain(a.T, b.T, c, -1.5, 0.5)
+        got = c.copy()
+        dp = lambda x: x.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+        O.lib().orc_gemm_packed_strided(m, n, k, dp(a), 1, m, dp(b), 1, k, dp(got), n, -1.5, 0.5, 3)
+        assert np.array_equal(got, want)
