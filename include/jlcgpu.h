@@ -316,7 +316,9 @@ typedef struct jlc_grouped_plan jlc_grouped_plan;
  * and columns are not skewed. */
 JLC_API int jlc_grouped_plan_create(jlc_ctx* ctx, const jlc_problem* probs, int64_t count, int precision, int flags,
                                     jlc_grouped_plan** out);
-/* enqueue one run on the context stream (graph replay when captured) */
+/* enqueue one run on the context stream (graph replay when captured); the
+ * FP64 tiles' waits are bounded, and one that runs out is reported by the
+ * next jlc_device_status */
 JLC_API int jlc_grouped_plan_run(jlc_grouped_plan* plan);
 JLC_API int jlc_grouped_plan_info(const jlc_grouped_plan* plan, int64_t* work_items, double* flops, int* tile_small,
                                   int* tile_large);

@@ -7,21 +7,23 @@
 // bidiagonalisation (HouseholderQR.java:167-210, BlockedHessenbergQR.java:
 // 277-345), each a gemm / gemmStrided* call.  Here a plan turns a problem
 // table into a work list once; every run is a single launch (optionally a
-// CUDA graph replay) in which persistent CTAs pull work items from an atomic
-// counter:
+// CUDA graph replay) of persistent CTAs, each with one producer warp and four
+// DMMA warps:
 //   * tile items: one 32x32 or 64x64 tile of C of one problem, FP64
-//     mma.sync (m16n8k8) over a 3-stage cp.async ring of 16 k-values; each
+//     mma.sync (m16n8k8) on k-blocks of 16 that the producer streams through
+//     a 12-slot cp.async ring without draining it between items; each
 //     operand is staged in the swizzled shared-memory layout that matches its
 //     global layout (K-major for row-major A / column-major B, MN-major
 //     otherwise), so the contiguous direction lands in 16-byte units and
 //     aligned operands move with 16-byte copies (8-byte copies otherwise,
-//     zero fill at ragged edges); alpha folded into the A fragments, beta
-//     fused in the epilogue;
+//     zero fill at ragged edges); alpha folded into the A fragments, C read
+//     when the item starts and beta fused in the epilogue;
 //   * tiny items: a batch of problems with m*n <= 64 and k <= 64 (the TINY
 //     and small SMALL shapes), one thread per output element running the
 //     reference's small-GEMM order (C <- beta*C, then an fma chain over p
 //     with alpha*a).
-// Items are ordered by decreasing cost (longest-processing-time first).  The
+// Items are ordered by decreasing cost (longest-processing-time first) and
+// dealt to the CTAs in serpentine rounds of the grid size.  The
 // tile shape of each shape class is chosen by an autotuner that times both
 // shapes on the plan's own problem shapes and caches the choice on disk,
 // keyed by device, SM count, library version and class.
@@ -255,26 +257,324 @@ __device__ void tiny_item(const jlc_problem* probs, const int* tiny_ids, int sta
     }
 }
 
-__global__ void __launch_bounds__(THREADS, 3) grouped_kernel(const jlc_problem* probs, const Item* items, int nitems,
-                                                          const int* tiny_ids, int* counter) {
-    extern __shared__ __align__(128) unsigned char smem_raw[];
-    char* smem = reinterpret_cast<char*>((reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~uintptr_t(127));
-    __shared__ int s_item;
-    for (;;) {
-        if (threadIdx.x == 0) s_item = atomicAdd(counter, 1);
-        __syncthreads();
-        const int it = s_item;
-        __syncthreads();
-        if (it >= nitems) return;
-        const Item w = items[it];
-        if (w.kind == KIND_TINY) {
-            tiny_item(probs, tiny_ids, w.prob, w.tm);
-        } else {
-            const jlc_problem P = probs[w.prob];
-            if (w.kind == KIND_T64) tile_dispatch<64, 64>(P, w.tm, w.tn, smem);
-            else tile_dispatch<32, 32>(P, w.tm, w.tn, smem);
+// ------------------------------------------------------ FP64 tiles, pipelined
+// One producer warp streams the k-blocks of a CTA's items, item after item,
+// through a ring of WS_STAGES shared-memory slots; four consumer warps run the
+// DMMA tiles.  The ring does not drain between items, so the next item's
+// first k-blocks load while the current item finishes; each consumer thread
+// reads its C elements when the item starts, so that read overlaps the
+// k-loop as well.  Items reach the producer in a fixed order (the longest-first
+// list dealt to the CTAs in serpentine rounds), so it reads the next item's
+// record while it streams the current one.
+//   full[s]   32 arrivals: each producer lane's cp.async into slot s landed
+//   empty[s]  4 arrivals: every consumer warp is done with slot s
+//   hfull[h]  1 arrival: item record h written
+//   hempty[h] 4 arrivals: every consumer warp has read item record h
+// Every wait is bounded; on a timeout the kernel records JLC_DEV_TIMEOUT and
+// unwinds.
+// The kernel comes in two builds: TMAX = 64 runs 32 x 32 and 64 x 64 tiles,
+// one CTA per SM (a 64 x 64 tile holds 2 x 32 accumulators and C values per
+// thread); TMAX = 32 runs 32 x 32 tiles only, two CTAs per SM.  A slot holds
+// one k-block of the largest tile.
+constexpr int WS_CONSUMERS = 128;
+constexpr int WS_THREADS = WS_CONSUMERS + 32;
+constexpr int WS_STAGES = 12;
+constexpr int WS_HDR = 4;
+__host__ __device__ constexpr int ws_slot(int tmax) { return 2 * tmax * 128; }
+__host__ __device__ constexpr int ws_smem(int tmax) { return WS_STAGES * ws_slot(tmax) + 128; }
+constexpr int KIND_END = 3;
+constexpr int TF_AK = 4, TF_BK = 8, TF_VA = 16, TF_VB = 32;
+
+// One work item as the kernel reads it: a tile of one problem with its
+// operand origins resolved, or a batch of tiny problems.
+struct alignas(16) TileItem {
+    const double* a;  // op(A) at row m0 of the tile
+    const double* b;  // op(B) at column n0 of the tile
+    double* c;        // C(m0, n0)
+    long long lda, ldb, ldc;
+    int rows, cols;   // valid rows / columns of the tile; tiny batch: first tiny index, count
+    int k;            // inner dimension (0 when alpha == 0)
+    int flags;        // kind in bits 0-1, then TF_* bits
+    double alpha, beta;
+};
+static_assert(sizeof(TileItem) == 80, "TileItem layout");
+
+__device__ __forceinline__ void cp_async_mbar_arrive(uint64_t* bar) {
+    asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
+// One k-block of one operand (ROWS rows x GBK k, x at the tile origin) by the
+// 32 producer lanes; layout and zero fill as load_operand.
+template <int ROWS, bool KMAJOR>
+__device__ __forceinline__ void ws_load(const double* x, long long ld, int nrows, int nk, char* s, int k0, bool vec,
+                                        int lane) {
+    if (vec) {
+#pragma unroll 4
+        for (int e = lane; e < ROWS * GBK / 2; e += 32) {
+            int r, c;
+            if (KMAJOR) {
+                r = e / (GBK / 2);
+                c = 2 * (e % (GBK / 2));
+            } else {
+                c = e / (ROWS / 2);
+                r = 2 * (e % (ROWS / 2));
+            }
+            const int gk = k0 + c;
+            const int valid = KMAJOR ? (r < nrows ? nk - gk : 0) : (gk < nk ? nrows - r : 0);
+            const int bytes = valid >= 2 ? 16 : (valid == 1 ? 8 : 0);
+            const double* src = bytes ? (KMAJOR ? x + r * ld + gk : x + (long long)gk * ld + r) : x;
+            cp_async16(s + op_off<KMAJOR>(r, c), src, bytes);
+        }
+    } else {
+#pragma unroll 4
+        for (int e = lane; e < ROWS * GBK; e += 32) {
+            const int r = KMAJOR ? e / GBK : e % ROWS;
+            const int c = KMAJOR ? e % GBK : e / ROWS;
+            const int gk = k0 + c;
+            const bool ok = r < nrows && gk < nk;
+            const double* src = ok ? (KMAJOR ? x + r * ld + gk : x + (long long)gk * ld + r) : x;
+            cp_async8(s + op_off<KMAJOR>(r, c), src, ok);
         }
     }
+}
+
+template <int BM, int BN, bool AK, bool BK>
+__device__ __forceinline__ void ws_load_block(const TileItem& w, char* slot, int k0, int lane) {
+    ws_load<BM, AK>(w.a, w.lda, w.rows, w.k, slot, k0, (w.flags & TF_VA) != 0, lane);
+    ws_load<BN, BK>(w.b, w.ldb, w.cols, w.k, slot + BM * 128, k0, (w.flags & TF_VB) != 0, lane);
+}
+
+struct WsRing {
+    char* slots;
+    int slot_bytes;
+    uint64_t* full;
+    uint64_t* empty;
+    int* status;
+    int stage = 0;
+    uint32_t phase = 0;
+    __device__ __forceinline__ void advance() {
+        if (++stage == WS_STAGES) {
+            stage = 0;
+            phase ^= 1u;
+        }
+    }
+};
+
+__device__ __forceinline__ int ws_item_index(int j) {
+    const int base = j * (int)gridDim.x;
+    return (j & 1) ? base + (int)gridDim.x - 1 - (int)blockIdx.x : base + (int)blockIdx.x;
+}
+
+template <int TMAX>
+__device__ void ws_producer(const TileItem* items, int nitems, WsRing ring, uint64_t* hfull, uint64_t* hempty,
+                            TileItem* hdr) {
+    const int lane = threadIdx.x & 31;
+    int hs = 0;
+    uint32_t hph = 0;
+    TileItem cur;
+    {
+        const int i0 = ws_item_index(0);
+        if (i0 < nitems) cur = items[i0];
+        else cur.flags = KIND_END;
+    }
+    for (int j = 0;; ++j) {
+        TileItem nxt;  // the next record is read while this item streams
+        const int in = ws_item_index(j + 1);
+        const int kind = cur.flags & 3;
+        if (kind != KIND_END) {
+            if (in < nitems) nxt = items[in];
+            else nxt.flags = KIND_END;
+        }
+        if (!mbar_wait(&hempty[hs], hph ^ 1u, ring.status)) break;
+        if (lane == 0) hdr[hs] = cur;
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&hfull[hs]);
+        if (++hs == WS_HDR) {
+            hs = 0;
+            hph ^= 1u;
+        }
+        if (kind == KIND_END) break;
+        if (kind != KIND_TINY) {
+            const int kblocks = (cur.k + GBK - 1) / GBK;
+            const int variant = (kind == KIND_T64 ? 4 : 0) + ((cur.flags & TF_AK) ? 2 : 0) + ((cur.flags & TF_BK) ? 1 : 0);
+            bool ok = true;
+            for (int kb = 0; kb < kblocks; ++kb) {
+                if (!mbar_wait(&ring.empty[ring.stage], ring.phase ^ 1u, ring.status)) {
+                    ok = false;
+                    break;
+                }
+                char* slot = ring.slots + ring.stage * ring.slot_bytes;
+                const int k0 = kb * GBK;
+                switch (TMAX == 64 ? variant : variant & 3) {
+                    case 0: ws_load_block<32, 32, false, false>(cur, slot, k0, lane); break;
+                    case 1: ws_load_block<32, 32, false, true>(cur, slot, k0, lane); break;
+                    case 2: ws_load_block<32, 32, true, false>(cur, slot, k0, lane); break;
+                    case 3: ws_load_block<32, 32, true, true>(cur, slot, k0, lane); break;
+                    case 4: ws_load_block<TMAX, TMAX, false, false>(cur, slot, k0, lane); break;
+                    case 5: ws_load_block<TMAX, TMAX, false, true>(cur, slot, k0, lane); break;
+                    case 6: ws_load_block<TMAX, TMAX, true, false>(cur, slot, k0, lane); break;
+                    default: ws_load_block<TMAX, TMAX, true, true>(cur, slot, k0, lane); break;
+                }
+                cp_async_mbar_arrive(&ring.full[ring.stage]);
+                ring.advance();
+            }
+            if (!ok) break;
+        }
+        cur = nxt;
+    }
+    cp_async_wait_all();  // no copy may land after the CTA has gone
+}
+
+// Runs one tile item on the consumer warps; false when a wait timed out.
+template <int BM, int BN, bool AK, bool BK>
+__device__ bool ws_tile(const TileItem& w, WsRing& ring) {
+    constexpr int WM = BM / 2, WN = BN / 2;  // 2 x 2 warps
+    constexpr int MT = WM / 16, NT = WN / 8;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int g = lane >> 2, t = lane & 3;
+    const int warp_m = warp >> 1, warp_n = warp & 1;
+    const int kblocks = (w.k + GBK - 1) / GBK;
+    const bool scale_a = w.alpha != 1.0, has_beta = w.beta != 0.0;
+
+    // C is read now and used in the epilogue, so the read overlaps the k-loop
+    double cv[MT][NT][4];
+#pragma unroll
+    for (int mt = 0; mt < MT; ++mt)
+#pragma unroll
+        for (int nt = 0; nt < NT; ++nt)
+#pragma unroll
+            for (int e = 0; e < 4; ++e) {
+                const int row = warp_m * WM + mt * 16 + g + 8 * (e >> 1);
+                const int col = warp_n * WN + nt * 8 + 2 * t + (e & 1);
+                cv[mt][nt][e] = (has_beta && row < w.rows && col < w.cols) ? w.c[row * w.ldc + col] : 0.0;
+            }
+    double acc[MT][NT][4];
+#pragma unroll
+    for (int i = 0; i < MT; ++i)
+#pragma unroll
+        for (int j = 0; j < NT; ++j)
+#pragma unroll
+            for (int e = 0; e < 4; ++e) acc[i][j][e] = 0.0;
+
+    for (int kb = 0; kb < kblocks; ++kb) {
+        if (!mbar_wait(&ring.full[ring.stage], ring.phase, ring.status)) return false;
+        const char* sA = ring.slots + ring.stage * ring.slot_bytes;
+        const char* sB = sA + BM * 128;
+#pragma unroll
+        for (int q = 0; q < GBK / 8; ++q) {
+            double bf[NT][2];
+#pragma unroll
+            for (int nt = 0; nt < NT; ++nt) {
+                const int c = warp_n * WN + nt * 8 + g;
+#pragma unroll
+                for (int j = 0; j < 2; ++j) bf[nt][j] = dmma::lds_b<BK>(sB, dmma::phys_k<8>(q, t, j), c);
+            }
+#pragma unroll
+            for (int mt = 0; mt < MT; ++mt) {
+                const int r = warp_m * WM + mt * 16 + g;
+                double af[4];
+#pragma unroll
+                for (int i = 0; i < 4; ++i) af[i] = dmma::lds_a<AK>(sA, r + 8 * (i & 1), dmma::phys_k<8>(q, t, i >> 1));
+                if (scale_a) {
+#pragma unroll
+                    for (int i = 0; i < 4; ++i) af[i] *= w.alpha;
+                }
+#pragma unroll
+                for (int nt = 0; nt < NT; ++nt) dmma::mma_f64<8>(acc[mt][nt], af, bf[nt]);
+            }
+        }
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&ring.empty[ring.stage]);
+        ring.advance();
+    }
+
+#pragma unroll
+    for (int mt = 0; mt < MT; ++mt)
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const int row = warp_m * WM + mt * 16 + g + 8 * h;
+            if (row >= w.rows) continue;
+            double* crow = w.c + row * w.ldc;
+#pragma unroll
+            for (int nt = 0; nt < NT; ++nt)
+#pragma unroll
+                for (int e = 0; e < 2; ++e) {
+                    const int col = warp_n * WN + nt * 8 + 2 * t + e;
+                    if (col < w.cols) {
+                        const double v = acc[mt][nt][2 * h + e];
+                        crow[col] = has_beta ? fma(w.beta, cv[mt][nt][2 * h + e], v) : v;
+                    }
+                }
+        }
+    return true;
+}
+
+template <int TMAX>
+__device__ void ws_consumer(const jlc_problem* probs, const int* tiny_ids, WsRing ring, uint64_t* hfull,
+                            uint64_t* hempty, const TileItem* hdr) {
+    const int lane = threadIdx.x & 31;
+    int hs = 0;
+    uint32_t hph = 0;
+    for (;;) {
+        if (!mbar_wait(&hfull[hs], hph, ring.status)) return;
+        const TileItem w = hdr[hs];
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&hempty[hs]);
+        if (++hs == WS_HDR) {
+            hs = 0;
+            hph ^= 1u;
+        }
+        const int kind = w.flags & 3;
+        if (kind == KIND_END) return;
+        if (kind == KIND_TINY) {
+            tiny_item(probs, tiny_ids, w.rows, w.cols);
+            continue;
+        }
+        const int variant = (kind == KIND_T64 ? 4 : 0) + ((w.flags & TF_AK) ? 2 : 0) + ((w.flags & TF_BK) ? 1 : 0);
+        bool ok;
+        switch (TMAX == 64 ? variant : variant & 3) {
+            case 0: ok = ws_tile<32, 32, false, false>(w, ring); break;
+            case 1: ok = ws_tile<32, 32, false, true>(w, ring); break;
+            case 2: ok = ws_tile<32, 32, true, false>(w, ring); break;
+            case 3: ok = ws_tile<32, 32, true, true>(w, ring); break;
+            case 4: ok = ws_tile<TMAX, TMAX, false, false>(w, ring); break;
+            case 5: ok = ws_tile<TMAX, TMAX, false, true>(w, ring); break;
+            case 6: ok = ws_tile<TMAX, TMAX, true, false>(w, ring); break;
+            default: ok = ws_tile<TMAX, TMAX, true, true>(w, ring); break;
+        }
+        if (!ok) return;
+    }
+}
+
+template <int TMAX>
+__global__ void __launch_bounds__(WS_THREADS, TMAX == 64 ? 1 : 2)
+    grouped_kernel(const jlc_problem* probs, const TileItem* items, int nitems, const int* tiny_ids, int* status) {
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    __shared__ __align__(8) uint64_t bars[2 * WS_STAGES + 2 * WS_HDR];
+    __shared__ TileItem hdr[WS_HDR];
+    WsRing ring;
+    ring.slots = reinterpret_cast<char*>((reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~uintptr_t(127));
+    ring.slot_bytes = ws_slot(TMAX);
+    ring.full = bars;
+    ring.empty = bars + WS_STAGES;
+    ring.status = status;
+    uint64_t* hfull = bars + 2 * WS_STAGES;
+    uint64_t* hempty = hfull + WS_HDR;
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < WS_STAGES; ++s) {
+            mbar_init(&ring.full[s], 32);
+            mbar_init(&ring.empty[s], WS_CONSUMERS / 32);
+        }
+        for (int h = 0; h < WS_HDR; ++h) {
+            mbar_init(&hfull[h], 1);
+            mbar_init(&hempty[h], WS_CONSUMERS / 32);
+        }
+        fence_barrier_init();
+    }
+    __syncthreads();
+    if (threadIdx.x >= WS_CONSUMERS) ws_producer<TMAX>(items, nitems, ring, hfull, hempty, hdr);
+    else ws_consumer<TMAX>(probs, tiny_ids, ring, hfull, hempty, hdr);
 }
 
 // ------------------------------------------------------ grouped Ozaki (residues)
@@ -680,7 +980,8 @@ struct jlc_grouped_plan {
     int* d_exps = nullptr;
     int* d_nonfinite = nullptr;
     jlc_problem* d_probs = nullptr;
-    jlc::grp::Item* d_items = nullptr;
+    jlc::grp::Item* d_items = nullptr;        // residue tiles
+    jlc::grp::TileItem* d_titems = nullptr;   // FP64 tiles
     int* d_tiny = nullptr;
     int* d_counter = nullptr;
     int nitems = 0;
@@ -688,6 +989,7 @@ struct jlc_grouped_plan {
     double flops = 0.0;
     int64_t n_int8 = 0, n_fp64 = 0;  // problems on residue tiles / on FP64 tiles
     int cfg[2] = {32, 64};
+    int tmax = 32;  // largest FP64 tile of the plan: picks the kernel build
     bool use_graph = false;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
@@ -730,6 +1032,7 @@ void free_plan_buffers(jlc_grouped_plan* pl) {
     if (pl->graph) cudaGraphDestroy(pl->graph);
     if (pl->d_probs) cudaFree(pl->d_probs);
     if (pl->d_items) cudaFree(pl->d_items);
+    if (pl->d_titems) cudaFree(pl->d_titems);
     if (pl->d_tiny) cudaFree(pl->d_tiny);
     if (pl->d_counter) cudaFree(pl->d_counter);
     if (pl->d_oz) cudaFree(pl->d_oz);
@@ -748,6 +1051,7 @@ void free_plan_buffers(jlc_grouped_plan* pl) {
     pl->graph = nullptr;
     pl->d_probs = nullptr;
     pl->d_items = nullptr;
+    pl->d_titems = nullptr;
     pl->d_tiny = nullptr;
     pl->d_counter = nullptr;
 }
@@ -760,10 +1064,41 @@ int upload(jlc_grouped_plan* pl, const std::vector<jlc_problem>& probs, const Wo
         if (e != cudaSuccess) return e;
         return bytes ? cudaMemcpyAsync(*dst, src, bytes, cudaMemcpyHostToDevice, st) : cudaSuccess;
     };
+    // the kernel's item records: operand origins of each tile resolved here
+    std::vector<TileItem> titems(wl.items.size());
+    for (size_t i = 0; i < wl.items.size(); ++i) {
+        const Item& it = wl.items[i];
+        TileItem& t = titems[i];
+        memset(&t, 0, sizeof(t));
+        if (it.kind == KIND_TINY) {
+            t.rows = it.prob;
+            t.cols = it.tm;
+            t.flags = KIND_TINY;
+            continue;
+        }
+        const jlc_problem& p = probs[it.prob];
+        const long long ts = it.kind == KIND_T64 ? 64 : 32;
+        const long long m0 = it.tm * ts, n0 = it.tn * ts;
+        const bool ak = p.layout_a == JLC_ROW_MAJOR, bk = p.layout_b == JLC_COL_MAJOR;
+        t.a = p.a ? (ak ? p.a + m0 * p.lda : p.a + m0) : nullptr;
+        t.b = p.b ? (bk ? p.b + n0 * p.ldb : p.b + n0) : nullptr;
+        t.c = p.c + m0 * p.ldc + n0;
+        t.lda = p.lda;
+        t.ldb = p.ldb;
+        t.ldc = p.ldc;
+        t.rows = (int)std::min<long long>(ts, p.m - m0);
+        t.cols = (int)std::min<long long>(ts, p.n - n0);
+        t.k = p.alpha == 0.0 ? 0 : (int)p.k;
+        t.alpha = p.alpha;
+        t.beta = p.beta;
+        // 16-byte copies need 16-byte aligned tile rows (origin and leading dimension)
+        const bool va = ((reinterpret_cast<uintptr_t>(t.a) & 15) == 0) && ((p.lda & 1) == 0);
+        const bool vb = ((reinterpret_cast<uintptr_t>(t.b) & 15) == 0) && ((p.ldb & 1) == 0);
+        t.flags = it.kind | (ak ? TF_AK : 0) | (bk ? TF_BK : 0) | (va ? TF_VA : 0) | (vb ? TF_VB : 0);
+    }
     cudaError_t e = alloc_copy((void**)&pl->d_probs, probs.data(), probs.size() * sizeof(jlc_problem));
-    if (e == cudaSuccess) e = alloc_copy((void**)&pl->d_items, wl.items.data(), wl.items.size() * sizeof(Item));
+    if (e == cudaSuccess) e = alloc_copy((void**)&pl->d_titems, titems.data(), titems.size() * sizeof(TileItem));
     if (e == cudaSuccess) e = alloc_copy((void**)&pl->d_tiny, wl.tiny.data(), wl.tiny.size() * sizeof(int));
-    if (e == cudaSuccess) e = cudaMalloc((void**)&pl->d_counter, sizeof(int));
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);  // host vectors are pageable and short-lived
     if (e != cudaSuccess) {
         cudaGetLastError();
@@ -771,9 +1106,17 @@ int upload(jlc_grouped_plan* pl, const std::vector<jlc_problem>& probs, const Wo
                     cudaGetErrorString(e));
     }
     pl->nitems = (int)wl.items.size();
+    pl->tmax = 32;
+    for (const Item& it : wl.items)
+        if (it.kind == KIND_T64) pl->tmax = 64;
     int per_sm = 0;
-    cudaFuncSetAttribute(grouped_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, grouped_kernel, THREADS, SMEM_BYTES);
+    if (pl->tmax == 64) {
+        cudaFuncSetAttribute(grouped_kernel<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, ws_smem(64));
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, grouped_kernel<64>, WS_THREADS, ws_smem(64));
+    } else {
+        cudaFuncSetAttribute(grouped_kernel<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, ws_smem(32));
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, grouped_kernel<32>, WS_THREADS, ws_smem(32));
+    }
     if (per_sm < 1) per_sm = 1;
     pl->grid = std::max(1, std::min(pl->nitems, ctx->sm_count * per_sm));
     return JLC_OK;
@@ -781,8 +1124,8 @@ int upload(jlc_grouped_plan* pl, const std::vector<jlc_problem>& probs, const Wo
 
 int launch_plan(jlc_grouped_plan* pl, cudaStream_t st) {
     if (pl->nitems == 0) return JLC_OK;
-    if (cudaMemsetAsync(pl->d_counter, 0, sizeof(int), st) != cudaSuccess) return JLC_E_CUDA;
     if (pl->oz) {
+        if (cudaMemsetAsync(pl->d_counter, 0, sizeof(int), st) != cudaSuccess) return JLC_E_CUDA;
         if (cudaMemsetAsync(pl->d_nonfinite, 0, (size_t)pl->count * sizeof(int), st) != cudaSuccess)
             return JLC_E_CUDA;
         if (pl->ntasks > 0)
@@ -796,8 +1139,12 @@ int launch_plan(jlc_grouped_plan* pl, cudaStream_t st) {
                                                                     pl->d_nonfinite, pl->d_counter);
         return cudaGetLastError() == cudaSuccess ? JLC_OK : JLC_E_LAUNCH;
     }
-    grouped_kernel<<<pl->grid, THREADS, SMEM_BYTES, st>>>(pl->d_probs, pl->d_items, pl->nitems, pl->d_tiny,
-                                                         pl->d_counter);
+    if (pl->tmax == 64)
+        grouped_kernel<64><<<pl->grid, WS_THREADS, ws_smem(64), st>>>(pl->d_probs, pl->d_titems, pl->nitems,
+                                                                     pl->d_tiny, pl->ctx->d_status);
+    else
+        grouped_kernel<32><<<pl->grid, WS_THREADS, ws_smem(32), st>>>(pl->d_probs, pl->d_titems, pl->nitems,
+                                                                     pl->d_tiny, pl->ctx->d_status);
     return cudaGetLastError() == cudaSuccess ? JLC_OK : JLC_E_LAUNCH;
 }
 
@@ -1104,6 +1451,7 @@ int jlc_dgemm_grouped_device(jlc_ctx* ctx, const jlc_problem* probs, int64_t cou
     cudaEventRecord(ctx->ev1, ctx->stream);
     cudaError_t e = cudaStreamSynchronize(ctx->stream);
     if (!rc && e != cudaSuccess) rc = gerr(ctx, JLC_E_CUDA, "grouped: %s", cudaGetErrorString(e));
+    if (!rc) rc = jlc_device_status(ctx);  // a bounded wait of the FP64 tiles that ran out
     if (!rc && rep) {
         float ms = 0.f;
         cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);

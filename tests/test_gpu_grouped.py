@@ -86,6 +86,36 @@ def test_grouped_mixed_batch(ctx, oracle):
     check_batch(oracle, probs, host, arena, "grouped")
 
 
+def test_grouped_small_tile_build_many_items(ctx, oracle):
+    """Only problems of the small class (max(m, n) <= 48): the plan runs the
+    32 x 32 build (two CTAs per SM) with several items per CTA, odd leading
+    dimensions (8-byte copies) beside even ones, and a few long products whose
+    k-blocks wrap the stage ring several times."""
+    rng = np.random.default_rng(17)
+    shapes = [tuple(int(x) for x in rng.integers(1, 49, size=3)) for _ in range(1400)]
+    shapes += [(32, 32, 2000), (48, 17, 1029), (5, 40, 777), (40, 40, 16), (33, 1, 100)]
+    probs, host, arena = make_batch(oracle, shapes, 19)
+    plan = ctx.grouped_plan(probs)
+    assert plan.info()["work_items"] > 2 * 296
+    plan.run()
+    ctx.synchronize()
+    check_batch(oracle, probs, host, arena, "small-tile build")
+    plan.close()
+
+
+def test_grouped_large_tile_long_k(ctx, oracle):
+    """64 x 64 tiles (the one-CTA-per-SM build) beside 32 x 32 ones, with k
+    long enough that one item's k-blocks wrap the stage ring, and alpha == 1
+    / beta == 0 (the unscaled paths)."""
+    shapes = [(130, 70, 3000), (64, 64, 16), (200, 90, 257), (49, 300, 1), (100, 100, 100)] + \
+             [(20, 30, 40)] * 50
+    probs, host, arena = make_batch(oracle, shapes, 23, alphas=[1.0] * len(shapes),
+                                    betas=[0.0, 1.0, -0.5, 0.0, 2.0] + [0.0] * 50)
+    rep = ctx.dgemm_grouped_device(probs)
+    assert rep["kernel"] == 4
+    check_batch(oracle, probs, host, arena, "large tiles")
+
+
 def test_grouped_plan_graph_replay_sees_new_data(ctx, oracle):
     import torch
     rng = np.random.default_rng(7)
