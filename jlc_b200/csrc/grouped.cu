@@ -7,26 +7,25 @@
 // bidiagonalisation (HouseholderQR.java:167-210, BlockedHessenbergQR.java:
 // 277-345), each a gemm / gemmStrided* call.  Here a plan turns a problem
 // table into a work list once; every run is a single launch (optionally a
-// CUDA graph replay) of persistent CTAs, each with one producer warp and four
-// DMMA warps:
-//   * tile items: one 32x32 or 64x64 tile of C of one problem, FP64
-//     mma.sync (m16n8k8) on k-blocks of 16 that the producer streams through
-//     a 12-slot cp.async ring without draining it between items; each
-//     operand is staged in the swizzled shared-memory layout that matches its
-//     global layout (K-major for row-major A / column-major B, MN-major
-//     otherwise), so the contiguous direction lands in 16-byte units and
-//     aligned operands move with 16-byte copies (8-byte copies otherwise,
-//     zero fill at ragged edges); alpha folded into the A fragments, C read
-//     when the item starts and beta fused in the epilogue;
+// CUDA graph replay) in which every warp of the persistent CTAs pulls work
+// items from an atomic counter on its own:
+//   * tile items: one 32x32 tile of C of one problem, FP64 mma.sync
+//     (m16n8k8) on k-blocks of 16 that the warp streams through its own ring
+//     of 2 or 3 cp.async slots; each operand is staged in the swizzled
+//     shared-memory layout that matches its global layout (K-major for
+//     row-major A / column-major B, MN-major otherwise), so the contiguous
+//     direction lands in 16-byte units and aligned operands move with 16-byte
+//     copies (8-byte copies otherwise, zero fill at ragged edges); alpha
+//     folded into the A fragments, beta fused in the epilogue;
 //   * tiny items: a batch of problems with m*n <= 64 and k <= 64 (the TINY
-//     and small SMALL shapes), one thread per output element running the
-//     reference's small-GEMM order (C <- beta*C, then an fma chain over p
-//     with alpha*a).
-// Items are ordered by decreasing cost (longest-processing-time first) and
-// dealt to the CTAs in serpentine rounds of the grid size.  The
-// tile shape of each shape class is chosen by an autotuner that times both
-// shapes on the plan's own problem shapes and caches the choice on disk,
-// keyed by device, SM count, library version and class.
+//     and small SMALL shapes) on one warp, one lane per output element (two
+//     rounds), running the reference's small-GEMM order (C <- beta*C, then an
+//     fma chain over p with alpha*a).
+// Items are ordered by decreasing cost (longest-processing-time first).  The
+// ring depth (2 slots per warp at three CTAs per SM, or 3 at two) is chosen
+// by an autotuner that times both on the plan's own problems and caches the
+// choice on disk, keyed by device, SM count, library version and the
+// batch's mean k (log2 bucket).
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -55,8 +54,7 @@ namespace grp {
 
 constexpr int THREADS = 128;
 constexpr int GBK = 16;  // k-values per stage (one 128-byte swizzled row per tile row)
-constexpr int TINY_ELEMS = THREADS;
-constexpr int KIND_TINY = 0, KIND_T32 = 1, KIND_T64 = 2;
+constexpr int KIND_TINY = 0, KIND_T32 = 1;
 constexpr int STAGES = 3;
 constexpr int SMEM_BYTES = STAGES * (64 + 64) * 128 + 128;
 
@@ -257,33 +255,23 @@ __device__ void tiny_item(const jlc_problem* probs, const int* tiny_ids, int sta
     }
 }
 
-// ------------------------------------------------------ FP64 tiles, pipelined
-// One producer warp streams the k-blocks of a CTA's items, item after item,
-// through a ring of WS_STAGES shared-memory slots; four consumer warps run the
-// DMMA tiles.  The ring does not drain between items, so the next item's
-// first k-blocks load while the current item finishes; each consumer thread
-// reads its C elements when the item starts, so that read overlaps the
-// k-loop as well.  Items reach the producer in a fixed order (the longest-first
-// list dealt to the CTAs in serpentine rounds), so it reads the next item's
-// record while it streams the current one.
-//   full[s]   32 arrivals: each producer lane's cp.async into slot s landed
-//   empty[s]  4 arrivals: every consumer warp is done with slot s
-//   hfull[h]  1 arrival: item record h written
-//   hempty[h] 4 arrivals: every consumer warp has read item record h
-// Every wait is bounded; on a timeout the kernel records JLC_DEV_TIMEOUT and
-// unwinds.
-// The kernel comes in two builds: TMAX = 64 runs 32 x 32 and 64 x 64 tiles,
-// one CTA per SM (a 64 x 64 tile holds 2 x 32 accumulators and C values per
-// thread); TMAX = 32 runs 32 x 32 tiles only, two CTAs per SM.  A slot holds
-// one k-block of the largest tile.
-constexpr int WS_CONSUMERS = 128;
-constexpr int WS_THREADS = WS_CONSUMERS + 32;
-constexpr int WS_STAGES = 12;
-constexpr int WS_HDR = 4;
-__host__ __device__ constexpr int ws_slot(int tmax) { return 2 * tmax * 128; }
-__host__ __device__ constexpr int ws_smem(int tmax) { return WS_STAGES * ws_slot(tmax) + 128; }
-constexpr int KIND_END = 3;
+// ------------------------------------------------------ FP64 tiles, one warp each
+// Every warp is its own worker: it takes an item (a 32 x 32 tile of one
+// problem, or a batch of tiny problems) from the shared counter, streams the
+// tile's k-blocks of 16 through its own ring of STAGES shared-memory slots
+// with cp.async, and runs FP64 mma.sync (m16n8k8) on them: 2 x 4 blocks of
+// 16 x 8, eight independent accumulator chains.  No CTA-wide barrier exists;
+// a warp waits only for its own copies, so the dozen warps of an SM overlap
+// one another's memory latency and the SM's DMMA pipe stays fed.  The next
+// item's index is fetched while the current one runs.  A tile with at most
+// 16 valid rows skips its second 16-row block, and columns are trimmed to
+// 8-column blocks, so ragged edges cost a 16 x 8 granule, not a 32 x 32 one.
+constexpr int WT_WARPS = 4;                  // warps per CTA
+constexpr int WT_THREADS = WT_WARPS * 32;
+constexpr int WT_SLOT = (32 + 32) * 128;     // one k-block of A and B: 8 KB
+constexpr int TINY_WARP_ELEMS = 64;          // elements of a tiny batch (two per lane)
 constexpr int TF_AK = 4, TF_BK = 8, TF_VA = 16, TF_VB = 32;
+__host__ __device__ constexpr int wt_smem(int stages) { return WT_WARPS * stages * WT_SLOT + 128; }
 
 // One work item as the kernel reads it: a tile of one problem with its
 // operand origins resolved, or a batch of tiny problems.
@@ -299,27 +287,25 @@ struct alignas(16) TileItem {
 };
 static_assert(sizeof(TileItem) == 80, "TileItem layout");
 
-__device__ __forceinline__ void cp_async_mbar_arrive(uint64_t* bar) {
-    asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];" ::"r"(smem_u32(bar)) : "memory");
-}
-__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
-
-// One k-block of one operand (ROWS rows x GBK k, x at the tile origin) by the
-// 32 producer lanes; layout and zero fill as load_operand.
-template <int ROWS, bool KMAJOR>
-__device__ __forceinline__ void ws_load(const double* x, long long ld, int nrows, int nk, char* s, int k0, bool vec,
-                                        int lane) {
+// One k-block of one operand (32 rows x GBK k, x at the tile origin, `live`
+// rows copied: rows past it are never read) by the 32 lanes of a warp;
+// layout and zero fill as load_operand.
+template <bool KMAJOR>
+__device__ __forceinline__ void wt_load(const double* x, long long ld, int nrows, int live, int nk, char* s, int k0,
+                                        bool vec, int lane) {
     if (vec) {
-#pragma unroll 4
-        for (int e = lane; e < ROWS * GBK / 2; e += 32) {
+#pragma unroll
+        for (int i = 0; i < 32 * GBK / 2 / 32; ++i) {
+            const int e = lane + 32 * i;
             int r, c;
             if (KMAJOR) {
                 r = e / (GBK / 2);
                 c = 2 * (e % (GBK / 2));
             } else {
-                c = e / (ROWS / 2);
-                r = 2 * (e % (ROWS / 2));
+                c = e / 16;
+                r = 2 * (e % 16);
             }
+            if (r >= live) continue;
             const int gk = k0 + c;
             const int valid = KMAJOR ? (r < nrows ? nk - gk : 0) : (gk < nk ? nrows - r : 0);
             const int bytes = valid >= 2 ? 16 : (valid == 1 ? 8 : 0);
@@ -328,9 +314,11 @@ __device__ __forceinline__ void ws_load(const double* x, long long ld, int nrows
         }
     } else {
 #pragma unroll 4
-        for (int e = lane; e < ROWS * GBK; e += 32) {
-            const int r = KMAJOR ? e / GBK : e % ROWS;
-            const int c = KMAJOR ? e % GBK : e / ROWS;
+        for (int i = 0; i < 32 * GBK / 32; ++i) {
+            const int e = lane + 32 * i;
+            const int r = KMAJOR ? e / GBK : e % 32;
+            const int c = KMAJOR ? e % GBK : e / 32;
+            if (r >= live) continue;
             const int gk = k0 + c;
             const bool ok = r < nrows && gk < nk;
             const double* src = ok ? (KMAJOR ? x + r * ld + gk : x + (long long)gk * ld + r) : x;
@@ -339,242 +327,139 @@ __device__ __forceinline__ void ws_load(const double* x, long long ld, int nrows
     }
 }
 
-template <int BM, int BN, bool AK, bool BK>
-__device__ __forceinline__ void ws_load_block(const TileItem& w, char* slot, int k0, int lane) {
-    ws_load<BM, AK>(w.a, w.lda, w.rows, w.k, slot, k0, (w.flags & TF_VA) != 0, lane);
-    ws_load<BN, BK>(w.b, w.ldb, w.cols, w.k, slot + BM * 128, k0, (w.flags & TF_VB) != 0, lane);
-}
-
-struct WsRing {
-    char* slots;
-    int slot_bytes;
-    uint64_t* full;
-    uint64_t* empty;
-    int* status;
-    int stage = 0;
-    uint32_t phase = 0;
-    __device__ __forceinline__ void advance() {
-        if (++stage == WS_STAGES) {
-            stage = 0;
-            phase ^= 1u;
-        }
-    }
-};
-
-__device__ __forceinline__ int ws_item_index(int j) {
-    const int base = j * (int)gridDim.x;
-    return (j & 1) ? base + (int)gridDim.x - 1 - (int)blockIdx.x : base + (int)blockIdx.x;
-}
-
-template <int TMAX>
-__device__ void ws_producer(const TileItem* items, int nitems, WsRing ring, uint64_t* hfull, uint64_t* hempty,
-                            TileItem* hdr) {
-    const int lane = threadIdx.x & 31;
-    int hs = 0;
-    uint32_t hph = 0;
-    TileItem cur;
-    {
-        const int i0 = ws_item_index(0);
-        if (i0 < nitems) cur = items[i0];
-        else cur.flags = KIND_END;
-    }
-    for (int j = 0;; ++j) {
-        TileItem nxt;  // the next record is read while this item streams
-        const int in = ws_item_index(j + 1);
-        const int kind = cur.flags & 3;
-        if (kind != KIND_END) {
-            if (in < nitems) nxt = items[in];
-            else nxt.flags = KIND_END;
-        }
-        if (!mbar_wait(&hempty[hs], hph ^ 1u, ring.status)) break;
-        if (lane == 0) hdr[hs] = cur;
-        __syncwarp();
-        if (lane == 0) mbar_arrive(&hfull[hs]);
-        if (++hs == WS_HDR) {
-            hs = 0;
-            hph ^= 1u;
-        }
-        if (kind == KIND_END) break;
-        if (kind != KIND_TINY) {
-            const int kblocks = (cur.k + GBK - 1) / GBK;
-            const int variant = (kind == KIND_T64 ? 4 : 0) + ((cur.flags & TF_AK) ? 2 : 0) + ((cur.flags & TF_BK) ? 1 : 0);
-            bool ok = true;
-            for (int kb = 0; kb < kblocks; ++kb) {
-                if (!mbar_wait(&ring.empty[ring.stage], ring.phase ^ 1u, ring.status)) {
-                    ok = false;
-                    break;
-                }
-                char* slot = ring.slots + ring.stage * ring.slot_bytes;
-                const int k0 = kb * GBK;
-                switch (TMAX == 64 ? variant : variant & 3) {
-                    case 0: ws_load_block<32, 32, false, false>(cur, slot, k0, lane); break;
-                    case 1: ws_load_block<32, 32, false, true>(cur, slot, k0, lane); break;
-                    case 2: ws_load_block<32, 32, true, false>(cur, slot, k0, lane); break;
-                    case 3: ws_load_block<32, 32, true, true>(cur, slot, k0, lane); break;
-                    case 4: ws_load_block<TMAX, TMAX, false, false>(cur, slot, k0, lane); break;
-                    case 5: ws_load_block<TMAX, TMAX, false, true>(cur, slot, k0, lane); break;
-                    case 6: ws_load_block<TMAX, TMAX, true, false>(cur, slot, k0, lane); break;
-                    default: ws_load_block<TMAX, TMAX, true, true>(cur, slot, k0, lane); break;
-                }
-                cp_async_mbar_arrive(&ring.full[ring.stage]);
-                ring.advance();
-            }
-            if (!ok) break;
-        }
-        cur = nxt;
-    }
-    cp_async_wait_all();  // no copy may land after the CTA has gone
-}
-
-// Runs one tile item on the consumer warps; false when a wait timed out.
-template <int BM, int BN, bool AK, bool BK>
-__device__ bool ws_tile(const TileItem& w, WsRing& ring) {
-    constexpr int WM = BM / 2, WN = BN / 2;  // 2 x 2 warps
-    constexpr int MT = WM / 16, NT = WN / 8;
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+template <bool AK, bool BK, int STAGES>
+__device__ void wt_tile(const TileItem& w, char* ring, int lane) {
     const int g = lane >> 2, t = lane & 3;
-    const int warp_m = warp >> 1, warp_n = warp & 1;
     const int kblocks = (w.k + GBK - 1) / GBK;
-    const bool scale_a = w.alpha != 1.0, has_beta = w.beta != 0.0;
-
-    // C is read now and used in the epilogue, so the read overlaps the k-loop
-    double cv[MT][NT][4];
+    const int mtv = w.rows > 16 ? 2 : 1;         // 16-row blocks with valid rows
+    const int ntv = (w.cols + 7) >> 3;           // 8-column blocks with valid columns
+    const int live_a = 16 * mtv, live_b = 8 * ntv;
+    const bool va = (w.flags & TF_VA) != 0, vb = (w.flags & TF_VB) != 0;
+    const bool scale_a = w.alpha != 1.0;
+    auto load = [&](int kb) {
+        char* sA = ring + (kb % STAGES) * WT_SLOT;
+        wt_load<AK>(w.a, w.lda, w.rows, live_a, w.k, sA, kb * GBK, va, lane);
+        wt_load<BK>(w.b, w.ldb, w.cols, live_b, w.k, sA + 32 * 128, kb * GBK, vb, lane);
+    };
+    double acc[2][4][4];
 #pragma unroll
-    for (int mt = 0; mt < MT; ++mt)
+    for (int i = 0; i < 2; ++i)
 #pragma unroll
-        for (int nt = 0; nt < NT; ++nt)
-#pragma unroll
-            for (int e = 0; e < 4; ++e) {
-                const int row = warp_m * WM + mt * 16 + g + 8 * (e >> 1);
-                const int col = warp_n * WN + nt * 8 + 2 * t + (e & 1);
-                cv[mt][nt][e] = (has_beta && row < w.rows && col < w.cols) ? w.c[row * w.ldc + col] : 0.0;
-            }
-    double acc[MT][NT][4];
-#pragma unroll
-    for (int i = 0; i < MT; ++i)
-#pragma unroll
-        for (int j = 0; j < NT; ++j)
+        for (int j = 0; j < 4; ++j)
 #pragma unroll
             for (int e = 0; e < 4; ++e) acc[i][j][e] = 0.0;
 
+    // the slots were last read by this warp's previous item
+    __syncwarp();
+#pragma unroll
+    for (int s = 0; s < STAGES - 1; ++s) {
+        if (s < kblocks) load(s);
+        cp_async_commit();
+    }
     for (int kb = 0; kb < kblocks; ++kb) {
-        if (!mbar_wait(&ring.full[ring.stage], ring.phase, ring.status)) return false;
-        const char* sA = ring.slots + ring.stage * ring.slot_bytes;
-        const char* sB = sA + BM * 128;
+        cp_async_wait<STAGES - 2>();  // this lane's copies of block kb have landed ...
+        __syncwarp();                 // ... and every lane's; block kb-1's slot is free
+        if (kb + STAGES - 1 < kblocks) load(kb + STAGES - 1);
+        cp_async_commit();
+        const char* sA = ring + (kb % STAGES) * WT_SLOT;
+        const char* sB = sA + 32 * 128;
 #pragma unroll
         for (int q = 0; q < GBK / 8; ++q) {
-            double bf[NT][2];
+            double bf[4][2];
 #pragma unroll
-            for (int nt = 0; nt < NT; ++nt) {
-                const int c = warp_n * WN + nt * 8 + g;
+            for (int nt = 0; nt < 4; ++nt)
 #pragma unroll
-                for (int j = 0; j < 2; ++j) bf[nt][j] = dmma::lds_b<BK>(sB, dmma::phys_k<8>(q, t, j), c);
-            }
+                for (int j = 0; j < 2; ++j)
+                    bf[nt][j] = nt < ntv ? dmma::lds_b<BK>(sB, dmma::phys_k<8>(q, t, j), nt * 8 + g) : 0.0;
 #pragma unroll
-            for (int mt = 0; mt < MT; ++mt) {
-                const int r = warp_m * WM + mt * 16 + g;
+            for (int mt = 0; mt < 2; ++mt) {
+                if (mt >= mtv) break;
                 double af[4];
 #pragma unroll
-                for (int i = 0; i < 4; ++i) af[i] = dmma::lds_a<AK>(sA, r + 8 * (i & 1), dmma::phys_k<8>(q, t, i >> 1));
+                for (int i = 0; i < 4; ++i)
+                    af[i] = dmma::lds_a<AK>(sA, mt * 16 + g + 8 * (i & 1), dmma::phys_k<8>(q, t, i >> 1));
                 if (scale_a) {
 #pragma unroll
                     for (int i = 0; i < 4; ++i) af[i] *= w.alpha;
                 }
 #pragma unroll
-                for (int nt = 0; nt < NT; ++nt) dmma::mma_f64<8>(acc[mt][nt], af, bf[nt]);
+                for (int nt = 0; nt < 4; ++nt)
+                    if (nt < ntv) dmma::mma_f64<8>(acc[mt][nt], af, bf[nt]);
             }
         }
-        __syncwarp();
-        if (lane == 0) mbar_arrive(&ring.empty[ring.stage]);
-        ring.advance();
     }
+    cp_async_wait<0>();
 
+    const bool has_beta = w.beta != 0.0;
 #pragma unroll
-    for (int mt = 0; mt < MT; ++mt)
+    for (int mt = 0; mt < 2; ++mt)
 #pragma unroll
         for (int h = 0; h < 2; ++h) {
-            const int row = warp_m * WM + mt * 16 + g + 8 * h;
+            const int row = mt * 16 + g + 8 * h;
             if (row >= w.rows) continue;
             double* crow = w.c + row * w.ldc;
 #pragma unroll
-            for (int nt = 0; nt < NT; ++nt)
+            for (int nt = 0; nt < 4; ++nt)
 #pragma unroll
                 for (int e = 0; e < 2; ++e) {
-                    const int col = warp_n * WN + nt * 8 + 2 * t + e;
+                    const int col = nt * 8 + 2 * t + e;
                     if (col < w.cols) {
                         const double v = acc[mt][nt][2 * h + e];
-                        crow[col] = has_beta ? fma(w.beta, cv[mt][nt][2 * h + e], v) : v;
+                        crow[col] = has_beta ? fma(w.beta, crow[col], v) : v;
                     }
                 }
         }
-    return true;
 }
 
-template <int TMAX>
-__device__ void ws_consumer(const jlc_problem* probs, const int* tiny_ids, WsRing ring, uint64_t* hfull,
-                            uint64_t* hempty, const TileItem* hdr) {
-    const int lane = threadIdx.x & 31;
-    int hs = 0;
-    uint32_t hph = 0;
-    for (;;) {
-        if (!mbar_wait(&hfull[hs], hph, ring.status)) return;
-        const TileItem w = hdr[hs];
-        __syncwarp();
-        if (lane == 0) mbar_arrive(&hempty[hs]);
-        if (++hs == WS_HDR) {
-            hs = 0;
-            hph ^= 1u;
+// A batch of tiny problems on one warp, elements lane and lane + 32.
+__device__ void tiny_warp_item(const jlc_problem* probs, const int* tiny_ids, int start, int count, int lane) {
+    int off = 0;
+    for (int q = 0; q < count; ++q) {
+        const jlc_problem& P = probs[tiny_ids[start + q]];
+        const int sz = (int)(P.m * P.n);
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const int e = lane + 32 * h - off;
+            if (e >= 0 && e < sz) {
+                const long long i = e / P.n, j = e % P.n;
+                double* cij = P.c + i * P.ldc + j;
+                double acc = (P.beta == 0.0) ? 0.0 : (P.beta == 1.0 ? *cij : *cij * P.beta);
+                if (P.alpha != 0.0)
+                    for (long long p = 0; p < P.k; ++p) acc = fma(P.alpha * elem_a(P, i, p), elem_b(P, p, j), acc);
+                *cij = acc;
+            }
         }
-        const int kind = w.flags & 3;
-        if (kind == KIND_END) return;
-        if (kind == KIND_TINY) {
-            tiny_item(probs, tiny_ids, w.rows, w.cols);
-            continue;
-        }
-        const int variant = (kind == KIND_T64 ? 4 : 0) + ((w.flags & TF_AK) ? 2 : 0) + ((w.flags & TF_BK) ? 1 : 0);
-        bool ok;
-        switch (TMAX == 64 ? variant : variant & 3) {
-            case 0: ok = ws_tile<32, 32, false, false>(w, ring); break;
-            case 1: ok = ws_tile<32, 32, false, true>(w, ring); break;
-            case 2: ok = ws_tile<32, 32, true, false>(w, ring); break;
-            case 3: ok = ws_tile<32, 32, true, true>(w, ring); break;
-            case 4: ok = ws_tile<TMAX, TMAX, false, false>(w, ring); break;
-            case 5: ok = ws_tile<TMAX, TMAX, false, true>(w, ring); break;
-            case 6: ok = ws_tile<TMAX, TMAX, true, false>(w, ring); break;
-            default: ok = ws_tile<TMAX, TMAX, true, true>(w, ring); break;
-        }
-        if (!ok) return;
+        off += sz;
     }
 }
 
-template <int TMAX>
-__global__ void __launch_bounds__(WS_THREADS, TMAX == 64 ? 1 : 2)
-    grouped_kernel(const jlc_problem* probs, const TileItem* items, int nitems, const int* tiny_ids, int* status) {
+template <int STAGES>
+__global__ void __launch_bounds__(WT_THREADS, STAGES == 2 ? 3 : 2)
+    grouped_kernel(const jlc_problem* probs, const TileItem* items, int nitems, const int* tiny_ids, int* counter) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
-    __shared__ __align__(8) uint64_t bars[2 * WS_STAGES + 2 * WS_HDR];
-    __shared__ TileItem hdr[WS_HDR];
-    WsRing ring;
-    ring.slots = reinterpret_cast<char*>((reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~uintptr_t(127));
-    ring.slot_bytes = ws_slot(TMAX);
-    ring.full = bars;
-    ring.empty = bars + WS_STAGES;
-    ring.status = status;
-    uint64_t* hfull = bars + 2 * WS_STAGES;
-    uint64_t* hempty = hfull + WS_HDR;
-    if (threadIdx.x == 0) {
-        for (int s = 0; s < WS_STAGES; ++s) {
-            mbar_init(&ring.full[s], 32);
-            mbar_init(&ring.empty[s], WS_CONSUMERS / 32);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    char* ring = reinterpret_cast<char*>((reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~uintptr_t(127)) +
+                 warp * STAGES * WT_SLOT;
+    int it = 0;
+    if (lane == 0) it = atomicAdd(counter, 1);
+    it = __shfl_sync(0xffffffffu, it, 0);
+    while (it < nitems) {
+        int nxt = 0;  // the next index arrives while this item runs
+        if (lane == 0) nxt = atomicAdd(counter, 1);
+        const TileItem w = items[it];
+        const int kind = w.flags & 3;
+        if (kind == KIND_TINY) {
+            tiny_warp_item(probs, tiny_ids, w.rows, w.cols, lane);
+        } else {
+            switch (((w.flags & TF_AK) ? 2 : 0) + ((w.flags & TF_BK) ? 1 : 0)) {
+                case 0: wt_tile<false, false, STAGES>(w, ring, lane); break;
+                case 1: wt_tile<false, true, STAGES>(w, ring, lane); break;
+                case 2: wt_tile<true, false, STAGES>(w, ring, lane); break;
+                default: wt_tile<true, true, STAGES>(w, ring, lane); break;
+            }
         }
-        for (int h = 0; h < WS_HDR; ++h) {
-            mbar_init(&hfull[h], 1);
-            mbar_init(&hempty[h], WS_CONSUMERS / 32);
-        }
-        fence_barrier_init();
+        it = __shfl_sync(0xffffffffu, nxt, 0);
     }
-    __syncthreads();
-    if (threadIdx.x >= WS_CONSUMERS) ws_producer<TMAX>(items, nitems, ring, hfull, hempty, hdr);
-    else ws_consumer<TMAX>(probs, tiny_ids, ring, hfull, hempty, hdr);
 }
 
 // ------------------------------------------------------ grouped Ozaki (residues)
@@ -861,7 +746,6 @@ __global__ void __launch_bounds__(THREADS, 3) grouped_oz_kernel(const jlc_proble
 
 // ------------------------------------------------------------------ host side
 bool is_tiny(const jlc_problem& p) { return p.m * p.n <= 64 && p.k <= 64; }
-int shape_class(const jlc_problem& p) { return std::max(p.m, p.n) <= 48 ? 0 : 1; }
 
 struct WorkList {
     std::vector<Item> items;
@@ -869,7 +753,7 @@ struct WorkList {
     double flops = 0.0;
 };
 
-void build_work(const std::vector<jlc_problem>& probs, const int cfg[2], int only_class, WorkList& wl) {
+void build_work(const std::vector<jlc_problem>& probs, WorkList& wl) {
     struct Costed {
         Item it;
         double cost;
@@ -889,9 +773,8 @@ void build_work(const std::vector<jlc_problem>& probs, const int cfg[2], int onl
         const double kk = p.alpha == 0.0 ? 0.0 : (double)p.k;
         wl.flops += 2.0 * p.m * p.n * kk;
         if (is_tiny(p)) {
-            if (only_class >= 0) continue;
             const int sz = (int)(p.m * p.n);
-            if (batch_elems + sz > TINY_ELEMS) flush_batch();
+            if (batch_elems + sz > TINY_WARP_ELEMS) flush_batch();
             if (batch_count == 0) batch_start = (int)wl.tiny.size();
             wl.tiny.push_back(i);
             ++batch_count;
@@ -899,13 +782,16 @@ void build_work(const std::vector<jlc_problem>& probs, const int cfg[2], int onl
             batch_cost += (double)sz * (kk + 1.0);
             continue;
         }
-        const int cls = shape_class(p);
-        if (only_class >= 0 && cls != only_class) continue;
-        const int ts = cfg[cls];
-        const int kind = ts == 64 ? KIND_T64 : KIND_T32;
-        const int tmn = (int)((p.m + ts - 1) / ts), tnn = (int)((p.n + ts - 1) / ts);
+        // cost: the 16 x 8 blocks the tile runs, times its k-blocks (+1 for
+        // the fixed cost of an item)
+        const int tmn = (int)((p.m + 31) / 32), tnn = (int)((p.n + 31) / 32);
         for (int a = 0; a < tmn; ++a)
-            for (int b = 0; b < tnn; ++b) v.push_back({Item{i, a, b, kind}, (double)ts * ts * (kk + 16.0)});
+            for (int b = 0; b < tnn; ++b) {
+                const long long rows = std::min<long long>(32, p.m - 32LL * a);
+                const long long cols = std::min<long long>(32, p.n - 32LL * b);
+                const double blocks = (rows > 16 ? 2.0 : 1.0) * (double)((cols + 7) / 8);
+                v.push_back({Item{i, a, b, KIND_T32}, blocks * (std::ceil(kk / GBK) + 1.0)});
+            }
     }
     flush_batch();
     std::stable_sort(v.begin(), v.end(), [](const Costed& x, const Costed& y) { return x.cost > y.cost; });
@@ -921,14 +807,14 @@ std::string tune_cache_path() {
 
 std::mutex g_tune_mu;
 
-std::string tune_key(int device, int sm_count, int cls) {
+std::string tune_key(int device, int sm_count, const char* what) {
     cudaDeviceProp prop;
     cudaGetDeviceProperties(&prop, device);
     std::ostringstream os;
     std::string name = prop.name;
     for (auto& ch : name)
         if (ch == ' ') ch = '_';
-    os << name << "|sm" << sm_count << "|v" << JLCGPU_VERSION << "|grouped-fp64|class" << cls;
+    os << name << "|sm" << sm_count << "|v" << JLCGPU_VERSION << "|grouped-fp64|" << what;
     return os.str();
 }
 
@@ -988,8 +874,8 @@ struct jlc_grouped_plan {
     int grid = 0;
     double flops = 0.0;
     int64_t n_int8 = 0, n_fp64 = 0;  // problems on residue tiles / on FP64 tiles
-    int cfg[2] = {32, 64};
-    int tmax = 32;  // largest FP64 tile of the plan: picks the kernel build
+    int tile = 32;    // FP64 tile edge (residue tiles: OZ_T)
+    int stages = 2;   // ring slots per warp of the FP64 tiles (autotuned)
     bool use_graph = false;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
@@ -1077,7 +963,7 @@ int upload(jlc_grouped_plan* pl, const std::vector<jlc_problem>& probs, const Wo
             continue;
         }
         const jlc_problem& p = probs[it.prob];
-        const long long ts = it.kind == KIND_T64 ? 64 : 32;
+        const long long ts = 32;
         const long long m0 = it.tm * ts, n0 = it.tn * ts;
         const bool ak = p.layout_a == JLC_ROW_MAJOR, bk = p.layout_b == JLC_COL_MAJOR;
         t.a = p.a ? (ak ? p.a + m0 * p.lda : p.a + m0) : nullptr;
@@ -1099,6 +985,7 @@ int upload(jlc_grouped_plan* pl, const std::vector<jlc_problem>& probs, const Wo
     cudaError_t e = alloc_copy((void**)&pl->d_probs, probs.data(), probs.size() * sizeof(jlc_problem));
     if (e == cudaSuccess) e = alloc_copy((void**)&pl->d_titems, titems.data(), titems.size() * sizeof(TileItem));
     if (e == cudaSuccess) e = alloc_copy((void**)&pl->d_tiny, wl.tiny.data(), wl.tiny.size() * sizeof(int));
+    if (e == cudaSuccess) e = cudaMalloc((void**)&pl->d_counter, sizeof(int));
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);  // host vectors are pageable and short-lived
     if (e != cudaSuccess) {
         cudaGetLastError();
@@ -1106,19 +993,16 @@ int upload(jlc_grouped_plan* pl, const std::vector<jlc_problem>& probs, const Wo
                     cudaGetErrorString(e));
     }
     pl->nitems = (int)wl.items.size();
-    pl->tmax = 32;
-    for (const Item& it : wl.items)
-        if (it.kind == KIND_T64) pl->tmax = 64;
     int per_sm = 0;
-    if (pl->tmax == 64) {
-        cudaFuncSetAttribute(grouped_kernel<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, ws_smem(64));
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, grouped_kernel<64>, WS_THREADS, ws_smem(64));
+    if (pl->stages == 3) {
+        cudaFuncSetAttribute(grouped_kernel<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, wt_smem(3));
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, grouped_kernel<3>, WT_THREADS, wt_smem(3));
     } else {
-        cudaFuncSetAttribute(grouped_kernel<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, ws_smem(32));
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, grouped_kernel<32>, WS_THREADS, ws_smem(32));
+        cudaFuncSetAttribute(grouped_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, wt_smem(2));
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, grouped_kernel<2>, WT_THREADS, wt_smem(2));
     }
     if (per_sm < 1) per_sm = 1;
-    pl->grid = std::max(1, std::min(pl->nitems, ctx->sm_count * per_sm));
+    pl->grid = std::max(1, std::min((pl->nitems + WT_WARPS - 1) / WT_WARPS, ctx->sm_count * per_sm));
     return JLC_OK;
 }
 
@@ -1139,56 +1023,50 @@ int launch_plan(jlc_grouped_plan* pl, cudaStream_t st) {
                                                                     pl->d_nonfinite, pl->d_counter);
         return cudaGetLastError() == cudaSuccess ? JLC_OK : JLC_E_LAUNCH;
     }
-    if (pl->tmax == 64)
-        grouped_kernel<64><<<pl->grid, WS_THREADS, ws_smem(64), st>>>(pl->d_probs, pl->d_titems, pl->nitems,
-                                                                     pl->d_tiny, pl->ctx->d_status);
+    if (cudaMemsetAsync(pl->d_counter, 0, sizeof(int), st) != cudaSuccess) return JLC_E_CUDA;
+    if (pl->stages == 3)
+        grouped_kernel<3><<<pl->grid, WT_THREADS, wt_smem(3), st>>>(pl->d_probs, pl->d_titems, pl->nitems,
+                                                                   pl->d_tiny, pl->d_counter);
     else
-        grouped_kernel<32><<<pl->grid, WS_THREADS, ws_smem(32), st>>>(pl->d_probs, pl->d_titems, pl->nitems,
-                                                                     pl->d_tiny, pl->ctx->d_status);
+        grouped_kernel<2><<<pl->grid, WT_THREADS, wt_smem(2), st>>>(pl->d_probs, pl->d_titems, pl->nitems,
+                                                                   pl->d_tiny, pl->d_counter);
     return cudaGetLastError() == cudaSuccess ? JLC_OK : JLC_E_LAUNCH;
 }
 
-// Times both tile shapes of one shape class on synthetic operands with the
-// plan's problem shapes (the caller's C is never touched) and returns the
-// faster tile size, or 0 when the class is empty.
-int autotune_class(jlc_ctx* ctx, const std::vector<jlc_problem>& probs, int cls) {
-    size_t ma = 0, mb = 0, mc = 0;
+// Times the plan's problems with both ring depths (2 slots per warp at three
+// CTAs per SM, 3 slots at two) and returns the faster, or 0 when there is
+// nothing to time.  The runs read the caller's A and B and write every C
+// into one scratch tile, so the caller's C is never touched.
+int autotune_stages(jlc_ctx* ctx, const std::vector<jlc_problem>& probs) {
+    size_t mc = 0;
     std::vector<jlc_problem> syn;
     for (const auto& p : probs) {
-        if (p.m == 0 || p.n == 0 || is_tiny(p) || shape_class(p) != cls) continue;
+        if (p.m == 0 || p.n == 0) continue;
         syn.push_back(p);
-        ma = std::max(ma, (size_t)(p.m * p.k));
-        mb = std::max(mb, (size_t)(p.k * p.n));
         mc = std::max(mc, (size_t)(p.m * p.n));
     }
     if (syn.empty()) return 0;
     double* buf = nullptr;
-    if (cudaMalloc(&buf, (ma + mb + mc + 3) * sizeof(double)) != cudaSuccess) {
+    if (cudaMalloc(&buf, (mc + 1) * sizeof(double)) != cudaSuccess) {
         cudaGetLastError();
         return 0;
     }
-    cudaMemsetAsync(buf, 0x3f, (ma + mb + mc + 3) * sizeof(double), ctx->stream);
     for (auto& p : syn) {
-        p.a = buf;
-        p.b = buf + ma + 1;
-        p.c = buf + ma + mb + 2;
-        p.lda = p.layout_a == JLC_ROW_MAJOR ? p.k : p.m;
-        p.ldb = p.layout_b == JLC_ROW_MAJOR ? p.n : p.k;
+        p.c = buf;
         p.ldc = p.n;
         p.beta = 0.0;
-        if (p.alpha == 0.0) p.alpha = 1.0;
     }
+    WorkList wl;
+    build_work(syn, wl);
     int best = 0;
     float best_ms = 1e30f;
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
-    for (int ts : {32, 64}) {
-        int cfg[2] = {ts, ts};
-        WorkList wl;
-        build_work(syn, cfg, cls, wl);
+    for (int stages : {2, 3}) {
         jlc_grouped_plan tmp;
         tmp.ctx = ctx;
+        tmp.stages = stages;
         if (upload(&tmp, syn, wl) != JLC_OK) {
             free_plan_buffers(&tmp);
             continue;
@@ -1206,7 +1084,7 @@ int autotune_class(jlc_ctx* ctx, const std::vector<jlc_problem>& probs, int cls)
         }
         if (t < best_ms) {
             best_ms = t;
-            best = ts;
+            best = stages;
         }
         free_plan_buffers(&tmp);
     }
@@ -1376,18 +1254,29 @@ int jlc_grouped_plan_create(jlc_ctx* ctx, const jlc_problem* probs, int64_t coun
             delete pl;
             return rc;
         }
-        pl->cfg[0] = pl->cfg[1] = OZ_T;
+        pl->tile = OZ_T;
         return finish_plan(pl, flags, out);
     }
-    for (int cls = 0; cls < 2; ++cls) {
-        const std::string key = tune_key(ctx->device, ctx->sm_count, cls);
-        int ts = (flags & JLC_GROUPED_AUTOTUNE) ? autotune_class(ctx, v, cls) : 0;
-        if (ts) tune_store(key, ts);
-        else ts = tune_lookup(key);
-        if (ts == 32 || ts == 64) pl->cfg[cls] = ts;
+    {
+        // the ring depth is tuned per batch profile: log2 of the mean k of
+        // the non-empty problems
+        double ksum = 0.0;
+        int64_t cnt = 0;
+        for (const jlc_problem& p : v)
+            if (p.m > 0 && p.n > 0) {
+                ksum += (double)p.k;
+                ++cnt;
+            }
+        const int kbucket = cnt ? (int)std::floor(std::log2(1.0 + ksum / (double)cnt)) : 0;
+        const std::string what = "stages|k" + std::to_string(kbucket);
+        const std::string key = tune_key(ctx->device, ctx->sm_count, what.c_str());
+        int stages = (flags & JLC_GROUPED_AUTOTUNE) ? autotune_stages(ctx, v) : 0;
+        if (stages) tune_store(key, stages);
+        else stages = tune_lookup(key);
+        if (stages == 2 || stages == 3) pl->stages = stages;
     }
     WorkList wl;
-    build_work(v, pl->cfg, -1, wl);
+    build_work(v, wl);
     pl->flops = wl.flops;
     for (const jlc_problem& p : v) pl->n_fp64 += (p.m > 0 && p.n > 0) ? 1 : 0;
     int rc = upload(pl, v, wl);
@@ -1419,8 +1308,8 @@ int jlc_grouped_plan_info(const jlc_grouped_plan* plan, int64_t* work_items, dou
     if (!plan) return JLC_E_ARG;
     if (work_items) *work_items = plan->nitems;
     if (flops) *flops = plan->flops;
-    if (tile_small) *tile_small = plan->cfg[0];
-    if (tile_large) *tile_large = plan->cfg[1];
+    if (tile_small) *tile_small = plan->tile;
+    if (tile_large) *tile_large = plan->tile;
     return JLC_OK;
 }
 

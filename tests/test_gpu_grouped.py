@@ -87,33 +87,54 @@ def test_grouped_mixed_batch(ctx, oracle):
 
 
 def test_grouped_small_tile_build_many_items(ctx, oracle):
-    """Only problems of the small class (max(m, n) <= 48): the plan runs the
-    32 x 32 build (two CTAs per SM) with several items per CTA, odd leading
-    dimensions (8-byte copies) beside even ones, and a few long products whose
-    k-blocks wrap the stage ring several times."""
+    """Many small problems (max(m, n) <= 48): several items per warp, odd
+    leading dimensions (8-byte copies) beside even ones, edge tiles trimmed to
+    16 rows and to 8-column blocks, and a few long products whose k-blocks
+    wrap the slot ring many times."""
     rng = np.random.default_rng(17)
     shapes = [tuple(int(x) for x in rng.integers(1, 49, size=3)) for _ in range(1400)]
     shapes += [(32, 32, 2000), (48, 17, 1029), (5, 40, 777), (40, 40, 16), (33, 1, 100)]
     probs, host, arena = make_batch(oracle, shapes, 19)
     plan = ctx.grouped_plan(probs)
-    assert plan.info()["work_items"] > 2 * 296
+    assert plan.info()["work_items"] > 1400
     plan.run()
     ctx.synchronize()
     check_batch(oracle, probs, host, arena, "small-tile build")
     plan.close()
 
 
-def test_grouped_large_tile_long_k(ctx, oracle):
-    """64 x 64 tiles (the one-CTA-per-SM build) beside 32 x 32 ones, with k
-    long enough that one item's k-blocks wrap the stage ring, and alpha == 1
-    / beta == 0 (the unscaled paths)."""
+def test_grouped_long_k_both_ring_depths(ctx, oracle, tmp_path):
+    """Problems of several tiles each with k long enough that one item's
+    k-blocks wrap the slot ring, beta 0 / 1 / other and alpha == 1 (the
+    unscaled path), run with both ring depths: the autotuner records its
+    choice in the cache, the cache is rewritten to the other depth and a plan
+    made without tuning reads it back."""
+    import torch
     shapes = [(130, 70, 3000), (64, 64, 16), (200, 90, 257), (49, 300, 1), (100, 100, 100)] + \
              [(20, 30, 40)] * 50
-    probs, host, arena = make_batch(oracle, shapes, 23, alphas=[1.0] * len(shapes),
-                                    betas=[0.0, 1.0, -0.5, 0.0, 2.0] + [0.0] * 50)
-    rep = ctx.dgemm_grouped_device(probs)
-    assert rep["kernel"] == 4
-    check_batch(oracle, probs, host, arena, "large tiles")
+    betas = [0.0, 1.0, -0.5, 0.0, 2.0] + [0.0] * 50
+    cache = tmp_path / "tune.txt"
+    os.environ["JLCGPU_TUNE_CACHE"] = str(cache)
+    try:
+        probs, host, arena = make_batch(oracle, shapes, 23, alphas=[1.0] * len(shapes), betas=betas)
+        saved = arena.clone()
+        plan = ctx.grouped_plan(probs, autotune=True)
+        plan.run()
+        ctx.synchronize()
+        check_batch(oracle, probs, host, arena, "tuned depth")
+        plan.close()
+        key, depth = cache.read_text().split()
+        other = "3" if depth == "2" else "2"
+        cache.write_text(f"{key} {other}\n")
+        arena.copy_(saved)
+        torch.cuda.synchronize()
+        plan = ctx.grouped_plan(probs)
+        plan.run()
+        ctx.synchronize()
+        check_batch(oracle, probs, host, arena, f"depth {other}")
+        plan.close()
+    finally:
+        os.environ.pop("JLCGPU_TUNE_CACHE", None)
 
 
 def test_grouped_plan_graph_replay_sees_new_data(ctx, oracle):
@@ -152,9 +173,10 @@ def test_grouped_autotune_writes_cache(ctx, oracle, tmp_path):
         probs, host, arena = make_batch(oracle, shapes, 13)
         plan = ctx.grouped_plan(probs, autotune=True)
         info = plan.info()
-        assert info["tile_small"] in (32, 64) and info["tile_large"] in (32, 64)
+        assert info["tile_small"] == 32 and info["tile_large"] == 32
         text = cache.read_text()
-        assert "class0" in text and "class1" in text
+        assert "grouped-fp64|stages|k" in text
+        assert text.split()[-1] in ("2", "3")
         plan.run()
         ctx.synchronize()
         check_batch(oracle, probs, host, arena, "autotuned")
