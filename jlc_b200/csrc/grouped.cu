@@ -15,8 +15,8 @@
 //     shared-memory layout that matches its global layout (K-major for
 //     row-major A / column-major B, MN-major otherwise), so the contiguous
 //     direction lands in 16-byte units and aligned operands move with 16-byte
-//     copies (8-byte copies otherwise, zero fill at ragged edges); alpha
-//     folded into the A fragments, beta fused in the epilogue;
+//     copies (8-byte copies otherwise, zero fill at ragged edges); alpha and
+//     beta applied in the epilogue, C = alpha * (A B) + beta * C;
 //   * tiny items: a batch of problems with m*n <= 64 and k <= 64 (the TINY
 //     and small SMALL shapes) on one warp, one lane per output element (two
 //     rounds), running the reference's small-GEMM order (C <- beta*C, then an
@@ -271,7 +271,7 @@ constexpr int WT_THREADS = WT_WARPS * 32;
 constexpr int WT_SLOT = (32 + 32) * 128;     // one k-block of A and B: 8 KB
 constexpr int TINY_WARP_ELEMS = 64;          // elements of a tiny batch (two per lane)
 constexpr int TF_AK = 4, TF_BK = 8, TF_VA = 16, TF_VB = 32;
-__host__ __device__ constexpr int wt_smem(int stages) { return WT_WARPS * stages * WT_SLOT + 128; }
+__host__ __device__ constexpr int wt_smem(int stages) { return WT_WARPS * (stages * WT_SLOT + 2 * 80) + 128; }
 
 // One work item as the kernel reads it: a tile of one problem with its
 // operand origins resolved, or a batch of tiny problems.
@@ -327,17 +327,39 @@ __device__ __forceinline__ void wt_load(const double* x, long long ld, int nrows
     }
 }
 
+// Block 0 of a tile item into ring slot `slot`, layouts chosen at run time
+// (used for the next item, whose layouts may differ from the current one's).
+__device__ __forceinline__ void wt_load_first(const TileItem& w, char* sA, int lane) {
+    const int live_a = w.rows > 16 ? 32 : 16, live_b = 8 * ((w.cols + 7) >> 3);
+    const bool va = (w.flags & TF_VA) != 0, vb = (w.flags & TF_VB) != 0;
+    if (w.flags & TF_AK) wt_load<true>(w.a, w.lda, w.rows, live_a, w.k, sA, 0, va, lane);
+    else wt_load<false>(w.a, w.lda, w.rows, live_a, w.k, sA, 0, va, lane);
+    if (w.flags & TF_BK) wt_load<true>(w.b, w.ldb, w.cols, live_b, w.k, sA + 32 * 128, 0, vb, lane);
+    else wt_load<false>(w.b, w.ldb, w.cols, live_b, w.k, sA + 32 * 128, 0, vb, lane);
+}
+
+// Per-warp state carried from item to item.
+struct WtState {
+    char* ring;
+    int base;         // ring position of the current item's block 0
+    bool first_in;    // the current item's block 0 is already in flight
+};
+
+// Runs one tile item on one warp.  `next` (shared memory, or null) is the
+// record of the warp's next item, copied by an older cp.async group: during
+// the last k-block its block 0 is loaded into the slot that follows, so the
+// next item starts with data in flight.
 template <bool AK, bool BK, int STAGES>
-__device__ void wt_tile(const TileItem& w, char* ring, int lane) {
+__device__ void wt_tile(const TileItem& w, WtState& st, const TileItem* next, int lane) {
     const int g = lane >> 2, t = lane & 3;
     const int kblocks = (w.k + GBK - 1) / GBK;
     const int mtv = w.rows > 16 ? 2 : 1;         // 16-row blocks with valid rows
     const int ntv = (w.cols + 7) >> 3;           // 8-column blocks with valid columns
     const int live_a = 16 * mtv, live_b = 8 * ntv;
     const bool va = (w.flags & TF_VA) != 0, vb = (w.flags & TF_VB) != 0;
-    const bool scale_a = w.alpha != 1.0;
+    auto slot = [&](int kb) { return st.ring + ((st.base + kb) % STAGES) * WT_SLOT; };
     auto load = [&](int kb) {
-        char* sA = ring + (kb % STAGES) * WT_SLOT;
+        char* sA = slot(kb);
         wt_load<AK>(w.a, w.lda, w.rows, live_a, w.k, sA, kb * GBK, va, lane);
         wt_load<BK>(w.b, w.ldb, w.cols, live_b, w.k, sA + 32 * 128, kb * GBK, vb, lane);
     };
@@ -353,15 +375,24 @@ __device__ void wt_tile(const TileItem& w, char* ring, int lane) {
     __syncwarp();
 #pragma unroll
     for (int s = 0; s < STAGES - 1; ++s) {
-        if (s < kblocks) load(s);
+        if (s < kblocks && !(s == 0 && st.first_in)) load(s);
         cp_async_commit();
     }
+    bool next_in = false;
     for (int kb = 0; kb < kblocks; ++kb) {
-        cp_async_wait<STAGES - 2>();  // this lane's copies of block kb have landed ...
+        cp_async_wait<STAGES - 2>();  // this lane's copies of block kb (and older groups) have landed ...
         __syncwarp();                 // ... and every lane's; block kb-1's slot is free
-        if (kb + STAGES - 1 < kblocks) load(kb + STAGES - 1);
+        if (kb + STAGES - 1 < kblocks) {
+            load(kb + STAGES - 1);
+        } else if (kb == kblocks - 1 && next != nullptr) {
+            const TileItem& nw = *next;
+            if ((nw.flags & 3) == KIND_T32 && nw.k > 0) {
+                wt_load_first(nw, slot(kblocks), lane);
+                next_in = true;
+            }
+        }
         cp_async_commit();
-        const char* sA = ring + (kb % STAGES) * WT_SLOT;
+        const char* sA = slot(kb);
         const char* sB = sA + 32 * 128;
 #pragma unroll
         for (int q = 0; q < GBK / 8; ++q) {
@@ -378,17 +409,14 @@ __device__ void wt_tile(const TileItem& w, char* ring, int lane) {
 #pragma unroll
                 for (int i = 0; i < 4; ++i)
                     af[i] = dmma::lds_a<AK>(sA, mt * 16 + g + 8 * (i & 1), dmma::phys_k<8>(q, t, i >> 1));
-                if (scale_a) {
-#pragma unroll
-                    for (int i = 0; i < 4; ++i) af[i] *= w.alpha;
-                }
 #pragma unroll
                 for (int nt = 0; nt < 4; ++nt)
                     if (nt < ntv) dmma::mma_f64<8>(acc[mt][nt], af, bf[nt]);
             }
         }
     }
-    cp_async_wait<0>();
+    st.base += kblocks;
+    st.first_in = next_in;
 
     const bool has_beta = w.beta != 0.0;
 #pragma unroll
@@ -404,7 +432,7 @@ __device__ void wt_tile(const TileItem& w, char* ring, int lane) {
                 for (int e = 0; e < 2; ++e) {
                     const int col = nt * 8 + 2 * t + e;
                     if (col < w.cols) {
-                        const double v = acc[mt][nt][2 * h + e];
+                        const double v = w.alpha * acc[mt][nt][2 * h + e];
                         crow[col] = has_beta ? fma(w.beta, crow[col], v) : v;
                     }
                 }
@@ -433,32 +461,64 @@ __device__ void tiny_warp_item(const jlc_problem* probs, const int* tiny_ids, in
     }
 }
 
+// C rows of a tile into L2 ahead of the epilogue (one 128-byte line per
+// lane and step, valid rows and columns only).
+__device__ __forceinline__ void wt_prefetch_c(const TileItem& w, int lane) {
+    const int row = lane;
+    if (row >= w.rows) return;
+    const double* r = w.c + row * w.ldc;
+    asm volatile("prefetch.global.L2 [%0];" ::"l"(r));
+    if (w.cols > 16) asm volatile("prefetch.global.L2 [%0];" ::"l"(r + 16));
+}
+
 template <int STAGES>
 __global__ void __launch_bounds__(WT_THREADS, STAGES == 2 ? 3 : 2)
     grouped_kernel(const jlc_problem* probs, const TileItem* items, int nitems, const int* tiny_ids, int* counter) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    char* ring = reinterpret_cast<char*>((reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~uintptr_t(127)) +
-                 warp * STAGES * WT_SLOT;
-    int it = 0;
-    if (lane == 0) it = atomicAdd(counter, 1);
-    it = __shfl_sync(0xffffffffu, it, 0);
-    while (it < nitems) {
-        int nxt = 0;  // the next index arrives while this item runs
-        if (lane == 0) nxt = atomicAdd(counter, 1);
-        const TileItem w = items[it];
+    char* base = reinterpret_cast<char*>((reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~uintptr_t(127));
+    WtState st{base + warp * STAGES * WT_SLOT, 0, false};
+    // two record buffers per warp, after all rings
+    TileItem* recs = reinterpret_cast<TileItem*>(base + WT_WARPS * STAGES * WT_SLOT) + 2 * warp;
+    int i0 = 0, i1 = 0;
+    if (lane == 0) {
+        i0 = atomicAdd(counter, 1);
+        i1 = atomicAdd(counter, 1);
+    }
+    int it = __shfl_sync(0xffffffffu, i0, 0);
+    int nx = __shfl_sync(0xffffffffu, i1, 0);
+    if (it >= nitems) return;
+    TileItem w = items[it];
+    int rb = 0;
+    for (;;) {
+        // the next record lands in shared memory while this item runs, and
+        // the index after it is fetched
+        const bool has_next = nx < nitems;
+        if (has_next && lane < 5)
+            cp_async16(reinterpret_cast<char*>(&recs[rb]) + 16 * lane,
+                       reinterpret_cast<const char*>(&items[nx]) + 16 * lane, 16);
+        cp_async_commit();
+        int nn = 0;
+        if (lane == 0 && has_next) nn = atomicAdd(counter, 1);
         const int kind = w.flags & 3;
         if (kind == KIND_TINY) {
             tiny_warp_item(probs, tiny_ids, w.rows, w.cols, lane);
         } else {
+            if (w.beta != 0.0) wt_prefetch_c(w, lane);
+            const TileItem* next = has_next ? &recs[rb] : nullptr;
             switch (((w.flags & TF_AK) ? 2 : 0) + ((w.flags & TF_BK) ? 1 : 0)) {
-                case 0: wt_tile<false, false, STAGES>(w, ring, lane); break;
-                case 1: wt_tile<false, true, STAGES>(w, ring, lane); break;
-                case 2: wt_tile<true, false, STAGES>(w, ring, lane); break;
-                default: wt_tile<true, true, STAGES>(w, ring, lane); break;
+                case 0: wt_tile<false, false, STAGES>(w, st, next, lane); break;
+                case 1: wt_tile<false, true, STAGES>(w, st, next, lane); break;
+                case 2: wt_tile<true, false, STAGES>(w, st, next, lane); break;
+                default: wt_tile<true, true, STAGES>(w, st, next, lane); break;
             }
         }
-        it = __shfl_sync(0xffffffffu, nxt, 0);
+        cp_async_wait<0>();  // the record (and the next item's first block, if started)
+        __syncwarp();
+        if (!has_next) break;
+        w = recs[rb];
+        rb ^= 1;
+        nx = __shfl_sync(0xffffffffu, nn, 0);
     }
 }
 
