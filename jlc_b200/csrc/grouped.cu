@@ -76,6 +76,12 @@ __device__ __forceinline__ void cp_async16(void* smem_dst, const void* src, int 
     const uint32_t d = smem_u32(smem_dst);
     asm volatile("cp.async.ca.shared.global [%0], [%1], 16, %2;" ::"r"(d), "l"(src), "r"(bytes) : "memory");
 }
+__device__ __forceinline__ void cp_async8_s(uint32_t d, const void* src, bool valid) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(d), "l"(src), "r"(valid ? 8 : 0) : "memory");
+}
+__device__ __forceinline__ void cp_async16_s(uint32_t d, const void* src, int bytes) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 16, %2;" ::"r"(d), "l"(src), "r"(bytes) : "memory");
+}
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 template <int N>
 __device__ __forceinline__ void cp_async_wait() {
@@ -287,60 +293,212 @@ struct alignas(16) TileItem {
 };
 static_assert(sizeof(TileItem) == 80, "TileItem layout");
 
-// One k-block of one operand (32 rows x GBK k, x at the tile origin, `live`
-// rows copied: rows past it are never read) by the 32 lanes of a warp;
-// layout and zero fill as load_operand.
+// Cooperative load of one operand's k-block (32 rows of op(X) x GBK k) by
+// the 32 lanes of a warp into the swizzled layouts of jlc_dmma.cuh.  Every
+// lane owns a fixed set of copies whose shared-memory offsets are a lane
+// constant (one of two or four, set per item) plus a compile-time immediate,
+// and whose sources step by a multiple of the leading dimension, so a copy
+// costs a pointer add and a predicate.  Rows past `live` (never read by the
+// item's MMAs) are skipped in whole 16-row chunks; rows past the operand's
+// edge and k past its end are zero-filled.
+//   K-major (X(i, p) = x[i * ld + p]), 16-byte pairs along k: lane -> rows
+//     (lane >> 3) + 4i, k pair 2 * (lane & 7), i = 0..7;
+//   K-major, 8-byte: rows (lane >> 4) + 2i, k lane & 15, i = 0..15;
+//   MN-major (X(i, p) = x[p * ld + i]), 16-byte pairs along rows: rows
+//     2 * (lane & 7) + 16 b0, k (lane >> 3) + 4 b1 + 8 b2, i = b0 + 2 b1 + 4 b2;
+//   MN-major, 8-byte: rows (lane & 15) + 16 b0, k (lane >> 4) + 2j, i = b0 + 2j.
 template <bool KMAJOR>
-__device__ __forceinline__ void wt_load(const double* x, long long ld, int nrows, int live, int nk, char* s, int k0,
-                                        bool vec, int lane) {
-    if (vec) {
+struct WtOperand {
+    const double* g;  // the lane's first source element at k = 0
+    long long ld;
+    uint32_t s[4];    // the lane's shared-memory offsets
+    int nrows;        // valid rows
+    int live;         // rows the MMAs read (16 or 32 for A, 8..32 for B)
+    int kl;           // the lane's first k
+    int rl;           // the lane's first row
+    bool vec;
+
+    __device__ __forceinline__ void init(const double* x, long long ld_, int nrows_, int nk, int live_, bool vec_,
+                                         int lane) {
+        ld = ld_;
+        nrows = nrows_;
+        live = live_;
+        vec = vec_;
+        if (KMAJOR) {
+            if (vec) {
+                rl = lane >> 3;
+                kl = 2 * (lane & 7);
+                const int p = lane & 7;
 #pragma unroll
-        for (int i = 0; i < 32 * GBK / 2 / 32; ++i) {
-            const int e = lane + 32 * i;
-            int r, c;
-            if (KMAJOR) {
-                r = e / (GBK / 2);
-                c = 2 * (e % (GBK / 2));
+                for (int h = 0; h < 2; ++h) s[h] = rl * 128 + h * 512 + ((p ^ (rl + 4 * h)) << 4);
+                s[2] = s[3] = 0;
             } else {
-                c = e / 16;
-                r = 2 * (e % 16);
+                rl = lane >> 4;
+                kl = lane & 15;
+#pragma unroll
+                for (int h = 0; h < 4; ++h)
+                    s[h] = rl * 128 + h * 256 + ((((kl >> 1) ^ (rl + 2 * h))) << 4) + ((kl & 1) << 3);
             }
-            if (r >= live) continue;
-            const int gk = k0 + c;
-            const int valid = KMAJOR ? (r < nrows ? nk - gk : 0) : (gk < nk ? nrows - r : 0);
-            const int bytes = valid >= 2 ? 16 : (valid == 1 ? 8 : 0);
-            const double* src = bytes ? (KMAJOR ? x + r * ld + gk : x + (long long)gk * ld + r) : x;
-            cp_async16(s + op_off<KMAJOR>(r, c), src, bytes);
+            g = x + rl * ld + kl;
+        } else {
+            if (vec) {
+                const int pl = lane & 7;
+                rl = 2 * pl;
+                kl = lane >> 3;
+#pragma unroll
+                for (int h = 0; h < 2; ++h) s[h] = kl * 128 + h * 512 + ((pl ^ (kl + 4 * h)) << 4);
+                s[2] = s[3] = 0;
+            } else {
+                rl = lane & 15;
+                kl = lane >> 4;
+#pragma unroll
+                for (int h = 0; h < 4; ++h)
+                    s[h] = (kl + 2 * h) * 128 + ((((rl >> 1) ^ (kl + 2 * h))) << 4) + ((rl & 1) << 3);
+            }
+            g = x + (long long)kl * ld + rl;
         }
+        // a lane whose first element lies outside the operand has no valid
+        // copy at any k-block: it zero-fills from the (valid) tile origin
+        if (rl >= nrows || kl >= nk) {
+            g = x;
+            nrows = 0;
+        }
+    }
+
+    // copies of k-block k0 into the operand tile at shared address `sx`
+    __device__ __forceinline__ void load(uint32_t sx, int k0, int nk) const {
+        if (KMAJOR) {
+            const double* src = g + k0;
+            if (vec) {
+                const int nv = nk - (k0 + kl);
+                const int kbytes = nv >= 2 ? 16 : (nv == 1 ? 8 : 0);
+                const long long step = 4 * ld;
+#pragma unroll
+                for (int i = 0; i < 8; ++i) {
+                    if (4 * i >= live) break;  // rows 4i..4i+3 and beyond are not read
+                    const int bytes = (rl + 4 * i < nrows) ? kbytes : 0;
+                    cp_async16_s(sx + s[i & 1] + (i >> 1) * 1024, bytes ? src : g, bytes);
+                    src += step;
+                }
+            } else {
+                const bool kok = k0 + kl < nk;
+                const long long step = 2 * ld;
+#pragma unroll
+                for (int i = 0; i < 16; ++i) {
+                    if (2 * i >= live) break;
+                    const bool ok = kok && (rl + 2 * i < nrows);
+                    cp_async8_s(sx + s[i & 3] + (i >> 2) * 1024, ok ? src : g, ok);
+                    src += step;
+                }
+            }
+        } else {
+            if (vec) {
+                const long long ld4 = 4 * ld;
+                const double* p0 = g + (long long)k0 * ld;
+                int mb[2];
+#pragma unroll
+                for (int b0 = 0; b0 < 2; ++b0) {
+                    const int v = nrows - (rl + 16 * b0);
+                    mb[b0] = v >= 2 ? 16 : (v == 1 ? 8 : 0);
+                }
+#pragma unroll
+                for (int b2 = 0; b2 < 2; ++b2)
+#pragma unroll
+                    for (int b1 = 0; b1 < 2; ++b1) {
+                        const double* src = p0 + (2 * b2 + b1) * ld4;
+                        const bool kok = k0 + kl + 4 * b1 + 8 * b2 < nk;
+#pragma unroll
+                        for (int b0 = 0; b0 < 2; ++b0) {
+                            if (16 * b0 >= live) break;
+                            const int bytes = kok ? mb[b0] : 0;
+                            cp_async16_s(sx + s[b1] + b0 * 2048 + b2 * 1024, bytes ? src + 16 * b0 : g, bytes);
+                        }
+                    }
+            } else {
+                const long long step = 2 * ld;
+                const double* src = g + (long long)k0 * ld;
+                bool mok[2];
+#pragma unroll
+                for (int b0 = 0; b0 < 2; ++b0) mok[b0] = rl + 16 * b0 < nrows;
+#pragma unroll
+                for (int j = 0; j < 8; ++j) {
+                    const bool kok = k0 + kl + 2 * j < nk;
+#pragma unroll
+                    for (int b0 = 0; b0 < 2; ++b0) {
+                        if (16 * b0 >= live) break;
+                        const bool ok = kok && mok[b0];
+                        cp_async8_s(sx + s[j & 3] + b0 * 2048 + (j >> 2) * 1024, ok ? src + 16 * b0 : g, ok);
+                    }
+                    src += step;
+                }
+            }
+        }
+    }
+};
+
+// The lane's fragment offsets in an operand tile (jlc_dmma.cuh layouts, the
+// k permutation phys_k<8>): a lane constant for each of up to four
+// (row-half, k-slot) combinations, the rest a compile-time immediate.
+//   A, K-major: element (16mt + g + 8h, 8q + 2t + j) at
+//     fa[q] + 2048 mt + 1024 h + 8 j  (j = 0, 1 adjacent: one 16-byte load)
+//   A, MN-major: at fa[2h + j] + 2048 mt + 1024 q
+//   B, K-major: element (k = 8q + 2t + j, n = 8nt + g) at fb[q] + 1024 nt + 8 j
+//   B, MN-major: at fb[2 (nt & 1) + j] + 2048 (nt >> 1) + 1024 q
+template <bool KMAJOR>
+__device__ __forceinline__ void frag_bases(uint32_t (&f)[4], int g, int t, bool is_a) {
+    if (KMAJOR) {
+#pragma unroll
+        for (int q = 0; q < 2; ++q) f[q] = g * 128 + (((4 * q + t) ^ g) << 4);
+        f[2] = f[3] = 0;
     } else {
-#pragma unroll 4
-        for (int i = 0; i < 32 * GBK / 32; ++i) {
-            const int e = lane + 32 * i;
-            const int r = KMAJOR ? e / GBK : e % 32;
-            const int c = KMAJOR ? e % GBK : e / 32;
-            if (r >= live) continue;
-            const int gk = k0 + c;
-            const bool ok = r < nrows && gk < nk;
-            const double* src = ok ? (KMAJOR ? x + r * ld + gk : x + (long long)gk * ld + r) : x;
-            cp_async8(s + op_off<KMAJOR>(r, c), src, ok);
-        }
+#pragma unroll
+        for (int h = 0; h < 2; ++h)
+#pragma unroll
+            for (int j = 0; j < 2; ++j) {
+                const int kk = 2 * t + j;                              // k & 7
+                const int half = is_a ? ((g >> 1) + 4 * h) : (4 * h + (g >> 1));  // (mn & 15) >> 1
+                f[2 * h + j] = kk * 128 + ((half ^ kk) << 4) + ((g & 1) << 3);
+            }
     }
 }
 
-// Block 0 of a tile item into ring slot `slot`, layouts chosen at run time
-// (used for the next item, whose layouts may differ from the current one's).
-__device__ __forceinline__ void wt_load_first(const TileItem& w, char* sA, int lane) {
+__device__ __forceinline__ double lds64(uint32_t a) {
+    double v;
+    asm volatile("ld.shared.f64 %0, [%1];" : "=d"(v) : "r"(a));
+    return v;
+}
+__device__ __forceinline__ void lds128(uint32_t a, double& x, double& y) {
+    asm volatile("ld.shared.v2.f64 {%0, %1}, [%2];" : "=d"(x), "=d"(y) : "r"(a));
+}
+
+// Block 0 of a tile item into the slot at shared address `sa`, layouts
+// chosen at run time (used for the next item, whose layouts may differ).
+__device__ __noinline__ void wt_load_first(const TileItem& w, uint32_t sa, int lane) {
     const int live_a = w.rows > 16 ? 32 : 16, live_b = 8 * ((w.cols + 7) >> 3);
     const bool va = (w.flags & TF_VA) != 0, vb = (w.flags & TF_VB) != 0;
-    if (w.flags & TF_AK) wt_load<true>(w.a, w.lda, w.rows, live_a, w.k, sA, 0, va, lane);
-    else wt_load<false>(w.a, w.lda, w.rows, live_a, w.k, sA, 0, va, lane);
-    if (w.flags & TF_BK) wt_load<true>(w.b, w.ldb, w.cols, live_b, w.k, sA + 32 * 128, 0, vb, lane);
-    else wt_load<false>(w.b, w.ldb, w.cols, live_b, w.k, sA + 32 * 128, 0, vb, lane);
+    if (w.flags & TF_AK) {
+        WtOperand<true> o;
+        o.init(w.a, w.lda, w.rows, w.k, live_a, va, lane);
+        o.load(sa, 0, w.k);
+    } else {
+        WtOperand<false> o;
+        o.init(w.a, w.lda, w.rows, w.k, live_a, va, lane);
+        o.load(sa, 0, w.k);
+    }
+    if (w.flags & TF_BK) {
+        WtOperand<true> o;
+        o.init(w.b, w.ldb, w.cols, w.k, live_b, vb, lane);
+        o.load(sa + 32 * 128, 0, w.k);
+    } else {
+        WtOperand<false> o;
+        o.init(w.b, w.ldb, w.cols, w.k, live_b, vb, lane);
+        o.load(sa + 32 * 128, 0, w.k);
+    }
 }
 
 // Per-warp state carried from item to item.
 struct WtState {
-    char* ring;
+    uint32_t ring;    // shared address of the warp's first slot
     int base;         // ring position of the current item's block 0
     bool first_in;    // the current item's block 0 is already in flight
 };
@@ -355,13 +513,18 @@ __device__ void wt_tile(const TileItem& w, WtState& st, const TileItem* next, in
     const int kblocks = (w.k + GBK - 1) / GBK;
     const int mtv = w.rows > 16 ? 2 : 1;         // 16-row blocks with valid rows
     const int ntv = (w.cols + 7) >> 3;           // 8-column blocks with valid columns
-    const int live_a = 16 * mtv, live_b = 8 * ntv;
-    const bool va = (w.flags & TF_VA) != 0, vb = (w.flags & TF_VB) != 0;
-    auto slot = [&](int kb) { return st.ring + ((st.base + kb) % STAGES) * WT_SLOT; };
+    WtOperand<AK> opa;
+    WtOperand<BK> opb;
+    opa.init(w.a, w.lda, w.rows, w.k, 16 * mtv, (w.flags & TF_VA) != 0, lane);
+    opb.init(w.b, w.ldb, w.cols, w.k, 8 * ntv, (w.flags & TF_VB) != 0, lane);
+    uint32_t fa[4], fb[4];
+    frag_bases<AK>(fa, g, t, true);
+    frag_bases<BK>(fb, g, t, false);
+    auto slot = [&](int kb) { return st.ring + (uint32_t)(((st.base + kb) % STAGES) * WT_SLOT); };
     auto load = [&](int kb) {
-        char* sA = slot(kb);
-        wt_load<AK>(w.a, w.lda, w.rows, live_a, w.k, sA, kb * GBK, va, lane);
-        wt_load<BK>(w.b, w.ldb, w.cols, live_b, w.k, sA + 32 * 128, kb * GBK, vb, lane);
+        const uint32_t sa = slot(kb);
+        opa.load(sa, kb * GBK, w.k);
+        opb.load(sa + 32 * 128, kb * GBK, w.k);
     };
     double acc[2][4][4];
 #pragma unroll
@@ -392,23 +555,35 @@ __device__ void wt_tile(const TileItem& w, WtState& st, const TileItem* next, in
             }
         }
         cp_async_commit();
-        const char* sA = slot(kb);
-        const char* sB = sA + 32 * 128;
+        const uint32_t sA = slot(kb), sB = sA + 32 * 128;
 #pragma unroll
         for (int q = 0; q < GBK / 8; ++q) {
             double bf[4][2];
 #pragma unroll
-            for (int nt = 0; nt < 4; ++nt)
+            for (int nt = 0; nt < 4; ++nt) {
+                if (nt < ntv) {
+                    if (BK) {
+                        lds128(sB + fb[q] + 1024 * nt, bf[nt][0], bf[nt][1]);
+                    } else {
 #pragma unroll
-                for (int j = 0; j < 2; ++j)
-                    bf[nt][j] = nt < ntv ? dmma::lds_b<BK>(sB, dmma::phys_k<8>(q, t, j), nt * 8 + g) : 0.0;
+                        for (int j = 0; j < 2; ++j)
+                            bf[nt][j] = lds64(sB + fb[2 * (nt & 1) + j] + 2048 * (nt >> 1) + 1024 * q);
+                    }
+                } else {
+                    bf[nt][0] = bf[nt][1] = 0.0;
+                }
+            }
 #pragma unroll
             for (int mt = 0; mt < 2; ++mt) {
                 if (mt >= mtv) break;
-                double af[4];
+                double af[4];  // (h, j) = (i & 1, i >> 1)
+                if (AK) {
+                    lds128(sA + fa[q] + 2048 * mt, af[0], af[2]);
+                    lds128(sA + fa[q] + 2048 * mt + 1024, af[1], af[3]);
+                } else {
 #pragma unroll
-                for (int i = 0; i < 4; ++i)
-                    af[i] = dmma::lds_a<AK>(sA, mt * 16 + g + 8 * (i & 1), dmma::phys_k<8>(q, t, i >> 1));
+                    for (int i = 0; i < 4; ++i) af[i] = lds64(sA + fa[2 * (i & 1) + (i >> 1)] + 2048 * mt + 1024 * q);
+                }
 #pragma unroll
                 for (int nt = 0; nt < 4; ++nt)
                     if (nt < ntv) dmma::mma_f64<8>(acc[mt][nt], af, bf[nt]);
@@ -477,7 +652,7 @@ __global__ void __launch_bounds__(WT_THREADS, STAGES == 2 ? 3 : 2)
     extern __shared__ __align__(128) unsigned char smem_raw[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     char* base = reinterpret_cast<char*>((reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~uintptr_t(127));
-    WtState st{base + warp * STAGES * WT_SLOT, 0, false};
+    WtState st{smem_u32(base + warp * STAGES * WT_SLOT), 0, false};
     // two record buffers per warp, after all rings
     TileItem* recs = reinterpret_cast<TileItem*>(base + WT_WARPS * STAGES * WT_SLOT) + 2 * warp;
     int i0 = 0, i1 = 0;
