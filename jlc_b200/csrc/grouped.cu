@@ -276,7 +276,7 @@ constexpr int WT_WARPS = 4;                  // warps per CTA
 constexpr int WT_THREADS = WT_WARPS * 32;
 constexpr int WT_SLOT = (32 + 32) * 128;     // one k-block of A and B: 8 KB
 constexpr int TINY_WARP_ELEMS = 64;          // elements of a tiny batch (two per lane)
-constexpr int TF_AK = 4, TF_BK = 8, TF_VA = 16, TF_VB = 32;
+constexpr int TF_AK = 4, TF_BK = 8, TF_VA = 16, TF_VB = 32, TF_VC = 64;
 __host__ __device__ constexpr int wt_smem(int stages) { return WT_WARPS * (stages * WT_SLOT + 2 * 80) + 128; }
 
 // One work item as the kernel reads it: a tile of one problem with its
@@ -593,25 +593,53 @@ __device__ void wt_tile(const TileItem& w, WtState& st, const TileItem* next, in
     st.base += kblocks;
     st.first_in = next_in;
 
+    // epilogue: every C value of the lane is read before any store, so the
+    // reads overlap one another (the stores of one row could otherwise order
+    // the reads of the next); 16-byte accesses where C's rows allow them
     const bool has_beta = w.beta != 0.0;
+    const bool vc = (w.flags & TF_VC) != 0;
+    double cv[2][2][4][2];
 #pragma unroll
     for (int mt = 0; mt < 2; ++mt)
 #pragma unroll
-        for (int h = 0; h < 2; ++h) {
-            const int row = mt * 16 + g + 8 * h;
-            if (row >= w.rows) continue;
-            double* crow = w.c + row * w.ldc;
+        for (int h = 0; h < 2; ++h)
 #pragma unroll
-            for (int nt = 0; nt < 4; ++nt)
+            for (int nt = 0; nt < 4; ++nt) {
+                cv[mt][h][nt][0] = cv[mt][h][nt][1] = 0.0;
+                const int row = mt * 16 + g + 8 * h, col = nt * 8 + 2 * t;
+                if (!has_beta || mt >= mtv || nt >= ntv || row >= w.rows) continue;
+                const double* p = w.c + row * w.ldc + col;
+                if (vc && col + 1 < w.cols) {
+                    asm volatile("ld.global.v2.f64 {%0, %1}, [%2];"
+                                 : "=d"(cv[mt][h][nt][0]), "=d"(cv[mt][h][nt][1])
+                                 : "l"(p));
+                } else {
+                    if (col < w.cols) cv[mt][h][nt][0] = p[0];
+                    if (col + 1 < w.cols) cv[mt][h][nt][1] = p[1];
+                }
+            }
+#pragma unroll
+    for (int mt = 0; mt < 2; ++mt)
+#pragma unroll
+        for (int h = 0; h < 2; ++h)
+#pragma unroll
+            for (int nt = 0; nt < 4; ++nt) {
+                const int row = mt * 16 + g + 8 * h, col = nt * 8 + 2 * t;
+                if (mt >= mtv || nt >= ntv || row >= w.rows) continue;
+                double* p = w.c + row * w.ldc + col;
+                double v[2];
 #pragma unroll
                 for (int e = 0; e < 2; ++e) {
-                    const int col = nt * 8 + 2 * t + e;
-                    if (col < w.cols) {
-                        const double v = w.alpha * acc[mt][nt][2 * h + e];
-                        crow[col] = has_beta ? fma(w.beta, crow[col], v) : v;
-                    }
+                    v[e] = w.alpha * acc[mt][nt][2 * h + e];
+                    if (has_beta) v[e] = fma(w.beta, cv[mt][h][nt][e], v[e]);
                 }
-        }
+                if (vc && col + 1 < w.cols) {
+                    asm volatile("st.global.v2.f64 [%0], {%1, %2};" ::"l"(p), "d"(v[0]), "d"(v[1]) : "memory");
+                } else {
+                    if (col < w.cols) p[0] = v[0];
+                    if (col + 1 < w.cols) p[1] = v[1];
+                }
+            }
 }
 
 // A batch of tiny problems on one warp, elements lane and lane + 32.
@@ -1215,7 +1243,9 @@ int upload(jlc_grouped_plan* pl, const std::vector<jlc_problem>& probs, const Wo
         // 16-byte copies need 16-byte aligned tile rows (origin and leading dimension)
         const bool va = ((reinterpret_cast<uintptr_t>(t.a) & 15) == 0) && ((p.lda & 1) == 0);
         const bool vb = ((reinterpret_cast<uintptr_t>(t.b) & 15) == 0) && ((p.ldb & 1) == 0);
-        t.flags = it.kind | (ak ? TF_AK : 0) | (bk ? TF_BK : 0) | (va ? TF_VA : 0) | (vb ? TF_VB : 0);
+        const bool vc = ((reinterpret_cast<uintptr_t>(t.c) & 15) == 0) && ((p.ldc & 1) == 0);
+        t.flags = it.kind | (ak ? TF_AK : 0) | (bk ? TF_BK : 0) | (va ? TF_VA : 0) | (vb ? TF_VB : 0) |
+                  (vc ? TF_VC : 0);
     }
     cudaError_t e = alloc_copy((void**)&pl->d_probs, probs.data(), probs.size() * sizeof(jlc_problem));
     if (e == cudaSuccess) e = alloc_copy((void**)&pl->d_titems, titems.data(), titems.size() * sizeof(TileItem));
