@@ -269,7 +269,10 @@ __device__ void tiny_item(const jlc_problem* probs, const int* tiny_ids, int sta
 // 16 x 8, eight independent accumulator chains.  No CTA-wide barrier exists;
 // a warp waits only for its own copies, so the dozen warps of an SM overlap
 // one another's memory latency and the SM's DMMA pipe stays fed.  The next
-// item's index is fetched while the current one runs.  A tile with at most
+// item's record is copied to shared memory, and the index after it fetched,
+// while the current item runs; C rows are prefetched to L2 when an item
+// starts, and the epilogue reads all of the lane's C values before its first
+// store.  A tile with at most
 // 16 valid rows skips its second 16-row block, and columns are trimmed to
 // 8-column blocks, so ragged edges cost a 16 x 8 granule, not a 32 x 32 one.
 constexpr int WT_WARPS = 4;                  // warps per CTA
@@ -365,16 +368,18 @@ struct WtOperand {
         }
     }
 
-    // copies of k-block k0 into the operand tile at shared address `sx`
-    __device__ __forceinline__ void load(uint32_t sx, int k0, int nk) const {
+    // Half H (0 or 1) of the lane's copies of k-block k0 into the operand
+    // tile at shared address `sx`; the halves are issued apart, between MMAs.
+    template <int H>
+    __device__ __forceinline__ void load_half(uint32_t sx, int k0, int nk) const {
         if (KMAJOR) {
-            const double* src = g + k0;
             if (vec) {
                 const int nv = nk - (k0 + kl);
                 const int kbytes = nv >= 2 ? 16 : (nv == 1 ? 8 : 0);
                 const long long step = 4 * ld;
+                const double* src = g + k0 + (long long)(4 * H) * step;
 #pragma unroll
-                for (int i = 0; i < 8; ++i) {
+                for (int i = 4 * H; i < 4 * H + 4; ++i) {
                     if (4 * i >= live) break;  // rows 4i..4i+3 and beyond are not read
                     const int bytes = (rl + 4 * i < nrows) ? kbytes : 0;
                     cp_async16_s(sx + s[i & 1] + (i >> 1) * 1024, bytes ? src : g, bytes);
@@ -383,8 +388,9 @@ struct WtOperand {
             } else {
                 const bool kok = k0 + kl < nk;
                 const long long step = 2 * ld;
+                const double* src = g + k0 + (long long)(8 * H) * step;
 #pragma unroll
-                for (int i = 0; i < 16; ++i) {
+                for (int i = 8 * H; i < 8 * H + 8; ++i) {
                     if (2 * i >= live) break;
                     const bool ok = kok && (rl + 2 * i < nrows);
                     cp_async8_s(sx + s[i & 3] + (i >> 2) * 1024, ok ? src : g, ok);
@@ -393,8 +399,9 @@ struct WtOperand {
             }
         } else {
             if (vec) {
+                // this half: k rows kl + 8H and kl + 8H + 4, both 16-row chunks
                 const long long ld4 = 4 * ld;
-                const double* p0 = g + (long long)k0 * ld;
+                const double* p0 = g + (long long)(k0 + 8 * H) * ld;
                 int mb[2];
 #pragma unroll
                 for (int b0 = 0; b0 < 2; ++b0) {
@@ -402,26 +409,25 @@ struct WtOperand {
                     mb[b0] = v >= 2 ? 16 : (v == 1 ? 8 : 0);
                 }
 #pragma unroll
-                for (int b2 = 0; b2 < 2; ++b2)
+                for (int b1 = 0; b1 < 2; ++b1) {
+                    const double* src = p0 + b1 * ld4;
+                    const bool kok = k0 + kl + 4 * b1 + 8 * H < nk;
 #pragma unroll
-                    for (int b1 = 0; b1 < 2; ++b1) {
-                        const double* src = p0 + (2 * b2 + b1) * ld4;
-                        const bool kok = k0 + kl + 4 * b1 + 8 * b2 < nk;
-#pragma unroll
-                        for (int b0 = 0; b0 < 2; ++b0) {
-                            if (16 * b0 >= live) break;
-                            const int bytes = kok ? mb[b0] : 0;
-                            cp_async16_s(sx + s[b1] + b0 * 2048 + b2 * 1024, bytes ? src + 16 * b0 : g, bytes);
-                        }
+                    for (int b0 = 0; b0 < 2; ++b0) {
+                        if (16 * b0 >= live) break;
+                        const int bytes = kok ? mb[b0] : 0;
+                        cp_async16_s(sx + s[b1] + b0 * 2048 + H * 1024, bytes ? src + 16 * b0 : g, bytes);
                     }
+                }
             } else {
+                // this half: k rows kl + 2j for j = 4H .. 4H + 3
                 const long long step = 2 * ld;
-                const double* src = g + (long long)k0 * ld;
+                const double* src = g + (long long)(k0 + 8 * H) * ld;
                 bool mok[2];
 #pragma unroll
                 for (int b0 = 0; b0 < 2; ++b0) mok[b0] = rl + 16 * b0 < nrows;
 #pragma unroll
-                for (int j = 0; j < 8; ++j) {
+                for (int j = 4 * H; j < 4 * H + 4; ++j) {
                     const bool kok = k0 + kl + 2 * j < nk;
 #pragma unroll
                     for (int b0 = 0; b0 < 2; ++b0) {
@@ -433,6 +439,11 @@ struct WtOperand {
                 }
             }
         }
+    }
+
+    __device__ __forceinline__ void load(uint32_t sx, int k0, int nk) const {
+        load_half<0>(sx, k0, nk);
+        load_half<1>(sx, k0, nk);
     }
 };
 
@@ -471,44 +482,10 @@ __device__ __forceinline__ void lds128(uint32_t a, double& x, double& y) {
     asm volatile("ld.shared.v2.f64 {%0, %1}, [%2];" : "=d"(x), "=d"(y) : "r"(a));
 }
 
-// Block 0 of a tile item into the slot at shared address `sa`, layouts
-// chosen at run time (used for the next item, whose layouts may differ).
-__device__ __noinline__ void wt_load_first(const TileItem& w, uint32_t sa, int lane) {
-    const int live_a = w.rows > 16 ? 32 : 16, live_b = 8 * ((w.cols + 7) >> 3);
-    const bool va = (w.flags & TF_VA) != 0, vb = (w.flags & TF_VB) != 0;
-    if (w.flags & TF_AK) {
-        WtOperand<true> o;
-        o.init(w.a, w.lda, w.rows, w.k, live_a, va, lane);
-        o.load(sa, 0, w.k);
-    } else {
-        WtOperand<false> o;
-        o.init(w.a, w.lda, w.rows, w.k, live_a, va, lane);
-        o.load(sa, 0, w.k);
-    }
-    if (w.flags & TF_BK) {
-        WtOperand<true> o;
-        o.init(w.b, w.ldb, w.cols, w.k, live_b, vb, lane);
-        o.load(sa + 32 * 128, 0, w.k);
-    } else {
-        WtOperand<false> o;
-        o.init(w.b, w.ldb, w.cols, w.k, live_b, vb, lane);
-        o.load(sa + 32 * 128, 0, w.k);
-    }
-}
-
-// Per-warp state carried from item to item.
-struct WtState {
-    uint32_t ring;    // shared address of the warp's first slot
-    int base;         // ring position of the current item's block 0
-    bool first_in;    // the current item's block 0 is already in flight
-};
-
-// Runs one tile item on one warp.  `next` (shared memory, or null) is the
-// record of the warp's next item, copied by an older cp.async group: during
-// the last k-block its block 0 is loaded into the slot that follows, so the
-// next item starts with data in flight.
+// Runs one tile item on one warp, streaming its k-blocks through the warp's
+// ring of STAGES slots at shared address `ring`.
 template <bool AK, bool BK, int STAGES>
-__device__ void wt_tile(const TileItem& w, WtState& st, const TileItem* next, int lane) {
+__device__ void wt_tile(const TileItem& w, uint32_t ring, int lane) {
     const int g = lane >> 2, t = lane & 3;
     const int kblocks = (w.k + GBK - 1) / GBK;
     const int mtv = w.rows > 16 ? 2 : 1;         // 16-row blocks with valid rows
@@ -520,7 +497,7 @@ __device__ void wt_tile(const TileItem& w, WtState& st, const TileItem* next, in
     uint32_t fa[4], fb[4];
     frag_bases<AK>(fa, g, t, true);
     frag_bases<BK>(fb, g, t, false);
-    auto slot = [&](int kb) { return st.ring + (uint32_t)(((st.base + kb) % STAGES) * WT_SLOT); };
+    auto slot = [&](int kb) { return ring + (uint32_t)((kb % STAGES) * WT_SLOT); };
     auto load = [&](int kb) {
         const uint32_t sa = slot(kb);
         opa.load(sa, kb * GBK, w.k);
@@ -538,23 +515,17 @@ __device__ void wt_tile(const TileItem& w, WtState& st, const TileItem* next, in
     __syncwarp();
 #pragma unroll
     for (int s = 0; s < STAGES - 1; ++s) {
-        if (s < kblocks && !(s == 0 && st.first_in)) load(s);
+        if (s < kblocks) load(s);
         cp_async_commit();
     }
-    bool next_in = false;
     for (int kb = 0; kb < kblocks; ++kb) {
         cp_async_wait<STAGES - 2>();  // this lane's copies of block kb (and older groups) have landed ...
         __syncwarp();                 // ... and every lane's; block kb-1's slot is free
-        if (kb + STAGES - 1 < kblocks) {
-            load(kb + STAGES - 1);
-        } else if (kb == kblocks - 1 && next != nullptr) {
-            const TileItem& nw = *next;
-            if ((nw.flags & 3) == KIND_T32 && nw.k > 0) {
-                wt_load_first(nw, slot(kblocks), lane);
-                next_in = true;
-            }
-        }
-        cp_async_commit();
+        // block kb + STAGES - 1 is copied in four parts, one after each group
+        // of MMAs: an in-order warp issues them while its MMAs occupy the pipe
+        const bool more = kb + STAGES - 1 < kblocks;
+        const uint32_t sn = slot(kb + STAGES - 1);
+        const int kn = (kb + STAGES - 1) * GBK;
         const uint32_t sA = slot(kb), sB = sA + 32 * 128;
 #pragma unroll
         for (int q = 0; q < GBK / 8; ++q) {
@@ -575,23 +546,31 @@ __device__ void wt_tile(const TileItem& w, WtState& st, const TileItem* next, in
             }
 #pragma unroll
             for (int mt = 0; mt < 2; ++mt) {
-                if (mt >= mtv) break;
-                double af[4];  // (h, j) = (i & 1, i >> 1)
-                if (AK) {
-                    lds128(sA + fa[q] + 2048 * mt, af[0], af[2]);
-                    lds128(sA + fa[q] + 2048 * mt + 1024, af[1], af[3]);
-                } else {
+                if (mt < mtv) {
+                    double af[4];  // (h, j) = (i & 1, i >> 1)
+                    if (AK) {
+                        lds128(sA + fa[q] + 2048 * mt, af[0], af[2]);
+                        lds128(sA + fa[q] + 2048 * mt + 1024, af[1], af[3]);
+                    } else {
 #pragma unroll
-                    for (int i = 0; i < 4; ++i) af[i] = lds64(sA + fa[2 * (i & 1) + (i >> 1)] + 2048 * mt + 1024 * q);
+                        for (int i = 0; i < 4; ++i)
+                            af[i] = lds64(sA + fa[2 * (i & 1) + (i >> 1)] + 2048 * mt + 1024 * q);
+                    }
+#pragma unroll
+                    for (int nt = 0; nt < 4; ++nt)
+                        if (nt < ntv) dmma::mma_f64<8>(acc[mt][nt], af, bf[nt]);
                 }
-#pragma unroll
-                for (int nt = 0; nt < 4; ++nt)
-                    if (nt < ntv) dmma::mma_f64<8>(acc[mt][nt], af, bf[nt]);
+                if (more) {
+                    if (q == 0 && mt == 0) opa.template load_half<0>(sn, kn, w.k);
+                    if (q == 0 && mt == 1) opa.template load_half<1>(sn, kn, w.k);
+                    if (q == 1 && mt == 0) opb.template load_half<0>(sn + 32 * 128, kn, w.k);
+                    if (q == 1 && mt == 1) opb.template load_half<1>(sn + 32 * 128, kn, w.k);
+                }
             }
         }
+        cp_async_commit();
     }
-    st.base += kblocks;
-    st.first_in = next_in;
+    cp_async_wait<0>();
 
     // epilogue: every C value of the lane is read before any store, so the
     // reads overlap one another (the stores of one row could otherwise order
@@ -680,7 +659,7 @@ __global__ void __launch_bounds__(WT_THREADS, STAGES == 2 ? 3 : 2)
     extern __shared__ __align__(128) unsigned char smem_raw[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     char* base = reinterpret_cast<char*>((reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~uintptr_t(127));
-    WtState st{smem_u32(base + warp * STAGES * WT_SLOT), 0, false};
+    const uint32_t ring = smem_u32(base + warp * STAGES * WT_SLOT);
     // two record buffers per warp, after all rings
     TileItem* recs = reinterpret_cast<TileItem*>(base + WT_WARPS * STAGES * WT_SLOT) + 2 * warp;
     int i0 = 0, i1 = 0;
@@ -708,15 +687,14 @@ __global__ void __launch_bounds__(WT_THREADS, STAGES == 2 ? 3 : 2)
             tiny_warp_item(probs, tiny_ids, w.rows, w.cols, lane);
         } else {
             if (w.beta != 0.0) wt_prefetch_c(w, lane);
-            const TileItem* next = has_next ? &recs[rb] : nullptr;
             switch (((w.flags & TF_AK) ? 2 : 0) + ((w.flags & TF_BK) ? 1 : 0)) {
-                case 0: wt_tile<false, false, STAGES>(w, st, next, lane); break;
-                case 1: wt_tile<false, true, STAGES>(w, st, next, lane); break;
-                case 2: wt_tile<true, false, STAGES>(w, st, next, lane); break;
-                default: wt_tile<true, true, STAGES>(w, st, next, lane); break;
+                case 0: wt_tile<false, false, STAGES>(w, ring, lane); break;
+                case 1: wt_tile<false, true, STAGES>(w, ring, lane); break;
+                case 2: wt_tile<true, false, STAGES>(w, ring, lane); break;
+                default: wt_tile<true, true, STAGES>(w, ring, lane); break;
             }
         }
-        cp_async_wait<0>();  // the record (and the next item's first block, if started)
+        cp_async_wait<0>();  // the next record
         __syncwarp();
         if (!has_next) break;
         w = recs[rb];
