@@ -370,72 +370,63 @@ struct WtOperand {
 
     // Half H (0 or 1) of the lane's copies of k-block k0 into the operand
     // tile at shared address `sx`; the halves are issued apart, between MMAs.
+    // Copies of rows past the operand's edge are not issued: those rows only
+    // reach output rows (of A) or columns (of B) that are never stored, so
+    // whatever the slot holds there is harmless.  k past the end is
+    // zero-filled (it reaches every output), from the lane's first element,
+    // which is in range.
     template <int H>
     __device__ __forceinline__ void load_half(uint32_t sx, int k0, int nk) const {
         if (KMAJOR) {
             if (vec) {
                 const int nv = nk - (k0 + kl);
                 const int kbytes = nv >= 2 ? 16 : (nv == 1 ? 8 : 0);
-                const long long step = 4 * ld;
-                const double* src = g + k0 + (long long)(4 * H) * step;
+                const long long step = kbytes ? 4 * ld : 0;
+                const double* src = kbytes ? g + k0 + (long long)(4 * H) * step : g;
 #pragma unroll
                 for (int i = 4 * H; i < 4 * H + 4; ++i) {
                     if (4 * i >= live) break;  // rows 4i..4i+3 and beyond are not read
-                    const int bytes = (rl + 4 * i < nrows) ? kbytes : 0;
-                    cp_async16_s(sx + s[i & 1] + (i >> 1) * 1024, bytes ? src : g, bytes);
+                    if (rl + 4 * i < nrows) cp_async16_s(sx + s[i & 1] + (i >> 1) * 1024, src, kbytes);
                     src += step;
                 }
             } else {
                 const bool kok = k0 + kl < nk;
-                const long long step = 2 * ld;
-                const double* src = g + k0 + (long long)(8 * H) * step;
+                const long long step = kok ? 2 * ld : 0;
+                const double* src = kok ? g + k0 + (long long)(8 * H) * step : g;
 #pragma unroll
                 for (int i = 8 * H; i < 8 * H + 8; ++i) {
                     if (2 * i >= live) break;
-                    const bool ok = kok && (rl + 2 * i < nrows);
-                    cp_async8_s(sx + s[i & 3] + (i >> 2) * 1024, ok ? src : g, ok);
+                    if (rl + 2 * i < nrows) cp_async8_s(sx + s[i & 3] + (i >> 2) * 1024, src, kok);
                     src += step;
                 }
             }
         } else {
             if (vec) {
                 // this half: k rows kl + 8H and kl + 8H + 4, both 16-row chunks
-                const long long ld4 = 4 * ld;
                 const double* p0 = g + (long long)(k0 + 8 * H) * ld;
-                int mb[2];
-#pragma unroll
-                for (int b0 = 0; b0 < 2; ++b0) {
-                    const int v = nrows - (rl + 16 * b0);
-                    mb[b0] = v >= 2 ? 16 : (v == 1 ? 8 : 0);
-                }
 #pragma unroll
                 for (int b1 = 0; b1 < 2; ++b1) {
-                    const double* src = p0 + b1 * ld4;
                     const bool kok = k0 + kl + 4 * b1 + 8 * H < nk;
+                    const double* src = kok ? p0 + b1 * 4 * ld : g;
 #pragma unroll
                     for (int b0 = 0; b0 < 2; ++b0) {
                         if (16 * b0 >= live) break;
-                        const int bytes = kok ? mb[b0] : 0;
-                        cp_async16_s(sx + s[b1] + b0 * 2048 + H * 1024, bytes ? src + 16 * b0 : g, bytes);
+                        const int v = nrows - (rl + 16 * b0);
+                        if (v > 0) cp_async16_s(sx + s[b1] + b0 * 2048 + H * 1024, src + 16 * b0, kok ? (v >= 2 ? 16 : 8) : 0);
                     }
                 }
             } else {
                 // this half: k rows kl + 2j for j = 4H .. 4H + 3
-                const long long step = 2 * ld;
-                const double* src = g + (long long)(k0 + 8 * H) * ld;
-                bool mok[2];
-#pragma unroll
-                for (int b0 = 0; b0 < 2; ++b0) mok[b0] = rl + 16 * b0 < nrows;
+                const double* p0 = g + (long long)(k0 + 8 * H) * ld;
 #pragma unroll
                 for (int j = 4 * H; j < 4 * H + 4; ++j) {
                     const bool kok = k0 + kl + 2 * j < nk;
+                    const double* src = kok ? p0 + (long long)(2 * (j - 4 * H)) * ld : g;
 #pragma unroll
                     for (int b0 = 0; b0 < 2; ++b0) {
                         if (16 * b0 >= live) break;
-                        const bool ok = kok && mok[b0];
-                        cp_async8_s(sx + s[j & 3] + b0 * 2048 + (j >> 2) * 1024, ok ? src + 16 * b0 : g, ok);
+                        if (rl + 16 * b0 < nrows) cp_async8_s(sx + s[j & 3] + b0 * 2048 + (j >> 2) * 1024, src + 16 * b0, kok);
                     }
-                    src += step;
                 }
             }
         }
