@@ -533,7 +533,8 @@ def run_grouped(args):
             "config": {"workload": f"{args.count} uneven DGEMMs, alpha/beta uniform[-2,2], row-major, 16-byte aligned "
                                    "matrices in one arena, CUDA-graph replay",
                        "work_items": info["work_items"], "tile_small": info["tile_small"],
-                       "tile_large": info["tile_large"], "flops_per_step": flops,
+                       "tile_large": info["tile_large"], "ring_slots_per_warp": info["stages"],
+                       "flops_per_step": flops,
                        "algorithmic_bytes_per_step": bytes_alg},
             "achieved_gbs": round(bytes_alg / (ms * 1e-3) / 1e9, 1),
             "gpu_launches": ctx.launch_count() - launches0, "clocks": clk.summary(),

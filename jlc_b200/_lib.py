@@ -126,6 +126,7 @@ SIGNATURES = {
     "jlc_grouped_plan_info": (_i, [_vp, ctypes.POINTER(_i64), ctypes.POINTER(_d), ctypes.POINTER(_i),
                                    ctypes.POINTER(_i)]),
     "jlc_grouped_plan_routes": (_i, [_vp, ctypes.POINTER(_i64), ctypes.POINTER(_i64)]),
+    "jlc_grouped_plan_stages": (_i, [_vp, ctypes.POINTER(_i)]),
     "jlc_grouped_plan_destroy": (None, [_vp]),
     "jlc_dgemm_grouped_device": (_i, [_vp, _PROB, _i64, _i, _REP]),
     "jlc_dgemm_ozaki_static": (_i, [_i, _i, _i64, _i64, _i64, _d, _dp, _i64, _dp, _i64, _d, _dp, _i64, _i, _vp,

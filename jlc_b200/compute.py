@@ -318,8 +318,10 @@ class GroupedPlan:
                                                           ctypes.byref(ts), ctypes.byref(tl)))
         n8, n64 = ctypes.c_int64(), ctypes.c_int64()
         self.ctx.check(self.ctx.lib.jlc_grouped_plan_routes(self.h, ctypes.byref(n8), ctypes.byref(n64)))
+        st = ctypes.c_int()
+        self.ctx.check(self.ctx.lib.jlc_grouped_plan_stages(self.h, ctypes.byref(st)))
         return {"work_items": items.value, "flops": flops.value, "tile_small": ts.value, "tile_large": tl.value,
-                "int8_problems": n8.value, "fp64_problems": n64.value}
+                "int8_problems": n8.value, "fp64_problems": n64.value, "stages": st.value}
 
     def close(self):
         if getattr(self, "h", None):

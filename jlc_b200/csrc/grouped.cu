@@ -1554,6 +1554,12 @@ int jlc_grouped_plan_routes(const jlc_grouped_plan* plan, int64_t* int8_problems
     return JLC_OK;
 }
 
+int jlc_grouped_plan_stages(const jlc_grouped_plan* plan, int* stages) {
+    if (!plan || !stages) return JLC_E_ARG;
+    *stages = plan->oz ? 0 : plan->stages;
+    return JLC_OK;
+}
+
 void jlc_grouped_plan_destroy(jlc_grouped_plan* plan) {
     if (!plan) return;
     if (plan->ctx) {
