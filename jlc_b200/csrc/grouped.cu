@@ -360,12 +360,10 @@ struct WtOperand {
             }
             g = x + (long long)kl * ld + rl;
         }
-        // a lane whose first element lies outside the operand has no valid
-        // copy at any k-block: it zero-fills from the (valid) tile origin
-        if (rl >= nrows || kl >= nk) {
-            g = x;
-            nrows = 0;
-        }
+        // a lane whose first element lies outside the operand addresses the
+        // (valid) tile origin instead: past the last row it issues no copy,
+        // past the last k it zero-fills every k-block it owns
+        if (rl >= nrows || kl >= nk) g = x;
     }
 
     // Half H (0 or 1) of the lane's copies of k-block k0 into the operand
