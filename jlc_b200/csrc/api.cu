@@ -668,14 +668,16 @@ struct QrWork {
     double *v, *g, *t, *w, *w2;
     long long ldv, ldw;
     void* panel_scratch;  // multi-CTA panel: partials, row records, barrier counter
+    double* gram;         // row-slab partials of G = V^T V
 };
 
 int qr_work(jlc_ctx* ctx, long long m, long long cols, QrWork& q) {
     q.ldv = round_up(m > 0 ? m : 1, 8);
     q.ldw = round_up(cols > 0 ? cols : 1, 8);
     const size_t doubles = (size_t)(q.ldv * kQrPanel + 2 * kQrPanel * kQrPanel + 2 * kQrPanel * q.ldw);
-    const size_t scratch = qr_panel_mp_scratch_bytes(ctx->sm_count > 0 ? ctx->sm_count : 1);
-    int rc = reserve(ctx, ctx->bufQ, doubles * sizeof(double) + scratch, "QR workspace");
+    const size_t scratch = round_up(qr_panel_mp_scratch_bytes(ctx->sm_count > 0 ? ctx->sm_count : 1), 256);
+    const size_t gram = qr_gram_scratch_bytes(ctx->sm_count);
+    int rc = reserve(ctx, ctx->bufQ, doubles * sizeof(double) + scratch + gram, "QR workspace");
     if (rc) return rc;
     q.v = static_cast<double*>(ctx->bufQ.ptr);
     q.g = q.v + q.ldv * kQrPanel;
@@ -683,6 +685,7 @@ int qr_work(jlc_ctx* ctx, long long m, long long cols, QrWork& q) {
     q.w = q.t + kQrPanel * kQrPanel;
     q.w2 = q.w + kQrPanel * q.ldw;
     q.panel_scratch = q.w2 + kQrPanel * q.ldw;
+    q.gram = reinterpret_cast<double*>(static_cast<char*>(q.panel_scratch) + scratch);
     return JLC_OK;
 }
 
@@ -697,18 +700,12 @@ int qr_panel_vt(jlc_ctx* ctx, const double* f, long long ldf, long long m, long 
         rc = launch_qr_pack_v(f, ldf, (int)m, (int)k0, kb, q.v, q.ldv, st);
     }
     if (rc) return set_err(ctx, rc, "QR: V packing launch failed");
-    // G (64 x 64, row-major) = V(k0:, :)^T V(k0:, :): op(A) = V^T as a row-major
-    // 64 x (m-k0) view, op(B) = V column-major
-    const long long rows = m - k0;
-    GemmDesc g{JLC_ROW_MAJOR, JLC_COL_MAJOR, kQrPanel, kQrPanel, rows, 1.0, 0.0, q.v + k0, q.ldv, q.v + k0, q.ldv,
-               q.g, kQrPanel};
-    rc = run_device(ctx, g, JLC_PREC_NATIVE, 0, nullptr);
-    if (rc) return rc;
-    {
-        Phase ph(ctx, JLC_PHASE_QR_VT);
-        rc = launch_qr_build_t(q.g, tau + k0, kb, q.t, st);
-    }
-    return rc ? set_err(ctx, rc, "QR: T launch failed") : JLC_OK;
+    // G (64 x 64, row-major) = V(k0:, :)^T V(k0:, :) over row slabs (a 64 x 64
+    // output is one tile of a GEMM, too few CTAs for k = m - k0), then T
+    Phase ph(ctx, JLC_PHASE_QR_VT);
+    rc = launch_qr_gram(q.v, q.ldv, (int)k0, (int)m, q.g, q.gram, ctx->sm_count, st);
+    if (!rc) rc = launch_qr_build_t(q.g, tau + k0, kb, q.t, st);
+    return rc ? set_err(ctx, rc, "QR: V^T V / T launch failed") : JLC_OK;
 }
 
 // C (rows k0.. of a column-major m x cols block, ld ldc) <- H C with

@@ -146,6 +146,17 @@ __global__ void __launch_bounds__(THREADS, 1)
                         }
                         continue;
                     }
+                    if (kb == kb0 && part == 0 && p.beta != 0.0) {
+                        // the tile's C rows into L2 ahead of its epilogue: whole
+                        // 16-byte units inside each row only
+                        const int rows = p.M - m0 < BM ? p.M - m0 : BM;
+                        const int cols = p.N - n0 < BN ? p.N - n0 : BN;
+                        for (int r = 0; r < rows; ++r) {
+                            const uintptr_t a0 = reinterpret_cast<uintptr_t>(p.C + (long long)(m0 + r) * p.ldc + n0);
+                            const uintptr_t lo = (a0 + 15) & ~uintptr_t(15), hi = (a0 + 8u * cols) & ~uintptr_t(15);
+                            if (hi > lo) l2_prefetch_bulk(reinterpret_cast<const void*>(lo), (uint32_t)(hi - lo));
+                        }
+                    }
                     char* sA = smem + stage * STAGE_BYTES;
                     char* sB = sA + A_STAGE;
                     const int k0 = kb * BK;
@@ -313,27 +324,50 @@ __global__ void __launch_bounds__(THREADS, 1)
             }
         }
         // fused epilogue: C = epi_scale*acc + beta * C_old (C_old not read when
-        // beta == 0); optional dot with dot_mat for the adjoint's d(alpha)
+        // beta == 0); optional dot with dot_mat for the adjoint's d(alpha).
+        // Per 16-row block, C_old of both of the lane's rows is read before
+        // either is stored (a store to one row would otherwise order the reads
+        // of the next: one memory latency per block, not per row).
         const int row0 = tm * BM + warp_m * WM;
         const int col0 = tn * BN + warp_n * WN;
+        constexpr int MB = 1;  // 16-row blocks per batch
 #pragma unroll
-        for (int mt = 0; mt < MT; ++mt) {
+        for (int mp = 0; mp < MT; mp += MB) {
+            double cold[MB][2][NT][2];
 #pragma unroll
-            for (int h = 0; h < 2; ++h) {
-                const int row = row0 + mt * 16 + g + 8 * h;
-                if (row >= p.M) continue;
-                double* crow = p.C + (long long)row * p.ldc;
-                const double* drow = p.dot_mat ? p.dot_mat + (long long)row * p.dot_ld : nullptr;
+            for (int mi = 0; mi < MB; ++mi)
 #pragma unroll
-                for (int nt = 0; nt < NT; ++nt) {
+                for (int h = 0; h < 2; ++h) {
+                    const int row = row0 + (mp + mi) * 16 + g + 8 * h;
+                    const double* crow = p.C + (long long)row * p.ldc;
 #pragma unroll
-                    for (int e = 0; e < 2; ++e) {
-                        const int col = col0 + nt * 8 + 2 * t + e;
-                        if (col < p.N) {
-                            const double a = acc[mt][nt][2 * h + e];
-                            if (drow) dot_acc = fma(drow[col], a, dot_acc);
-                            const double v = p.epi_scale == 1.0 ? a : p.epi_scale * a;
-                            crow[col] = (p.beta == 0.0) ? v : fma(p.beta, crow[col], v);
+                    for (int nt = 0; nt < NT; ++nt)
+#pragma unroll
+                        for (int e = 0; e < 2; ++e) {
+                            const int col = col0 + nt * 8 + 2 * t + e;
+                            cold[mi][h][nt][e] = (p.beta != 0.0 && row < p.M && col < p.N) ? crow[col] : 0.0;
+                        }
+                }
+#pragma unroll
+            for (int mi = 0; mi < MB; ++mi) {
+                const int mt = mp + mi;
+#pragma unroll
+                for (int h = 0; h < 2; ++h) {
+                    const int row = row0 + mt * 16 + g + 8 * h;
+                    if (row >= p.M) continue;
+                    double* crow = p.C + (long long)row * p.ldc;
+                    const double* drow = p.dot_mat ? p.dot_mat + (long long)row * p.dot_ld : nullptr;
+#pragma unroll
+                    for (int nt = 0; nt < NT; ++nt) {
+#pragma unroll
+                        for (int e = 0; e < 2; ++e) {
+                            const int col = col0 + nt * 8 + 2 * t + e;
+                            if (col < p.N) {
+                                const double a = acc[mt][nt][2 * h + e];
+                                if (drow) dot_acc = fma(drow[col], a, dot_acc);
+                                const double v = p.epi_scale == 1.0 ? a : p.epi_scale * a;
+                                crow[col] = (p.beta == 0.0) ? v : fma(p.beta, cold[mi][h][nt][e], v);
+                            }
                         }
                     }
                 }

@@ -83,6 +83,11 @@ int launch_qr_panel(double* a, long long lda, int m, int k0, int kb, double* tau
 int launch_qr_pack_v(const double* a, long long lda, int m, int k0, int kb, double* v, long long ldv,
                      cudaStream_t st);
 int launch_qr_build_t(const double* g, const double* tau, int kb, double* t, cudaStream_t st);
+// G = V^T V (64 x 64, row-major) over rows [r0, r1) of the packed V; scratch
+// holds qr_gram_scratch_bytes(sm_count)
+size_t qr_gram_scratch_bytes(int sm_count);
+int launch_qr_gram(const double* v, long long ldv, int r0, int r1, double* g, double* scratch, int sm_count,
+                   cudaStream_t st);
 int launch_set_identity(double* q, long long ldq, long long m, long long cols, cudaStream_t st);
 // blocked Hessenberg reduction kernels (hess.cu)
 size_t hess_work_doubles(long long n);

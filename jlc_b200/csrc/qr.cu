@@ -15,6 +15,8 @@
 //                      factorisation is deterministic;
 //   qr_pack_v_kernel:  V = the panel's reflectors with unit diagonal and zeros
 //                      above it (packV, HouseholderQR.java:445-471);
+//   qr_gram_partial_kernel / qr_gram_sum_kernel: G = V^T V over row slabs,
+//                      one CTA per slab, partials added in slab order;
 //   qr_build_t_kernel: T from the Gram matrix G = V^T V and tau: the
 //                      reference's recurrence (buildT, :300-325) inside
 //                      16 x 16 diagonal blocks, joined blockwise.
@@ -646,6 +648,61 @@ __global__ void qr_pack_v_kernel(const double* A, long long lda, int m, int k0, 
     V[e] = v;
 }
 
+// G = V^T V (64 x 64, row-major) over rows [r0, r1) of the packed V
+// (column-major, ld ldv), in two launches: every CTA sums its slab of rows,
+// 32 rows at a time staged in shared memory, into a 64 x 64 partial (each
+// thread a 4 x 4 block of it, the rows in order); a second launch adds the
+// partials in slab order.  The result does not depend on timing.
+constexpr int GR_THREADS = 256, GR_CHUNK = 32;
+
+__global__ void __launch_bounds__(GR_THREADS) qr_gram_partial_kernel(const double* V, long long ldv, int r0, int r1,
+                                                                     int slab, double* part) {
+    __shared__ double sv[GR_CHUNK][64 + 1];
+    const int tid = threadIdx.x;
+    const int bi = (tid >> 4) * 4, bj = (tid & 15) * 4;  // this thread's 4 x 4 block of G
+    double acc[4][4];
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int b = 0; b < 4; ++b) acc[a][b] = 0.0;
+    const int s0 = r0 + blockIdx.x * slab;
+    const int s1 = s0 + slab < r1 ? s0 + slab : r1;
+    for (int c0 = s0; c0 < s1; c0 += GR_CHUNK) {
+        const int n = s1 - c0 < GR_CHUNK ? s1 - c0 : GR_CHUNK;
+        __syncthreads();  // the previous chunk has been read
+        for (int e = tid; e < GR_CHUNK * 64; e += GR_THREADS) {
+            const int r = e % GR_CHUNK, c = e / GR_CHUNK;  // consecutive threads, consecutive rows
+            sv[r][c] = r < n ? V[(long long)c * ldv + c0 + r] : 0.0;
+        }
+        __syncthreads();
+        for (int r = 0; r < n; ++r) {
+            double x[4], y[4];
+#pragma unroll
+            for (int a = 0; a < 4; ++a) {
+                x[a] = sv[r][bi + a];
+                y[a] = sv[r][bj + a];
+            }
+#pragma unroll
+            for (int a = 0; a < 4; ++a)
+#pragma unroll
+                for (int b = 0; b < 4; ++b) acc[a][b] = fma(x[a], y[b], acc[a][b]);
+        }
+    }
+    double* out = part + (size_t)blockIdx.x * 64 * 64;
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int b = 0; b < 4; ++b) out[(bi + a) * 64 + bj + b] = acc[a][b];
+}
+
+__global__ void qr_gram_sum_kernel(const double* part, int parts, double* G) {
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= 64 * 64) return;
+    double s = part[e];
+    for (int q = 1; q < parts; ++q) s += part[(size_t)q * 64 * 64 + e];
+    G[e] = s;
+}
+
 // T (64 x 64, row-major, upper triangular) from G = V^T V (row-major) and tau,
 // the factor of H_0 H_1 ... H_63 = I - V T V^T.  The reference builds it
 // column by column: T[i][i] = tau_i, T[r][i] = sum_{c=r}^{i-1} T[r][c] t0[c][i]
@@ -823,6 +880,21 @@ int launch_set_identity(double* q, long long ldq, long long m, long long cols, c
         return JLC_E_LAUNCH;
     const long long d = m < cols ? m : cols;
     qr::set_diag_kernel<<<(unsigned)((d + 255) / 256), 256, 0, st>>>(q, ldq, d);
+    return cudaGetLastError() == cudaSuccess ? JLC_OK : JLC_E_LAUNCH;
+}
+
+size_t qr_gram_scratch_bytes(int sm_count) { return (size_t)(sm_count > 0 ? sm_count : 1) * 64 * 64 * sizeof(double); }
+
+int launch_qr_gram(const double* v, long long ldv, int r0, int r1, double* g, double* scratch, int sm_count,
+                   cudaStream_t st) {
+    const int rows = r1 - r0;
+    int parts = (rows + qr::GR_CHUNK - 1) / qr::GR_CHUNK;
+    if (parts > sm_count) parts = sm_count;
+    if (parts < 1) parts = 1;
+    const int slab = (rows + parts - 1) / parts;
+    parts = rows > 0 ? (rows + slab - 1) / slab : 1;
+    qr::qr_gram_partial_kernel<<<parts, qr::GR_THREADS, 0, st>>>(v, ldv, r0, r1, rows > 0 ? slab : 0, scratch);
+    qr::qr_gram_sum_kernel<<<(64 * 64 + 255) / 256, 256, 0, st>>>(scratch, parts, g);
     return cudaGetLastError() == cudaSuccess ? JLC_OK : JLC_E_LAUNCH;
 }
 
