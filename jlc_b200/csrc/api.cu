@@ -73,13 +73,6 @@ int copy_failed(jlc_ctx* ctx, cudaError_t e, const char* what) {
     return rc;
 }
 
-// a host <-> device copy of a host entry (and the copy test hook)
-cudaError_t copy2d(jlc_ctx* ctx, void* dst, size_t dpitch, const void* src, size_t spitch, size_t width,
-                   size_t height, cudaMemcpyKind kind, cudaStream_t st) {
-    if (fault_hit(ctx, JLC_FAULT_COPY)) return cudaErrorUnknown;
-    return cudaMemcpy2DAsync(dst, dpitch, src, spitch, width, height, kind, st);
-}
-
 // Phase markers for the profiler: begin() records the start event of a new
 // record, end() its stop event.  Both are no-ops when profiling is off or the
 // record buffer is full.
@@ -130,6 +123,13 @@ void report_init(jlc_report* rep) {
 }  // namespace
 
 namespace jlc {
+
+// a host <-> device copy of a host entry (and the copy test hook)
+cudaError_t copy2d(jlc_ctx* ctx, void* dst, size_t dpitch, const void* src, size_t spitch, size_t width,
+                   size_t height, cudaMemcpyKind kind, cudaStream_t st) {
+    if (fault_hit(ctx, JLC_FAULT_COPY)) return cudaErrorUnknown;
+    return cudaMemcpy2DAsync(dst, dpitch, src, spitch, width, height, kind, st);
+}
 // The matrix-vector form of a GEMM with n == 1 or m == 1.
 GemvDesc gemv_desc(const GemmDesc& g) {
     GemvDesc v;
@@ -402,6 +402,15 @@ int run_host_pipelined(jlc_ctx* ctx, int la, int lb, long long m, long long n, l
                        int64_t& h2d, int64_t& d2h) {
     int rc = pipe_ready(ctx);
     if (rc) return rc;
+    // pageable operands go through the context's pinned chunks (staging.cu)
+    const bool pa = host_pageable(a), pb = host_pageable(b), pc = host_pageable(c);
+    if ((pa || pb || pc) && !ctx->stager) ctx->stager = stager_create();  // null: the driver stages instead
+    auto h2d_copy = [&](bool pageable, void* dst, long long dp, const void* src, long long sp, long long w,
+                        long long h) {
+        return pageable ? staged_h2d(ctx, dst, (size_t)dp, src, (size_t)sp, (size_t)w, (size_t)h, ctx->cin)
+                        : copy2d(ctx, dst, (size_t)dp, src, (size_t)sp, (size_t)w, (size_t)h, cudaMemcpyHostToDevice,
+                                 ctx->cin);
+    };
     const int maxb = jlc_ctx::kPipeMaxBlocks;
     long long rb = round_up((m + maxb - 1) / maxb, 128);
     if (rb < kPipeBlockRows) rb = kPipeBlockRows;
@@ -412,6 +421,7 @@ int run_host_pipelined(jlc_ctx* ctx, int la, int lb, long long m, long long n, l
         cudaStreamSynchronize(ci);
         cudaStreamSynchronize(cs);
         cudaStreamSynchronize(co);
+        stager_abort(ctx);
     };
     cudaError_t e = cudaEventRecord(ctx->ev0, cs);
     if (e == cudaSuccess) e = cudaStreamWaitEvent(ci, ctx->ev0, 0);
@@ -419,7 +429,7 @@ int run_host_pipelined(jlc_ctx* ctx, int la, int lb, long long m, long long n, l
     if (e != cudaSuccess) return cuda_err(ctx, e, "pipeline start");
     {
         Phase ph(ctx, JLC_PHASE_H2D, ci);
-        e = copy2d(ctx, ctx->bufB.ptr, dldb * 8, b, ldb * 8, b_cols * 8, b_rows, cudaMemcpyHostToDevice, ci);
+        e = h2d_copy(pb, ctx->bufB.ptr, dldb * 8, b, ldb * 8, b_cols * 8, b_rows);
     }
     if (e != cudaSuccess) {
         drain();
@@ -443,16 +453,14 @@ int run_host_pipelined(jlc_ctx* ctx, int la, int lb, long long m, long long n, l
         {
             Phase ph(ctx, JLC_PHASE_H2D, ci);
             if (la == JLC_ROW_MAJOR) {
-                e = copy2d(ctx, dA + r0 * dlda, dlda * 8, a + r0 * lda, lda * 8, k * 8, mr, cudaMemcpyHostToDevice,
-                           ci);
+                e = h2d_copy(pa, dA + r0 * dlda, dlda * 8, a + r0 * lda, lda * 8, k * 8, mr);
                 blk_a = dA + r0 * dlda;
             } else {
-                e = copy2d(ctx, dA + r0, dlda * 8, a + r0, lda * 8, mr * 8, k, cudaMemcpyHostToDevice, ci);
+                e = h2d_copy(pa, dA + r0, dlda * 8, a + r0, lda * 8, mr * 8, k);
                 blk_a = dA + r0;
             }
             if (e == cudaSuccess && beta != 0.0)
-                e = copy2d(ctx, dC + r0 * dldc, dldc * 8, c + r0 * ldc, ldc * 8, n * 8, mr, cudaMemcpyHostToDevice,
-                           ci);
+                e = h2d_copy(pc, dC + r0 * dldc, dldc * 8, c + r0 * ldc, ldc * 8, n * 8, mr);
         }
         if (e == cudaSuccess) e = cudaEventRecord(ctx->pev[i], ci);
         if (e == cudaSuccess) e = cudaStreamWaitEvent(cs, ctx->pev[i], 0);
@@ -482,13 +490,22 @@ int run_host_pipelined(jlc_ctx* ctx, int la, int lb, long long m, long long n, l
         e = cudaStreamWaitEvent(co, ctx->pev[maxb + i], 0);
         if (e == cudaSuccess) {
             Phase ph(ctx, JLC_PHASE_D2H, co);
-            e = copy2d(ctx, c + r0 * ldc, ldc * 8, dC + r0 * dldc, dldc * 8, n * 8, mr, cudaMemcpyDeviceToHost, co);
+            e = pc ? staged_d2h(ctx, c + r0 * ldc, ldc * 8, dC + r0 * dldc, dldc * 8, n * 8, mr, co)
+                   : copy2d(ctx, c + r0 * ldc, ldc * 8, dC + r0 * dldc, dldc * 8, n * 8, mr, cudaMemcpyDeviceToHost,
+                            co);
         }
         if (e != cudaSuccess) {
             drain();
             return cuda_err(ctx, e, "copy C block to host");
         }
         d2h += mr * n * 8;
+    }
+    if (pc) {
+        e = stager_flush(ctx);  // the host copies of the last chunks of C
+        if (e != cudaSuccess) {
+            drain();
+            return cuda_err(ctx, e, "copy C to host");
+        }
     }
     e = cudaEventRecord(ctx->pev[2 * maxb], co);
     if (e == cudaSuccess) e = cudaStreamWaitEvent(cs, ctx->pev[2 * maxb], 0);
@@ -889,6 +906,7 @@ void jlc_destroy(jlc_ctx* ctx) {
     if (ctx->ws.ptr) cudaFree(ctx->ws.ptr);
     if (ctx->d_status) cudaFree(ctx->d_status);
     if (ctx->d_flags) cudaFree(ctx->d_flags);
+    stager_destroy(ctx->stager);
     for (int i = 0; i < 2 * jlc_ctx::kMaxRec; ++i)
         if (ctx->rec_ev[i]) cudaEventDestroy(ctx->rec_ev[i]);
     if (ctx->ev0) cudaEventDestroy(ctx->ev0);

@@ -221,6 +221,27 @@ struct DevBuf {
     size_t bytes = 0;
 };
 
+namespace jlc {
+// Pinned staging of host entries on pageable memory (staging.cu).
+struct HostStager;
+HostStager* stager_create();
+void stager_destroy(HostStager* s);
+bool host_pageable(const void* p);
+// a host <-> device copy of a host entry (and the copy test hook)
+cudaError_t copy2d(jlc_ctx* ctx, void* dst, size_t dpitch, const void* src, size_t spitch, size_t width,
+                   size_t height, cudaMemcpyKind kind, cudaStream_t st);
+// rows x width bytes between pageable host memory and the device through the
+// context's pinned chunks (direct when the context has none)
+cudaError_t staged_h2d(jlc_ctx* ctx, void* dst, size_t dpitch, const void* src, size_t spitch, size_t width,
+                       size_t rows, cudaStream_t st);
+cudaError_t staged_d2h(jlc_ctx* ctx, void* dst, size_t dpitch, const void* src, size_t spitch, size_t width,
+                       size_t rows, cudaStream_t st);
+// waits for every staged device -> host chunk and copies it out
+cudaError_t stager_flush(jlc_ctx* ctx);
+// forgets staged device -> host chunks not yet copied out (after a failure)
+void stager_abort(jlc_ctx* ctx);
+}  // namespace jlc
+
 struct jlc_ctx {
     using Workspace = jlc::Workspace;
     int device = 0;
@@ -240,6 +261,7 @@ struct jlc_ctx {
     static constexpr int kPipeMaxBlocks = 16;
     cudaStream_t cin = nullptr, cout = nullptr;
     cudaEvent_t pev[2 * kPipeMaxBlocks + 1] = {};
+    jlc::HostStager* stager = nullptr;  // pinned chunks for pageable operands (created on first use)
     int dmma_k = 8;
     int qr_cluster_max = 0;  // largest QR panel cluster on this device (0: not queried yet)
     // profiler: event pairs around phases, reused from a pool

@@ -99,3 +99,42 @@ def test_pipeline_repeated_calls_and_small_shapes(ctx, oracle):
         got = C.copy()
         ctx.dgemm(JLC_ROW_MAJOR, JLC_ROW_MAJOR, m, n, k, 0.5, A, k, B, n, 0.0, got, n)
         np.testing.assert_array_equal(got, want)
+
+
+@pytest.mark.parametrize("pinned", ["none", "a_only", "all"])
+def test_pipeline_staging_through_pinned_chunks(ctx, oracle, pinned):
+    """Operands larger than the context's 32 MB pinned chunks, so the staging
+    ring of the pageable path wraps several times on the way in and out; A
+    stored with lda > k (every staged row is a strided 2-D copy); beta != 0
+    (C is staged both ways).  Pinned operands take the direct copies instead,
+    and a mix of the two works.  The result equals the device entry's."""
+    import torch
+    m, n, k = 6000, 1400, 1500
+    lda = k + 37
+    Abuf = oracle.uniform((m, lda), 61)
+    A = Abuf[:, :k]
+    B = oracle.uniform((k, n), 62)
+    C = oracle.uniform((m, n), 63)
+    want, _ = _device_result(ctx, JLC_ROW_MAJOR, JLC_ROW_MAJOR, m, n, k, -0.5, np.ascontiguousarray(A), k, B, n,
+                             0.25, C, JLC_PREC_NATIVE)
+
+    def host(x):
+        if pinned == "none" or (pinned == "a_only" and x is not Abuf):
+            return x.copy()
+        t = torch.empty(x.shape, dtype=torch.float64).pin_memory()
+        t.numpy()[...] = x
+        return t.numpy()
+
+    a_h, b_h, c_h = host(Abuf), host(B), host(C)
+    rep = ctx.dgemm(JLC_ROW_MAJOR, JLC_ROW_MAJOR, m, n, k, -0.5, a_h, lda, b_h, n, 0.25, c_h, n,
+                    precision=JLC_PREC_NATIVE)
+    np.testing.assert_array_equal(c_h, want)
+    assert rep["h2d_bytes"] == (m * k + k * n + m * n) * 8 and rep["d2h_bytes"] == m * n * 8
+    # the same context again (chunks reused), and a product whose C is smaller than one chunk
+    c2 = C[:2048, :700].copy()
+    want2, _ = _device_result(ctx, JLC_ROW_MAJOR, JLC_ROW_MAJOR, 2048, 700, k, 1.0, np.ascontiguousarray(A[:2048]),
+                              k, np.ascontiguousarray(B[:, :700]), 700, 1.0, c2, JLC_PREC_NATIVE)
+    got2 = c2.copy()
+    ctx.dgemm(JLC_ROW_MAJOR, JLC_ROW_MAJOR, 2048, 700, k, 1.0, Abuf[:2048].copy(), lda,
+              np.ascontiguousarray(B[:, :700]), 700, 1.0, got2, 700, precision=JLC_PREC_NATIVE)
+    np.testing.assert_array_equal(got2, want2)
