@@ -369,8 +369,9 @@ def run_ours(args):
         pg = statistics.mean(pg_ms)
         e2e["pageable"] = {"value": round(world * flops / (pg * 1e-3) / 1e9, 1), "unit": "GFLOP/s",
                            "ms_per_step": round(pg, 3), "steps": len(pg_ms), "clock": "host wall clock per call",
-                           "path": "jlc_gemm on pageable numpy buffers (the driver stages the copies through its "
-                                   "own pinned memory), same copies inside the timed region"}
+                           "path": "jlc_gemm on pageable numpy buffers (the library stages the copies through "
+                                   "its ring of pinned chunks, filled and drained by host threads), same copies "
+                                   "inside the timed region"}
         del a_pg, b_pg, c_pg
 
     if rank != 0:
