@@ -52,18 +52,21 @@ __global__ void hess_clear_kernel(double* h, long long ldh, int n) {
 // ---------------------------------------------------------------------------
 // All reflectors of a panel in one cooperative launch.  The m rows (global
 // rows k+1..n-1) are split into slabs of `slab` rows (a multiple of 32), one
-// per CTA.  Per reflector j every CTA works on its own rows and three bounded
+// per CTA.  Per reflector j every CTA works on its own rows and two bounded
 // grid barriers join the reductions:
 //   1. w = A e_col - Y V^T e_col on its rows, its part of u = V^T w;
 //   2. u summed over the CTAs' parts in a fixed order (so every CTA gets the
-//      same bits), z = T^T u, w -= V z, its part of sigma (and x0 from the
-//      CTA that holds row j);
-//   3. sigma summed, the reflector (computed identically in every CTA), v_j
-//      on its rows, its part of s = V_{j-1}^T v_j;
-// then s summed, T's column j (CTA 0), and, with v_j complete, the GEMV
-// A_sub v_j over its rows (every column of the trailing block) and
-// y_j = tau_j (A_sub v_j - Y s) on its rows.  The next reflector reads only
-// its own rows of Y and row j of V, which every CTA wrote before barrier 3.
+//      same bits), z = T^T u, w -= V z, its parts of sigma = |tail|^2 and of
+//      q = V^T tail (tail: the rows below j), and x0 from the CTA that holds
+//      row j;
+// then sigma and q summed, the reflector (computed identically in every CTA),
+// v_j = tail / v0 on its rows, s = V^T v_j = V[j, :] + q / v0, T's column j
+// (CTA 0), and the GEMV over its rows of every column of the trailing block,
+// taken from w itself -- A v_j = A e_j + (A tail) / v0, all of w being written
+// before barrier 2 -- and y_j = tau_j (A v_j - Y s).  w alternates between
+// two buffers by reflector parity, since a CTA may still read the previous w
+// while others write the next.  The next reflector reads its own rows of Y,
+// row j of V written by earlier reflectors, and v_j's unit entry from tau.
 constexpr int PT = 512;           // threads of the cooperative panel kernel
 constexpr int PWARPS = PT / 32;
 
@@ -106,9 +109,18 @@ __global__ void __launch_bounds__(PT, 1) hess_panel_kernel(const PanelArgs p) {
     const int ra = blockIdx.x * p.slab, rb = min(p.m, ra + p.slab);
     const int r0 = p.k + 1, P = gridDim.x;
     unsigned target = 0;
+    double t_prev = 0.0;  // tau of the previous reflector (the same bits in every CTA)
     for (int j = 0; j < p.pw; ++j) {
         const int col = p.k + j;
-        if (tid < PW) vrow[tid] = (tid < j) ? p.V[(j - 1) + (long long)tid * p.ldv] : 0.0;
+        // w is double-buffered by reflector parity: other CTAs may still read
+        // the previous reflector's w in their GEMV while this one is written
+        double* wb = p.wbuf + (long long)(j & 1) * p.ldv;
+        // row j-1 of V: entries of earlier reflectors were fenced by the
+        // previous reflector's barriers; v_{j-1}'s own entry there is its unit
+        // diagonal, known from tau without reading what another CTA wrote
+        if (tid < PW)
+            vrow[tid] = (tid < j - 1) ? p.V[(j - 1) + (long long)tid * p.ldv]
+                                      : (tid == j - 1 && t_prev != 0.0 ? 1.0 : 0.0);
         __syncthreads();
         // 1. w and this CTA's part of V^T w
         double part[PW];
@@ -117,7 +129,7 @@ __global__ void __launch_bounds__(PT, 1) hess_panel_kernel(const PanelArgs p) {
         for (int r = ra + tid; r < rb; r += PT) {
             double w = p.h[(long long)(r0 + r) + (long long)col * p.ldh];
             for (int i = 0; i < j; ++i) w -= p.Y[r + (long long)i * p.ldv] * vrow[i];
-            p.wbuf[r] = w;
+            wb[r] = w;
 #pragma unroll
             for (int i = 0; i < PW; ++i)
                 if (i < j) part[i] += p.V[r + (long long)i * p.ldv] * w;
@@ -125,7 +137,8 @@ __global__ void __launch_bounds__(PT, 1) hess_panel_kernel(const PanelArgs p) {
         block_sum_to(part, j, red, p.part_u + (long long)blockIdx.x * PW);
         target += P;
         if (!grid_barrier(p.counter, target, p.status, &s_ok)) return;
-        // 2. u in a fixed order, z = T^T u, w -= V z, sigma part, x0
+        // 2. u in a fixed order, z = T^T u, w -= V z; this CTA's parts of
+        //    sigma = |tail|^2 and of q = V^T tail (tail: rows > j), and x0
         if (tid < j) {
             double acc = 0.0;
             for (int b = 0; b < P; ++b) acc += p.part_u[(long long)b * PW + tid];
@@ -139,60 +152,63 @@ __global__ void __launch_bounds__(PT, 1) hess_panel_kernel(const PanelArgs p) {
         }
         __syncthreads();
         double sig = 0.0;
+#pragma unroll
+        for (int i = 0; i < PW; ++i) part[i] = 0.0;
         for (int r = ra + tid; r < rb; r += PT) {
-            double w = p.wbuf[r];
+            double w = wb[r];
             for (int i = 0; i < j; ++i) w -= p.V[r + (long long)i * p.ldv] * z[i];
-            p.wbuf[r] = w;
-            if (r == j) *p.x0rec = w;
-            else if (r > j) sig += w * w;
+            wb[r] = w;
+            if (r == j) {
+                *p.x0rec = w;
+            } else if (r > j) {
+                sig += w * w;
+#pragma unroll
+                for (int i = 0; i < PW; ++i)
+                    if (i < j) part[i] += p.V[r + (long long)i * p.ldv] * w;
+            }
         }
+        block_sum_to(part, j, red, p.part_s + (long long)blockIdx.x * PW);
         sig = warp_sum(sig);
+        __syncthreads();  // red is reused
         if (lane == 0) red[warp][0] = sig;
         __syncthreads();
         if (tid == 0) {
-            double t = 0.0;
-            for (int w = 0; w < PWARPS; ++w) t += red[w][0];
-            p.part_sig[blockIdx.x] = t;
+            double tt = 0.0;
+            for (int w = 0; w < PWARPS; ++w) tt += red[w][0];
+            p.part_sig[blockIdx.x] = tt;
         }
         target += P;
         if (!grid_barrier(p.counter, target, p.status, &s_ok)) return;
-        // 3. the reflector (the same bits in every CTA), v_j, part of V^T v_j
+        // 3. the reflector (the same bits in every CTA); v_j = tail / v0 on
+        //    this CTA's rows; s = V^T v_j = V[j, :] + q / v0
         if (tid == 0) {
             double sigma = 0.0;
             for (int b = 0; b < P; ++b) sigma += p.part_sig[b];
             const double x0 = *p.x0rec;
-            double t = 0.0, v0 = 0.0;
+            double tt = 0.0, v0 = 0.0;
             if (sigma > p.eps) {
                 const double mu = sqrt(x0 * x0 + sigma);
                 const double beta = -copysign(mu, x0);
                 v0 = x0 - beta;
                 const double v0sq = v0 * v0;
-                if (v0sq > p.eps) t = 2.0 * v0sq / (sigma + v0sq);
+                if (v0sq > p.eps) tt = 2.0 * v0sq / (sigma + v0sq);
             }
             sc[2] = v0;
-            sc[3] = t;
+            sc[3] = tt;
         }
         __syncthreads();
         const double v0 = sc[2], t = sc[3];
-#pragma unroll
-        for (int i = 0; i < PW; ++i) part[i] = 0.0;
-        double* vj = p.V + (long long)j * p.ldv;
-        for (int r = ra + tid; r < rb; r += PT) {
-            double v = 0.0;
-            if (t != 0.0) v = r < j ? 0.0 : (r == j ? 1.0 : p.wbuf[r] / v0);
-            vj[r] = v;
-#pragma unroll
-            for (int i = 0; i < PW; ++i)
-                if (i < j) part[i] += p.V[r + (long long)i * p.ldv] * v;
-        }
-        block_sum_to(part, j, red, p.part_s + (long long)blockIdx.x * PW);
-        target += P;
-        if (!grid_barrier(p.counter, target, p.status, &s_ok)) return;
-        // 4. s, T's column j, then y_j on this CTA's rows
+        t_prev = t;
         if (tid < j) {
             double acc = 0.0;
             for (int b = 0; b < P; ++b) acc += p.part_s[(long long)b * PW + tid];
-            s[tid] = acc;
+            s[tid] = t != 0.0 ? p.V[j + (long long)tid * p.ldv] + acc / v0 : 0.0;
+        }
+        double* vj = p.V + (long long)j * p.ldv;
+        for (int r = ra + tid; r < rb; r += PT) {
+            double v = 0.0;
+            if (t != 0.0) v = r < j ? 0.0 : (r == j ? 1.0 : wb[r] / v0);
+            vj[r] = v;
         }
         __syncthreads();
         if (blockIdx.x == 0 && tid < PW) {
@@ -208,31 +224,38 @@ __global__ void __launch_bounds__(PT, 1) hess_panel_kernel(const PanelArgs p) {
             p.T[i * PW + j] = val;
             if (i == 0) p.tau[j] = t;
         }
-        // GEMV over the trailing block: lanes walk 32 rows, warps the columns
-        for (int c0 = ra; c0 < rb; c0 += 32) {
-            const int r = c0 + lane;
-            double acc = 0.0;
-            if (t != 0.0 && r < rb) {
-                const double* arow = p.h + (long long)(r0 + r) + (long long)r0 * p.ldh;
-                int c = j + warp;
-                for (; c + 3 * PWARPS < p.m; c += 4 * PWARPS) {
-                    const double a0 = arow[(long long)c * p.ldh];
-                    const double a1 = arow[(long long)(c + PWARPS) * p.ldh];
-                    const double a2 = arow[(long long)(c + 2 * PWARPS) * p.ldh];
-                    const double a3 = arow[(long long)(c + 3 * PWARPS) * p.ldh];
-                    acc += a0 * vj[c] + a1 * vj[c + PWARPS] + a2 * vj[c + 2 * PWARPS] + a3 * vj[c + 3 * PWARPS];
+        // GEMV over the trailing block with v_j = e_j + tail / v0, from w (all
+        // of it written before the barrier): A v_j = A e_j + (A tail) / v0.
+        // Lanes walk 32 rows, warps the columns.
+        if (t != 0.0) {
+            for (int c0 = ra; c0 < rb; c0 += 32) {
+                const int r = c0 + lane;
+                double acc = 0.0;
+                if (r < rb) {
+                    const double* arow = p.h + (long long)(r0 + r) + (long long)r0 * p.ldh;
+                    int c = j + 1 + warp;
+                    for (; c + 3 * PWARPS < p.m; c += 4 * PWARPS) {
+                        const double a0 = arow[(long long)c * p.ldh];
+                        const double a1 = arow[(long long)(c + PWARPS) * p.ldh];
+                        const double a2 = arow[(long long)(c + 2 * PWARPS) * p.ldh];
+                        const double a3 = arow[(long long)(c + 3 * PWARPS) * p.ldh];
+                        acc += a0 * wb[c] + a1 * wb[c + PWARPS] + a2 * wb[c + 2 * PWARPS] + a3 * wb[c + 3 * PWARPS];
+                    }
+                    for (; c < p.m; c += PWARPS) acc += arow[(long long)c * p.ldh] * wb[c];
                 }
-                for (; c < p.m; c += PWARPS) acc += arow[(long long)c * p.ldh] * vj[c];
+                ypart[warp][lane] = acc;
+                __syncthreads();
+                if (warp == 0 && r < rb) {
+                    double y = 0.0;
+                    for (int w = 0; w < PWARPS; ++w) y += ypart[w][lane];
+                    y = p.h[(long long)(r0 + r) + (long long)(r0 + j) * p.ldh] + y / v0;
+                    for (int i = 0; i < j; ++i) y -= p.Y[r + (long long)i * p.ldv] * s[i];
+                    p.Y[r + (long long)j * p.ldv] = t * y;
+                }
+                __syncthreads();
             }
-            ypart[warp][lane] = acc;
-            __syncthreads();
-            if (warp == 0 && r < rb) {
-                double y = 0.0;
-                for (int w = 0; w < PWARPS; ++w) y += ypart[w][lane];
-                for (int i = 0; i < j; ++i) y -= p.Y[r + (long long)i * p.ldv] * s[i];
-                p.Y[r + (long long)j * p.ldv] = t * y;
-            }
-            __syncthreads();
+        } else {
+            for (int r = ra + tid; r < rb; r += PT) p.Y[r + (long long)j * p.ldv] = 0.0;
         }
     }
 }
