@@ -226,26 +226,41 @@ __global__ void __launch_bounds__(PT, 1) hess_panel_kernel(const PanelArgs p) {
         }
         // GEMV over the trailing block with v_j = e_j + tail / v0, from w (all
         // of it written before the barrier): A v_j = A e_j + (A tail) / v0.
-        // Lanes walk 32 rows, warps the columns.
+        // Lanes walk 32 rows; each warp a contiguous range of columns, 32 at
+        // a time: w of the 32 columns in one load, spread by shuffles, and 16
+        // column loads in flight per lane (a warp's loads are 256-byte row
+        // segments of consecutive columns).
         if (t != 0.0) {
+            const int ncols = p.m - (j + 1);
+            const int per = (ncols + PWARPS - 1) / PWARPS;
+            const int cw0 = j + 1 + warp * per, cw1 = min(p.m, cw0 + per);
             for (int c0 = ra; c0 < rb; c0 += 32) {
                 const int r = c0 + lane;
+                const bool rv = r < rb;
+                // rows past the slab read row ra (in range) and are discarded
+                const double* arow = p.h + (long long)(r0 + (rv ? r : ra)) + (long long)r0 * p.ldh;
                 double acc = 0.0;
-                if (r < rb) {
-                    const double* arow = p.h + (long long)(r0 + r) + (long long)r0 * p.ldh;
-                    int c = j + 1 + warp;
-                    for (; c + 3 * PWARPS < p.m; c += 4 * PWARPS) {
-                        const double a0 = arow[(long long)c * p.ldh];
-                        const double a1 = arow[(long long)(c + PWARPS) * p.ldh];
-                        const double a2 = arow[(long long)(c + 2 * PWARPS) * p.ldh];
-                        const double a3 = arow[(long long)(c + 3 * PWARPS) * p.ldh];
-                        acc += a0 * wb[c] + a1 * wb[c + PWARPS] + a2 * wb[c + 2 * PWARPS] + a3 * wb[c + 3 * PWARPS];
+                for (int cb = cw0; cb < cw1; cb += 32) {
+                    const int nc = min(32, cw1 - cb);
+                    const double wv = lane < nc ? wb[cb + lane] : 0.0;
+                    const double* ac = arow + (long long)cb * p.ldh;
+                    if (nc == 32) {
+#pragma unroll
+                        for (int h = 0; h < 32; h += 16) {
+                            double av[16];
+#pragma unroll
+                            for (int u = 0; u < 16; ++u) av[u] = ac[(long long)(h + u) * p.ldh];
+#pragma unroll
+                            for (int u = 0; u < 16; ++u) acc = fma(av[u], __shfl_sync(0xffffffffu, wv, h + u), acc);
+                        }
+                    } else {
+                        for (int u = 0; u < nc; ++u)
+                            acc = fma(ac[(long long)u * p.ldh], __shfl_sync(0xffffffffu, wv, u), acc);
                     }
-                    for (; c < p.m; c += PWARPS) acc += arow[(long long)c * p.ldh] * wb[c];
                 }
-                ypart[warp][lane] = acc;
+                ypart[warp][lane] = rv ? acc : 0.0;
                 __syncthreads();
-                if (warp == 0 && r < rb) {
+                if (warp == 0 && rv) {
                     double y = 0.0;
                     for (int w = 0; w < PWARPS; ++w) y += ypart[w][lane];
                     y = p.h[(long long)(r0 + r) + (long long)(r0 + j) * p.ldh] + y / v0;
