@@ -68,6 +68,7 @@ __global__ void hess_clear_kernel(double* h, long long ldh, int n) {
 // while others write the next.  The next reflector reads its own rows of Y,
 // row j of V written by earlier reflectors, and v_j's unit entry from tau.
 constexpr int PT = 512;           // threads of the cooperative panel kernel
+constexpr int kHessMaxDynSmem = 160 * 1024;  // V and Y rows of a slab of up to 320 rows
 constexpr int PWARPS = PT / 32;
 
 struct PanelArgs {
@@ -80,6 +81,7 @@ struct PanelArgs {
     unsigned* counter;                           // zero at launch
     int* status;
     double eps;
+    int cache_rows;  // the CTA's rows of V and Y live in dynamic shared memory
 };
 
 __device__ void block_sum_to(double (&part)[PW], int cnt, double (*red)[PW], double* out_row) {
@@ -99,8 +101,19 @@ __device__ void block_sum_to(double (&part)[PW], int cnt, double (*red)[PW], dou
     }
 }
 
+// Sum over the P CTAs of column i of a [P][PW] partial array, every CTA the
+// same bits: lanes take CTAs lane, lane + 32, ... in order, then a butterfly.
+__device__ __forceinline__ double cta_sum(const double* part, int P, int i) {
+    const int lane = threadIdx.x & 31;
+    double acc = 0.0;
+    for (int b = lane; b < P; b += 32) acc += part[(long long)b * PW + i];
+    return warp_sum(acc);
+}
+
 __global__ void __launch_bounds__(PT, 1) hess_panel_kernel(const PanelArgs p) {
+    extern __shared__ double dyn[];  // the CTA's rows of V and Y: column i at [i * slab] (when cached)
     __shared__ double vrow[PW], u[PW], z[PW], s[PW];
+    __shared__ double sT[PW][PW];    // this CTA's copy of T (computed here with CTA 0's bits)
     __shared__ double red[PWARPS][PW];
     __shared__ double sc[4];
     __shared__ double ypart[PWARPS][32];
@@ -108,8 +121,16 @@ __global__ void __launch_bounds__(PT, 1) hess_panel_kernel(const PanelArgs p) {
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int ra = blockIdx.x * p.slab, rb = min(p.m, ra + p.slab);
     const int r0 = p.k + 1, P = gridDim.x;
+    // V(r, i) = Vb[(r - ra) + i * vs], Y likewise: shared memory when the slab
+    // fits, else the global arrays
+    const bool cached = p.cache_rows;
+    double* Vb = cached ? dyn : p.V + ra;
+    double* Yb = cached ? dyn + (long long)p.slab * PW : p.Y + ra;
+    const long long vs = cached ? p.slab : p.ldv;
+    for (int e = tid; e < PW * PW; e += PT) sT[e / PW][e % PW] = 0.0;
     unsigned target = 0;
     double t_prev = 0.0;  // tau of the previous reflector (the same bits in every CTA)
+    __syncthreads();
     for (int j = 0; j < p.pw; ++j) {
         const int col = p.k + j;
         // w is double-buffered by reflector parity: other CTAs may still read
@@ -127,27 +148,28 @@ __global__ void __launch_bounds__(PT, 1) hess_panel_kernel(const PanelArgs p) {
 #pragma unroll
         for (int i = 0; i < PW; ++i) part[i] = 0.0;
         for (int r = ra + tid; r < rb; r += PT) {
+            const int rl = r - ra;
             double w = p.h[(long long)(r0 + r) + (long long)col * p.ldh];
-            for (int i = 0; i < j; ++i) w -= p.Y[r + (long long)i * p.ldv] * vrow[i];
+            for (int i = 0; i < j; ++i) w -= Yb[rl + i * vs] * vrow[i];
             wb[r] = w;
 #pragma unroll
             for (int i = 0; i < PW; ++i)
-                if (i < j) part[i] += p.V[r + (long long)i * p.ldv] * w;
+                if (i < j) part[i] += Vb[rl + i * vs] * w;
         }
         block_sum_to(part, j, red, p.part_u + (long long)blockIdx.x * PW);
         target += P;
         if (!grid_barrier(p.counter, target, p.status, &s_ok)) return;
-        // 2. u in a fixed order, z = T^T u, w -= V z; this CTA's parts of
-        //    sigma = |tail|^2 and of q = V^T tail (tail: rows > j), and x0
-        if (tid < j) {
-            double acc = 0.0;
-            for (int b = 0; b < P; ++b) acc += p.part_u[(long long)b * PW + tid];
-            u[tid] = acc;
+        // 2. u summed over the CTAs (warp i: u[i]), z = T^T u, w -= V z; this
+        //    CTA's parts of sigma = |tail|^2 and of q = V^T tail (tail: rows
+        //    below j), and x0
+        for (int i = warp; i < j; i += PWARPS) {
+            const double v = cta_sum(p.part_u, P, i);
+            if (lane == 0) u[i] = v;
         }
         __syncthreads();
         if (tid < j) {
             double acc = 0.0;
-            for (int l = 0; l <= tid; ++l) acc += p.T[l * PW + tid] * u[l];
+            for (int l = 0; l <= tid; ++l) acc += sT[l][tid] * u[l];
             z[tid] = acc;
         }
         __syncthreads();
@@ -155,8 +177,9 @@ __global__ void __launch_bounds__(PT, 1) hess_panel_kernel(const PanelArgs p) {
 #pragma unroll
         for (int i = 0; i < PW; ++i) part[i] = 0.0;
         for (int r = ra + tid; r < rb; r += PT) {
+            const int rl = r - ra;
             double w = wb[r];
-            for (int i = 0; i < j; ++i) w -= p.V[r + (long long)i * p.ldv] * z[i];
+            for (int i = 0; i < j; ++i) w -= Vb[rl + i * vs] * z[i];
             wb[r] = w;
             if (r == j) {
                 *p.x0rec = w;
@@ -164,7 +187,7 @@ __global__ void __launch_bounds__(PT, 1) hess_panel_kernel(const PanelArgs p) {
                 sig += w * w;
 #pragma unroll
                 for (int i = 0; i < PW; ++i)
-                    if (i < j) part[i] += p.V[r + (long long)i * p.ldv] * w;
+                    if (i < j) part[i] += Vb[rl + i * vs] * w;
             }
         }
         block_sum_to(part, j, red, p.part_s + (long long)blockIdx.x * PW);
@@ -180,49 +203,56 @@ __global__ void __launch_bounds__(PT, 1) hess_panel_kernel(const PanelArgs p) {
         target += P;
         if (!grid_barrier(p.counter, target, p.status, &s_ok)) return;
         // 3. the reflector (the same bits in every CTA); v_j = tail / v0 on
-        //    this CTA's rows; s = V^T v_j = V[j, :] + q / v0
-        if (tid == 0) {
-            double sigma = 0.0;
-            for (int b = 0; b < P; ++b) sigma += p.part_sig[b];
-            const double x0 = *p.x0rec;
-            double tt = 0.0, v0 = 0.0;
-            if (sigma > p.eps) {
-                const double mu = sqrt(x0 * x0 + sigma);
-                const double beta = -copysign(mu, x0);
-                v0 = x0 - beta;
-                const double v0sq = v0 * v0;
-                if (v0sq > p.eps) tt = 2.0 * v0sq / (sigma + v0sq);
+        //    this CTA's rows; s = V^T v_j = V[j, :] + q / v0; T's column j
+        if (warp == 0) {
+            double acc = 0.0;
+            for (int b = lane; b < P; b += 32) acc += p.part_sig[b];
+            const double sigma = warp_sum(acc);
+            if (lane == 0) {
+                const double x0 = *p.x0rec;
+                double tt = 0.0, v0 = 0.0;
+                if (sigma > p.eps) {
+                    const double mu = sqrt(x0 * x0 + sigma);
+                    const double beta = -copysign(mu, x0);
+                    v0 = x0 - beta;
+                    const double v0sq = v0 * v0;
+                    if (v0sq > p.eps) tt = 2.0 * v0sq / (sigma + v0sq);
+                }
+                sc[2] = v0;
+                sc[3] = tt;
             }
-            sc[2] = v0;
-            sc[3] = tt;
+        }
+        for (int i = warp; i < j; i += PWARPS) {
+            const double v = cta_sum(p.part_s, P, i);
+            if (lane == 0) u[i] = v;  // q, in u's place
         }
         __syncthreads();
         const double v0 = sc[2], t = sc[3];
         t_prev = t;
-        if (tid < j) {
-            double acc = 0.0;
-            for (int b = 0; b < P; ++b) acc += p.part_s[(long long)b * PW + tid];
-            s[tid] = t != 0.0 ? p.V[j + (long long)tid * p.ldv] + acc / v0 : 0.0;
-        }
+        if (tid < j) s[tid] = t != 0.0 ? p.V[j + (long long)tid * p.ldv] + u[tid] / v0 : 0.0;
         double* vj = p.V + (long long)j * p.ldv;
         for (int r = ra + tid; r < rb; r += PT) {
             double v = 0.0;
             if (t != 0.0) v = r < j ? 0.0 : (r == j ? 1.0 : wb[r] / v0);
             vj[r] = v;
+            if (cached) Vb[(r - ra) + j * vs] = v;
         }
         __syncthreads();
-        if (blockIdx.x == 0 && tid < PW) {
+        if (tid < PW) {
             const int i = tid;
             double val = 0.0;
             if (i < j) {
                 double acc = 0.0;
-                for (int l = i; l < j; ++l) acc += p.T[i * PW + l] * s[l];
+                for (int l = i; l < j; ++l) acc += sT[i][l] * s[l];
                 val = -t * acc;
             } else if (i == j) {
                 val = t;
             }
-            p.T[i * PW + j] = val;
-            if (i == 0) p.tau[j] = t;
+            sT[i][j] = val;
+            if (blockIdx.x == 0) {
+                p.T[i * PW + j] = val;
+                if (i == 0) p.tau[j] = t;
+            }
         }
         // GEMV over the trailing block with v_j = e_j + tail / v0, from w (all
         // of it written before the barrier): A v_j = A e_j + (A tail) / v0.
@@ -249,13 +279,13 @@ __global__ void __launch_bounds__(PT, 1) hess_panel_kernel(const PanelArgs p) {
                         for (int h = 0; h < 32; h += 16) {
                             double av[16];
 #pragma unroll
-                            for (int u = 0; u < 16; ++u) av[u] = ac[(long long)(h + u) * p.ldh];
+                            for (int q = 0; q < 16; ++q) av[q] = ac[(long long)(h + q) * p.ldh];
 #pragma unroll
-                            for (int u = 0; u < 16; ++u) acc = fma(av[u], __shfl_sync(0xffffffffu, wv, h + u), acc);
+                            for (int q = 0; q < 16; ++q) acc = fma(av[q], __shfl_sync(0xffffffffu, wv, h + q), acc);
                         }
                     } else {
-                        for (int u = 0; u < nc; ++u)
-                            acc = fma(ac[(long long)u * p.ldh], __shfl_sync(0xffffffffu, wv, u), acc);
+                        for (int q = 0; q < nc; ++q)
+                            acc = fma(ac[(long long)q * p.ldh], __shfl_sync(0xffffffffu, wv, q), acc);
                     }
                 }
                 ypart[warp][lane] = rv ? acc : 0.0;
@@ -264,14 +294,20 @@ __global__ void __launch_bounds__(PT, 1) hess_panel_kernel(const PanelArgs p) {
                     double y = 0.0;
                     for (int w = 0; w < PWARPS; ++w) y += ypart[w][lane];
                     y = p.h[(long long)(r0 + r) + (long long)(r0 + j) * p.ldh] + y / v0;
-                    for (int i = 0; i < j; ++i) y -= p.Y[r + (long long)i * p.ldv] * s[i];
+                    const int rl = r - ra;
+                    for (int i = 0; i < j; ++i) y -= Yb[rl + i * vs] * s[i];
                     p.Y[r + (long long)j * p.ldv] = t * y;
+                    if (cached) Yb[rl + j * vs] = t * y;
                 }
                 __syncthreads();
             }
         } else {
-            for (int r = ra + tid; r < rb; r += PT) p.Y[r + (long long)j * p.ldv] = 0.0;
+            for (int r = ra + tid; r < rb; r += PT) {
+                p.Y[r + (long long)j * p.ldv] = 0.0;
+                if (cached) Yb[(r - ra) + j * vs] = 0.0;
+            }
         }
+        __syncthreads();  // sT, s, u and the cached rows are read again next reflector
     }
 }
 
@@ -318,9 +354,17 @@ int launch_hess_panel(const double* h, long long ldh, int n, int k, int pw, doub
     a.counter = reinterpret_cast<unsigned*>(a.x0rec + 8);
     a.status = status;
     a.eps = 1e-12;
+    // the slab's rows of V and Y in shared memory while they fit
+    const size_t dyn = (size_t)a.slab * PW * 2 * sizeof(double);
+    a.cache_rows = dyn <= (size_t)kHessMaxDynSmem;
+    if (a.cache_rows &&
+        cudaFuncSetAttribute((const void*)hess_panel_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             kHessMaxDynSmem) != cudaSuccess)
+        return JLC_E_LAUNCH;
     if (cudaMemsetAsync(a.counter, 0, sizeof(unsigned), st) != cudaSuccess) return JLC_E_CUDA;
     void* args[] = {&a};
-    cudaError_t e = cudaLaunchCooperativeKernel((const void*)hess_panel_kernel, dim3(P), dim3(PT), args, 0, st);
+    cudaError_t e = cudaLaunchCooperativeKernel((const void*)hess_panel_kernel, dim3(P), dim3(PT), args,
+                                                a.cache_rows ? dyn : 0, st);
     return e == cudaSuccess ? JLC_OK : JLC_E_LAUNCH;
 }
 
