@@ -110,19 +110,22 @@ __device__ __forceinline__ bool grid_barrier(unsigned* counter, unsigned target,
     __syncthreads();
     if (threadIdx.x == 0) {
         asm volatile("red.release.gpu.global.add.u32 [%0], %1;" ::"l"(counter), "r"(1u) : "memory");
-        const uint64_t t0 = globaltimer_ns();
-        const uint64_t limit = wait_limit_ns(status);
         int ok = 1;
-        for (unsigned it = 0; ld_acquire_u32(counter) < target; ++it) {
-            if ((it & 63u) == 0u) {
-                if (*(volatile int*)status != 0) {
-                    ok = 0;
-                    break;
-                }
-                if (globaltimer_ns() - t0 > limit) {
-                    atomicOr(status, JLC_DEV_TIMEOUT);
-                    ok = 0;
-                    break;
+        if (ld_acquire_u32(counter) < target) {
+            // not complete at the first poll: only now the clock and the limit
+            const uint64_t t0 = globaltimer_ns();
+            const uint64_t limit = wait_limit_ns(status);
+            for (unsigned it = 0; ld_acquire_u32(counter) < target; ++it) {
+                if ((it & 63u) == 0u) {
+                    if (*(volatile int*)status != 0) {
+                        ok = 0;
+                        break;
+                    }
+                    if (globaltimer_ns() - t0 > limit) {
+                        atomicOr(status, JLC_DEV_TIMEOUT);
+                        ok = 0;
+                        break;
+                    }
                 }
             }
         }
