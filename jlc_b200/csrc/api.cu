@@ -840,7 +840,8 @@ int jlc_autotune_splitk(jlc_ctx* ctx, int64_t m, int64_t n, int64_t k, int* spli
     if (!ctx || !split || m < 2 || n < 2 || k < 1 || m > (1 << 20) || n > (1 << 20) || k > (1 << 20))
         return set_err(ctx, JLC_E_ARG, "autotune_splitk: bad arguments");
     cudaSetDevice(ctx->device);
-    const long long tiles = ((m + 127) / 128) * ((n + 127) / 128), kbl = (k + 15) / 16;
+    const long long bm = dmma_bm(m);
+    const long long tiles = ((m + bm - 1) / bm) * ((n + 127) / 128), kbl = (k + 15) / 16;
     const long long lda = round_up(k, 8), ldb = round_up(n, 8), ldc = n;
     int rc = reserve(ctx, ctx->bufA, (size_t)(m * lda) * 8, "autotune A");
     if (!rc) rc = reserve(ctx, ctx->bufB, (size_t)(k * ldb) * 8, "autotune B");

@@ -60,6 +60,24 @@ constexpr int A_STAGE = BM * BK * 8;  // 16 KB
 constexpr int B_STAGE = BN * BK * 8;  // 16 KB
 constexpr int STAGE_BYTES = A_STAGE + B_STAGE;
 constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024 + 2 * STAGES * 8 + MMA_WARPS * 8;
+
+// Tile shapes of the kernel: 128 x 128 (2 x 4 warps of 64 x 32), and for
+// products with few rows -- the panel GEMMs of blocked factorisations, 32 or
+// 64 rows -- 64 x 128 or 32 x 128 (1 x 8 warps of 64 x 16 or 32 x 16), so
+// that a thin product does not run 128-row tiles that are mostly empty.
+// Smaller tiles take more ring stages in the same shared memory.
+template <int TBM>
+struct Cfg {
+    static constexpr int BM = TBM;
+    static constexpr int WARPS_M = TBM >= 128 ? 2 : 1, WARPS_N = MMA_WARPS / WARPS_M;
+    static constexpr int WM = BM / WARPS_M, WN = BN / WARPS_N;
+    static constexpr int MT = WM / 16, NT = WN / 8;
+    static constexpr int A_STAGE = BM * BK * 8;
+    static constexpr int STAGE_BYTES = A_STAGE + B_STAGE;
+    static constexpr int STAGES = (160 * 1024) / STAGE_BYTES;
+    static constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024 + 2 * STAGES * 8 + MMA_WARPS * 8;
+};
+static_assert(Cfg<128>::STAGES == STAGES && Cfg<128>::SMEM_BYTES == SMEM_BYTES, "128-row tile");
 constexpr int RASTER_GROUP = 8;
 
 struct Params {
@@ -94,10 +112,14 @@ __device__ __forceinline__ void drain_wait(uint64_t* bar, uint32_t parity, int* 
     }
 }
 
-template <bool A_KMAJOR, bool B_KMAJOR, int MMA_K>
+template <bool A_KMAJOR, bool B_KMAJOR, int MMA_K, int TBM>
 __global__ void __launch_bounds__(THREADS, 1)
     dgemm_dmma_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB,
                       const Params p) {
+    // this instance's tile shape (shadows the 128-row defaults)
+    using C = Cfg<TBM>;
+    constexpr int BM = C::BM, WARPS_N = C::WARPS_N, WM = C::WM, WN = C::WN, MT = C::MT, NT = C::NT;
+    constexpr int A_STAGE = C::A_STAGE, STAGE_BYTES = C::STAGE_BYTES, STAGES = C::STAGES;
     if (p.gate != nullptr && (p.gate[kFlagNonfiniteA] | p.gate[kFlagFallback] | p.gate[kFlagNonfiniteB]) == 0) return;
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     char* smem = reinterpret_cast<char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
@@ -389,20 +411,25 @@ __global__ void __launch_bounds__(THREADS, 1)
     }
 }
 
-template <bool AK, bool BK_, int MK>
+template <bool AK, bool BK_, int MK, int TBM>
 static int launch_variant(const CUtensorMap& ma, const CUtensorMap& mb, const Params& p, int grid,
                           cudaStream_t st) {
-    auto kern = dgemm_dmma_kernel<AK, BK_, MK>;
-    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES);
+    auto kern = dgemm_dmma_kernel<AK, BK_, MK, TBM>;
+    constexpr int smem = Cfg<TBM>::SMEM_BYTES;
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     if (e != cudaSuccess) return JLC_E_LAUNCH;
-    kern<<<grid, THREADS, SMEM_BYTES, st>>>(ma, mb, p);
+    kern<<<grid, THREADS, smem, st>>>(ma, mb, p);
     return cudaGetLastError() == cudaSuccess ? JLC_OK : JLC_E_LAUNCH;
 }
 
 }  // namespace dmma
 
+// tile height for an m-row product: 32 or 64 rows for thin products, else 128
+int dmma_bm(long long m) { return m <= 32 ? 32 : (m <= 64 ? 64 : 128); }
+
 int dmma_grid(long long m, long long n, int sm_count) {
-    const long long tiles = ((m + dmma::BM - 1) / dmma::BM) * ((n + dmma::BN - 1) / dmma::BN);
+    const long long bm = dmma_bm(m);
+    const long long tiles = ((m + bm - 1) / bm) * ((n + dmma::BN - 1) / dmma::BN);
     return (int)(tiles < sm_count ? tiles : sm_count);
 }
 
@@ -450,7 +477,8 @@ int dmma_splitk_tuned(int sm_count, long long tiles, long long kbl) {
 // block sums in the same order as the single-shot call.
 int dmma_splitk(long long m, long long n, long long k, int sm_count) {
     using namespace dmma;
-    const long long tiles = ((m + BM - 1) / BM) * ((n + BN - 1) / BN);
+    const long long bm = dmma_bm(m);
+    const long long tiles = ((m + bm - 1) / bm) * ((n + BN - 1) / BN);
     const long long kbl = (k + BK - 1) / BK;
     const int tuned = dmma_splitk_tuned(sm_count, tiles, kbl);
     if (tuned > 0 && dmma_splitk_legal(tiles, kbl, tuned, sm_count)) return tuned;
@@ -476,9 +504,10 @@ int dmma_splitk(long long m, long long n, long long k, int sm_count) {
 size_t dmma_splitk_bytes(long long m, long long n, int ksplit) {
     using namespace dmma;
     if (ksplit < 2) return 0;
-    const long long tiles = ((m + BM - 1) / BM) * ((n + BN - 1) / BN);
+    const long long bm = dmma_bm(m);
+    const long long tiles = ((m + bm - 1) / bm) * ((n + BN - 1) / BN);
     const int s = ksplit;
-    return (size_t)(tiles * s) * BM * BN * sizeof(double) + (size_t)tiles * sizeof(int);
+    return (size_t)(tiles * s) * bm * BN * sizeof(double) + (size_t)tiles * sizeof(int);
 }
 
 int launch_dgemm_dmma(const GemmDesc& g, cudaStream_t st, int sm_count, int* status, const int* gate,
@@ -490,10 +519,11 @@ int launch_dgemm_dmma(const GemmDesc& g, cudaStream_t st, int sm_count, int* sta
     }
     const bool a_k = g.layout_a == 0;  // row-major A: k contiguous
     const bool b_k = g.layout_b == 1;  // column-major B: k contiguous
+    const int bm = dmma_bm(g.m);
     CUtensorMap ma, mb;
     int rc;
     if (a_k)
-        rc = make_tmap_2d(&ma, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 8, (void*)g.a, g.k, g.m, g.lda, BK, BM,
+        rc = make_tmap_2d(&ma, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 8, (void*)g.a, g.k, g.m, g.lda, BK, bm,
                           CU_TENSOR_MAP_SWIZZLE_128B, err, errlen);
     else
         rc = make_tmap_2d(&ma, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 8, (void*)g.a, g.m, g.k, g.lda, 16, BK,
@@ -519,7 +549,7 @@ int launch_dgemm_dmma(const GemmDesc& g, cudaStream_t st, int sm_count, int* sta
     p.dot_mat = g.dot_mat;
     p.dot_ld = g.dot_ld;
     p.dot_partials = g.dot_partials;
-    p.tiles_m = (int)((g.m + BM - 1) / BM);
+    p.tiles_m = (int)((g.m + bm - 1) / bm);
     p.tiles_n = (int)((g.n + BN - 1) / BN);
     p.num_tiles = p.tiles_m * p.tiles_n;
     p.k_blocks = (int)((g.k + BK - 1) / BK);
@@ -538,7 +568,7 @@ int launch_dgemm_dmma(const GemmDesc& g, cudaStream_t st, int sm_count, int* sta
             p.ksplit = s;
             p.part = static_cast<double*>(splitk_ws);
             p.counters = reinterpret_cast<int*>(static_cast<char*>(splitk_ws) +
-                                                (size_t)p.num_tiles * s * BM * BN * sizeof(double));
+                                                (size_t)p.num_tiles * s * bm * BN * sizeof(double));
             if (cudaMemsetAsync(p.counters, 0, (size_t)p.num_tiles * sizeof(int), st) != cudaSuccess) {
                 snprintf(err, errlen, "split-K counters: %s", cudaGetErrorString(cudaGetLastError()));
                 return JLC_E_LAUNCH;
@@ -548,17 +578,21 @@ int launch_dgemm_dmma(const GemmDesc& g, cudaStream_t st, int sm_count, int* sta
     const int units = p.num_tiles * p.ksplit;
     const int grid = units < sm_count ? units : sm_count;
 
-#define JLC_DMMA_DISPATCH(MK)                                                     \
-    if (a_k && b_k) rc = launch_variant<true, true, MK>(ma, mb, p, grid, st);      \
-    else if (a_k) rc = launch_variant<true, false, MK>(ma, mb, p, grid, st);       \
-    else if (b_k) rc = launch_variant<false, true, MK>(ma, mb, p, grid, st);       \
-    else rc = launch_variant<false, false, MK>(ma, mb, p, grid, st);
-    if (mma_k == 4) {
-        JLC_DMMA_DISPATCH(4)
+#define JLC_DMMA_DISPATCH(MK, TB)                                                     \
+    if (a_k && b_k) rc = launch_variant<true, true, MK, TB>(ma, mb, p, grid, st);      \
+    else if (a_k) rc = launch_variant<true, false, MK, TB>(ma, mb, p, grid, st);       \
+    else if (b_k) rc = launch_variant<false, true, MK, TB>(ma, mb, p, grid, st);       \
+    else rc = launch_variant<false, false, MK, TB>(ma, mb, p, grid, st);
+    if (bm == 32) {
+        JLC_DMMA_DISPATCH(8, 32)  // thin tiles: the default k step only
+    } else if (bm == 64) {
+        JLC_DMMA_DISPATCH(8, 64)
+    } else if (mma_k == 4) {
+        JLC_DMMA_DISPATCH(4, 128)
     } else if (mma_k == 16) {
-        JLC_DMMA_DISPATCH(16)
+        JLC_DMMA_DISPATCH(16, 128)
     } else {
-        JLC_DMMA_DISPATCH(8)
+        JLC_DMMA_DISPATCH(8, 128)
     }
 #undef JLC_DMMA_DISPATCH
     if (rc) snprintf(err, errlen, "DMMA kernel launch failed: %s", cudaGetErrorString(cudaGetLastError()));

@@ -50,6 +50,8 @@ struct GemmDesc {
 // number of CTAs the DMMA / Ozaki GEMM kernels launch for this shape (the
 // length of dot_partials they fill)
 int dmma_grid(long long m, long long n, int sm_count);
+// tile height the DMMA kernel uses for an m-row product (32, 64 or 128)
+int dmma_bm(long long m);
 int ozaki_grid(long long m, long long n, int sm_count);
 
 // Grow-only device scratch owned by a context.

@@ -386,3 +386,30 @@ def test_splitk_autotune_caches_and_is_used(ctx, oracle, tmp_path, monkeypatch):
         outs.append(dC.cpu().numpy())
     np.testing.assert_array_equal(outs[0], outs[1])
     assert_fp64_bound("tuned split-K", outs[0], A, B, None, 1.0, 0.0)
+
+
+@pytest.mark.parametrize("m", [2, 20, 32, 33, 50, 64, 65])
+@pytest.mark.parametrize("la,lb", [(0, 0), (0, 1), (1, 0), (1, 1)])
+def test_thin_tiles(ctx, oracle, m, la, lb):
+    """Products of at most 64 rows run 32- or 64-row tiles (the panel GEMMs of
+    the blocked factorisations): every operand order, rows on and just past
+    the tile heights, beta != 0, and a k long enough for split-K.  Inside the
+    FP64 bound, and the same bits on a second run."""
+    import torch
+    n, k = 1000, 3000
+    A = oracle.uniform((m, k), 81 + m)
+    B = oracle.uniform((k, n), 82)
+    C = oracle.uniform((m, n), 83)
+    a_store = A if la == 0 else np.ascontiguousarray(A.T)
+    b_store = B if lb == 0 else np.ascontiguousarray(B.T)
+    dA, dB = torch.from_numpy(a_store).cuda(), torch.from_numpy(b_store).cuda()
+    runs = []
+    for _ in range(2):
+        dC = torch.from_numpy(C.copy()).cuda()
+        rep = ctx.dgemm_device(la, lb, m, n, k, -0.5, dA.data_ptr(), a_store.shape[1], dB.data_ptr(),
+                               b_store.shape[1], 1.25, dC.data_ptr(), n, precision=0)
+        ctx.synchronize()
+        assert rep["kernel"] == 1
+        runs.append(dC.cpu().numpy())
+    np.testing.assert_array_equal(runs[1], runs[0])
+    assert_fp64_bound(f"thin {m} {la}{lb}", runs[0], A, B, C, -0.5, 1.25)
