@@ -1204,15 +1204,19 @@ int hess_apply_left(jlc_ctx* ctx, double* h, long long ldh, long long n, long lo
 
 int hess_apply_right(jlc_ctx* ctx, double* mat, long long ldm, long long n, long long k, int pw, const double* V,
                      long long ldv, const double* T, double* W, double* W2, int precision) {
+    // W = X V and W2 = W T are formed transposed, W^T = V^T X^T (pw x n) and
+    // W2^T = T^T W^T, so that their GEMMs have pw rows (thin tiles) rather
+    // than pw columns; W and W2 hold them row-major with leading dimension ldv
     const long long m = n - k - 1;
     double* b = mat + (k + 1) * ldm;
-    GemmDesc w{JLC_COL_MAJOR, JLC_COL_MAJOR, n, pw, m, 1.0, 0.0, b, ldm, V, ldv, W, kHessPanel};
+    GemmDesc w{JLC_ROW_MAJOR, JLC_ROW_MAJOR, pw, n, m, 1.0, 0.0, V, ldv, b, ldm, W, ldv};
     int rc = run_device(ctx, w, precision, 0, nullptr);
     if (rc) return rc;
-    GemmDesc t{JLC_ROW_MAJOR, JLC_ROW_MAJOR, n, pw, pw, 1.0, 0.0, W, kHessPanel, T, kHessPanel, W2, kHessPanel};
+    GemmDesc t{JLC_COL_MAJOR, JLC_ROW_MAJOR, pw, n, pw, 1.0, 0.0, T, kHessPanel, W, ldv, W2, ldv};
     rc = run_device(ctx, t, JLC_PREC_NATIVE, 0, nullptr);
     if (rc) return rc;
-    GemmDesc u{JLC_COL_MAJOR, JLC_COL_MAJOR, m, n, pw, -1.0, 1.0, V, ldv, W2, kHessPanel, b, ldm};
+    // X_sub^T (the column-major block read row-major) -= V W2^T
+    GemmDesc u{JLC_COL_MAJOR, JLC_ROW_MAJOR, m, n, pw, -1.0, 1.0, V, ldv, W2, ldv, b, ldm};
     return run_device(ctx, u, precision, 0, nullptr);
 }
 
