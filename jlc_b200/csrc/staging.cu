@@ -14,6 +14,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstdlib>
 #include <condition_variable>
 #include <cstring>
 #include <functional>
@@ -142,8 +143,14 @@ HostStager* stager_create() {
              cudaEventCreateWithFlags(&s->done[i], cudaEventDisableTiming) == cudaSuccess;
     }
     if (ok) {
+        // workers beside the calling thread: JLCGPU_STAGING_THREADS - 1 when
+        // set, else half the host's hardware threads (at most 7)
         const unsigned hw = std::thread::hardware_concurrency();
-        const int workers = (int)std::min(7u, hw > 2 ? hw / 2 - 1 : 0u);
+        int workers = (int)std::min(7u, hw > 2 ? hw / 2 - 1 : 0u);
+        if (const char* env = getenv("JLCGPU_STAGING_THREADS")) {
+            const int t = atoi(env);
+            if (t >= 1 && t <= 64) workers = t - 1;
+        }
         s->pool = new (std::nothrow) CopyPool(workers);
         ok = s->pool != nullptr;
     }
