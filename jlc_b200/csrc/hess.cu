@@ -112,7 +112,7 @@ __device__ __forceinline__ double cta_sum(const double* part, int P, int i) {
 
 __global__ void __launch_bounds__(PT, 1) hess_panel_kernel(const PanelArgs p) {
     extern __shared__ double dyn[];  // the CTA's rows of V and Y: column i at [i * slab] (when cached)
-    __shared__ double vrow[PW], u[PW], z[PW], s[PW];
+    __shared__ double vrow[PW], vnext[PW], u[PW], z[PW], s[PW];
     __shared__ double sT[PW][PW];    // this CTA's copy of T (computed here with CTA 0's bits)
     __shared__ double red[PWARPS][PW];
     __shared__ double sc[4];
@@ -129,20 +129,23 @@ __global__ void __launch_bounds__(PT, 1) hess_panel_kernel(const PanelArgs p) {
     const long long vs = cached ? p.slab : p.ldv;
     for (int e = tid; e < PW * PW; e += PT) sT[e / PW][e % PW] = 0.0;
     unsigned target = 0;
-    double t_prev = 0.0;  // tau of the previous reflector (the same bits in every CTA)
+    double t_prev = 0.0, v0_prev = 0.0;  // the previous reflector's (the same bits in every CTA)
+    // all rows of a slab of at most 32 sit in warp 0: its sums go straight out
+    const bool one_warp = p.slab <= 32;
+    if (tid < PW) vrow[tid] = 0.0;
     __syncthreads();
     for (int j = 0; j < p.pw; ++j) {
         const int col = p.k + j;
         // w is double-buffered by reflector parity: other CTAs may still read
         // the previous reflector's w in their GEMV while this one is written
         double* wb = p.wbuf + (long long)(j & 1) * p.ldv;
-        // row j-1 of V: entries of earlier reflectors were fenced by the
-        // previous reflector's barriers; v_{j-1}'s own entry there is its unit
-        // diagonal, known from tau without reading what another CTA wrote
-        if (tid < PW)
-            vrow[tid] = (tid < j - 1) ? p.V[(j - 1) + (long long)tid * p.ldv]
-                                      : (tid == j - 1 && t_prev != 0.0 ? 1.0 : 0.0);
-        __syncthreads();
+        // row j of V (for s below, and as the next reflector's vrow), read
+        // now: entries of reflectors before j-1 were fenced by the previous
+        // reflector's barriers; v_{j-1}'s entry there is recomputed from the
+        // previous w exactly as its owner computed it
+        if (tid < j - 1) vnext[tid] = p.V[j + (long long)tid * p.ldv];
+        else if (tid == j - 1)
+            vnext[tid] = t_prev != 0.0 ? p.wbuf[(long long)((j - 1) & 1) * p.ldv + j] / v0_prev : 0.0;
         // 1. w and this CTA's part of V^T w
         double part[PW];
 #pragma unroll
@@ -156,7 +159,19 @@ __global__ void __launch_bounds__(PT, 1) hess_panel_kernel(const PanelArgs p) {
             for (int i = 0; i < PW; ++i)
                 if (i < j) part[i] += Vb[rl + i * vs] * w;
         }
-        block_sum_to(part, j, red, p.part_u + (long long)blockIdx.x * PW);
+        if (one_warp) {
+            if (warp == 0) {
+                double* out = p.part_u + (long long)blockIdx.x * PW;
+#pragma unroll
+                for (int i = 0; i < PW; ++i)
+                    if (i < j) {
+                        const double v = warp_sum(part[i]);
+                        if (lane == 0) out[i] = v;
+                    }
+            }
+        } else {
+            block_sum_to(part, j, red, p.part_u + (long long)blockIdx.x * PW);
+        }
         target += P;
         if (!grid_barrier(p.counter, target, p.status, &s_ok)) return;
         // 2. u summed over the CTAs (warp i: u[i]), z = T^T u, w -= V z; this
@@ -190,15 +205,29 @@ __global__ void __launch_bounds__(PT, 1) hess_panel_kernel(const PanelArgs p) {
                     if (i < j) part[i] += Vb[rl + i * vs] * w;
             }
         }
-        block_sum_to(part, j, red, p.part_s + (long long)blockIdx.x * PW);
-        sig = warp_sum(sig);
-        __syncthreads();  // red is reused
-        if (lane == 0) red[warp][0] = sig;
-        __syncthreads();
-        if (tid == 0) {
-            double tt = 0.0;
-            for (int w = 0; w < PWARPS; ++w) tt += red[w][0];
-            p.part_sig[blockIdx.x] = tt;
+        if (one_warp) {
+            if (warp == 0) {
+                double* out = p.part_s + (long long)blockIdx.x * PW;
+#pragma unroll
+                for (int i = 0; i < PW; ++i)
+                    if (i < j) {
+                        const double v = warp_sum(part[i]);
+                        if (lane == 0) out[i] = v;
+                    }
+                sig = warp_sum(sig);
+                if (lane == 0) p.part_sig[blockIdx.x] = sig;
+            }
+        } else {
+            block_sum_to(part, j, red, p.part_s + (long long)blockIdx.x * PW);
+            sig = warp_sum(sig);
+            __syncthreads();  // red is reused
+            if (lane == 0) red[warp][0] = sig;
+            __syncthreads();
+            if (tid == 0) {
+                double tt = 0.0;
+                for (int w = 0; w < PWARPS; ++w) tt += red[w][0];
+                p.part_sig[blockIdx.x] = tt;
+            }
         }
         target += P;
         if (!grid_barrier(p.counter, target, p.status, &s_ok)) return;
@@ -229,7 +258,8 @@ __global__ void __launch_bounds__(PT, 1) hess_panel_kernel(const PanelArgs p) {
         __syncthreads();
         const double v0 = sc[2], t = sc[3];
         t_prev = t;
-        if (tid < j) s[tid] = t != 0.0 ? p.V[j + (long long)tid * p.ldv] + u[tid] / v0 : 0.0;
+        v0_prev = v0;
+        if (tid < j) s[tid] = t != 0.0 ? vnext[tid] + u[tid] / v0 : 0.0;
         double* vj = p.V + (long long)j * p.ldv;
         for (int r = ra + tid; r < rb; r += PT) {
             double v = 0.0;
@@ -307,7 +337,9 @@ __global__ void __launch_bounds__(PT, 1) hess_panel_kernel(const PanelArgs p) {
                 if (cached) Yb[(r - ra) + j * vs] = 0.0;
             }
         }
-        __syncthreads();  // sT, s, u and the cached rows are read again next reflector
+        // the next reflector's vrow: row j of V, whose entry j is v_j's unit diagonal
+        if (tid < PW) vrow[tid] = tid < j ? vnext[tid] : (tid == j && t != 0.0 ? 1.0 : 0.0);
+        __syncthreads();  // sT, s, u, vrow and the cached rows are read again next reflector
     }
 }
 
