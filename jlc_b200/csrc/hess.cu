@@ -130,8 +130,6 @@ __global__ void __launch_bounds__(PT, 1) hess_panel_kernel(const PanelArgs p) {
     for (int e = tid; e < PW * PW; e += PT) sT[e / PW][e % PW] = 0.0;
     unsigned target = 0;
     double t_prev = 0.0, v0_prev = 0.0;  // the previous reflector's (the same bits in every CTA)
-    // all rows of a slab of at most 32 sit in warp 0: its sums go straight out
-    const bool one_warp = p.slab <= 32;
     if (tid < PW) vrow[tid] = 0.0;
     __syncthreads();
     for (int j = 0; j < p.pw; ++j) {
@@ -143,9 +141,12 @@ __global__ void __launch_bounds__(PT, 1) hess_panel_kernel(const PanelArgs p) {
         // now: entries of reflectors before j-1 were fenced by the previous
         // reflector's barriers; v_{j-1}'s entry there is recomputed from the
         // previous w exactly as its owner computed it
-        if (tid < j - 1) vnext[tid] = p.V[j + (long long)tid * p.ldv];
-        else if (tid == j - 1)
-            vnext[tid] = t_prev != 0.0 ? p.wbuf[(long long)((j - 1) & 1) * p.ldv + j] / v0_prev : 0.0;
+        // (by the last warp, while warp 0 starts on the rows)
+        if (warp == PWARPS - 1) {
+            if (lane < j - 1) vnext[lane] = p.V[j + (long long)lane * p.ldv];
+            else if (lane == j - 1)
+                vnext[lane] = t_prev != 0.0 ? p.wbuf[(long long)((j - 1) & 1) * p.ldv + j] / v0_prev : 0.0;
+        }
         // 1. w and this CTA's part of V^T w
         double part[PW];
 #pragma unroll
@@ -159,19 +160,7 @@ __global__ void __launch_bounds__(PT, 1) hess_panel_kernel(const PanelArgs p) {
             for (int i = 0; i < PW; ++i)
                 if (i < j) part[i] += Vb[rl + i * vs] * w;
         }
-        if (one_warp) {
-            if (warp == 0) {
-                double* out = p.part_u + (long long)blockIdx.x * PW;
-#pragma unroll
-                for (int i = 0; i < PW; ++i)
-                    if (i < j) {
-                        const double v = warp_sum(part[i]);
-                        if (lane == 0) out[i] = v;
-                    }
-            }
-        } else {
-            block_sum_to(part, j, red, p.part_u + (long long)blockIdx.x * PW);
-        }
+        block_sum_to(part, j, red, p.part_u + (long long)blockIdx.x * PW);
         target += P;
         if (!grid_barrier(p.counter, target, p.status, &s_ok)) return;
         // 2. u summed over the CTAs (warp i: u[i]), z = T^T u, w -= V z; this
@@ -205,29 +194,15 @@ __global__ void __launch_bounds__(PT, 1) hess_panel_kernel(const PanelArgs p) {
                     if (i < j) part[i] += Vb[rl + i * vs] * w;
             }
         }
-        if (one_warp) {
-            if (warp == 0) {
-                double* out = p.part_s + (long long)blockIdx.x * PW;
-#pragma unroll
-                for (int i = 0; i < PW; ++i)
-                    if (i < j) {
-                        const double v = warp_sum(part[i]);
-                        if (lane == 0) out[i] = v;
-                    }
-                sig = warp_sum(sig);
-                if (lane == 0) p.part_sig[blockIdx.x] = sig;
-            }
-        } else {
-            block_sum_to(part, j, red, p.part_s + (long long)blockIdx.x * PW);
-            sig = warp_sum(sig);
-            __syncthreads();  // red is reused
-            if (lane == 0) red[warp][0] = sig;
-            __syncthreads();
-            if (tid == 0) {
-                double tt = 0.0;
-                for (int w = 0; w < PWARPS; ++w) tt += red[w][0];
-                p.part_sig[blockIdx.x] = tt;
-            }
+        block_sum_to(part, j, red, p.part_s + (long long)blockIdx.x * PW);
+        sig = warp_sum(sig);
+        __syncthreads();  // red is reused
+        if (lane == 0) red[warp][0] = sig;
+        __syncthreads();
+        if (tid == 0) {
+            double tt = 0.0;
+            for (int w = 0; w < PWARPS; ++w) tt += red[w][0];
+            p.part_sig[blockIdx.x] = tt;
         }
         target += P;
         if (!grid_barrier(p.counter, target, p.status, &s_ok)) return;
