@@ -48,6 +48,8 @@ def parse():
     p.add_argument("--count", type=int, default=20000, help="grouped workload: number of problems")
     p.add_argument("--mnk", default="16384,1,16384", help="shape workload: m,n,k of one device product")
     p.add_argument("--precision", type=int, default=0, help="shape workload: JLC_PREC_* of the product")
+    p.add_argument("--layouts", default="rr",
+                   help="shape workload: storage of A and B, r (row-major) or c (column-major) each")
     p.add_argument("--sizes", default="128,256,512", help="harness workload: square sizes")
     p.add_argument("--iters", type=int, default=25, help="harness workload: timed iterations per backend")
     p.add_argument("--warmups", type=int, default=8, help="harness workload: warm-up iterations per backend")
@@ -1015,15 +1017,17 @@ def run_shape(args):
     ctx.set_stream(stream.cuda_stream)
     g = torch.Generator(device="cuda")
     g.manual_seed(20260604)
+    la, lb = (0 if x == "r" else 1 for x in args.layouts)
     with torch.cuda.stream(stream):
-        A = torch.rand((m, k), dtype=torch.float64, device="cuda", generator=g) * 2 - 1
-        B = torch.rand((k, n), dtype=torch.float64, device="cuda", generator=g) * 2 - 1
+        # op(A) is m x k, op(B) k x n; a column-major operand is stored as its transpose
+        A = torch.rand((m, k) if la == 0 else (k, m), dtype=torch.float64, device="cuda", generator=g) * 2 - 1
+        B = torch.rand((k, n) if lb == 0 else (n, k), dtype=torch.float64, device="cuda", generator=g) * 2 - 1
         C = torch.zeros((m, n), dtype=torch.float64, device="cuda")
     stream.synchronize()
 
     def call(report=False):
-        return ctx.dgemm_device(0, 0, m, n, k, 1.0, A.data_ptr(), k, B.data_ptr(), n, 0.0, C.data_ptr(), n,
-                                precision=args.precision, report=report)
+        return ctx.dgemm_device(la, lb, m, n, k, 1.0, A.data_ptr(), A.shape[1], B.data_ptr(), B.shape[1], 0.0,
+                                C.data_ptr(), n, precision=args.precision, report=report)
 
     rep = call(report=True)
     for _ in range(args.warmup - 1):
@@ -1037,7 +1041,8 @@ def run_shape(args):
     e1.synchronize()
     ms = e0.elapsed_time(e1) / args.steps
     nbytes = 8.0 * (m * k + k * n + m * n)
-    print(json.dumps({"workload": "shape", "m": m, "n": n, "k": k, "precision": args.precision,
+    print(json.dumps({"workload": "shape", "m": m, "n": n, "k": k, "layouts": args.layouts,
+                      "precision": args.precision,
                       "kernel": rep["kernel"], "ms": round(ms, 4),
                       "gflops": round(2.0 * m * n * k / (ms * 1e-3) / 1e9, 1),
                       "gbs_algorithmic": round(nbytes / (ms * 1e-3) / 1e9, 1)}), flush=True)
