@@ -794,22 +794,26 @@ __global__ void __launch_bounds__(SPLIT_THREADS) split_rows_kernel(const double*
 }
 
 // MN-major source: element (i, p) is src[p*ld + i].  Pass 1: max over p.
+constexpr int COLMAX_INFLIGHT = 16;
 __global__ void __launch_bounds__(SPLIT_THREADS) colmax_kernel(const double* src, long long ld, int cols, int K,
                                                                 int kchunk, unsigned long long* maxbits,
                                                                 int* nonfinite) {
     const int i = blockIdx.x * SPLIT_THREADS + threadIdx.x;
     if (i >= cols) return;
     const int p0 = blockIdx.y * kchunk, p1 = min(K, p0 + kchunk);
-    // eight independent loads in flight per thread (the pass is latency-bound)
-    double mx[8] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+    // COLMAX_INFLIGHT independent loads per thread (the pass is latency-bound)
+    constexpr int F = COLMAX_INFLIGHT;
+    double mx[F];
+#pragma unroll
+    for (int u = 0; u < F; ++u) mx[u] = 0.0;
     bool bad = false;
     int pp = p0;
-    for (; pp + 8 <= p1; pp += 8) {
-        double x[8];
+    for (; pp + F <= p1; pp += F) {
+        double x[F];
 #pragma unroll
-        for (int u = 0; u < 8; ++u) x[u] = src[(long long)(pp + u) * ld + i];
+        for (int u = 0; u < F; ++u) x[u] = __ldg(src + (long long)(pp + u) * ld + i);
 #pragma unroll
-        for (int u = 0; u < 8; ++u) {
+        for (int u = 0; u < F; ++u) {
             bad |= !isfinite(x[u]);
             mx[u] = fmax(mx[u], fabs(x[u]));
         }
@@ -820,12 +824,13 @@ __global__ void __launch_bounds__(SPLIT_THREADS) colmax_kernel(const double* src
         mx[0] = fmax(mx[0], fabs(x));
     }
 #pragma unroll
-    for (int u = 1; u < 8; ++u) mx[0] = fmax(mx[0], mx[u]);
+    for (int u = 1; u < F; ++u) mx[0] = fmax(mx[0], mx[u]);
     if (bad) atomicOr(nonfinite, 1);
     atomicMax(&maxbits[i], (unsigned long long)__double_as_longlong(mx[0]));
 }
 
-// Pass 2: 32 (i) x 128 (p) tiles through shared memory, written K-major.
+// Pass 2: 32 (i) x 128 (p) tiles through shared memory, written K-major;
+// a 1-D grid, block b covering p tile b % ptiles of column tile b / ptiles.
 // mag / l1 / exps_in / run_if as for split_rows_kernel (l1 accumulates with
 // atomics over the p tiles and must start at zero).
 constexpr int TR_I = 32, TR_P = 128;
@@ -840,7 +845,11 @@ __global__ void __launch_bounds__(SPLIT_THREADS, 4) split_cols_kernel(const doub
     // element (p, i) sits at column i ^ (p/4): the loads (lanes along i) and
     // the encoder's reads (lanes along p/4) both hit 32 distinct banks pairs
     __shared__ double tile[TR_P][TR_I];
-    const int i0 = blockIdx.x * TR_I, p0 = blockIdx.y * TR_P;
+    // consecutive blocks walk p within one column tile, so the blocks in
+    // flight write long runs of each column's row of every plane
+    const int ptiles = (K + TR_P - 1) / TR_P;
+    const int pt = (int)(blockIdx.x % (unsigned)ptiles);
+    const int i0 = (int)(blockIdx.x / (unsigned)ptiles) * TR_I, p0 = pt * TR_P;
     constexpr int LOADS = TR_I * TR_P / SPLIT_THREADS;
     double ld_v[LOADS];  // every load of the tile is in flight before the first store
 #pragma unroll
@@ -867,7 +876,7 @@ __global__ void __launch_bounds__(SPLIT_THREADS, 4) split_cols_kernel(const doub
         double l1s = 0.0;
         if (gi < cols && gp < K) {
             const int ex = exps_in ? exps_in[gi] : frexp_exp(__longlong_as_double((long long)maxbits[gi]));
-            if (!exps_in && blockIdx.y == 0 && q == 0) exps[gi] = ex;
+            if (!exps_in && pt == 0 && q == 0) exps[gi] = ex;
             const Pow2 sc = pow2_split(shift - ex);
             double v[4];
 #pragma unroll
@@ -944,7 +953,7 @@ int split_operand(const double* src, long long ld, bool kmajor, int rows, int K,
         if (!exps_in) {
             cudaMemsetAsync(maxbits, 0, (size_t)rows * 8, st);
             const int cblocks = (rows + SPLIT_THREADS - 1) / SPLIT_THREADS;
-            int ksplit = (4 * sm_count + cblocks - 1) / cblocks;
+            int ksplit = (8 * sm_count + cblocks - 1) / cblocks;
             if (ksplit < 1) ksplit = 1;
             int kchunk = (K + ksplit - 1) / ksplit;
             if (kchunk < 16) kchunk = 16;
@@ -954,7 +963,9 @@ int split_operand(const double* src, long long ld, bool kmajor, int rows, int K,
             *launches += 1;
         }
         if (l1) cudaMemsetAsync(l1, 0, (size_t)rows * 8, st);
-        const dim3 grid((rows + TR_I - 1) / TR_I, (K + TR_P - 1) / TR_P);
+        const long long nblk = (long long)((rows + TR_I - 1) / TR_I) * ((K + TR_P - 1) / TR_P);
+        if (nblk > 0x7fffffffLL) return JLC_E_ARG;
+        const unsigned grid = (unsigned)nblk;
         if (crt)
             split_cols_kernel<true><<<grid, SPLIT_THREADS, 0, st>>>(src, ld, rows, K, Kp, count, shift, maxbits, out,
                                                                    exps, mag, l1, exps_in, run_if);
