@@ -435,6 +435,9 @@ def run_ours(args):
                      "achieved": round(achieved_tops, 1), "peak": round(int8_sustained, 1),
                      "unit": "TFLOP/s", "frac": round(achieved_tops / int8_sustained, 4),
                      "traffic": traffic,
+                     "traffic_source": (f"dram__bytes_read.sum + dram__bytes_write.sum per launch from the committed "
+                                        f"ncu capture profiles/ozaki_crt_gemm_{size}.txt, not measured in this run"
+                                        if traffic is not None else None),
                      "peak_source": "INT8 dense tcgen05 rate sustained over 3 s of back-to-back probe launches "
                                     "(second half, at the power limit) in this run: the kernel is timed inside "
                                     "a long step under sw_power_cap (MEASURED_PEAKS.json has no INT8 figure)",
