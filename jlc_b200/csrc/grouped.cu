@@ -471,6 +471,78 @@ __device__ __forceinline__ void lds128(uint32_t a, double& x, double& y) {
     asm volatile("ld.shared.v2.f64 {%0, %1}, [%2];" : "=d"(x), "=d"(y) : "r"(a));
 }
 
+// Epilogue of a 32 x 32 tile held by one warp as 2 x 4 blocks of 16 x 8:
+// C = alpha * acc + beta * C over the tile's valid rows and columns, with
+// mtv 16-row and ntv 8-column blocks computed; vc: C's rows allow 16-byte
+// accesses.
+// C values of a 32 x 32 tile held by one warp as 2 x 4 blocks of 16 x 8 (the
+// lane's elements of the mtv 16-row x ntv 8-column blocks computed; zero
+// where beta == 0, whose C is not read); vc: C's rows allow 16-byte accesses.
+__device__ __forceinline__ void wt_load_c(double (&cv)[2][2][4][2], const double* c, long long ldc, int rows, int cols,
+                                          bool vc, double beta, int mtv, int ntv, int lane) {
+    const int g = lane >> 2, t = lane & 3;
+    const bool has_beta = beta != 0.0;
+#pragma unroll
+    for (int mt = 0; mt < 2; ++mt)
+#pragma unroll
+        for (int h = 0; h < 2; ++h)
+#pragma unroll
+            for (int nt = 0; nt < 4; ++nt) {
+                cv[mt][h][nt][0] = cv[mt][h][nt][1] = 0.0;
+                const int row = mt * 16 + g + 8 * h, col = nt * 8 + 2 * t;
+                if (!has_beta || mt >= mtv || nt >= ntv || row >= rows) continue;
+                const double* p = c + row * ldc + col;
+                if (vc && col + 1 < cols) {
+                    asm volatile("ld.global.v2.f64 {%0, %1}, [%2];"
+                                 : "=d"(cv[mt][h][nt][0]), "=d"(cv[mt][h][nt][1])
+                                 : "l"(p));
+                } else {
+                    if (col < cols) cv[mt][h][nt][0] = p[0];
+                    if (col + 1 < cols) cv[mt][h][nt][1] = p[1];
+                }
+            }
+}
+
+// C = alpha * acc + beta * cv over the tile's valid rows and columns.
+__device__ __forceinline__ void wt_store_c(const double (&cv)[2][2][4][2], const double (&acc)[2][4][4], double* c,
+                                           long long ldc, int rows, int cols, bool vc, double alpha, double beta,
+                                           int mtv, int ntv, int lane) {
+    const int g = lane >> 2, t = lane & 3;
+    const bool has_beta = beta != 0.0;
+#pragma unroll
+    for (int mt = 0; mt < 2; ++mt)
+#pragma unroll
+        for (int h = 0; h < 2; ++h)
+#pragma unroll
+            for (int nt = 0; nt < 4; ++nt) {
+                const int row = mt * 16 + g + 8 * h, col = nt * 8 + 2 * t;
+                if (mt >= mtv || nt >= ntv || row >= rows) continue;
+                double* p = c + row * ldc + col;
+                double v[2];
+#pragma unroll
+                for (int e = 0; e < 2; ++e) {
+                    v[e] = alpha * acc[mt][nt][2 * h + e];
+                    if (has_beta) v[e] = fma(beta, cv[mt][h][nt][e], v[e]);
+                }
+                if (vc && col + 1 < cols) {
+                    asm volatile("st.global.v2.f64 [%0], {%1, %2};" ::"l"(p), "d"(v[0]), "d"(v[1]) : "memory");
+                } else {
+                    if (col < cols) p[0] = v[0];
+                    if (col + 1 < cols) p[1] = v[1];
+                }
+            }
+}
+
+// Epilogue of a 32 x 32 warp tile: every C value of the lane is read before
+// any store, so the reads overlap one another (the stores of one row could
+// otherwise order the reads of the next).
+__device__ __forceinline__ void wt_epilogue(double* c, long long ldc, int rows, int cols, bool vc, double alpha,
+                                            double beta, const double (&acc)[2][4][4], int mtv, int ntv, int lane) {
+    double cv[2][2][4][2];
+    wt_load_c(cv, c, ldc, rows, cols, vc, beta, mtv, ntv, lane);
+    wt_store_c(cv, acc, c, ldc, rows, cols, vc, alpha, beta, mtv, ntv, lane);
+}
+
 // Runs one tile item on one warp, streaming its k-blocks through the warp's
 // ring of STAGES slots at shared address `ring`.
 template <bool AK, bool BK, int STAGES>
@@ -561,53 +633,7 @@ __device__ void wt_tile(const TileItem& w, uint32_t ring, int lane) {
     }
     cp_async_wait<0>();
 
-    // epilogue: every C value of the lane is read before any store, so the
-    // reads overlap one another (the stores of one row could otherwise order
-    // the reads of the next); 16-byte accesses where C's rows allow them
-    const bool has_beta = w.beta != 0.0;
-    const bool vc = (w.flags & TF_VC) != 0;
-    double cv[2][2][4][2];
-#pragma unroll
-    for (int mt = 0; mt < 2; ++mt)
-#pragma unroll
-        for (int h = 0; h < 2; ++h)
-#pragma unroll
-            for (int nt = 0; nt < 4; ++nt) {
-                cv[mt][h][nt][0] = cv[mt][h][nt][1] = 0.0;
-                const int row = mt * 16 + g + 8 * h, col = nt * 8 + 2 * t;
-                if (!has_beta || mt >= mtv || nt >= ntv || row >= w.rows) continue;
-                const double* p = w.c + row * w.ldc + col;
-                if (vc && col + 1 < w.cols) {
-                    asm volatile("ld.global.v2.f64 {%0, %1}, [%2];"
-                                 : "=d"(cv[mt][h][nt][0]), "=d"(cv[mt][h][nt][1])
-                                 : "l"(p));
-                } else {
-                    if (col < w.cols) cv[mt][h][nt][0] = p[0];
-                    if (col + 1 < w.cols) cv[mt][h][nt][1] = p[1];
-                }
-            }
-#pragma unroll
-    for (int mt = 0; mt < 2; ++mt)
-#pragma unroll
-        for (int h = 0; h < 2; ++h)
-#pragma unroll
-            for (int nt = 0; nt < 4; ++nt) {
-                const int row = mt * 16 + g + 8 * h, col = nt * 8 + 2 * t;
-                if (mt >= mtv || nt >= ntv || row >= w.rows) continue;
-                double* p = w.c + row * w.ldc + col;
-                double v[2];
-#pragma unroll
-                for (int e = 0; e < 2; ++e) {
-                    v[e] = w.alpha * acc[mt][nt][2 * h + e];
-                    if (has_beta) v[e] = fma(w.beta, cv[mt][h][nt][e], v[e]);
-                }
-                if (vc && col + 1 < w.cols) {
-                    asm volatile("st.global.v2.f64 [%0], {%1, %2};" ::"l"(p), "d"(v[0]), "d"(v[1]) : "memory");
-                } else {
-                    if (col < w.cols) p[0] = v[0];
-                    if (col + 1 < w.cols) p[1] = v[1];
-                }
-            }
+    wt_epilogue(w.c, w.ldc, w.rows, w.cols, (w.flags & TF_VC) != 0, w.alpha, w.beta, acc, mtv, ntv, lane);
 }
 
 // A batch of tiny problems on one warp, elements lane and lane + 32.
@@ -689,6 +715,361 @@ __global__ void __launch_bounds__(WT_THREADS, STAGES == 2 ? 3 : 2)
         w = recs[rb];
         rb ^= 1;
         nx = __shfl_sync(0xffffffffu, nn, 0);
+    }
+}
+
+// ------------------------------------------------------ FP64 CTA tiles, 64 x 64
+// Problems with more than 32 rows and more than 32 columns run as 64 x 64 tile
+// items on CTAs of two copy warps and four DMMA warps, so that the DMMA warps'
+// instruction streams hold fragment loads and MMAs only.
+//   * Copy warp A (warp 4) takes items from its own counter and hands each
+//     item's record to the other warps through a queue of CT_Q records in
+//     shared memory (a full and an empty barrier per record).  The two copy
+//     warps stream the item's k-blocks -- 64 x 16 of op(A) (warp 4) and 16 x
+//     64 of op(B) (warp 5), 16 KB, in the layouts of jlc_dmma.cuh -- into a
+//     ring of CT_STAGES slots with cp.async; each lane's copies complete on
+//     the slot's full barrier (cp.async.mbarrier.arrive.noinc), and the ring
+//     runs on across items.  One copy warp alone was measured busy issuing
+//     copies two thirds of the time while the DMMA warps waited for data.
+//   * DMMA warp q owns the 32 x 32 quadrant (q >> 1, q & 1) of the tile: it
+//     waits for a slot, runs the slot's m16n8k8 MMAs on its quadrant (trimmed
+//     to 16-row x 8-column blocks as the warp tiles are) and passes the slot
+//     back on its empty barrier.  A quadrant without valid rows or columns
+//     issues no MMAs but still passes every slot back.
+//   * Every wait is bounded by the status block's limit; a warp that gives up
+//     records JLC_DEV_TIMEOUT and leaves, and the copy warp first waits for
+//     its own copies in flight.
+constexpr int CT_CONS = 4;                      // DMMA warps
+constexpr int CT_THREADS = (CT_CONS + 2) * 32;  // + the copy warps of A and B
+constexpr int CT_STAGES = 4;
+constexpr int CT_SLOT = (64 + 64) * 128;  // one k-block of A and B: 16 KB
+constexpr int CT_Q = 4;                   // item records in flight
+constexpr int CT_BARS = 2 * CT_STAGES + 2 * CT_Q;
+constexpr int CT_SMEM = CT_STAGES * CT_SLOT + CT_Q * (int)sizeof(TileItem) + CT_BARS * 8 + 128;
+constexpr int KIND_C64 = 2;
+
+__device__ __forceinline__ void cp_async_mbar_arrive(uint64_t* bar) {
+    asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
+// One operand's k-block (64 rows of op(X) x GBK k) copied by the 32 lanes of
+// the copy warp.  The lane mappings are those of WtOperand with twice the row
+// groups (K-major: 16 or 32 copies per lane, MN-major: 4 row chunks of 16);
+// rows at or past nrows are not copied, k at or past nk is zero-filled.
+template <bool KMAJOR>
+struct CtOperand {
+    const double* g;  // the lane's first source element at k = 0
+    long long ld;
+    uint32_t s[4];
+    int nrows, kl, rl;
+    bool vec;
+
+    __device__ __forceinline__ void init(const double* x, long long ld_, int nrows_, int nk, bool vec_, int lane) {
+        ld = ld_;
+        nrows = nrows_;
+        vec = vec_;
+        if (KMAJOR) {
+            if (vec) {
+                rl = lane >> 3;
+                kl = 2 * (lane & 7);
+                const int p = lane & 7;
+#pragma unroll
+                for (int h = 0; h < 2; ++h) s[h] = rl * 128 + h * 512 + ((p ^ (rl + 4 * h)) << 4);
+                s[2] = s[3] = 0;
+            } else {
+                rl = lane >> 4;
+                kl = lane & 15;
+#pragma unroll
+                for (int h = 0; h < 4; ++h)
+                    s[h] = rl * 128 + h * 256 + ((((kl >> 1) ^ (rl + 2 * h))) << 4) + ((kl & 1) << 3);
+            }
+            g = x + rl * ld + kl;
+        } else {
+            if (vec) {
+                const int pl = lane & 7;
+                rl = 2 * pl;
+                kl = lane >> 3;
+#pragma unroll
+                for (int h = 0; h < 2; ++h) s[h] = kl * 128 + h * 512 + ((pl ^ (kl + 4 * h)) << 4);
+                s[2] = s[3] = 0;
+            } else {
+                rl = lane & 15;
+                kl = lane >> 4;
+#pragma unroll
+                for (int h = 0; h < 4; ++h)
+                    s[h] = (kl + 2 * h) * 128 + ((((rl >> 1) ^ (kl + 2 * h))) << 4) + ((rl & 1) << 3);
+            }
+            g = x + (long long)kl * ld + rl;
+        }
+        if (rl >= nrows || kl >= nk) g = x;  // no copy past the last row; zero fill past the last k
+    }
+
+    __device__ __forceinline__ void load(uint32_t sx, int k0, int nk) const {
+        if (KMAJOR) {
+            if (vec) {
+                const int nv = nk - (k0 + kl);
+                const int kbytes = nv >= 2 ? 16 : (nv == 1 ? 8 : 0);
+                const long long step = kbytes ? 4 * ld : 0;
+                const double* src = kbytes ? g + k0 : g;
+#pragma unroll
+                for (int i = 0; i < 16; ++i) {
+                    if (rl + 4 * i < nrows) cp_async16_s(sx + s[i & 1] + (i >> 1) * 1024, src, kbytes);
+                    src += step;
+                }
+            } else {
+                const bool kok = k0 + kl < nk;
+                const long long step = kok ? 2 * ld : 0;
+                const double* src = kok ? g + k0 : g;
+#pragma unroll
+                for (int i = 0; i < 32; ++i) {
+                    if (rl + 2 * i < nrows) cp_async8_s(sx + s[i & 3] + (i >> 2) * 1024, src, kok);
+                    src += step;
+                }
+            }
+        } else {
+            if (vec) {
+#pragma unroll
+                for (int b2 = 0; b2 < 2; ++b2)
+#pragma unroll
+                    for (int b1 = 0; b1 < 2; ++b1) {
+                        const int kk = k0 + kl + 4 * b1 + 8 * b2;
+                        const bool kok = kk < nk;
+                        const double* src = kok ? g + (long long)(k0 + 4 * b1 + 8 * b2) * ld : g;
+#pragma unroll
+                        for (int b0 = 0; b0 < 4; ++b0) {
+                            const int v = nrows - (rl + 16 * b0);
+                            if (v > 0)
+                                cp_async16_s(sx + s[b1] + b0 * 2048 + b2 * 1024, src + 16 * b0,
+                                             kok ? (v >= 2 ? 16 : 8) : 0);
+                        }
+                    }
+            } else {
+#pragma unroll
+                for (int j = 0; j < 8; ++j) {
+                    const bool kok = k0 + kl + 2 * j < nk;
+                    const double* src = kok ? g + (long long)(k0 + 2 * j) * ld : g;
+#pragma unroll
+                    for (int b0 = 0; b0 < 4; ++b0)
+                        if (rl + 16 * b0 < nrows) cp_async8_s(sx + s[j & 3] + b0 * 2048 + (j >> 2) * 1024, src + 16 * b0, kok);
+                }
+            }
+        }
+    }
+};
+
+// Copy warp: streams one item's k-blocks into the ring.  pidx counts the
+// k-blocks this CTA has produced; slot pidx % CT_STAGES is reused once the
+// DMMA warps have passed back its previous fill.  Returns false when a wait
+// gave up.
+// Copy warp of one operand (op(A) rows, or op(B)^T rows when !IS_A):
+// streams one item's k-blocks into the ring.  pidx counts the k-blocks this
+// warp has copied; slot pidx % CT_STAGES is reused once the DMMA warps have
+// passed back its previous fill.  Returns false when a wait gave up.
+template <bool KMAJOR, bool IS_A>
+__device__ bool ct_produce(const TileItem& w, uint32_t ring, uint64_t* full, uint64_t* empty, uint32_t& pidx,
+                           int* status, int lane) {
+    const int kblocks = (w.k + GBK - 1) / GBK;
+    CtOperand<KMAJOR> op;
+    if (IS_A) op.init(w.a, w.lda, w.rows, w.k, (w.flags & TF_VA) != 0, lane);
+    else op.init(w.b, w.ldb, w.cols, w.k, (w.flags & TF_VB) != 0, lane);
+    const uint32_t base = ring + (IS_A ? 0 : 64 * 128);
+    for (int kb = 0; kb < kblocks; ++kb, ++pidx) {
+        const uint32_t st = pidx % CT_STAGES, round = pidx / CT_STAGES;
+        bool ok = round == 0 || mbar_wait_sleep(&empty[st], (round - 1) & 1, status);
+        if (__any_sync(0xffffffffu, !ok)) return false;
+        op.load(base + st * CT_SLOT, kb * GBK, w.k);
+        cp_async_mbar_arrive(&full[st]);
+    }
+    return true;
+}
+
+// The MMAs of one slot on a quadrant: 2 k-steps of 8, mtv 16-row x ntv
+// 8-column blocks (FULL: all 2 x 4, no block tests).
+template <bool AK, bool BK, bool FULL>
+__device__ __forceinline__ void ct_mma_block(double (&acc)[2][4][4], uint32_t sA, uint32_t sB, const uint32_t (&fa)[4],
+                                             const uint32_t (&fb)[4], int mtv, int ntv) {
+#pragma unroll
+    for (int q = 0; q < GBK / 8; ++q) {
+        double bf[4][2];
+#pragma unroll
+        for (int nt = 0; nt < 4; ++nt) {
+            if (FULL || nt < ntv) {
+                if (BK) {
+                    lds128(sB + fb[q] + 1024 * nt, bf[nt][0], bf[nt][1]);
+                } else {
+#pragma unroll
+                    for (int j = 0; j < 2; ++j)
+                        bf[nt][j] = lds64(sB + fb[2 * (nt & 1) + j] + 2048 * (nt >> 1) + 1024 * q);
+                }
+            } else {
+                bf[nt][0] = bf[nt][1] = 0.0;
+            }
+        }
+#pragma unroll
+        for (int mt = 0; mt < 2; ++mt) {
+            if (FULL || mt < mtv) {
+                double af[4];
+                if (AK) {
+                    lds128(sA + fa[q] + 2048 * mt, af[0], af[2]);
+                    lds128(sA + fa[q] + 2048 * mt + 1024, af[1], af[3]);
+                } else {
+#pragma unroll
+                    for (int i = 0; i < 4; ++i)
+                        af[i] = lds64(sA + fa[2 * (i & 1) + (i >> 1)] + 2048 * mt + 1024 * q);
+                }
+#pragma unroll
+                for (int nt = 0; nt < 4; ++nt)
+                    if (FULL || nt < ntv) dmma::mma_f64<8>(acc[mt][nt], af, bf[nt]);
+            }
+        }
+    }
+}
+
+// One slot on a DMMA warp: wait for its copies, run the quadrant's MMAs (qa,
+// qb: the quadrant's A and B tiles in slot 0), pass the slot back.  Returns
+// false when the wait gave up; the warp leaves as one.
+template <bool AK, bool BK>
+__device__ __forceinline__ bool ct_slot(double (&acc)[2][4][4], uint32_t qa, uint32_t qb, const uint32_t (&fa)[4],
+                                        const uint32_t (&fb)[4], int mtv, int ntv, uint64_t* full, uint64_t* empty,
+                                        uint32_t& cidx, int* status, int lane) {
+    const uint32_t st = cidx % CT_STAGES;
+    const bool ok = mbar_wait_sleep(&full[st], (cidx / CT_STAGES) & 1, status);
+    if (__any_sync(0xffffffffu, !ok)) return false;
+    const uint32_t off = st * CT_SLOT;
+    if (mtv == 2 && ntv == 4) ct_mma_block<AK, BK, true>(acc, qa + off, qb + off, fa, fb, 2, 4);
+    else if (mtv > 0 && ntv > 0) ct_mma_block<AK, BK, false>(acc, qa + off, qb + off, fa, fb, mtv, ntv);
+    __syncwarp();  // every lane's fragment loads of the slot are done
+    if (lane == 0) mbar_arrive(&empty[st]);
+    ++cidx;
+    return true;
+}
+
+// DMMA warp: one item's k-blocks on quadrant (wm, wn), then its epilogue.
+// cidx counts the k-blocks this warp has consumed.  Returns false when a
+// wait gave up.
+// The record stays in the queue (shared memory) until the item is done: the
+// warp keeps only the few fields its k-loop needs in registers.
+template <bool AK, bool BK>
+__device__ bool ct_consume(const TileItem& w, int wm, int wn, uint32_t ring, uint64_t* full, uint64_t* empty,
+                           uint32_t& cidx, int* status, int lane) {
+    const int g = lane >> 2, t = lane & 3;
+    const int kblocks = (w.k + GBK - 1) / GBK;
+    const int qrows = min(32, w.rows - 32 * wm), qcols = min(32, w.cols - 32 * wn);  // the quadrant's
+    const int mtv = qrows > 16 ? 2 : (qrows > 0 ? 1 : 0);
+    const int ntv = qcols > 0 ? (qcols + 7) >> 3 : 0;
+    const bool active = mtv > 0 && ntv > 0;
+    if (active && w.beta != 0.0 && lane < qrows) {
+        // C rows of the quadrant into L2 ahead of the epilogue
+        const double* r = w.c + (long long)(32 * wm + lane) * w.ldc + 32 * wn;
+        asm volatile("prefetch.global.L2 [%0];" ::"l"(r));
+        if (qcols > 16) asm volatile("prefetch.global.L2 [%0];" ::"l"(r + 16));
+    }
+    uint32_t fa[4], fb[4];
+    frag_bases<AK>(fa, g, t, true);
+    frag_bases<BK>(fb, g, t, false);
+    double acc[2][4][4];
+#pragma unroll
+    for (int i = 0; i < 2; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+#pragma unroll
+            for (int e = 0; e < 4; ++e) acc[i][j][e] = 0.0;
+    double* const qc = w.c + (long long)(32 * wm) * w.ldc + 32 * wn;
+    const uint32_t qa = ring + 4096 * wm, qb = ring + 64 * 128 + 4096 * wn;  // the quadrant in slot 0
+    for (int kb = 0; kb < kblocks; ++kb)
+        if (!ct_slot<AK, BK>(acc, qa, qb, fa, fb, mtv, ntv, full, empty, cidx, status, lane)) return false;
+    if (active)
+        wt_epilogue(qc, w.ldc, qrows, qcols, (w.flags & TF_VC) != 0, w.alpha, w.beta, acc, mtv, ntv, lane);
+    return true;
+}
+
+__global__ void __maxnreg__(168)
+    grouped_cta_kernel(const TileItem* items, int nitems, int* counter, int* status) {
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    char* base = reinterpret_cast<char*>((reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~uintptr_t(127));
+    const uint32_t ring = smem_u32(base);
+    TileItem* recs = reinterpret_cast<TileItem*>(base + CT_STAGES * CT_SLOT);
+    uint64_t* bars = reinterpret_cast<uint64_t*>(base + CT_STAGES * CT_SLOT + CT_Q * sizeof(TileItem));
+    uint64_t* full = bars;
+    uint64_t* empty = bars + CT_STAGES;
+    uint64_t* qfull = bars + 2 * CT_STAGES;
+    uint64_t* qempty = bars + 2 * CT_STAGES + CT_Q;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < CT_STAGES; ++s) {
+            mbar_init(&full[s], 64);       // one cp.async arrival per lane of each copy warp
+            mbar_init(&empty[s], CT_CONS);  // one arrival per DMMA warp
+        }
+        for (int q = 0; q < CT_Q; ++q) {
+            mbar_init(&qfull[q], 1);
+            mbar_init(&qempty[q], CT_CONS + 1);  // the DMMA warps and copy warp B
+        }
+    }
+    __syncthreads();
+    if (warp == CT_CONS) {
+        // copy warp A: takes the items
+        uint32_t pidx = 0;
+        for (uint32_t n = 0;; ++n) {
+            const uint32_t q = n % CT_Q;
+            int it = 0;
+            if (lane == 0) it = atomicAdd(counter, 1);
+            it = __shfl_sync(0xffffffffu, it, 0);
+            bool ok = n < CT_Q || mbar_wait_sleep(&qempty[q], ((n / CT_Q) - 1) & 1, status);
+            ok = !__any_sync(0xffffffffu, !ok);
+            const bool last = !ok || it >= nitems;
+            if (lane == 0) {
+                if (last) recs[q].k = -1;  // no more items: the DMMA warps leave
+                else recs[q] = items[it];
+                mbar_arrive(&qfull[q]);
+            }
+            if (last) break;
+            __syncwarp();
+            const TileItem w = recs[q];
+            const bool done = (w.flags & TF_AK) ? ct_produce<true, true>(w, ring, full, empty, pidx, status, lane)
+                                                : ct_produce<false, true>(w, ring, full, empty, pidx, status, lane);
+            if (!done) break;
+        }
+        cp_async_wait_all();  // no copy of this CTA outlives it
+        return;
+    }
+    if (warp == CT_CONS + 1) {
+        // copy warp B: reads each record as the DMMA warps do
+        uint32_t pidx = 0;
+        for (uint32_t n = 0;; ++n) {
+            const uint32_t q = n % CT_Q;
+            const bool ok = mbar_wait_sleep(&qfull[q], (n / CT_Q) & 1, status);
+            if (__any_sync(0xffffffffu, !ok)) break;
+            const TileItem w = recs[q];
+            if (w.k < 0) break;
+            const bool done = (w.flags & TF_BK) ? ct_produce<true, false>(w, ring, full, empty, pidx, status, lane)
+                                                : ct_produce<false, false>(w, ring, full, empty, pidx, status, lane);
+            if (!done) break;
+            __syncwarp();  // every lane has read the record before its slot is passed back
+            if (lane == 0) mbar_arrive(&qempty[q]);
+        }
+        cp_async_wait_all();
+        return;
+    }
+    // DMMA warps
+    const int wm = warp >> 1, wn = warp & 1;
+    uint32_t cidx = 0;
+    for (uint32_t n = 0;; ++n) {
+        const uint32_t q = n % CT_Q;
+        const bool ok = mbar_wait_sleep(&qfull[q], (n / CT_Q) & 1, status);
+        if (__any_sync(0xffffffffu, !ok)) break;
+        const TileItem& w = recs[q];
+        if (w.k < 0) break;
+        bool done;
+        switch (((w.flags & TF_AK) ? 2 : 0) + ((w.flags & TF_BK) ? 1 : 0)) {
+            case 0: done = ct_consume<false, false>(w, wm, wn, ring, full, empty, cidx, status, lane); break;
+            case 1: done = ct_consume<false, true>(w, wm, wn, ring, full, empty, cidx, status, lane); break;
+            case 2: done = ct_consume<true, false>(w, wm, wn, ring, full, empty, cidx, status, lane); break;
+            default: done = ct_consume<true, true>(w, wm, wn, ring, full, empty, cidx, status, lane); break;
+        }
+        if (!done) break;
+        __syncwarp();  // every lane is done with the record before its slot is passed back
+        if (lane == 0) mbar_arrive(&qempty[q]);
     }
 }
 
@@ -978,17 +1359,26 @@ __global__ void __launch_bounds__(THREADS, 3) grouped_oz_kernel(const jlc_proble
 bool is_tiny(const jlc_problem& p) { return p.m * p.n <= 64 && p.k <= 64; }
 
 struct WorkList {
-    std::vector<Item> items;
+    std::vector<Item> items;   // warp items: 32 x 32 tiles and tiny batches
+    std::vector<Item> citems;  // CTA items: 64 x 64 tiles
     std::vector<int> tiny;
     double flops = 0.0;
 };
+
+// 64 x 64 CTA tiles for problems with more than 32 rows and 32 columns;
+// JLCGPU_GROUPED_CTA=0 runs every problem on the warp tiles instead.
+bool cta_tiles_enabled() {
+    const char* e = getenv("JLCGPU_GROUPED_CTA");
+    return !(e && e[0] == '0');
+}
 
 void build_work(const std::vector<jlc_problem>& probs, WorkList& wl) {
     struct Costed {
         Item it;
         double cost;
     };
-    std::vector<Costed> v;
+    std::vector<Costed> v, vc;
+    const bool cta = cta_tiles_enabled();
     int batch_start = -1, batch_count = 0, batch_elems = 0;
     double batch_cost = 0.0;
     auto flush_batch = [&] {
@@ -1014,6 +1404,22 @@ void build_work(const std::vector<jlc_problem>& probs, WorkList& wl) {
         }
         // cost: the 16 x 8 blocks the tile runs, times its k-blocks (+1 for
         // the fixed cost of an item)
+        auto blocks_of = [](long long rows, long long cols) {
+            return rows <= 0 || cols <= 0 ? 0.0 : (rows > 16 ? 2.0 : 1.0) * (double)((cols + 7) / 8);
+        };
+        if (cta && p.m > 32 && p.n > 32) {
+            const int tmc = (int)((p.m + 63) / 64), tnc = (int)((p.n + 63) / 64);
+            for (int a = 0; a < tmc; ++a)
+                for (int b = 0; b < tnc; ++b) {
+                    const long long rows = std::min<long long>(64, p.m - 64LL * a);
+                    const long long cols = std::min<long long>(64, p.n - 64LL * b);
+                    const double blocks = blocks_of(std::min(32LL, rows), std::min(32LL, cols)) +
+                                          blocks_of(std::min(32LL, rows), cols - 32) +
+                                          blocks_of(rows - 32, std::min(32LL, cols)) + blocks_of(rows - 32, cols - 32);
+                    vc.push_back({Item{i, a, b, KIND_C64}, blocks * (std::ceil(kk / GBK) + 1.0)});
+                }
+            continue;
+        }
         const int tmn = (int)((p.m + 31) / 32), tnn = (int)((p.n + 31) / 32);
         for (int a = 0; a < tmn; ++a)
             for (int b = 0; b < tnn; ++b) {
@@ -1024,9 +1430,13 @@ void build_work(const std::vector<jlc_problem>& probs, WorkList& wl) {
             }
     }
     flush_batch();
-    std::stable_sort(v.begin(), v.end(), [](const Costed& x, const Costed& y) { return x.cost > y.cost; });
+    auto longest_first = [](const Costed& x, const Costed& y) { return x.cost > y.cost; };
+    std::stable_sort(v.begin(), v.end(), longest_first);
+    std::stable_sort(vc.begin(), vc.end(), longest_first);
     wl.items.reserve(v.size());
     for (auto& c : v) wl.items.push_back(c.it);
+    wl.citems.reserve(vc.size());
+    for (auto& c : vc) wl.citems.push_back(c.it);
 }
 
 std::string tune_cache_path() {
@@ -1097,11 +1507,18 @@ struct jlc_grouped_plan {
     int* d_nonfinite = nullptr;
     jlc_problem* d_probs = nullptr;
     jlc::grp::Item* d_items = nullptr;        // residue tiles
-    jlc::grp::TileItem* d_titems = nullptr;   // FP64 tiles
+    jlc::grp::TileItem* d_titems = nullptr;   // FP64 tiles: warp items
+    jlc::grp::TileItem* d_citems = nullptr;   // FP64 tiles: 64 x 64 CTA items
     int* d_tiny = nullptr;
     int* d_counter = nullptr;
     int nitems = 0;
     int grid = 0;
+    int nitems_c = 0;  // CTA items (their counter is d_counter[1])
+    int grid_c = 0;
+    // with both kinds of items the warp tiles run on a second stream beside
+    // the CTA tiles, so that they fill the SMs the CTA tiles' tail frees
+    cudaStream_t side = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     double flops = 0.0;
     int64_t n_int8 = 0, n_fp64 = 0;  // problems on residue tiles / on FP64 tiles
     int tile = 32;    // FP64 tile edge (residue tiles: OZ_T)
@@ -1146,9 +1563,15 @@ int check_problem(jlc_ctx* ctx, const jlc_problem& p, int64_t i) {
 void free_plan_buffers(jlc_grouped_plan* pl) {
     if (pl->exec) cudaGraphExecDestroy(pl->exec);
     if (pl->graph) cudaGraphDestroy(pl->graph);
+    if (pl->ev_fork) cudaEventDestroy(pl->ev_fork);
+    if (pl->ev_join) cudaEventDestroy(pl->ev_join);
+    if (pl->side) cudaStreamDestroy(pl->side);
+    pl->ev_fork = pl->ev_join = nullptr;
+    pl->side = nullptr;
     if (pl->d_probs) cudaFree(pl->d_probs);
     if (pl->d_items) cudaFree(pl->d_items);
     if (pl->d_titems) cudaFree(pl->d_titems);
+    if (pl->d_citems) cudaFree(pl->d_citems);
     if (pl->d_tiny) cudaFree(pl->d_tiny);
     if (pl->d_counter) cudaFree(pl->d_counter);
     if (pl->d_oz) cudaFree(pl->d_oz);
@@ -1168,6 +1591,7 @@ void free_plan_buffers(jlc_grouped_plan* pl) {
     pl->d_probs = nullptr;
     pl->d_items = nullptr;
     pl->d_titems = nullptr;
+    pl->d_citems = nullptr;
     pl->d_tiny = nullptr;
     pl->d_counter = nullptr;
 }
@@ -1180,20 +1604,17 @@ int upload(jlc_grouped_plan* pl, const std::vector<jlc_problem>& probs, const Wo
         if (e != cudaSuccess) return e;
         return bytes ? cudaMemcpyAsync(*dst, src, bytes, cudaMemcpyHostToDevice, st) : cudaSuccess;
     };
-    // the kernel's item records: operand origins of each tile resolved here
-    std::vector<TileItem> titems(wl.items.size());
-    for (size_t i = 0; i < wl.items.size(); ++i) {
-        const Item& it = wl.items[i];
-        TileItem& t = titems[i];
+    // the kernels' item records: operand origins of each tile resolved here
+    auto to_record = [&](const Item& it, TileItem& t) {
         memset(&t, 0, sizeof(t));
         if (it.kind == KIND_TINY) {
             t.rows = it.prob;
             t.cols = it.tm;
             t.flags = KIND_TINY;
-            continue;
+            return;
         }
         const jlc_problem& p = probs[it.prob];
-        const long long ts = 32;
+        const long long ts = it.kind == KIND_C64 ? 64 : 32;
         const long long m0 = it.tm * ts, n0 = it.tn * ts;
         const bool ak = p.layout_a == JLC_ROW_MAJOR, bk = p.layout_b == JLC_COL_MAJOR;
         t.a = p.a ? (ak ? p.a + m0 * p.lda : p.a + m0) : nullptr;
@@ -1213,11 +1634,15 @@ int upload(jlc_grouped_plan* pl, const std::vector<jlc_problem>& probs, const Wo
         const bool vc = ((reinterpret_cast<uintptr_t>(t.c) & 15) == 0) && ((p.ldc & 1) == 0);
         t.flags = it.kind | (ak ? TF_AK : 0) | (bk ? TF_BK : 0) | (va ? TF_VA : 0) | (vb ? TF_VB : 0) |
                   (vc ? TF_VC : 0);
-    }
+    };
+    std::vector<TileItem> titems(wl.items.size()), citems(wl.citems.size());
+    for (size_t i = 0; i < wl.items.size(); ++i) to_record(wl.items[i], titems[i]);
+    for (size_t i = 0; i < wl.citems.size(); ++i) to_record(wl.citems[i], citems[i]);
     cudaError_t e = alloc_copy((void**)&pl->d_probs, probs.data(), probs.size() * sizeof(jlc_problem));
     if (e == cudaSuccess) e = alloc_copy((void**)&pl->d_titems, titems.data(), titems.size() * sizeof(TileItem));
+    if (e == cudaSuccess) e = alloc_copy((void**)&pl->d_citems, citems.data(), citems.size() * sizeof(TileItem));
     if (e == cudaSuccess) e = alloc_copy((void**)&pl->d_tiny, wl.tiny.data(), wl.tiny.size() * sizeof(int));
-    if (e == cudaSuccess) e = cudaMalloc((void**)&pl->d_counter, sizeof(int));
+    if (e == cudaSuccess) e = cudaMalloc((void**)&pl->d_counter, 2 * sizeof(int));
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);  // host vectors are pageable and short-lived
     if (e != cudaSuccess) {
         cudaGetLastError();
@@ -1225,7 +1650,24 @@ int upload(jlc_grouped_plan* pl, const std::vector<jlc_problem>& probs, const Wo
                     cudaGetErrorString(e));
     }
     pl->nitems = (int)wl.items.size();
+    pl->nitems_c = (int)wl.citems.size();
+    if (pl->nitems > 0 && pl->nitems_c > 0) {
+        e = cudaStreamCreateWithFlags(&pl->side, cudaStreamNonBlocking);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&pl->ev_fork, cudaEventDisableTiming);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&pl->ev_join, cudaEventDisableTiming);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            return gerr(ctx, JLC_E_CUDA, "grouped plan streams: %s", cudaGetErrorString(e));
+        }
+    }
     int per_sm = 0;
+    if (pl->nitems_c > 0) {
+        cudaFuncSetAttribute(grouped_cta_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, CT_SMEM);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, grouped_cta_kernel, CT_THREADS, CT_SMEM);
+        if (per_sm < 1) per_sm = 1;
+        pl->grid_c = std::max(1, std::min(pl->nitems_c, ctx->sm_count * per_sm));
+    }
+    per_sm = 0;
     if (pl->stages == 3) {
         cudaFuncSetAttribute(grouped_kernel<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, wt_smem(3));
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, grouped_kernel<3>, WT_THREADS, wt_smem(3));
@@ -1239,7 +1681,7 @@ int upload(jlc_grouped_plan* pl, const std::vector<jlc_problem>& probs, const Wo
 }
 
 int launch_plan(jlc_grouped_plan* pl, cudaStream_t st) {
-    if (pl->nitems == 0) return JLC_OK;
+    if (pl->nitems == 0 && pl->nitems_c == 0) return JLC_OK;
     if (pl->oz) {
         if (cudaMemsetAsync(pl->d_counter, 0, sizeof(int), st) != cudaSuccess) return JLC_E_CUDA;
         if (cudaMemsetAsync(pl->d_nonfinite, 0, (size_t)pl->count * sizeof(int), st) != cudaSuccess)
@@ -1255,13 +1697,30 @@ int launch_plan(jlc_grouped_plan* pl, cudaStream_t st) {
                                                                     pl->d_nonfinite, pl->d_counter);
         return cudaGetLastError() == cudaSuccess ? JLC_OK : JLC_E_LAUNCH;
     }
-    if (cudaMemsetAsync(pl->d_counter, 0, sizeof(int), st) != cudaSuccess) return JLC_E_CUDA;
-    if (pl->stages == 3)
-        grouped_kernel<3><<<pl->grid, WT_THREADS, wt_smem(3), st>>>(pl->d_probs, pl->d_titems, pl->nitems,
-                                                                   pl->d_tiny, pl->d_counter);
-    else
-        grouped_kernel<2><<<pl->grid, WT_THREADS, wt_smem(2), st>>>(pl->d_probs, pl->d_titems, pl->nitems,
-                                                                   pl->d_tiny, pl->d_counter);
+    if (cudaMemsetAsync(pl->d_counter, 0, 2 * sizeof(int), st) != cudaSuccess) return JLC_E_CUDA;
+    // CTA tiles first on the caller's stream; the warp tiles on the side
+    // stream, forked after the counters are cleared and joined at the end
+    cudaStream_t wst = st;
+    if (pl->side) {
+        if (cudaEventRecord(pl->ev_fork, st) != cudaSuccess || cudaStreamWaitEvent(pl->side, pl->ev_fork, 0) != cudaSuccess)
+            return JLC_E_CUDA;
+        wst = pl->side;
+    }
+    if (pl->nitems_c > 0)
+        grouped_cta_kernel<<<pl->grid_c, CT_THREADS, CT_SMEM, st>>>(pl->d_citems, pl->nitems_c, pl->d_counter + 1,
+                                                                    pl->ctx->d_status);
+    if (pl->nitems > 0) {
+        if (pl->stages == 3)
+            grouped_kernel<3><<<pl->grid, WT_THREADS, wt_smem(3), wst>>>(pl->d_probs, pl->d_titems, pl->nitems,
+                                                                        pl->d_tiny, pl->d_counter);
+        else
+            grouped_kernel<2><<<pl->grid, WT_THREADS, wt_smem(2), wst>>>(pl->d_probs, pl->d_titems, pl->nitems,
+                                                                        pl->d_tiny, pl->d_counter);
+    }
+    if (pl->side) {
+        if (cudaEventRecord(pl->ev_join, pl->side) != cudaSuccess || cudaStreamWaitEvent(st, pl->ev_join, 0) != cudaSuccess)
+            return JLC_E_CUDA;
+    }
     return cudaGetLastError() == cudaSuccess ? JLC_OK : JLC_E_LAUNCH;
 }
 
@@ -1525,8 +1984,8 @@ int jlc_grouped_plan_run(jlc_grouped_plan* plan) {
     if (!plan || !plan->ctx) return JLC_E_ARG;
     jlc_ctx* ctx = plan->ctx;
     cudaSetDevice(ctx->device);
-    if (plan->nitems == 0) return JLC_OK;
-    ctx->launches += 1;
+    if (plan->nitems == 0 && plan->nitems_c == 0) return JLC_OK;
+    ctx->launches += (plan->nitems > 0) + (plan->nitems_c > 0);
     if (plan->use_graph) {
         cudaError_t e = cudaGraphLaunch(plan->exec, ctx->stream);
         return e == cudaSuccess ? JLC_OK : gerr(ctx, JLC_E_LAUNCH, "graph launch: %s", cudaGetErrorString(e));
@@ -1538,10 +1997,10 @@ int jlc_grouped_plan_run(jlc_grouped_plan* plan) {
 int jlc_grouped_plan_info(const jlc_grouped_plan* plan, int64_t* work_items, double* flops, int* tile_small,
                           int* tile_large) {
     if (!plan) return JLC_E_ARG;
-    if (work_items) *work_items = plan->nitems;
+    if (work_items) *work_items = (int64_t)plan->nitems + plan->nitems_c;
     if (flops) *flops = plan->flops;
     if (tile_small) *tile_small = plan->tile;
-    if (tile_large) *tile_large = plan->tile;
+    if (tile_large) *tile_large = plan->nitems_c > 0 ? 64 : plan->tile;
     return JLC_OK;
 }
 

@@ -94,6 +94,41 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int* s
     }
 }
 
+// try_wait with a suspend-time hint: a thread whose phase has not completed
+// may sleep up to hint_ns (it resumes when the phase completes) instead of
+// returning at once, so a waiting warp does not spend the SM's issue slots.
+__device__ __forceinline__ bool mbar_try_wait_hint(uint32_t bar, uint32_t parity, uint32_t hint_ns) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(bar), "r"(parity), "r"(hint_ns)
+        : "memory");
+    return ok != 0;
+}
+
+// Bounded wait like mbar_wait for roles that are often ahead of their
+// partners (a copy warp waiting for a free slot, MMA warps waiting for
+// data): every try sleeps up to 20 us, and the status word and the clock are
+// checked after each try that failed.
+__device__ __forceinline__ bool mbar_wait_sleep(uint64_t* bar, uint32_t parity, int* status) {
+    constexpr uint32_t kHintNs = 20000;
+    const uint32_t b = smem_u32(bar);
+    if (mbar_try_wait_hint(b, parity, kHintNs)) return true;
+    const uint64_t t0 = globaltimer_ns();
+    const uint64_t limit = wait_limit_ns(status);
+    for (;;) {
+        if (mbar_try_wait_hint(b, parity, kHintNs)) return true;
+        if (*(volatile int*)status != 0) return false;
+        if (globaltimer_ns() - t0 > limit) {
+            atomicOr(status, JLC_DEV_TIMEOUT);
+            return false;
+        }
+    }
+}
+
 __device__ __forceinline__ unsigned ld_acquire_u32(const unsigned* p) {
     unsigned v;
     asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");

@@ -173,7 +173,8 @@ def test_grouped_autotune_writes_cache(ctx, oracle, tmp_path):
         probs, host, arena = make_batch(oracle, shapes, 13)
         plan = ctx.grouped_plan(probs, autotune=True)
         info = plan.info()
-        assert info["tile_small"] == 32 and info["tile_large"] == 32
+        # problems above 32 rows and columns run as 64 x 64 CTA tiles
+        assert info["tile_small"] == 32 and info["tile_large"] == 64
         text = cache.read_text()
         assert "grouped-fp64|stages|k" in text
         assert text.split()[-1] in ("2", "3")
@@ -183,6 +184,57 @@ def test_grouped_autotune_writes_cache(ctx, oracle, tmp_path):
         plan.close()
     finally:
         os.environ.pop("JLCGPU_TUNE_CACHE", None)
+
+
+def test_grouped_cta_tiles_many_items(ctx, oracle):
+    """Problems above 32 rows and 32 columns run as 64 x 64 items on CTAs of
+    a copy warp and four DMMA warps.  Thousands of items (more than the
+    persistent grid holds, so every CTA's record queue and slot ring wrap many
+    times), all four operand layouts, odd and even leading dimensions (8- and
+    16-byte copies), ragged edges in every quadrant, alpha == 0, k == 0 and
+    k == 1, and a few long products; the same batch on the warp tiles alone
+    (JLCGPU_GROUPED_CTA=0) as well.  Both inside the FP64 bound."""
+    import torch
+    rng = np.random.default_rng(41)
+    shapes = [(int(rng.integers(33, 200)), int(rng.integers(33, 200)), int(rng.integers(1, 300)))
+              for _ in range(700)]
+    shapes += [(33, 33, 1), (64, 64, 16), (65, 97, 0), (200, 40, 2500), (40, 200, 1777), (129, 129, 129)]
+    layouts = [(i % 2, (i // 2) % 2) for i in range(len(shapes))]
+    alphas = [float(x) for x in rng.uniform(-2, 2, size=len(shapes))]
+    alphas[5] = 0.0
+    betas = [float(x) for x in rng.uniform(-2, 2, size=len(shapes))]
+    betas[7] = 0.0
+    probs, host, arena = make_batch(oracle, shapes, 37, layouts=layouts, alphas=alphas, betas=betas)
+    saved = arena.clone()
+    plan = ctx.grouped_plan(probs, graph=True)
+    info = plan.info()
+    assert info["tile_large"] == 64 and info["work_items"] > 2000
+    plan.run()
+    ctx.synchronize()
+    check_batch(oracle, probs, host, arena, "CTA tiles")
+    # graph replay (the counters are reset inside the graph) on the first
+    # run's results as C
+    flat = arena.cpu().numpy()
+    host2 = []
+    for p, (m, n, k, la, lb, alpha, beta, A, B, C) in zip(probs, host):
+        o = (p["c"] - arena.data_ptr()) // 8
+        host2.append((m, n, k, la, lb, alpha, beta, A, B, flat[o:o + m * n].reshape(m, n).copy()))
+    plan.run()
+    ctx.synchronize()
+    check_batch(oracle, probs, host2, arena, "CTA tiles, graph replay")
+    plan.close()
+    arena.copy_(saved)
+    torch.cuda.synchronize()
+    os.environ["JLCGPU_GROUPED_CTA"] = "0"
+    try:
+        plan = ctx.grouped_plan(probs)
+    finally:
+        os.environ.pop("JLCGPU_GROUPED_CTA", None)
+    assert plan.info()["tile_large"] == 32
+    plan.run()
+    ctx.synchronize()
+    check_batch(oracle, probs, host, arena, "warp tiles")
+    plan.close()
 
 
 def test_grouped_rejects_bad_problem(ctx):
