@@ -328,6 +328,7 @@ JLC_API int jlc_grouped_plan_routes(const jlc_grouped_plan* plan, int64_t* int8_
 /* slots per warp in the FP64 tiles' copy ring (2 or 3; 0 for a residue
  * plan), as the autotuner or the tuning cache chose it (new) */
 JLC_API int jlc_grouped_plan_stages(const jlc_grouped_plan* plan, int* stages);
+/* releases a plan; every plan must be destroyed before its context */
 JLC_API void jlc_grouped_plan_destroy(jlc_grouped_plan* plan);
 /* one-shot: plan, run, synchronise, destroy */
 JLC_API int jlc_dgemm_grouped_device(jlc_ctx* ctx, const jlc_problem* probs, int64_t count, int precision,

@@ -18,6 +18,7 @@ non-empty message, as the reference throws IllegalArgumentException.
 from __future__ import annotations
 
 import ctypes
+import weakref
 import threading
 
 import numpy as np
@@ -48,9 +49,14 @@ class Context:
             raise JlcError(rc, f"jlc_init(device={device}) failed")
         self.h = h
         self.device = device
+        # grouped plans made on this context: a plan refers to its context,
+        # so closing the context closes them first
+        self._plans = weakref.WeakSet()
 
     def close(self):
         if getattr(self, "h", None):
+            for plan in list(getattr(self, "_plans", ())):
+                plan.close()
             self.lib.jlc_destroy(self.h)
             self.h = None
 
@@ -307,6 +313,7 @@ class GroupedPlan:
         ctx.check(ctx.lib.jlc_grouped_plan_create(ctx.h, self.problems, len(self.problems), int(precision), flags,
                                                   ctypes.byref(h)))
         self.h = h
+        ctx._plans.add(self)
 
     def run(self):
         self.ctx.check(self.ctx.lib.jlc_grouped_plan_run(self.h))
@@ -324,9 +331,10 @@ class GroupedPlan:
                 "int8_problems": n8.value, "fp64_problems": n64.value, "stages": st.value}
 
     def close(self):
-        if getattr(self, "h", None):
+        # a plan outlived by its context was closed with it
+        if getattr(self, "h", None) and getattr(self.ctx, "h", None):
             self.ctx.lib.jlc_grouped_plan_destroy(self.h)
-            self.h = None
+        self.h = None
 
     def __del__(self):
         try:

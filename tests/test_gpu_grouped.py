@@ -187,8 +187,9 @@ def test_grouped_autotune_writes_cache(ctx, oracle, tmp_path):
 
 
 def test_grouped_cta_tiles_many_items(ctx, oracle):
-    """Problems above 32 rows and 32 columns run as 64 x 64 items on CTAs of
-    a copy warp and four DMMA warps.  Thousands of items (more than the
+    """Problems above 32 rows and 32 columns run as 64 x 64 items of four
+    32 x 32 quadrants on CTAs of two copy warps and four DMMA warps; the rest
+    (at most 32 rows or columns) on warp tiles beside them.  Thousands of items (more than the
     persistent grid holds, so every CTA's record queue and slot ring wrap many
     times), all four operand layouts, odd and even leading dimensions (8- and
     16-byte copies), ragged edges in every quadrant, alpha == 0, k == 0 and
@@ -199,6 +200,10 @@ def test_grouped_cta_tiles_many_items(ctx, oracle):
     shapes = [(int(rng.integers(33, 200)), int(rng.integers(33, 200)), int(rng.integers(1, 300)))
               for _ in range(700)]
     shapes += [(33, 33, 1), (64, 64, 16), (65, 97, 0), (200, 40, 2500), (40, 200, 1777), (129, 129, 129)]
+    # at most 32 rows or at most 32 columns (warp tiles), 1 included
+    shapes += [(int(rng.integers(1, 33)), int(rng.integers(33, 400)), int(rng.integers(1, 300))) for _ in range(150)]
+    shapes += [(int(rng.integers(33, 400)), int(rng.integers(1, 33)), int(rng.integers(1, 300))) for _ in range(150)]
+    shapes += [(1, 513, 40), (513, 1, 40), (32, 129, 1000), (129, 32, 1000)]
     layouts = [(i % 2, (i // 2) % 2) for i in range(len(shapes))]
     alphas = [float(x) for x in rng.uniform(-2, 2, size=len(shapes))]
     alphas[5] = 0.0
