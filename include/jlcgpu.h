@@ -193,8 +193,10 @@ JLC_API int jlc_set_wait_limit(jlc_ctx* ctx, double seconds);
  *   JLC_FAULT_ALLOC   a device buffer request reports JLC_E_OOM (nothing allocated)
  *   JLC_FAULT_LAUNCH  a GEMM dispatch reports JLC_E_LAUNCH before launching
  *   JLC_FAULT_COPY    a host<->device copy of a host entry reports JLC_E_CUDA
- *   JLC_FAULT_WAIT    the next FP64 GEMM kernel leaves one stage unloaded, so
- *                     one of its bounded waits runs out (JLC_E_TIMEOUT)
+ *   JLC_FAULT_WAIT    the next FP64 GEMM kernel leaves one stage unloaded, or
+ *                     the next run of a grouped plan with 64 x 64 items (not
+ *                     graph-captured) leaves one slot unreported, so one of
+ *                     its bounded waits runs out (JLC_E_TIMEOUT)
  * JLC_FAULT_NONE clears it.  All faults are made on the host or by a wait
  * that nothing satisfies; none faults the GPU.  The environment variable
  * JLCGPU_FAULT=alloc|launch|copy|wait[:after] arms one at jlc_init.  A host

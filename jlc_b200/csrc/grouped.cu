@@ -868,7 +868,7 @@ struct CtOperand {
 // passed back its previous fill.  Returns false when a wait gave up.
 template <bool KMAJOR, bool IS_A>
 __device__ bool ct_produce(const TileItem& w, uint32_t ring, uint64_t* full, uint64_t* empty, uint32_t& pidx,
-                           int* status, int lane) {
+                           int* status, int lane, bool withhold = false) {
     const int kblocks = (w.k + GBK - 1) / GBK;
     CtOperand<KMAJOR> op;
     if (IS_A) op.init(w.a, w.lda, w.rows, w.k, (w.flags & TF_VA) != 0, lane);
@@ -879,7 +879,10 @@ __device__ bool ct_produce(const TileItem& w, uint32_t ring, uint64_t* full, uin
         bool ok = round == 0 || mbar_wait_sleep(&empty[st], (round - 1) & 1, status);
         if (__any_sync(0xffffffffu, !ok)) return false;
         op.load(base + st * CT_SLOT, kb * GBK, w.k);
-        cp_async_mbar_arrive(&full[st]);
+        // test hook: the first slot's copies are issued but never reported,
+        // so its full barrier stays incomplete and the DMMA warps' bounded
+        // wait runs out
+        if (!(withhold && pidx == 0)) cp_async_mbar_arrive(&full[st]);
     }
     return true;
 }
@@ -984,8 +987,11 @@ __device__ bool ct_consume(const TileItem& w, int wm, int wn, uint32_t ring, uin
     return true;
 }
 
+// withhold: test hook (JLC_FAULT_WAIT) -- CTA 0's copy warp B leaves its first
+// slot unreported, so a bounded wait runs out and the launch reports
+// JLC_DEV_TIMEOUT.
 __global__ void __maxnreg__(168)
-    grouped_cta_kernel(const TileItem* items, int nitems, int* counter, int* status) {
+    grouped_cta_kernel(const TileItem* items, int nitems, int* counter, int* status, int withhold) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
     char* base = reinterpret_cast<char*>((reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~uintptr_t(127));
     const uint32_t ring = smem_u32(base);
@@ -1042,8 +1048,10 @@ __global__ void __maxnreg__(168)
             if (__any_sync(0xffffffffu, !ok)) break;
             const TileItem w = recs[q];
             if (w.k < 0) break;
-            const bool done = (w.flags & TF_BK) ? ct_produce<true, false>(w, ring, full, empty, pidx, status, lane)
-                                                : ct_produce<false, false>(w, ring, full, empty, pidx, status, lane);
+            const bool hold = withhold != 0 && blockIdx.x == 0;
+            const bool done = (w.flags & TF_BK)
+                                  ? ct_produce<true, false>(w, ring, full, empty, pidx, status, lane, hold)
+                                  : ct_produce<false, false>(w, ring, full, empty, pidx, status, lane, hold);
             if (!done) break;
             __syncwarp();  // every lane has read the record before its slot is passed back
             if (lane == 0) mbar_arrive(&qempty[q]);
@@ -1680,7 +1688,7 @@ int upload(jlc_grouped_plan* pl, const std::vector<jlc_problem>& probs, const Wo
     return JLC_OK;
 }
 
-int launch_plan(jlc_grouped_plan* pl, cudaStream_t st) {
+int launch_plan(jlc_grouped_plan* pl, cudaStream_t st, bool withhold = false) {
     if (pl->nitems == 0 && pl->nitems_c == 0) return JLC_OK;
     if (pl->oz) {
         if (cudaMemsetAsync(pl->d_counter, 0, sizeof(int), st) != cudaSuccess) return JLC_E_CUDA;
@@ -1708,7 +1716,7 @@ int launch_plan(jlc_grouped_plan* pl, cudaStream_t st) {
     }
     if (pl->nitems_c > 0)
         grouped_cta_kernel<<<pl->grid_c, CT_THREADS, CT_SMEM, st>>>(pl->d_citems, pl->nitems_c, pl->d_counter + 1,
-                                                                    pl->ctx->d_status);
+                                                                    pl->ctx->d_status, withhold ? 1 : 0);
     if (pl->nitems > 0) {
         if (pl->stages == 3)
             grouped_kernel<3><<<pl->grid, WT_THREADS, wt_smem(3), wst>>>(pl->d_probs, pl->d_titems, pl->nitems,
@@ -1990,7 +1998,10 @@ int jlc_grouped_plan_run(jlc_grouped_plan* plan) {
         cudaError_t e = cudaGraphLaunch(plan->exec, ctx->stream);
         return e == cudaSuccess ? JLC_OK : gerr(ctx, JLC_E_LAUNCH, "graph launch: %s", cudaGetErrorString(e));
     }
-    int rc = launch_plan(plan, ctx->stream);
+    // the JLC_FAULT_WAIT hook reaches a plan that launches its CTA items
+    // itself (a captured graph holds fixed kernel arguments)
+    const bool withhold = plan->nitems_c > 0 && fault_hit(ctx, JLC_FAULT_WAIT);
+    int rc = launch_plan(plan, ctx->stream, withhold);
     return rc ? gerr(ctx, rc, "grouped launch failed") : JLC_OK;
 }
 

@@ -12,6 +12,9 @@ the caller falls back; the next call works.  Here:
     kernel leaves one stage unloaded (a barrier nothing completes), the kernel
     unwinds, the call reports JLC_E_TIMEOUT within the limit rather than the
     4 s default, and the context computes correctly afterwards;
+  * the same hook on a grouped plan: CTA 0 of the 64 x 64 tile kernel leaves
+    one slot's copies unreported, every warp's bounded wait ends, the run
+    reports JLC_E_TIMEOUT, and the plan runs correctly afterwards;
   * JLCGPU_FAULT arms the same hook when a context is created.
 """
 import os
@@ -96,6 +99,41 @@ def test_bounded_wait_runs_out_and_context_recovers(ctx, oracle):
         assert_fp64_bound("after timeout", dC.cpu().numpy(), A, B, None, 1.0, 0.0)
     finally:
         ctx.set_wait_limit(0.0)
+
+
+def test_grouped_wait_runs_out_and_plan_recovers(ctx, oracle):
+    import torch
+    from jlc_b200 import JlcError
+    shapes = [(100, 90, 200), (64, 64, 64), (130, 70, 300)] * 6
+    mats = [(oracle.uniform((m, k), 1561 + 3 * i), oracle.uniform((k, n), 1562 + 3 * i),
+             oracle.uniform((m, n), 1563 + 3 * i)) for i, (m, n, k) in enumerate(shapes)]
+    dev = [tuple(torch.from_numpy(x).cuda() for x in t) for t in mats]
+    probs = [dict(m=m, n=n, k=k, layout_a=0, layout_b=0, lda=k, ldb=n, ldc=n, alpha=1.0, beta=0.5,
+                  a=dA.data_ptr(), b=dB.data_ptr(), c=dC.data_ptr())
+             for (m, n, k), (dA, dB, dC) in zip(shapes, dev)]
+    plan = ctx.grouped_plan(probs)
+    assert plan.info()["tile_large"] == 64
+    ctx.set_wait_limit(0.05)
+    try:
+        ctx.inject_fault(WAIT, 0)
+        t0 = time.perf_counter()
+        plan.run()
+        with pytest.raises(JlcError) as exc:
+            ctx.synchronize()
+        elapsed = time.perf_counter() - t0
+        assert exc.value.code == E_TIMEOUT, exc.value
+        assert elapsed < 2.0, f"the wait ran {elapsed:.2f} s: the 50 ms limit was not applied"
+        # C again as it was; the next run of the same plan computes correctly
+        for (A, B, C), (dA, dB, dC) in zip(mats, dev):
+            dC.copy_(torch.from_numpy(C))
+        torch.cuda.synchronize()
+        plan.run()
+        ctx.synchronize()
+        for (m, n, k), (A, B, C), (dA, dB, dC) in zip(shapes, mats, dev):
+            assert_fp64_bound(f"grouped after timeout {m}x{n}x{k}", dC.cpu().numpy(), A, B, C, 1.0, 0.5)
+    finally:
+        ctx.set_wait_limit(0.0)
+        plan.close()
 
 
 def test_timeout_through_the_host_entry_returns_false(oracle):
