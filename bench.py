@@ -42,7 +42,7 @@ def parse():
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--workload", default="dgemm",
-                   choices=["dgemm", "grouped", "configs", "harness", "qr", "shape", "hessenberg"],
+                   choices=["dgemm", "grouped", "configs", "harness", "qr", "shape", "hessenberg", "bidiag"],
                    help="dgemm: the 8192^3 headline; grouped: 20,000 uneven problems in one launch; "
                         "configs: one line per C1-C5 shape (rate and accuracy), one GPU")
     p.add_argument("--count", type=int, default=20000, help="grouped workload: number of problems")
@@ -837,6 +837,75 @@ def run_hessenberg(args):
     return 0
 
 
+def bidiag_cpu_baseline(n):
+    """The oracle's restatement of Bidiagonalization.decompose (one column and
+    one row reflector per step applied to the whole trailing matrix and to U
+    and V, numpy rank-1 updates on the host) on an n x n uniform[-1,1) matrix."""
+    import numpy as np
+    from oracle import oracle as O
+    a = np.random.default_rng(20260604).uniform(-1.0, 1.0, (n, n))
+    t0 = time.perf_counter()
+    O.bidiagonalize(a)
+    dt = time.perf_counter() - t0
+    return {"value": round(16.0 / 3.0 * n ** 3 / dt / 1e9, 2), "unit": "GFLOP/s", "cores": os.cpu_count() or 1,
+            "kind": "port",
+            "sample": f"one {n}x{n} reduction (B, U and V) through the numpy restatement of "
+                      f"Bidiagonalization.decompose (rank-1 updates per reflector), {dt:.1f} s"}
+
+
+def run_bidiag(args):
+    """Device Golub-Kahan bidiagonalisation of a size x size uniform[-1,1)
+    matrix with U and V formed (Bidiagonalization.decompose): device time per
+    reduction (the matrix restored, untimed, before each), FLOPs 8n^3/3 for B
+    and 4n^3/3 each for U and V, and the device time of the reflector launch."""
+    import statistics
+    import torch
+    import jlc_b200
+    world, rank, local = dist_env()
+    if rank != 0:
+        return 0
+    torch.cuda.set_device(local)
+    ctx = jlc_b200.Context(local)
+    n = args.size
+    g = torch.Generator(device="cuda")
+    g.manual_seed(20260604)
+    a0 = torch.rand((n, n), dtype=torch.float64, device="cuda", generator=g) * 2 - 1
+    a = torch.empty_like(a0)
+    u = torch.empty_like(a0)
+    v = torch.empty_like(a0)
+    d = torch.empty(n, dtype=torch.float64, device="cuda")
+    e = torch.empty(max(n - 1, 1), dtype=torch.float64, device="cuda")
+    flops = 16.0 / 3.0 * n ** 3
+    times, phases = [], []
+    for it in range(args.warmup + args.steps):
+        a.copy_(a0)
+        torch.cuda.synchronize()
+        ctx.set_profiling(it >= args.warmup)
+        rep = ctx.bidiag_device(n, n, a.data_ptr(), n, d.data_ptr(), e.data_ptr(), u.data_ptr(), n, v.data_ptr(), n)
+        if it >= args.warmup:
+            recs = ctx.profile_collect()
+            times.append(rep["device_ms"])
+            per = {}
+            for name, t in recs:
+                per[name] = per.get(name, 0.0) + t
+            phases.append(per)
+    ctx.set_profiling(False)
+    ms = statistics.median(times)
+    cpu = None if args.no_cpu_baseline else bidiag_cpu_baseline(min(n, 512))
+    line = {"metric": f"Golub-Kahan bidiagonalisation GFLOP/s ({n}x{n}, FP64, B, U and V, device-resident)",
+            "value": round(flops / (ms * 1e-3) / 1e9, 1), "unit": "GFLOP/s", "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(ms, 3), "higher_is_better": True, "dtype": "f64",
+            "data": "synthetic uniform[-1,1) (torch Philox, seed 20260604), device resident",
+            "config": {"workload": f"bidiagonalisation {n}x{n} with U and V: one cooperative launch for the "
+                                   "reflectors, U and V by blocked WY on the DMMA route"},
+            "phase_ms": {name: round(statistics.median(p.get(name, 0.0) for p in phases), 3)
+                         for name in sorted({nm for p in phases for nm in p})},
+            "cpu_baseline": cpu}
+    print(json.dumps(line), flush=True)
+    ctx.close()
+    return 0
+
+
 # ----------------------------------------------------------------------------- harness (report port)
 HARNESS_BACKENDS = ["blas3-naive", "blas3-simd-1t", "blas3-parallel", "opt-1t", "opt-parallel", "cuda",
                     "cuda-ozaki"]
@@ -1071,6 +1140,8 @@ def main():
         return run_shape(args)
     if args.workload == "hessenberg":
         return run_hessenberg(args)
+    if args.workload == "bidiag":
+        return run_bidiag(args)
     if args.workload == "qr":
         return run_qr(args)
     return run_ours(args)

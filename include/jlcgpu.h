@@ -226,6 +226,7 @@ JLC_API int jlc_inject_fault(jlc_ctx* ctx, int kind, int after);
 #define JLC_PHASE_QR_PANEL 12   /* blocked QR: one panel's factorisation kernel */
 #define JLC_PHASE_QR_VT 13      /* blocked QR: V packing and the T factor (the Gram GEMM is a dmma phase) */
 #define JLC_PHASE_HESS_PANEL 17     /* Hessenberg: one panel's reflectors (column, GEMV, Y updates) */
+#define JLC_PHASE_BIDIAG 18         /* bidiagonalisation: the reflectors' cooperative launch */
 #define JLC_PHASE_OZAKI_CERT 14     /* Ozaki accuracy certificate (magnitude product, route decision) */
 #define JLC_PHASE_OZAKI_SPLIT_HI 15 /* split at the higher count (runs only when the certificate picks it) */
 #define JLC_PHASE_OZAKI_GEMM_HI 16  /* INT8 GEMM at the higher count (likewise) */
@@ -353,6 +354,24 @@ JLC_API int jlc_qr_factor_device(jlc_ctx* ctx, int64_t m, int64_t n, double* a, 
  * HouseholderQR.java:387-441), blocked with the same WY form. */
 JLC_API int jlc_qr_build_q_device(jlc_ctx* ctx, int64_t m, int64_t n, int64_t qcols, const double* f, int64_t ldf,
                                   const double* tau, double* q, int64_t ldq, int precision, jlc_report* rep);
+
+/* ---------------------------------------------------------------- bidiagonalisation (device) */
+/* Reduces the column-major m x n matrix A (m >= n, lda >= m) on the device to
+ * upper bidiagonal B = U^T A V, as Bidiagonalization.decomposeUpper does
+ * (decomposition/bidiagonal/Bidiagonalization.java:180-309): per column a
+ * Householder reflector from the left, per row one from the right, each with
+ * the reference's recipe (scaled norm of the whole vector, beta =
+ * -copysign(norm, x0), tau = (beta - x0) / beta, none when the norm or |tau|
+ * is at most Double.MIN_NORMAL).  d (n) and e (n - 1) receive the diagonal and
+ * superdiagonal of B.  On return A holds the column reflectors' tails below
+ * the diagonal and the row reflectors' tails beyond the superdiagonal.  U
+ * (m x m, ldu >= m) and V (n x n, ldv >= n) are formed when not null, on the
+ * GEMM route (blocked WY, precision as for the QR trailing updates).  Wide
+ * matrices go through their transpose, as the reference's decompose does.
+ * Rows are split at most 256 per SM.  New: the reference runs this on the CPU
+ * only. */
+JLC_API int jlc_bidiag_device(jlc_ctx* ctx, int64_t m, int64_t n, double* a, int64_t lda, double* d, double* e,
+                              double* u, int64_t ldu, double* v, int64_t ldv, int precision, jlc_report* rep);
 
 /* ---------------------------------------------------------------- Hessenberg reduction (device) */
 /* Reduces the column-major n x n matrix A (lda >= n) on the device, in place,

@@ -12,13 +12,14 @@ from ._lib import (JLC_COL_MAJOR, JLC_KERNEL_DMMA, JLC_KERNEL_GEMV, JLC_KERNEL_G
                    JlcLibraryMissing, LIB_PATH, load)
 from .compute import (BLAS3Kernels, Context, CudaGemm, DispatchPolicy, IllegalArgumentException, JlcError, Matrix,
                       OffHeapMatrix, OptimizedBLAS3, default_context)
-from .decomposition import (ArithmeticException, BlockedHessenbergQR, HessenbergResult, HouseholderQR, QRResult,
-                            UnsupportedOperationException)
+from .decomposition import (ArithmeticException, Bidiagonalization, BidiagonalizationResult, BlockedHessenbergQR,
+                            HessenbergResult, HouseholderQR, QRResult, UnsupportedOperationException)
 from .dispatch import BlockedMultiply, CpuRouteUnavailable, CudaContext, CudaSupport, GemmDispatch
 
 __all__ = [
     "BLAS3Kernels", "BlockedMultiply", "Context", "CpuRouteUnavailable", "CudaContext", "CudaGemm", "CudaSupport",
     "GemmDispatch", "DispatchPolicy", "ArithmeticException", "BlockedHessenbergQR", "HessenbergResult",
+    "Bidiagonalization", "BidiagonalizationResult",
     "HouseholderQR", "IllegalArgumentException", "JlcError",
     "QRResult", "UnsupportedOperationException",
     "JlcLibraryMissing", "Matrix", "OffHeapMatrix", "OptimizedBLAS3", "default_context", "load", "LIB_PATH",

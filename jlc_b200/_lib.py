@@ -112,6 +112,7 @@ SIGNATURES = {
     "jlc_profile_timeline": (_i, [_vp, ctypes.POINTER(_i), ctypes.POINTER(_d), ctypes.POINTER(_d), _i]),
     "jlc_qr_factor_device": (_i, [_vp, _i64, _i64, _dp, _i64, _dp, _i, _REP]),
     "jlc_hessenberg_device": (_i, [_vp, _i64, _dp, _i64, _dp, _i64, _i, _REP]),
+    "jlc_bidiag_device": (_i, [_vp, _i64, _i64, _dp, _i64, _dp, _dp, _dp, _i64, _dp, _i64, _i, _REP]),
     "jlc_qr_build_q_device": (_i, [_vp, _i64, _i64, _i64, _dp, _i64, _dp, _dp, _i64, _i, _REP]),
     "jlc_launch_count": (_i, [_vp, ctypes.POINTER(_i64)]),
     "jlc_check_fp64_bound_device": (_i, [_vp, _i, _i, _i64, _i64, _i64, _d, _dp, _i64, _dp, _i64, _d, _dp, _i64,
@@ -135,7 +136,7 @@ SIGNATURES = {
 
 PHASES = {1: "dmma", 2: "gemv", 3: "ozaki_gemm", 4: "grouped", 5: "ozaki_split", 6: "scale", 7: "fp64_gated", 8: "h2d",
           9: "d2h", 11: "reduce", 12: "qr_panel", 13: "qr_vt", 14: "ozaki_cert", 15: "ozaki_split_hi",
-          16: "ozaki_gemm_hi", 17: "hess_panel"}
+          16: "ozaki_gemm_hi", 17: "hess_panel", 18: "bidiag_reflectors"}
 
 _lib = None
 

@@ -24,7 +24,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-fvisibility=hidden", "--expt-relaxed-constexpr",
          "-I", INCLUDE, "-I", CSRC]
 SOURCES = ["api.cu", "dgemm_dmma.cu", "gemv.cu", "ozaki.cu", "verify.cu", "peaks.cu", "noalloc.cu", "grouped.cu", "adjoint.cu",
-           "qr.cu", "hess.cu", "staging.cu"]
+           "qr.cu", "hess.cu", "staging.cu", "bidiag.cu"]
 # the double-double check must not have its expressions contracted into fma
 PER_FILE_FLAGS = {"verify.cu": ["--fmad=false"]}
 

@@ -271,6 +271,16 @@ class Context:
                                                   ctypes.byref(rep)))
         return rep.as_dict()
 
+    def bidiag_device(self, m, n, a_ptr, lda, d_ptr, e_ptr, u_ptr, ldu, v_ptr, ldv,
+                      precision=L.JLC_PREC_NATIVE) -> dict:
+        """Golub-Kahan bidiagonalisation of the column-major m x n matrix at
+        a_ptr (m >= n), in place; d_ptr / e_ptr receive B's diagonal and
+        superdiagonal, u_ptr / v_ptr (or None) U and V with A = U B V^T."""
+        rep = L.Report()
+        self.check(self.lib.jlc_bidiag_device(self.h, m, n, a_ptr, lda, d_ptr, e_ptr, u_ptr, ldu, v_ptr, ldv,
+                                              int(precision), ctypes.byref(rep)))
+        return rep.as_dict()
+
     def qr_build_q_device(self, m, n, qcols, f_ptr, ldf, tau_ptr, q_ptr, ldq, precision=L.JLC_PREC_NATIVE) -> dict:
         """Q (column-major m x qcols) of a factorisation from qr_factor_device."""
         rep = L.Report()

@@ -1220,6 +1220,33 @@ int hess_apply_right(jlc_ctx* ctx, double* mat, long long ldm, long long n, long
     return run_device(ctx, u, precision, 0, nullptr);
 }
 
+}  // extern "C"
+
+namespace {
+// Q (first qcols columns) of the reflectors stored in f (below its diagonal,
+// QR style) with scales tau, enqueued on the context stream without a sync:
+// the identity, then the panels' block reflectors in reverse order.
+int qr_build_q_enqueue(jlc_ctx* ctx, long long m, long long n, long long qcols, const double* f, long long ldf,
+                       const double* tau, double* q_out, long long ldq, int precision) {
+    const long long kmax = m < n ? m : n;
+    QrWork q;
+    int rc = qr_work(ctx, m, qcols, q);
+    if (rc) return rc;
+    rc = launch_set_identity(q_out, ldq, m, qcols, ctx->stream);
+    if (rc) return set_err(ctx, rc, "QR: identity launch failed");
+    for (long long k0 = (kmax - 1) / kQrPanel * kQrPanel; k0 >= 0 && kmax > 0; k0 -= kQrPanel) {
+        const int kb = (int)(kmax - k0 < kQrPanel ? kmax - k0 : kQrPanel);
+        if (k0 >= qcols) continue;
+        rc = qr_panel_vt(ctx, f, ldf, m, k0, kb, tau, q, precision);
+        if (!rc) rc = qr_apply_wy(ctx, m, k0, qcols - k0, q_out + k0 * ldq, ldq, false, q, precision);
+        if (rc) return rc;
+    }
+    return JLC_OK;
+}
+}  // namespace
+
+extern "C" {
+
 int jlc_hessenberg_device(jlc_ctx* ctx, int64_t n, double* a, int64_t lda, double* q, int64_t ldq, int precision,
                           jlc_report* rep) {
     report_init(rep);
@@ -1293,22 +1320,76 @@ int jlc_qr_build_q_device(jlc_ctx* ctx, int64_t m, int64_t n, int64_t qcols, con
     if (m > INT32_MAX / 2 || n > INT32_MAX / 2) return set_err(ctx, JLC_E_UNSUPPORTED, "dimension above 2^30");
     cudaSetDevice(ctx->device);
     ctx->err[0] = 0;
-    QrWork q;
-    int rc = qr_work(ctx, m, qcols, q);
-    if (rc) return rc;
     cudaEventRecord(ctx->ev0, ctx->stream);
-    // Q = I (first qcols columns), then the panels' H applied in reverse order;
-    // panel k0 changes only rows and columns from k0 on
-    rc = launch_set_identity(q_out, ldq, m, qcols, ctx->stream);
-    if (rc) return set_err(ctx, rc, "QR: identity launch failed");
-    for (long long k0 = (kmax - 1) / kQrPanel * kQrPanel; k0 >= 0 && kmax > 0; k0 -= kQrPanel) {
-        const int kb = (int)(kmax - k0 < kQrPanel ? kmax - k0 : kQrPanel);
-        if (k0 >= qcols) continue;
-        rc = qr_panel_vt(ctx, f, ldf, m, k0, kb, tau, q, precision);
-        if (!rc) rc = qr_apply_wy(ctx, m, k0, qcols - k0, q_out + k0 * ldq, ldq, false, q, precision);
-        if (rc) return rc;
-    }
+    int rc = qr_build_q_enqueue(ctx, m, n, qcols, f, ldf, tau, q_out, ldq, precision);
+    if (rc) return rc;
     cudaEventRecord(ctx->ev1, ctx->stream);
+    rc = finish_sync(ctx);
+    if (rc) return rc;
+    if (rep) {
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
+        rep->device_ms = ms;
+        rep->kernel = JLC_KERNEL_DMMA;
+    }
+    return JLC_OK;
+}
+
+int jlc_bidiag_device(jlc_ctx* ctx, int64_t m, int64_t n, double* a, int64_t lda, double* d, double* e, double* u,
+                      int64_t ldu, double* v, int64_t ldv, int precision, jlc_report* rep) {
+    report_init(rep);
+    if (!ctx) return JLC_E_ARG;
+    if (m < 0 || n < 0) return set_err(ctx, JLC_E_ARG, "dimensions must be non-negative");
+    if (n > m) return set_err(ctx, JLC_E_ARG, "need m >= n (a wide matrix is reduced through its transpose)");
+    if (m > 0 && n > 0 && (!a || lda < m)) return set_err(ctx, JLC_E_ARG, "A must not be null and lda must be >= m");
+    if (n > 0 && (!d || (n > 1 && !e))) return set_err(ctx, JLC_E_ARG, "d and e must not be null");
+    if (u && ldu < m) return set_err(ctx, JLC_E_ARG, "ldu must be >= m");
+    if (v && ldv < n) return set_err(ctx, JLC_E_ARG, "ldv must be >= n");
+    if (m > INT32_MAX / 4) return set_err(ctx, JLC_E_UNSUPPORTED, "dimension above 2^29");
+    cudaSetDevice(ctx->device);
+    ctx->err[0] = 0;
+    cudaStream_t st = ctx->stream;
+    int slab = 0;
+    if (m > 0 && n > 0 && bidiag_grid((int)m, ctx->sm_count, &slab) == 0)
+        return set_err(ctx, JLC_E_UNSUPPORTED, "bidiagonalisation: more than 256 rows per SM");
+    cudaEventRecord(ctx->ev0, st);
+    int rc = JLC_OK;
+    if (m > 0 && n > 0) {
+        // workspace: tau of the column and row reflectors, the kernel's
+        // partials, and the row reflectors rearranged as a QR factor
+        const long long ldw = n > 1 ? round_up(n - 1, 8) : 8;
+        const size_t kdoubles = bidiag_work_doubles((int)m, (int)n, ctx->sm_count);
+        const size_t wdoubles = v ? (size_t)ldw * (size_t)(n > 1 ? n - 1 : 1) : 0;
+        if ((rc = reserve(ctx, ctx->bufH, (2 * (size_t)n + kdoubles + wdoubles) * sizeof(double),
+                          "bidiagonalisation workspace")))
+            return rc;
+        double* tauq = static_cast<double*>(ctx->bufH.ptr);
+        double* taup = tauq + n;
+        double* kwork = taup + n;
+        double* wr = kwork + kdoubles;
+        {
+            Phase ph(ctx, JLC_PHASE_BIDIAG);
+            rc = launch_bidiag(a, lda, (int)m, (int)n, d, e, tauq, taup, kwork, ctx->sm_count, ctx->d_status, st);
+            if (rc) return set_err(ctx, rc, "bidiagonalisation: launch failed");
+            ctx->launches += 1;
+        }
+        // U = H_0 H_1 ... H_{n-1}: the column reflectors sit below the diagonal as in a QR factor
+        if (u && (rc = qr_build_q_enqueue(ctx, m, n, m, a, lda, tauq, u, ldu, precision))) return rc;
+        if (v) {
+            // V = diag(1, G_0 ... G_{n-2}): row k's reflector acts on columns k+1..
+            if ((rc = launch_set_identity(v, ldv, n, n, st))) return set_err(ctx, rc, "identity launch failed");
+            if (n > 1) {
+                if ((rc = launch_bidiag_right_factor(a, lda, (int)n, wr, ldw, st)))
+                    return set_err(ctx, rc, "bidiagonalisation: right factor launch failed");
+                if ((rc = qr_build_q_enqueue(ctx, n - 1, n - 1, n - 1, wr, ldw, taup, v + 1 + ldv, ldv, precision)))
+                    return rc;
+            }
+        }
+    } else {
+        if (u && (rc = launch_set_identity(u, ldu, m, m, st))) return set_err(ctx, rc, "identity launch failed");
+        if (v && (rc = launch_set_identity(v, ldv, n, n, st))) return set_err(ctx, rc, "identity launch failed");
+    }
+    cudaEventRecord(ctx->ev1, st);
     rc = finish_sync(ctx);
     if (rc) return rc;
     if (rep) {

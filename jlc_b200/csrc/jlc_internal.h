@@ -93,6 +93,14 @@ int launch_qr_gram(const double* v, long long ldv, int r0, int r1, double* g, do
 int launch_set_identity(double* q, long long ldq, long long m, long long cols, cudaStream_t st);
 // blocked Hessenberg reduction kernels (hess.cu)
 size_t hess_work_doubles(long long n);
+// Golub-Kahan bidiagonalisation (bidiag.cu): rows per CTA and CTA count (0:
+// too many rows), the kernel's workspace in doubles, the cooperative launch,
+// and the row reflectors rearranged as the columns of a QR factor.
+int bidiag_grid(int m, int sm_count, int* slab);
+size_t bidiag_work_doubles(int m, int n, int sm_count);
+int launch_bidiag(double* a, long long lda, int m, int n, double* d, double* e, double* tauq, double* taup,
+                  double* work, int sm_count, int* status, cudaStream_t st);
+int launch_bidiag_right_factor(const double* a, long long lda, int n, double* w, long long ldw, cudaStream_t st);
 int launch_hess_clear(double* h, long long ldh, int n, cudaStream_t st);
 // all reflectors of one panel in one cooperative launch (rows in slabs over
 // up to sm_count CTAs); scratch of hess_panel_scratch_bytes

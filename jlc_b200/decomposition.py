@@ -159,3 +159,77 @@ class BlockedHessenbergQR:
         h = np.ascontiguousarray(ht.cpu().numpy().T)
         q = np.ascontiguousarray(qt.cpu().numpy().T)
         return HessenbergResult(a, Matrix.wrap(h.ravel(), n, n), Matrix.wrap(q.ravel(), n, n))
+
+
+class BidiagonalizationResult:
+    """decomposition/result/BidiagonalizationResult.java: the input, U, B and V
+    with A = U B V^T."""
+
+    def __init__(self, a: Matrix, u: Matrix, b: Matrix, v: Matrix):
+        self._a, self._u, self._b, self._v = a, u, b, v
+
+    def getA(self) -> Matrix:
+        return self._a
+
+    def getU(self) -> Matrix:
+        return self._u
+
+    def getB(self) -> Matrix:
+        return self._b
+
+    def getV(self) -> Matrix:
+        return self._v
+
+    def reconstruct(self) -> Matrix:
+        u, b, v = self._u.to_numpy(), self._b.to_numpy(), self._v.to_numpy()
+        r = u @ b @ v.T
+        return Matrix.wrap(np.ascontiguousarray(r).ravel(), r.shape[0], r.shape[1])
+
+    def residualNorm(self) -> float:
+        a = self._a.to_numpy()
+        return float(np.linalg.norm(a - self.reconstruct().to_numpy()) / max(np.linalg.norm(a), 1e-300))
+
+
+class Bidiagonalization:
+    """decomposition/bidiagonal/Bidiagonalization.java:155-309 on the device:
+    the matrix goes to the device once (column-major), jlc_bidiag_device
+    reduces it there (one cooperative launch for the reflectors, U and V on the
+    GEMM route), and U, B and V come back.  B is upper bidiagonal for m >= n;
+    a wide matrix goes through its transpose and B comes back lower
+    bidiagonal, as in the reference."""
+
+    def decompose(self, a: Matrix, ctx=None, precision: int = L.JLC_PREC_NATIVE) -> BidiagonalizationResult:
+        if a is None:
+            raise IllegalArgumentException("Matrix must not be null")
+        x = a.to_numpy()
+        m, n = x.shape
+        if m >= n:
+            u, b, v = _bidiag_upper(x, ctx or default_context(), precision)
+            return BidiagonalizationResult(a, _wrap(u), _wrap(b), _wrap(v))
+        u, b, v = _bidiag_upper(np.ascontiguousarray(x.T), ctx or default_context(), precision)
+        return BidiagonalizationResult(a, _wrap(v), _wrap(np.ascontiguousarray(b.T)), _wrap(u))
+
+
+def _wrap(x):
+    return Matrix.wrap(np.ascontiguousarray(x).ravel(), x.shape[0], x.shape[1])
+
+
+def _bidiag_upper(x, ctx, precision):
+    """U, B, V of a tall (m >= n) row-major array through jlc_bidiag_device."""
+    import torch
+    m, n = x.shape
+    if m == 0 or n == 0:
+        return np.eye(m), np.zeros((m, n)), np.eye(n)
+    dev = torch.device("cuda", ctx.device)
+    at = torch.from_numpy(np.ascontiguousarray(x.T)).to(dev)  # column-major A
+    d = torch.empty(n, dtype=torch.float64, device=dev)
+    e = torch.empty(max(n - 1, 1), dtype=torch.float64, device=dev)
+    ut = torch.empty((m, m), dtype=torch.float64, device=dev)
+    vt = torch.empty((n, n), dtype=torch.float64, device=dev)
+    ctx.bidiag_device(m, n, at.data_ptr(), m, d.data_ptr(), e.data_ptr(), ut.data_ptr(), m, vt.data_ptr(), n,
+                      precision)
+    b = np.zeros((m, n))
+    b[np.arange(n), np.arange(n)] = d.cpu().numpy()
+    if n > 1:
+        b[np.arange(n - 1), np.arange(1, n)] = e.cpu().numpy()[:n - 1]
+    return (np.ascontiguousarray(ut.cpu().numpy().T), b, np.ascontiguousarray(vt.cpu().numpy().T))

@@ -256,6 +256,72 @@ def blocked_hessenberg_c(a, threads: int = 0):
     return h, q
 
 
+# ------------------------------------------------------------- Golub-Kahan bidiagonalisation
+BIDIAG_SAFE_MIN = 2.2250738585072014e-308  # Double.MIN_NORMAL (Bidiagonalization.java:128)
+
+
+def _bidiag_reflector(x):
+    """The reference's dlarfg-style recipe (Bidiagonalization.java:205-229):
+    scale/ssq norm over the whole vector (x0 included), beta = -xnorm for
+    x0 >= 0 else xnorm, tau = (beta - x0) / beta, v = x / (x0 - beta) with
+    v0 = 1.  Returns (tau, beta, v) or None when xnorm or |tau| is at most
+    Double.MIN_NORMAL (no reflector)."""
+    x0 = float(x[0])
+    scale, ssq = abs(x0), 1.0
+    for xi in x[1:]:
+        a = abs(float(xi))
+        if a > scale:
+            t = scale / a
+            ssq = 1.0 + ssq * t * t
+            scale = a
+        elif a > 0.0:
+            t = a / scale
+            ssq += t * t
+    xnorm = scale * np.sqrt(ssq)
+    if not xnorm > BIDIAG_SAFE_MIN:
+        return None
+    beta = -xnorm if x0 >= 0.0 else xnorm
+    tau = (beta - x0) / beta
+    if not abs(tau) > BIDIAG_SAFE_MIN:
+        return None
+    v = np.asarray(x, dtype=np.float64) * (1.0 / (x0 - beta))
+    v[0] = 1.0
+    return tau, beta, v
+
+
+def bidiagonalize(a):
+    """Bidiagonalization.decompose (decomposition/bidiagonal/Bidiagonalization.java:155-309):
+    Golub-Kahan reduction A = U B V^T, one column and one row reflector per
+    step applied to the whole trailing matrix (and to U and V from the right),
+    B upper bidiagonal for m >= n; a wide matrix goes through its transpose and
+    B comes back lower bidiagonal.  Returns (U, B, V)."""
+    a = np.asarray(a, dtype=np.float64)
+    m, n = a.shape
+    if m < n:
+        ut, bt, vt = bidiagonalize(a.T)
+        return vt, bt.T.copy(), ut
+    b = a.copy()
+    u = np.eye(m)
+    v = np.eye(n)
+    for k in range(min(m, n)):
+        r = _bidiag_reflector(b[k:, k])
+        if r is not None:
+            tau, beta, h = r
+            b[k:, k:] -= tau * np.outer(h, h @ b[k:, k:])
+            u[:, k:] -= tau * np.outer(u[:, k:] @ h, h)
+            b[k, k] = beta
+            b[k + 1:, k] = 0.0
+        if k < n - 1:
+            r = _bidiag_reflector(b[k, k + 1:])
+            if r is not None:
+                tau, beta, g = r
+                b[k:, k + 1:] -= tau * np.outer(b[k:, k + 1:] @ g, g)
+                v[:, k + 1:] -= tau * np.outer(v[:, k + 1:] @ g, g)
+                b[k, k + 1] = beta
+                b[k, k + 2:] = 0.0
+    return u, b, v
+
+
 def normal(shape, seed: int) -> np.ndarray:
     n = int(np.prod(shape))
     out = np.empty(n, dtype=np.float64)
