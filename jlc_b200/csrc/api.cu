@@ -1349,8 +1349,8 @@ int jlc_bidiag_device(jlc_ctx* ctx, int64_t m, int64_t n, double* a, int64_t lda
     cudaSetDevice(ctx->device);
     ctx->err[0] = 0;
     cudaStream_t st = ctx->stream;
-    int slab = 0;
-    if (m > 0 && n > 0 && bidiag_grid((int)m, ctx->sm_count, &slab) == 0)
+    int rows_per_cta = 0;
+    if (m > 0 && n > 0 && bidiag_grid((int)m, ctx->sm_count, &rows_per_cta) == 0)
         return set_err(ctx, JLC_E_UNSUPPORTED, "bidiagonalisation: more than 256 rows per SM");
     cudaEventRecord(ctx->ev0, st);
     int rc = JLC_OK;

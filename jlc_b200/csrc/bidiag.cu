@@ -12,8 +12,9 @@
 //     rows k.. of B from the right (and to V).
 // That is a BLAS-2 algorithm: every reflector touches the whole trailing
 // matrix.  Here all n steps run in one cooperative launch.  The m rows are
-// split into slabs of at most 256 rows, one per CTA, and four bounded grid
-// barriers join the reductions of each step:
+// dealt to the CTAs (at most one per SM) in chunks of 8, round robin, so that
+// every CTA keeps rows in play as the trailing matrix shrinks; a CTA holds at
+// most 256 rows.  Four bounded grid barriers join the reductions of each step:
 //   1. each CTA's scale/ssq of its rows of column k, merged by every CTA in
 //      the same fixed order (so all derive the same beta, tau, 1/(x0 - beta));
 //   2. each CTA's v on its rows (stored below the diagonal, as QR stores its
@@ -41,14 +42,15 @@ namespace bidiag {
 
 constexpr int BT = 256;  // threads per CTA
 constexpr int WARPS = BT / 32;
-constexpr int CH = 8;  // loads a thread keeps in flight in the passes over the trailing matrix
+constexpr int CH = 16;  // loads a thread keeps in flight in the row passes and the cross-CTA sums
+constexpr int RC = 8;   // rows per chunk: CTA p holds row chunks p, p + P, p + 2P, ...
 constexpr double kSafeMin = 2.2250738585072014e-308;  // Double.MIN_NORMAL
 
 struct Args {
     double* a;  // column-major m x n, m >= n
     long long lda;
     int m, n;
-    int slab;      // rows per CTA
+    int nloc;      // rows per CTA (a multiple of RC, at most BT): its chunks, the last ones possibly past m
     double* d;     // n: the diagonal of B
     double* e;     // n - 1: the superdiagonal of B
     double* tauq;  // n: the column reflectors' tau
@@ -143,7 +145,7 @@ __global__ void __launch_bounds__(BT, 1) bidiag_kernel(const Args p) {
     __shared__ double s_red[2 * WARPS];
     __shared__ double s_sc[4];
     __shared__ double s_x[BT];
-    __shared__ double s_v[BT];  // the column reflector on this CTA's rows (index r - r0)
+    __shared__ double s_v[BT];  // the column reflector on this CTA's rows (by local row)
     __shared__ int s_ok;
     // the matrix and the vectors never alias, and each is reached through its
     // own pointer only: loads may pass earlier stores
@@ -152,23 +154,28 @@ __global__ void __launch_bounds__(BT, 1) bidiag_kernel(const Args p) {
     double* __restrict__ W = p.w;
     const int P = gridDim.x, cta = blockIdx.x;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int r0 = cta * p.slab, r1 = min(p.m, r0 + p.slab);
+    const int m = p.m, n = p.n, nloc = p.nloc, nchunk = nloc / RC;
+    // local row l of this CTA: row chunks cta, cta + P, cta + 2P, ... of RC rows
+    auto grow = [&](int l) { return ((l / RC) * P + cta) * RC + (l % RC); };
     unsigned nbar = 0;
     auto barrier = [&]() -> bool {
         ++nbar;
         return grid_barrier(p.counter, nbar * (unsigned)P, p.status, &s_ok);
     };
-    // the row-reflector phase: thread -> (row of the slab, part of the columns)
-    const int nparts = BT / p.slab > 0 ? BT / p.slab : 1;
-    const int rloc = threadIdx.x % p.slab, rpart = threadIdx.x / p.slab;
+    // the row-reflector phase: thread -> (local row, part of the columns)
+    const int nparts = BT / nloc > 0 ? BT / nloc : 1;
+    const int rloc = threadIdx.x % nloc, rpart = threadIdx.x / nloc;
 
-    for (int k = 0; k < p.n; ++k) {
+    for (int k = 0; k < n; ++k) {
         double* col = A + (long long)k * p.lda;
         __syncthreads();  // the previous step's row updates of this CTA are done
         // 1. scale/ssq of this CTA's rows k.. of column k
         {
             Ssq acc{0.0, 0.0};
-            for (int r = max(r0, k) + threadIdx.x; r < r1; r += BT) acc = ssq_add(acc, col[r]);
+            for (int l = threadIdx.x; l < nloc; l += BT) {
+                const int g = grow(l);
+                if (g >= k && g < m) acc = ssq_add(acc, col[g]);
+            }
             const Ssq t = cta_merge(acc, s_red);
             if (threadIdx.x == 0) {
                 p.part[2 * cta] = t.s;
@@ -193,67 +200,85 @@ __global__ void __launch_bounds__(BT, 1) bidiag_kernel(const Args p) {
         __syncthreads();
         const double tau = s_sc[0], inv = s_sc[2];
         const bool lact = tau != 0.0;
-        // 2. v on this CTA's rows (v_k = 1), the tails stored in column k;
-        //    partial dots of v with the trailing columns, one column per lane
-        //    (each lane walks down its column: the loads are independent and
-        //    no cross-lane sum is needed)
-        const int rs = max(r0, k);  // this CTA's first row in play
+        // this CTA's first chunk with rows at or past k
+        const int kc = k / RC;
+        const int i0 = kc > cta ? (kc - cta + P - 1) / P : 0;
+        // 2. v on this CTA's rows (v_k = 1, 0 above k), the tails stored in
+        //    column k; partial dots of v with the trailing columns, one column
+        //    per lane (each lane walks down its column, a chunk of RC loads in
+        //    flight, and no cross-lane sum is needed)
         if (lact) {
-            for (int r = r0 + threadIdx.x; r < r1; r += BT) {
-                const double x = r > k ? col[r] * inv : (r == k ? 1.0 : 0.0);
-                s_v[r - r0] = x;
-                if (r > k) col[r] = x;
+            for (int l = threadIdx.x; l < nloc; l += BT) {
+                const int g = grow(l);
+                const bool tail = g > k && g < m;
+                const double x = tail ? col[g] * inv : (g == k ? 1.0 : 0.0);
+                s_v[l] = x;
+                if (tail) col[g] = x;
             }
         }
         __syncthreads();
         if (lact) {
-            for (int j = k + 1 + 32 * warp + lane; j < p.n; j += 32 * WARPS) {
+            for (int j = k + 1 + threadIdx.x; j < n; j += BT) {
                 const double* aj = A + (long long)j * p.lda;
                 double s = 0.0;
-                int r = rs;
-                for (; r + CH <= r1; r += CH) {  // CH loads in flight, then their FMAs
-                    double x[CH];
+                for (int i = i0; i < nchunk; ++i) {
+                    const int g0 = (i * P + cta) * RC;
+                    if (g0 + RC <= m) {
+                        double x[RC];
 #pragma unroll
-                    for (int t = 0; t < CH; ++t) x[t] = aj[r + t];
+                        for (int t = 0; t < RC; ++t) x[t] = aj[g0 + t];
 #pragma unroll
-                    for (int t = 0; t < CH; ++t) s = fma(s_v[r + t - r0], x[t], s);
+                        for (int t = 0; t < RC; ++t) s = fma(s_v[i * RC + t], x[t], s);
+                    } else {
+                        for (int g = g0; g < m; ++g) s = fma(s_v[i * RC + g - g0], aj[g], s);
+                    }
                 }
-                for (; r < r1; ++r) s = fma(s_v[r - r0], aj[r], s);
-                p.wpart[(long long)cta * p.n + j] = s;
+                p.wpart[(long long)cta * n + j] = s;
             }
         }
         if (!barrier()) return;
         // 3. w_j = tau * sum over the CTAs' dots, in CTA order; a share of the columns per thread
         if (lact) {
-            for (int j = k + 1 + cta * BT + threadIdx.x; j < p.n; j += P * BT) {
+            for (int j = k + 1 + cta * BT + threadIdx.x; j < n; j += P * BT) {
                 double s = 0.0;
-                for (int q = 0; q < P; ++q) s += p.wpart[(long long)q * p.n + j];
+                int q = 0;
+                for (; q + CH <= P; q += CH) {  // CH loads in flight, added in CTA order
+                    double x[CH];
+#pragma unroll
+                    for (int t = 0; t < CH; ++t) x[t] = p.wpart[(long long)(q + t) * n + j];
+#pragma unroll
+                    for (int t = 0; t < CH; ++t) s += x[t];
+                }
+                for (; q < P; ++q) s += p.wpart[(long long)q * n + j];
                 W[j] = tau * s;
             }
         }
         if (!barrier()) return;
         // 4. A -= v w^T on this CTA's rows k.., one column per lane
         if (lact) {
-            for (int j = k + 1 + 32 * warp + lane; j < p.n; j += 32 * WARPS) {
+            for (int j = k + 1 + threadIdx.x; j < n; j += BT) {
                 double* aj = A + (long long)j * p.lda;
                 const double wj = W[j];
-                int r = rs;
-                for (; r + CH <= r1; r += CH) {
-                    double x[CH];
+                for (int i = i0; i < nchunk; ++i) {
+                    const int g0 = (i * P + cta) * RC;
+                    if (g0 + RC <= m) {
+                        double x[RC];
 #pragma unroll
-                    for (int t = 0; t < CH; ++t) x[t] = aj[r + t];
+                        for (int t = 0; t < RC; ++t) x[t] = aj[g0 + t];
 #pragma unroll
-                    for (int t = 0; t < CH; ++t) aj[r + t] = fma(-s_v[r + t - r0], wj, x[t]);
+                        for (int t = 0; t < RC; ++t) aj[g0 + t] = fma(-s_v[i * RC + t], wj, x[t]);
+                    } else {
+                        for (int g = g0; g < m; ++g) aj[g] = fma(-s_v[i * RC + g - g0], wj, aj[g]);
+                    }
                 }
-                for (; r < r1; ++r) aj[r] = fma(-s_v[r - r0], wj, aj[r]);
             }
         }
-        if (k + 1 >= p.n) break;
+        if (k + 1 >= n) break;
         // the row reflector of row k, by the CTA that holds the row
-        if (k >= r0 && k < r1) {
+        if (kc % P == cta) {
             __syncthreads();  // row k's updated entries
             Ssq acc{0.0, 0.0};
-            for (int j = k + 1 + threadIdx.x; j < p.n; j += BT) acc = ssq_add(acc, A[k + (long long)j * p.lda]);
+            for (int j = k + 1 + threadIdx.x; j < n; j += BT) acc = ssq_add(acc, A[k + (long long)j * p.lda]);
             const Ssq t = cta_merge(acc, s_red);
             if (threadIdx.x == 0) {
                 const double xnorm = t.s == 0.0 ? 0.0 : t.s * sqrt(t.q);
@@ -269,7 +294,7 @@ __global__ void __launch_bounds__(BT, 1) bidiag_kernel(const Args p) {
             __syncthreads();
             if (s_sc[0] != 0.0) {
                 const double ir = s_sc[2];
-                for (int j = k + 2 + threadIdx.x; j < p.n; j += BT) {
+                for (int j = k + 2 + threadIdx.x; j < n; j += BT) {
                     double* q = A + k + (long long)j * p.lda;
                     const double uj = *q * ir;
                     *q = uj;
@@ -281,14 +306,13 @@ __global__ void __launch_bounds__(BT, 1) bidiag_kernel(const Args p) {
         // the row reflector on this CTA's rows below k: x_r = tau_p * A(r, k+1:) u
         const double taur = p.rec[0];
         if (taur != 0.0) {
-            const int rb = max(r0, k + 1);
-            const int r = r0 + rloc;
-            const bool live = rpart < nparts && r >= rb && r < r1;
+            const int r = grow(rloc);
+            const bool live = rpart < nparts && r > k && r < m;
             double x = 0.0;
             if (live) {
                 const double* ar = A + r;
                 int j = k + 1 + rpart;
-                for (; j + (CH - 1) * nparts < p.n; j += CH * nparts) {
+                for (; j + (CH - 1) * nparts < n; j += CH * nparts) {
                     double y[CH], uu[CH];
 #pragma unroll
                     for (int t = 0; t < CH; ++t) {
@@ -298,13 +322,13 @@ __global__ void __launch_bounds__(BT, 1) bidiag_kernel(const Args p) {
 #pragma unroll
                     for (int t = 0; t < CH; ++t) x = fma(y[t], uu[t], x);
                 }
-                for (; j < p.n; j += nparts) x = fma(ar[(long long)j * p.lda], U[j], x);
+                for (; j < n; j += nparts) x = fma(ar[(long long)j * p.lda], U[j], x);
             }
             s_x[threadIdx.x] = x;
             __syncthreads();
             if (live && rpart == 0) {
                 double s = 0.0;
-                for (int q = 0; q < nparts; ++q) s += s_x[rloc + q * p.slab];
+                for (int q = 0; q < nparts; ++q) s += s_x[rloc + q * nloc];
                 s_x[rloc] = taur * s;
             }
             __syncthreads();
@@ -312,7 +336,7 @@ __global__ void __launch_bounds__(BT, 1) bidiag_kernel(const Args p) {
                 const double xr = s_x[rloc];
                 double* ar = A + r;
                 int j = k + 1 + rpart;
-                for (; j + (CH - 1) * nparts < p.n; j += CH * nparts) {
+                for (; j + (CH - 1) * nparts < n; j += CH * nparts) {
                     double y[CH], uu[CH];
 #pragma unroll
                     for (int t = 0; t < CH; ++t) {
@@ -322,7 +346,7 @@ __global__ void __launch_bounds__(BT, 1) bidiag_kernel(const Args p) {
 #pragma unroll
                     for (int t = 0; t < CH; ++t) ar[(long long)(j + t * nparts) * p.lda] = fma(-xr, uu[t], y[t]);
                 }
-                for (; j < p.n; j += nparts) {
+                for (; j < n; j += nparts) {
                     double* q = ar + (long long)j * p.lda;
                     *q = fma(-xr, U[j], *q);
                 }
@@ -341,14 +365,17 @@ __global__ void bidiag_right_factor_kernel(const double* a, long long lda, int n
 
 }  // namespace bidiag
 
-// Rows per CTA and the number of CTAs for an m-row reduction (0 if m needs
-// slabs above 256 rows).
-int bidiag_grid(int m, int sm_count, int* slab) {
-    int sl = (m + sm_count - 1) / sm_count;
-    if (sl < 32) sl = 32;
-    if (sl > bidiag::BT) return 0;
-    *slab = sl;
-    return (m + sl - 1) / sl;
+// The number of CTAs for an m-row reduction and the rows each holds (row
+// chunks of RC dealt round robin, so that every CTA keeps rows in play to the
+// last steps); 0 when a CTA would hold more than 256 rows.
+int bidiag_grid(int m, int sm_count, int* nloc) {
+    using namespace bidiag;
+    const int chunks = (m + RC - 1) / RC;
+    const int P = chunks < sm_count ? chunks : sm_count;
+    const int per = (chunks + P - 1) / P;
+    if (per * RC > BT) return 0;
+    *nloc = per * RC;
+    return P;
 }
 
 size_t bidiag_work_doubles(int m, int n, int sm_count) {
@@ -360,14 +387,14 @@ int launch_bidiag(double* a, long long lda, int m, int n, double* d, double* e, 
                   double* work, int sm_count, int* status, cudaStream_t st) {
     using namespace bidiag;
     Args p;
-    int slab = 0;
-    const int P = bidiag_grid(m, sm_count, &slab);
+    int nloc = 0;
+    const int P = bidiag_grid(m, sm_count, &nloc);
     if (P == 0) return JLC_E_UNSUPPORTED;
     p.a = a;
     p.lda = lda;
     p.m = m;
     p.n = n;
-    p.slab = slab;
+    p.nloc = nloc;
     p.d = d;
     p.e = e;
     p.tauq = tauq;

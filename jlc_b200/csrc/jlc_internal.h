@@ -96,7 +96,7 @@ size_t hess_work_doubles(long long n);
 // Golub-Kahan bidiagonalisation (bidiag.cu): rows per CTA and CTA count (0:
 // too many rows), the kernel's workspace in doubles, the cooperative launch,
 // and the row reflectors rearranged as the columns of a QR factor.
-int bidiag_grid(int m, int sm_count, int* slab);
+int bidiag_grid(int m, int sm_count, int* rows_per_cta);
 size_t bidiag_work_doubles(int m, int n, int sm_count);
 int launch_bidiag(double* a, long long lda, int m, int n, double* d, double* e, double* tauq, double* taup,
                   double* work, int sm_count, int* status, cudaStream_t st);
