@@ -64,6 +64,18 @@ def test_null_context_is_an_argument_error(lib):
     a = np.zeros(4)
     rc = lib.jlc_gemm(None, a.ctypes.data, a.ctypes.data, a.ctypes.data, 2, 2, 2, 1.0, 0.0, 0, None)
     assert rc == -1
+    rc = lib.jlc_bidiag_device(None, 2, 2, a.ctypes.data, 2, a.ctypes.data, a.ctypes.data, None, 2, None, 2, 0,
+                               None)
+    assert rc == -1
+
+
+def test_decomposition_mirrors_reject_null_before_any_device_call():
+    # Bidiagonalization.decompose and BlockedHessenbergQR.decompose: "Matrix must not be null"
+    from jlc_b200 import Bidiagonalization, BlockedHessenbergQR, IllegalArgumentException
+    for f in (lambda: Bidiagonalization().decompose(None), lambda: BlockedHessenbergQR.decompose(None)):
+        with pytest.raises(IllegalArgumentException) as e:
+            f()
+        assert "must not be null" in str(e.value)
 
 
 def test_mirror_validates_before_any_device_call():
